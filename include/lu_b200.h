@@ -1,0 +1,177 @@
+/*
+ * lu_b200.h -- C ABI of the B200-native no-pivot LU library (liblu_b200.so).
+ *
+ * Drop-in boundary for the lu_nopiv entry points of flipflapflop/remifa.
+ * Every function is plain C: device pointers are void*, sizes are int64_t,
+ * streams are CUDA streams, nothing throws.  All matrices are column-major
+ * (element (i, j) at a[i + j*lda]).  Factorizations are in place: the strict
+ * lower triangle holds the unit-lower L, the upper triangle holds U, and no
+ * pivoting is performed.
+ *
+ * Each entry point names the reference interface (file:line, paths inside
+ * the reference project) that it replaces.  remifa_b200/include_cpp/
+ * remifa_shim.hxx maps the reference's C++ template names onto these.
+ */
+#ifndef LU_B200_H
+#define LU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LU_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LU_API __attribute__((visibility("default")))
+#else
+#define LU_API
+#endif
+
+/* Same type as cudaStream_t / CUstream (an opaque driver handle). */
+typedef struct CUstream_st* lu_stream_t;
+
+typedef enum lu_status {
+  LU_SUCCESS = 0,
+  LU_ERR_INVALID_ARG = 1,   /* bad size, leading dimension, pointer or option */
+  LU_ERR_CUDA = 2,          /* a CUDA runtime/driver call failed */
+  LU_ERR_ALLOC = 3,         /* device allocation failed */
+  LU_ERR_UNSUPPORTED = 4,   /* valid but unimplemented combination */
+  LU_ERR_WORKSPACE = 5,     /* caller workspace too small */
+  LU_ERR_NOT_CONVERGED = 6, /* iterative refinement did not reach its target */
+  LU_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+  LU_ERR_NO_DEVICE = 8      /* no usable sm_100 device */
+} lu_status;
+
+/* Storage types. */
+typedef enum lu_dtype {
+  LU_F32 = 0,
+  LU_F16 = 1,
+  LU_BF16 = 2,
+  LU_E4M3 = 3,
+  LU_F64 = 4
+} lu_dtype;
+
+/* Update compute types.  0..3 keep the reference's enum values
+ * (remifa::compute_type, src/utils.hxx:18-24); 4..6 are new tensor-core
+ * update kinds (operands rounded as named, fp32 accumulation). */
+typedef enum lu_compute {
+  LU_COMPUTE_FP32 = 0,       /* SIMT fp32, fp32 accumulation */
+  LU_COMPUTE_FP16 = 1,       /* fp16 in, fp16 out (W = fp16 only) */
+  LU_COMPUTE_TC32 = 2,       /* tensor cores: fp16 operands, fp32 accumulate */
+  LU_COMPUTE_TC16 = 3,       /* tensor cores: fp16 operands, fp16 result */
+  LU_COMPUTE_TC32_BF16 = 4,  /* tensor cores: bf16 operands, fp32 accumulate */
+  LU_COMPUTE_TC32_E4M3 = 5,  /* tensor cores: e4m3 operands with a power-of-two
+                                scale per 128-row / 128-column tile */
+  LU_COMPUTE_TC32_SPLIT = 6  /* compensated split fp16: hi*hi + hi*lo + lo*hi */
+} lu_compute;
+
+typedef enum lu_variant {
+  LU_RIGHT_LOOKING = 0, /* remifa::lu_nopiv_rl (src/lu_nopiv.hxx:44-208) */
+  LU_LEFT_LOOKING = 1   /* remifa::lu_nopiv_ll (src/lu_nopiv_ll.hxx:41-582) */
+} lu_variant;
+
+typedef struct lu_opts {
+  int64_t nb;           /* outer block size (reference runtime nb, default 256) */
+  int32_t ib;           /* inner block size: 8 (the reference's compile-time ib) */
+  int32_t inner_update; /* lu_compute for updates inside the outer block */
+  int32_t outer_update; /* lu_compute for the trailing (Schur) update */
+  int32_t variant;      /* lu_variant */
+  int32_t lookahead;    /* 1: factor panel k+1 while update k runs */
+  int32_t diag_width;   /* width of the one-CTA diagonal factorization
+                           (multiple of 8, <= 128; 0 = default 128) */
+  int32_t reserved[8];
+} lu_opts;
+
+/* Defaults: nb = 256, ib = 8, FP32/FP32, right-looking, look-ahead on. */
+LU_API void lu_opts_default(lu_opts* opts);
+
+LU_API const char* lu_status_string(lu_status s);
+LU_API int lu_abi_version(void);
+/* Message of the last CUDA failure seen by this thread (empty if none). */
+LU_API const char* lu_last_error(void);
+
+/* Bytes of device workspace lu_nopiv_rl_c / lu_nopiv_ll_c need for these
+ * arguments (replaces the reference's internal cudaMalloc,
+ * src/lu_nopiv.hxx:111 and src/lu_nopiv_ll.hxx:162-190). */
+LU_API lu_status lu_workspace_size(const lu_opts* opts, int64_t m, int64_t n,
+                            lu_dtype dtype_a, size_t* bytes);
+
+/* In-place no-pivot LU, right-looking.
+ * Replaces remifa::lu_nopiv_rl<T,I,O,ib,use_cutlass,CpyType>
+ * (src/lu_nopiv.hxx:44-63).
+ *   m, n      : matrix size (square: m == n, as the reference's inner loop
+ *               assumes, src/lu_nopiv_inner_rl.hxx:124-129)
+ *   d_a, lda  : device matrix of type dtype_a (LU_F32 or LU_F16)
+ *   d_info    : device int; 0 on success, k > 0 if the k-th pivot (1-based)
+ *               was zero or not finite (the factorization still completes)
+ *   d_a_lowp  : optional fp16 m x n buffer (ld_lowp); when given it receives
+ *               the fp16 copy of the factors the reference leaves in its
+ *               d_a_cpy argument.  Unlike the reference it is never required.
+ *   workspace : device memory of lu_workspace_size bytes, or NULL to let the
+ *               library allocate stream-ordered memory (cudaMallocAsync).
+ * Asynchronous with respect to the host: work is queued on `stream`; call
+ * cudaStreamSynchronize before reading d_a. */
+LU_API lu_status lu_nopiv_rl_c(const lu_opts* opts, lu_stream_t stream, int64_t m,
+                        int64_t n, void* d_a, lu_dtype dtype_a, int64_t lda,
+                        int* d_info, void* d_a_lowp, int64_t ld_lowp,
+                        void* workspace, size_t ws_bytes);
+
+/* In-place no-pivot LU, left-looking (Crout).
+ * Replaces remifa::lu_nopiv_ll<...> (src/lu_nopiv_ll.hxx:41-66) and its 30
+ * wrappers lu_nopiv_ll_* (src/lu_nopiv_ll.hxx:586-793). Arguments as
+ * lu_nopiv_rl_c. */
+LU_API lu_status lu_nopiv_ll_c(const lu_opts* opts, lu_stream_t stream, int64_t m,
+                        int64_t n, void* d_a, lu_dtype dtype_a, int64_t lda,
+                        int* d_info, void* d_a_lowp, int64_t ld_lowp,
+                        void* workspace, size_t ws_bytes);
+
+/* Panel kernel: factors the n x n (n <= 8) diagonal tile whose copy is d,
+ * applies it to the m - n rows below (L, in l) and the m - n columns to its
+ * right (U, in u).  stat receives n.
+ * Replaces remifa::lu_nopiv_panel<T,8> (src/lu_nopiv.cuh:12-19,
+ * src/lu_nopiv.cu:364-400).  dtype: LU_F32 or LU_F16. */
+LU_API lu_status lu_panel_c(lu_stream_t stream, lu_dtype dtype, int64_t m, int64_t n,
+                     const void* d, int64_t ldd, void* l, int64_t ldl, void* u,
+                     int64_t ldu, int* stat);
+
+/* Cast copy out = round(a * 2^scale_log2), m x n column-major.
+ * Replaces remifa::convert<TA,TAO> (src/convert.cuh:17-18,
+ * src/convert.cu:324-387).  Supported (in -> out): f32 -> f16/bf16/e4m3/f32,
+ * f16 -> f32, f64 -> f16, f16 -> f64, f32 -> f64, f64 -> f32.  Rounding is
+ * to nearest even; e4m3 saturates to +-448. */
+LU_API lu_status lu_convert_c(lu_stream_t stream, int64_t m, int64_t n, const void* a,
+                       lu_dtype type_a, int64_t lda, void* out,
+                       lu_dtype type_out, int64_t ldout, int scale_log2);
+
+/* C = alpha * A * B + beta * C (no transposes), A m x k, B k x n.
+ * Replaces remifa::gemmex<Impl,Op,Acc,In,Out> (src/gemm.cuh:24-40,
+ * src/gemm.cu:17-316) without cuBLAS:
+ *   LU_COMPUTE_FP32 : A, B, C fp32; SIMT fp32.  With alpha = -1, beta = 1
+ *                     the result is C - sum_t fma-chain(A[i,t] B[t,j]).
+ *   LU_COMPUTE_TC32 / _BF16 / _E4M3 / _SPLIT : A, B fp32 (rounded on the
+ *                     fly to the operand type by the library), C fp32,
+ *                     tcgen05 tensor cores, fp32 accumulation.
+ * workspace/ws_bytes: scratch for the rounded operand copies (NULL: the
+ * library allocates stream-ordered memory). */
+LU_API lu_status lu_gemm_update_c(lu_stream_t stream, lu_compute compute, int64_t m,
+                           int64_t n, int64_t k, double alpha, const void* a,
+                           int64_t lda, const void* b, int64_t ldb,
+                           double beta, void* c, int64_t ldc, void* workspace,
+                           size_t ws_bytes);
+
+/* Seeded, counter-based test-matrix generator (bit-identical to the CPU
+ * oracle): kind 0: r_ij = U[-1,1); kind 1: r_ij ~ N(0,1)/sqrt(n);
+ * a_ii = alpha * sum_{j!=i} |r_ij|; all entries * 2^kscale; row i scaled by
+ * 2^-round(gamma_bits * i / (n-1)).  New: the reference generates on the host
+ * (tests/genmat.hxx:69-102). */
+LU_API lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
+                          int64_t lda, uint64_t seed, int kind, double alpha,
+                          int kscale, double gamma_bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LU_B200_H */

@@ -1,0 +1,20 @@
+"""remifa_b200: B200-native (sm_100a) no-pivot LU factorization.
+
+A drop-in for the lu_nopiv entry points of flipflapflop/remifa.  The compute
+lives in liblu_b200.so (hand-written CUDA for sm_100a behind the C ABI in
+include/lu_b200.h); this package is the thin Python host layer over it.
+"""
+from . import _lib
+from .api import (FP16, FP32, TC16, TC32, align_lda, colmajor, colmajor_empty,
+                  compute_type, convert, gemmex, gen_matrix, ld, lu_nopiv_ll,
+                  lu_nopiv_panel, lu_nopiv_rl, make_opts, workspace_size)
+
+__all__ = [
+    "FP16", "FP32", "TC16", "TC32", "align_lda", "colmajor", "colmajor_empty",
+    "compute_type", "convert", "gemmex", "gen_matrix", "ld", "lu_nopiv_ll",
+    "lu_nopiv_panel", "lu_nopiv_rl", "make_opts", "workspace_size",
+]
+
+
+def library_path() -> str:
+    return _lib.LIB_PATH

@@ -1,0 +1,206 @@
+"""Host-side mirror of the reference's lu_nopiv interface over the C ABI.
+
+The reference (flipflapflop/remifa) exposes C++ templates; this module keeps
+their names and argument meaning for Python callers, on column-major torch
+CUDA tensors (a 2-D tensor with stride(0) == 1; its leading dimension is
+stride(1)).  PyTorch only supplies device memory and the current stream; all
+work runs in liblu_b200.so.
+
+    remifa::lu_nopiv_rl       (src/lu_nopiv.hxx:44-63)     -> lu_nopiv_rl
+    remifa::lu_nopiv_ll       (src/lu_nopiv_ll.hxx:41-66)  -> lu_nopiv_ll
+    remifa::lu_nopiv_panel    (src/lu_nopiv.cuh:12-19)     -> lu_nopiv_panel
+    remifa::convert           (src/convert.cuh:17-18)      -> convert
+    remifa::gemmex            (src/gemm.cuh:24-40)         -> gemmex
+    remifa::align_lda         (src/utils.hxx:48-62)        -> align_lda
+    remifa::compute_type      (src/utils.hxx:18-24)        -> compute_type
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import torch
+
+from . import _lib
+
+
+class compute_type(enum.IntEnum):
+    """Update compute types; FP32..TC16 keep the reference's values."""
+    FP32 = _lib.COMPUTE_FP32
+    FP16 = _lib.COMPUTE_FP16
+    TC32 = _lib.COMPUTE_TC32
+    TC16 = _lib.COMPUTE_TC16
+    TC32_BF16 = _lib.COMPUTE_TC32_BF16
+    TC32_E4M3 = _lib.COMPUTE_TC32_E4M3
+    TC32_SPLIT = _lib.COMPUTE_TC32_SPLIT
+
+
+FP32, FP16, TC32, TC16 = (compute_type.FP32, compute_type.FP16,
+                          compute_type.TC32, compute_type.TC16)
+
+_DTYPES = {
+    torch.float32: _lib.F32,
+    torch.float16: _lib.F16,
+    torch.bfloat16: _lib.BF16,
+    torch.float8_e4m3fn: _lib.E4M3,
+    torch.float64: _lib.F64,
+}
+
+
+def align_lda(m: int, itemsize: int = 4) -> int:
+    """Smallest multiple of 64 bytes (in elements) >= m, as the reference's
+    align_lda (src/utils.hxx:48-62)."""
+    t = 64 // itemsize
+    return t * ((m - 1) // t + 1) if m > 0 else t
+
+
+def colmajor_empty(m: int, n: int, lda: int | None = None,
+                   dtype=torch.float32, device="cuda") -> torch.Tensor:
+    """An m x n column-major tensor with leading dimension lda."""
+    lda = m if lda is None else lda
+    if lda < max(1, m):
+        raise ValueError("lda < m")
+    buf = torch.empty((max(n, 1), lda), dtype=dtype, device=device)
+    return buf.t()[:m, :n]
+
+
+def colmajor(t: torch.Tensor, lda: int | None = None) -> torch.Tensor:
+    """Column-major copy of a 2-D tensor (same device and dtype)."""
+    m, n = t.shape
+    out = colmajor_empty(m, n, lda, t.dtype, t.device)
+    out.copy_(t)
+    return out
+
+
+def ld(t: torch.Tensor) -> int:
+    """Leading dimension of a column-major 2-D tensor."""
+    if t.dim() != 2 or (t.stride(0) != 1 and t.shape[0] > 1):
+        raise ValueError("expected a column-major 2-D tensor (stride(0) == 1)")
+    return max(t.stride(1), t.shape[0], 1)
+
+
+def _ptr(t: torch.Tensor | None):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    s = torch.cuda.current_stream() if stream is None else stream
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def make_opts(nb: int = 256, inner=FP32, outer=FP32, lookahead: bool = True,
+              diag_width: int = 0, variant: int = _lib.RIGHT_LOOKING) -> _lib.LuOpts:
+    o = _lib.LuOpts()
+    _lib.lib().lu_opts_default(ctypes.byref(o))
+    o.nb = int(nb)
+    o.inner_update = int(inner)
+    o.outer_update = int(outer)
+    o.lookahead = int(bool(lookahead))
+    o.diag_width = int(diag_width)
+    o.variant = int(variant)
+    return o
+
+
+def workspace_size(n: int, nb: int = 256, inner=FP32, outer=FP32,
+                   variant: int = _lib.RIGHT_LOOKING, dtype=torch.float32,
+                   lookahead: bool = True) -> int:
+    o = make_opts(nb, inner, outer, lookahead, variant=variant)
+    sz = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().lu_workspace_size(ctypes.byref(o), n, n, _DTYPES[dtype],
+                                            ctypes.byref(sz)), "lu_workspace_size")
+    return sz.value
+
+
+def _factor(fn_name: str, variant: int, a: torch.Tensor, nb: int, inner, outer,
+            a_cpy, info, lookahead, diag_width, workspace, stream):
+    if not a.is_cuda:
+        raise ValueError(f"{fn_name}: the matrix must be a CUDA tensor")
+    m, n = a.shape
+    lda = ld(a)
+    if info is None:
+        info = torch.zeros(1, dtype=torch.int32, device=a.device)
+    o = make_opts(nb, inner, outer, lookahead, diag_width, variant)
+    ws_ptr, ws_bytes = None, 0
+    if workspace is not None:
+        ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
+    st = getattr(_lib.lib(), fn_name)(
+        ctypes.byref(o), _stream(stream), m, n, _ptr(a), _DTYPES[a.dtype], lda,
+        _ptr(info), _ptr(a_cpy), ld(a_cpy) if a_cpy is not None else 0,
+        ws_ptr, ws_bytes)
+    _lib.check(st, fn_name)
+    return info
+
+
+def lu_nopiv_rl(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
+                a_cpy: torch.Tensor | None = None, info: torch.Tensor | None = None,
+                lookahead: bool = True, diag_width: int = 0,
+                workspace: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """In-place right-looking no-pivot LU of the column-major CUDA matrix `a`
+    (remifa::lu_nopiv_rl).  Returns the device info tensor (0 = success,
+    k > 0 = first bad pivot, 1-based).  Asynchronous on `stream`."""
+    return _factor("lu_nopiv_rl_c", _lib.RIGHT_LOOKING, a, nb, inner, outer,
+                   a_cpy, info, lookahead, diag_width, workspace, stream)
+
+
+def lu_nopiv_ll(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
+                a_cpy: torch.Tensor | None = None, info: torch.Tensor | None = None,
+                lookahead: bool = True, diag_width: int = 0,
+                workspace: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """In-place left-looking (Crout) no-pivot LU (remifa::lu_nopiv_ll)."""
+    return _factor("lu_nopiv_ll_c", _lib.LEFT_LOOKING, a, nb, inner, outer,
+                   a_cpy, info, lookahead, diag_width, workspace, stream)
+
+
+def lu_nopiv_panel(m: int, n: int, d: torch.Tensor, l: torch.Tensor,
+                   u: torch.Tensor, stat: torch.Tensor | None = None,
+                   stream=None) -> None:
+    """remifa::lu_nopiv_panel<float,8>: factor the n x n tile copy `d`, apply
+    it to the L rows (in `l`) and U columns (in `u`) of an m-row panel."""
+    if stat is None:
+        stat = torch.zeros(1, dtype=torch.int32, device=l.device)
+    st = _lib.lib().lu_panel_c(_stream(stream), _DTYPES[l.dtype], m, n, _ptr(d),
+                               ld(d), _ptr(l), ld(l), _ptr(u), ld(u), _ptr(stat))
+    _lib.check(st, "lu_panel_c")
+
+
+def convert(a: torch.Tensor, out: torch.Tensor, scale_log2: int = 0,
+            stream=None) -> torch.Tensor:
+    """remifa::convert: out = round(a * 2^scale_log2) (column-major)."""
+    m, n = a.shape
+    if tuple(out.shape) != (m, n):
+        raise ValueError("convert: shape mismatch")
+    st = _lib.lib().lu_convert_c(_stream(stream), m, n, _ptr(a), _DTYPES[a.dtype],
+                                 ld(a), _ptr(out), _DTYPES[out.dtype], ld(out),
+                                 int(scale_log2))
+    _lib.check(st, "lu_convert_c")
+    return out
+
+
+def gemmex(compute, alpha: float, a: torch.Tensor, b: torch.Tensor, beta: float,
+           c: torch.Tensor, workspace: torch.Tensor | None = None,
+           stream=None) -> torch.Tensor:
+    """remifa::gemmex: c = alpha * a @ b + beta * c (column-major fp32)."""
+    m, k = a.shape
+    k2, n = b.shape
+    if k != k2 or tuple(c.shape) != (m, n):
+        raise ValueError("gemmex: shape mismatch")
+    ws_ptr, ws_bytes = None, 0
+    if workspace is not None:
+        ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
+    st = _lib.lib().lu_gemm_update_c(_stream(stream), int(compute), m, n, k,
+                                     float(alpha), _ptr(a), ld(a), _ptr(b), ld(b),
+                                     float(beta), _ptr(c), ld(c), ws_ptr, ws_bytes)
+    _lib.check(st, "lu_gemm_update_c")
+    return c
+
+
+def gen_matrix(n: int, seed: int, kind: int = 0, alpha: float = 2.0,
+               kscale: int = 0, gamma_bits: float = 0.0, lda: int | None = None,
+               device="cuda", stream=None) -> torch.Tensor:
+    """Seeded diagonally dominant test matrix generated on the device
+    (identical to the CPU generator of the tests)."""
+    a = colmajor_empty(n, n, lda, torch.float32, device)
+    st = _lib.lib().lu_gen_matrix_c(_stream(stream), n, _ptr(a), ld(a), seed, kind,
+                                    float(alpha), int(kscale), float(gamma_bits))
+    _lib.check(st, "lu_gen_matrix_c")
+    return a

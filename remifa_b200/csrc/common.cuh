@@ -1,0 +1,60 @@
+// Shared helpers for the sm_100a kernels and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "lu_b200.h"
+
+namespace lub {
+
+// Sentinel stored in the "first bad pivot" word before a factorization.
+constexpr int kNoBadPivot = 0x7f7f7f7f;
+
+#define LUB_CUDA_TRY(expr)                                              \
+  do {                                                                  \
+    cudaError_t _e = (expr);                                            \
+    if (_e != cudaSuccess) {                                            \
+      ::lub::record_cuda_error(_e, #expr, __FILE__, __LINE__);          \
+      return LU_ERR_CUDA;                                               \
+    }                                                                   \
+  } while (0)
+
+#define LUB_LAUNCH_CHECK()                                              \
+  do {                                                                  \
+    cudaError_t _e = cudaGetLastError();                                \
+    if (_e != cudaSuccess) {                                            \
+      ::lub::record_cuda_error(_e, "kernel launch", __FILE__, __LINE__); \
+      return LU_ERR_CUDA;                                               \
+    }                                                                   \
+  } while (0)
+
+#define LUB_TRY(expr)                       \
+  do {                                      \
+    lu_status _s = (expr);                  \
+    if (_s != LU_SUCCESS) return _s;        \
+  } while (0)
+
+void record_cuda_error(cudaError_t e, const char* what, const char* file,
+                       int line);
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// ---- device helpers -------------------------------------------------------
+
+// Record the 1-based global index of a zero / non-finite pivot.
+__device__ __forceinline__ void note_pivot(float d, int64_t col0,
+                                           int* first_bad) {
+  if (first_bad != nullptr && !(fabsf(d) > 0.0f && isfinite(d)))
+    atomicMin(first_bad, (int)(col0 + 1));
+}
+
+}  // namespace lub

@@ -1,0 +1,39 @@
+// Factorization drivers (host C++) shared by the C-ABI layer.
+#pragma once
+
+#include "common.cuh"
+
+namespace lub {
+
+// Everything a factorization call needs to know before enqueueing work.
+struct Plan {
+  int64_t n = 0;
+  int64_t nb = 256;
+  int diag_w = 128;
+  lu_compute inner = LU_COMPUTE_FP32;
+  lu_compute outer = LU_COMPUTE_FP32;
+  lu_variant variant = LU_RIGHT_LOOKING;
+  bool lookahead = true;
+  lu_dtype dtype = LU_F32;
+  // workspace layout (byte offsets into one device allocation)
+  size_t off_status = 0;    // int first_bad
+  size_t off_lcopy = 0;     // low-precision L21 copy (row-major)
+  size_t off_ucopy = 0;     // low-precision U12 copy (column-major)
+  size_t off_scales = 0;    // int per-tile scales (fp8)
+  size_t lcopy_bytes = 0, ucopy_bytes = 0, scale_bytes = 0;
+  size_t ws_bytes = 0;
+};
+
+lu_status check_device();
+lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
+                    Plan* p);
+lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
+                    void* d_a, lu_dtype dtype_a, int64_t lda, int* d_info,
+                    void* d_a_lowp, int64_t ld_lowp, void* workspace,
+                    size_t ws_bytes);
+lu_status gemm_update(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
+                      int64_t k, double alpha, const float* a, int64_t lda,
+                      const float* b, int64_t ldb, double beta, float* c,
+                      int64_t ldc, void* workspace, size_t ws_bytes);
+
+}  // namespace lub

@@ -1,0 +1,192 @@
+// FP32 SIMT update C = alpha*A*B + beta*C for the FP32 plain path.
+//
+// Replaces the reference's cublasSgemm call (src/gemm.cu:17-35) used for the
+// outer Schur update (src/lu_nopiv.hxx:185-192) and the K = 8 inner updates
+// (src/lu_nopiv_inner_rl.hxx:155-190).  No tensor cores: the FP32 plain path
+// must stay FP32-faithful.
+//
+// Accumulation order, per output element: acc = fma(A[i,t], B[t,j], acc) for
+// t = 0..K-1 from acc = 0, then C = C - acc (alpha = -1, beta = 1).  With
+// CHUNK8 the K range is consumed in blocks of 8 and C -= acc after every
+// block, which is how the reference's sequence of rank-8 updates inside an
+// outer block composes; this lets one launch apply several inner steps while
+// every element still sees the reference's sequence.
+//
+// Tiling: 128 x 128 per CTA, 256 threads with an 8 x 8 register tile each
+// (rows tx*4..+3 and 64+tx*4..+3, columns likewise), K staged 8 at a time
+// through double-buffered shared memory.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace lub {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 8, NT = 256;
+
+template <bool CHUNK8, bool VEC>
+__global__ void __launch_bounds__(NT)
+sgemm_update_kernel(int64_t M, int64_t N, int64_t K, float alpha,
+                    const float* __restrict__ A, int64_t lda,
+                    const float* __restrict__ B, int64_t ldb, float beta,
+                    float* __restrict__ C, int64_t ldc) {
+  __shared__ __align__(16) float As[2][BK][BM];
+  __shared__ __align__(16) float Bs[2][BK][BN];
+
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  const int64_t m0 = (int64_t)blockIdx.x * BM;
+  const int64_t n0 = (int64_t)blockIdx.y * BN;
+
+  // loader coordinates
+  // A tile BM x BK: thread loads 4 consecutive rows of one column.
+  const int a_col = tid / 32;         // 0..7
+  const int a_row = (tid % 32) * 4;   // 0..124
+  // B tile BK x BN: thread loads 4 consecutive k of one column.
+  const int b_col = tid / 2;          // 0..127
+  const int b_k = (tid % 2) * 4;      // 0 or 4
+
+  float ra[4], rb[4];
+  auto load_tiles = [&](int64_t k0) {
+    const int64_t ak = k0 + a_col;
+    const int64_t ar = m0 + a_row;
+    if (VEC && ak < K && ar + 3 < M) {
+      const float4 v = *reinterpret_cast<const float4*>(A + ar + ak * lda);
+      ra[0] = v.x; ra[1] = v.y; ra[2] = v.z; ra[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        ra[i] = (ak < K && ar + i < M) ? A[ar + i + ak * lda] : 0.0f;
+    }
+    const int64_t bc = n0 + b_col;
+    const int64_t bk = k0 + b_k;
+    if (VEC && bc < N && bk + 3 < K) {
+      const float4 v = *reinterpret_cast<const float4*>(B + bk + bc * ldb);
+      rb[0] = v.x; rb[1] = v.y; rb[2] = v.z; rb[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        rb[i] = (bc < N && bk + i < K) ? B[bk + i + bc * ldb] : 0.0f;
+    }
+  };
+  auto store_tiles = [&](int buf) {
+    *reinterpret_cast<float4*>(&As[buf][a_col][a_row]) =
+        make_float4(ra[0], ra[1], ra[2], ra[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) Bs[buf][b_k + i][b_col] = rb[i];
+  };
+
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+  // output coordinates of this thread
+  auto row_of = [&](int i) -> int64_t {
+    return m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+  };
+  auto col_of = [&](int j) -> int64_t {
+    return n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+  };
+
+  float cr[CHUNK8 ? 8 : 1][CHUNK8 ? 8 : 1];
+  if constexpr (CHUNK8) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int64_t r = row_of(i), c = col_of(j);
+        cr[i][j] = (r < M && c < N) ? C[r + c * ldc] : 0.0f;
+      }
+  }
+
+  const int64_t nk = (K + BK - 1) / BK;
+  load_tiles(0);
+  store_tiles(0);
+  __syncthreads();
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int buf = (int)(kt & 1);
+    if (kt + 1 < nk) load_tiles((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      float a[8], b[8];
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][k][64 + tx * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][k][64 + ty * 4]);
+      a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
+      a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
+      b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
+      b[4] = b1.x; b[5] = b1.y; b[6] = b1.z; b[7] = b1.w;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+    }
+    if constexpr (CHUNK8) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          cr[i][j] = __fsub_rn(cr[i][j], acc[i][j]);
+          acc[i][j] = 0.0f;
+        }
+    }
+    if (kt + 1 < nk) {
+      store_tiles(buf ^ 1);
+      __syncthreads();
+    }
+  }
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t r = row_of(i);
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int64_t c = col_of(j);
+      if (c >= N) continue;
+      float* p = C + r + c * ldc;
+      if constexpr (CHUNK8) {
+        *p = cr[i][j];
+      } else {
+        if (alpha == -1.0f && beta == 1.0f)
+          *p = __fsub_rn(*p, acc[i][j]);
+        else if (beta == 0.0f)
+          *p = __fmul_rn(alpha, acc[i][j]);
+        else
+          *p = __fmaf_rn(alpha, acc[i][j], __fmul_rn(beta, *p));
+      }
+    }
+  }
+}
+
+}  // namespace
+
+lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,
+                              float alpha, const float* A, int64_t lda,
+                              const float* B, int64_t ldb, float beta, float* C,
+                              int64_t ldc, bool chunk8) {
+  if (M <= 0 || N <= 0) return LU_SUCCESS;
+  if (K <= 0) return LU_SUCCESS;  // nothing to accumulate (beta == 1 callers)
+  if (chunk8 && !(alpha == -1.0f && beta == 1.0f)) return LU_ERR_INVALID_ARG;
+  const bool vec = (lda % 4 == 0) && (ldb % 4 == 0) &&
+                   ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0);
+  dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN));
+  if (grid.y > 65535) return LU_ERR_INVALID_ARG;
+  if (chunk8) {
+    if (vec)
+      sgemm_update_kernel<true, true><<<grid, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      sgemm_update_kernel<true, false><<<grid, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  } else {
+    if (vec)
+      sgemm_update_kernel<false, true><<<grid, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      sgemm_update_kernel<false, false><<<grid, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  }
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+}  // namespace lub

@@ -1,0 +1,43 @@
+// Internal launchers shared between the kernel files and the drivers.
+#pragma once
+
+#include "common.cuh"
+
+namespace lub {
+
+// panel.cu
+size_t diag_smem_bytes(int w);
+lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
+                             int64_t col0, int* first_bad);
+lu_status launch_lpanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
+                        int64_t M, int w);
+lu_status launch_upanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
+                        int64_t N, int w);
+lu_status launch_ref_panel(cudaStream_t st, int64_t m, int n, const float* d,
+                           int64_t ldd, float* l, int64_t ldl, float* u,
+                           int64_t ldu, int* stat);
+
+// gemm_simt.cu
+lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,
+                              float alpha, const float* A, int64_t lda,
+                              const float* B, int64_t ldb, float beta, float* C,
+                              int64_t ldc, bool chunk8);
+
+// convert.cu
+lu_status launch_convert(cudaStream_t st, int64_t m, int64_t n, const void* a,
+                         lu_dtype ta, int64_t lda, void* out, lu_dtype tout,
+                         int64_t ldout, int scale_log2);
+
+// gen.cu
+lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
+                            uint64_t seed, int kind, double alpha, int kscale,
+                            double gamma_bits);
+
+// misc.cu
+lu_status launch_fill_int(cudaStream_t st, int* p, int v, int64_t count);
+lu_status launch_finalize_info(cudaStream_t st, const int* first_bad, int* info);
+
+// Set the dynamic shared-memory limit of `func` for the current device.
+cudaError_t set_smem_limit(const void* func, size_t bytes);
+
+}  // namespace lub

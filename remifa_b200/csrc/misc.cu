@@ -1,0 +1,86 @@
+// Small utilities shared by the drivers: status words, error recording,
+// per-device attributes.
+#include "common.cuh"
+#include "kernels.cuh"
+
+#include <mutex>
+#include <unordered_map>
+
+namespace lub {
+namespace {
+
+__global__ void fill_int_kernel(int* p, int v, int64_t count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) p[i] = v;
+}
+
+// LAPACK-style info: 0, or the 1-based column of the first bad pivot.
+__global__ void finalize_info_kernel(const int* first_bad, int* info) {
+  const int f = *first_bad;
+  *info = (f == kNoBadPivot) ? 0 : f;
+}
+
+std::mutex g_mu;
+thread_local char g_last_error[512] = {0};
+
+}  // namespace
+
+void record_cuda_error(cudaError_t e, const char* what, const char* file,
+                       int line) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s failed: %s (%s:%d)",
+                what, cudaGetErrorString(e), file, line);
+  if (std::getenv("LU_B200_VERBOSE")) std::fprintf(stderr, "[lu_b200] %s\n", g_last_error);
+}
+
+const char* last_error_message() { return g_last_error; }
+
+int sm_count() {
+  static std::unordered_map<int, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 148;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  cache[dev] = n;
+  return n;
+}
+
+cudaError_t set_smem_limit(const void* func, size_t bytes) {
+  // The attribute is per (function, device); remember the largest value set.
+  static std::unordered_map<uint64_t, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t key = ((uint64_t)(uintptr_t)func) ^ ((uint64_t)dev << 56);
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  }
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)bytes);
+  if (e == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    done[key] = bytes;
+  }
+  return e;
+}
+
+lu_status launch_fill_int(cudaStream_t st, int* p, int v, int64_t count) {
+  if (count <= 0) return LU_SUCCESS;
+  fill_int_kernel<<<(unsigned)ceil_div(count, 256), 256, 0, st>>>(p, v, count);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+lu_status launch_finalize_info(cudaStream_t st, const int* first_bad,
+                               int* info) {
+  finalize_info_kernel<<<1, 1, 0, st>>>(first_bad, info);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+}  // namespace lub

@@ -1,0 +1,98 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every symbol
+include/lu_b200.h declares, validates arguments before touching a device, and
+refuses to run without an sm_100 device (no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from remifa_b200 import _lib
+import remifa_b200 as rb
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "lu_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    return re.findall(r"LU_API\s+[\w\s\*]+?\b(lu_\w+)\s*\(", src)
+
+
+def test_library_exports_every_declared_symbol(built):
+    names = declared_functions()
+    assert len(names) >= 10
+    L = _lib.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    # the ctypes table covers the whole header
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def test_opts_default_and_version(built):
+    o = _lib.LuOpts()
+    _lib.lib().lu_opts_default(ctypes.byref(o))
+    assert (o.nb, o.ib, o.inner_update, o.outer_update, o.variant, o.lookahead) == \
+        (256, 8, 0, 0, 0, 1)
+    assert _lib.lib().lu_abi_version() == 1
+    for s in range(9):
+        assert _lib.lib().lu_status_string(s)
+
+
+def _ws(o, m, n, dtype=_lib.F32):
+    sz = ctypes.c_size_t(0)
+    st = _lib.lib().lu_workspace_size(ctypes.byref(o), m, n, dtype, ctypes.byref(sz))
+    return st, sz.value
+
+
+def test_workspace_size_validation(built):
+    o = rb.make_opts()
+    st, sz = _ws(o, 1024, 1024)
+    assert st == _lib.SUCCESS and sz > 0
+    assert _ws(o, 1024, 512)[0] == _lib.ERR_UNSUPPORTED      # square only
+    o.nb = 100
+    assert _ws(o, 64, 64)[0] == _lib.ERR_INVALID_ARG          # nb % 8 != 0
+    o = rb.make_opts()
+    o.ib = 4
+    assert _ws(o, 64, 64)[0] == _lib.ERR_UNSUPPORTED          # ib is 8
+    o = rb.make_opts(diag_width=129)
+    assert _ws(o, 64, 64)[0] == _lib.ERR_INVALID_ARG
+
+
+def _rl(m=64, n=64, a=1, lda=64, info=1, dtype=_lib.F32, ws=None, ws_bytes=0):
+    o = rb.make_opts()
+    return _lib.lib().lu_nopiv_rl_c(ctypes.byref(o), None, m, n,
+                                    ctypes.c_void_p(a) if a else None, dtype, lda,
+                                    ctypes.c_void_p(info) if info else None,
+                                    None, 0, ws, ws_bytes)
+
+
+def test_factor_argument_validation_without_device(built):
+    # argument errors are reported before any device call
+    assert _rl(info=0) == _lib.ERR_INVALID_ARG
+    assert _rl(lda=10) == _lib.ERR_INVALID_ARG
+    assert _rl(a=0) == _lib.ERR_INVALID_ARG
+    assert _rl(m=-1) == _lib.ERR_INVALID_ARG
+    assert _rl(ws=ctypes.c_void_p(64), ws_bytes=1) in (_lib.ERR_WORKSPACE,
+                                                       _lib.ERR_NO_DEVICE)
+
+
+def test_no_cpu_fallback(built):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    # valid arguments, no device: the call must fail, not compute on the host
+    assert _rl() == _lib.ERR_NO_DEVICE
+    st = _lib.lib().lu_convert_c(None, 4, 4, ctypes.c_void_p(1), _lib.F32, 4,
+                                 ctypes.c_void_p(1), _lib.F16, 4, 0)
+    assert st == _lib.ERR_NO_DEVICE
+
+
+def test_python_layer_raises_like_reference(built):
+    with pytest.raises(ValueError):
+        _lib.check(_lib.ERR_INVALID_ARG, "x")
+    with pytest.raises(NotImplementedError):
+        _lib.check(_lib.ERR_UNSUPPORTED, "x")
+    with pytest.raises(RuntimeError):
+        _lib.check(_lib.ERR_CUDA, "x")
+    assert rb.align_lda(100) == 112 and rb.align_lda(16) == 16
+    assert rb.align_lda(100, 2) == 128

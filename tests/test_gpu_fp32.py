@@ -1,0 +1,228 @@
+"""GPU parity of the FP32 plain path against the oracle (bit for bit) and the
+reference's own compiled kernels (oracle/_ref), all through the C ABI."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import remifa_b200 as rb
+
+pytestmark = pytest.mark.gpu
+
+REF_SO = os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref",
+                      "libremifa_ref.so")
+
+
+def to_dev(a: np.ndarray, lda: int | None = None) -> torch.Tensor:
+    m, n = a.shape
+    t = rb.colmajor_empty(m, n, lda if lda is not None else O.ld(a), torch.float32)
+    t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+    return t
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    return np.asfortranarray(t.cpu().numpy())
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference library not built")
+    L = ctypes.CDLL(REF_SO)
+    vp, i64, i = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    L.ref_panel_f32.argtypes = [vp, i, i, vp, i, vp, i, vp, i, vp]
+    L.ref_convert_f32_f16.argtypes = [vp, i, i, vp, i, vp, i]
+    L.ref_lu_nopiv_rl_f32.argtypes = [vp, i64, i64, i64, vp, i64, vp, i, i, vp, i64]
+    return L
+
+
+def _st():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# ------------------------------------------------------------ generator
+
+@pytest.mark.parametrize("n,kind,kscale,gamma", [(1, 0, 0, 0.0), (7, 1, 0, 0.0),
+                                                  (64, 0, 8, 0.0), (257, 1, 0, 12.0),
+                                                  (300, 1, 8, 20.0)])
+def test_gen_matrix_bit_exact(built, n, kind, kscale, gamma):
+    lda = n + 3
+    g = rb.gen_matrix(n, seed=42, kind=kind, alpha=1.5, kscale=kscale,
+                      gamma_bits=gamma, lda=lda)
+    torch.cuda.synchronize()
+    want = O.gen_matrix(n, seed=42, kind=kind, alpha=1.5, kscale=kscale,
+                        gamma_bits=gamma, lda=lda)
+    np.testing.assert_array_equal(to_host(g), want)
+
+
+# ------------------------------------------------------------ convert
+
+@pytest.mark.parametrize("dt,fmt", [(torch.float16, 1), (torch.bfloat16, 2),
+                                    (torch.float8_e4m3fn, 3)])
+@pytest.mark.parametrize("m,n,lda", [(64, 33, 64), (37, 5, 41), (4096, 3, 4096)])
+def test_convert_bit_exact(built, dt, fmt, m, n, lda):
+    rng = np.random.default_rng(m + n)
+    a = O.colmajor(m, n, lda)
+    a[:, :] = (rng.standard_normal((m, n)) * 300).astype(np.float32)
+    for s in (0, -3):
+        da = to_dev(a)
+        out = rb.colmajor_empty(m, n, lda, dt)
+        rb.convert(da, out, scale_log2=s)
+        got = out.float().cpu().numpy()
+        want = O.round_fmt(a, fmt, s)
+        if dt == torch.float16:  # overflow -> inf in both
+            np.testing.assert_array_equal(got, want)
+        else:
+            np.testing.assert_array_equal(got, want)
+
+
+def test_convert_f16_matches_reference(built, ref):
+    rng = np.random.default_rng(3)
+    m, n = 128, 40
+    a = np.asfortranarray((rng.standard_normal((m, n)) * 2e4).astype(np.float32))
+    da = to_dev(a)
+    mine = rb.colmajor_empty(m, n, m, torch.float16)
+    rb.convert(da, mine)
+    theirs = torch.zeros((n, m), dtype=torch.float16, device="cuda")
+    ref.ref_convert_f32_f16(_st(), m, n, ctypes.c_void_p(da.data_ptr()), m,
+                            ctypes.c_void_p(theirs.data_ptr()), m)
+    torch.cuda.synchronize()
+    assert torch.equal(mine.t().contiguous().view(torch.int16),
+                       theirs.view(torch.int16))
+
+
+# ------------------------------------------------------------ panel
+
+@pytest.mark.parametrize("m,n", [(8, 8), (48, 8), (1000, 8), (20, 5), (9, 1)])
+def test_panel_bit_exact_vs_oracle(built, m, n):
+    a = O.gen_matrix(m, seed=m, kind=0, alpha=2.0, lda=m + 1)
+    d = np.asfortranarray(a[:n, :n].copy())
+    want = np.array(a, copy=True, order="F")
+    O.panel(m, n, d, want)
+    da, dd = to_dev(a), to_dev(d)
+    stat = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rb.lu_nopiv_panel(m, n, dd, da, da, stat)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(da), want)
+    assert int(stat.item()) == n
+
+
+def test_panel_bit_exact_vs_reference(built, ref):
+    m = 520
+    a = O.gen_diagdom(m, lda=m)
+    d = np.asfortranarray(a[:8, :8].copy())
+    mine, theirs, dd = to_dev(a), to_dev(a), to_dev(d)
+    rb.lu_nopiv_panel(m, 8, dd, mine, mine)
+    stat = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ref.ref_panel_f32(_st(), m, 8, ctypes.c_void_p(dd.data_ptr()), 8,
+                      ctypes.c_void_p(theirs.data_ptr()), m,
+                      ctypes.c_void_p(theirs.data_ptr()), m,
+                      ctypes.c_void_p(stat.data_ptr()))
+    torch.cuda.synchronize()
+    assert torch.equal(mine, theirs)
+
+
+# ------------------------------------------------------------ gemm
+
+@pytest.mark.parametrize("m,n,k,lda", [(128, 128, 8, 128), (300, 77, 256, 301),
+                                       (1, 1, 1, 1), (513, 1029, 64, 516)])
+def test_gemmex_fp32_bit_exact(built, m, n, k, lda):
+    rng = np.random.default_rng(k)
+    A = O.colmajor(m, k, lda); A[:, :] = rng.standard_normal((m, k)).astype(np.float32)
+    B = O.colmajor(k, n, max(k, 1)); B[:, :] = rng.standard_normal((k, n)).astype(np.float32)
+    C = O.colmajor(m, n, lda); C[:, :] = rng.standard_normal((m, n)).astype(np.float32)
+    want = np.array(C, copy=True, order="F")
+    O.gemm_sub(A, B, want)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    rb.gemmex(rb.FP32, -1.0, dA, dB, 1.0, dC)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(dC), want)
+
+
+# ------------------------------------------------------------ factorization
+
+CASES = [(1, 256, 0), (7, 256, 0), (8, 8, 0), (9, 8, 0), (63, 64, 0), (64, 64, 0),
+         (65, 64, 0), (200, 256, 0), (257, 256, 0), (520, 256, 0), (520, 64, 8),
+         (1024, 256, 64), (1024, 128, 128), (777, 136, 24)]
+
+
+@pytest.mark.parametrize("n,nb,dw", CASES)
+def test_lu_rl_fp32_bit_exact_vs_oracle(built, n, nb, dw):
+    a = (O.gen_matrix(n, seed=n + nb, kind=1, alpha=1.5, lda=n + 5) if n > 1
+         else np.asfortranarray(np.array([[3.0]], np.float32)))
+    want = O.lu_rl(a, nb=nb)
+    da = to_dev(a)
+    info = rb.lu_nopiv_rl(da, nb=nb, diag_width=dw)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(da), want)
+    assert int(info.item()) == 0
+
+
+def test_lu_rl_fp32_bit_exact_diagdom_4096(built):
+    n = 4096
+    a = O.gen_diagdom(n, lda=n)
+    want = O.lu_rl(a, nb=256)
+    da = to_dev(a)
+    rb.lu_nopiv_rl(da, nb=256)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(da), want)
+
+
+@pytest.mark.parametrize("n,nb", [(1024, 256), (4096, 256)])
+def test_lu_rl_fp32_vs_reference_gpu(built, ref, n, nb):
+    """Same input through the reference's own lu_nopiv_rl (cuBLAS) and ours:
+    factors within a stated tolerance, errors within a factor of 4."""
+    a = O.gen_diagdom(n, lda=n)
+    mine, theirs = to_dev(a), to_dev(a)
+    rb.lu_nopiv_rl(mine, nb=nb)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = ref.ref_lu_nopiv_rl_f32(_st(), n, n, nb, ctypes.c_void_p(theirs.data_ptr()),
+                                 n, ctypes.c_void_p(info.data_ptr()), 0, 0, None, 0)
+    assert rc == 0
+    torch.cuda.synchronize()
+    lm, lr = to_host(mine), to_host(theirs)
+    U32 = 2.0 ** -24
+    rel = np.abs(lm - lr).max() / np.abs(lr).max()
+    assert rel <= 4 * n * U32, rel
+    x1 = np.ones(n, np.float32)
+    b = O.gen_rhs(a, x1)
+    e_m = O.nwerr(a, b, O.lu_solve_f32(lm, b))
+    e_r = O.nwerr(a, b, O.lu_solve_f32(lr, b))
+    assert e_m <= 4 * e_r and e_r <= 4 * e_m, (e_m, e_r)
+
+
+def test_zero_pivot_reported(built):
+    n = 64
+    a = O.gen_matrix(n, seed=1, kind=0, alpha=2.0)
+    a[:, 20] = 0.0
+    a[20, :] = 0.0  # column 20 of the factor is exactly zero -> pivot 21
+    da = to_dev(a)
+    info = rb.lu_nopiv_rl(da, nb=32)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 21
+
+
+def test_lowp_copy_side_effect(built):
+    n = 100
+    a = O.gen_matrix(n, seed=4, kind=0, alpha=2.0)
+    da = to_dev(a)
+    cpy = rb.colmajor_empty(n, n, 104, torch.float16)
+    rb.lu_nopiv_rl(da, nb=64, a_cpy=cpy)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(cpy.float().cpu().numpy(),
+                                  O.round_fmt(to_host(da), 1))
+
+
+def test_workspace_caller_provided(built):
+    n = 300
+    a = O.gen_matrix(n, seed=8, kind=1, alpha=2.0)
+    ws = torch.empty(rb.workspace_size(n), dtype=torch.uint8, device="cuda")
+    da = to_dev(a)
+    rb.lu_nopiv_rl(da, nb=128, workspace=ws)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(da), O.lu_rl(a, nb=128))
+    with pytest.raises(RuntimeError):
+        rb.lu_nopiv_rl(to_dev(a), nb=128, workspace=ws[:1])

@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the no-pivot LU hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+    python bench.py --impl reference ...   (the CPU restatement, host cores)
+
+One step = one in-place factorization of a fresh, HBM-resident copy of the
+workload matrix (each step factors its own copy, so no input reuse; a copy
+is 1 GiB at n = 16384, far larger than the 126 MB L2).  For N > 1 (torchrun)
+every rank factors its own matrices: replicas, no data-path collective;
+time is the max over ranks.  Prints one JSON line on rank 0.
+
+Fields beyond the value: `e2e` times the same factorization through the
+public API from pinned host memory (H2D of A, factorization, D2H of the
+factors), `roofline` reports the dominant kernel against the measured HBM
+peak, `cpu_baseline` the CPU restatement of the reference algorithm on a
+bounded sample of the same workload, `clocks` the SM clocks sampled during
+the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # Mixed-precision reference path: fp32 storage, fp16 tensor-core Schur
+    # update, fp32 accumulation, right-looking, nb = 256, n = 16384; matrix
+    # A = R + D, R ~ N(0,1)/sqrt(n), row dominance 1.5.
+    "lu_tc32_rl_n16384": dict(n=16384, nb=256, outer="TC32", kind=1, alpha=1.5,
+                              kscale=0, oracle_fmt=1),
+    # Plain FP32 right-looking, n = 4096, nb = 256, U[-1,1] + dominance 2.
+    "lu_fp32_rl_n4096": dict(n=4096, nb=256, outer="FP32", kind=0, alpha=2.0,
+                             kscale=0, oracle_fmt=0),
+    # FP32 plain path at the mixed path's size (the comparison point of the
+    # time-to-solution target).
+    "lu_fp32_rl_n16384": dict(n=16384, nb=256, outer="FP32", kind=1, alpha=1.5,
+                              kscale=0, oracle_fmt=0),
+    "lu_bf16_rl_n16384": dict(n=16384, nb=256, outer="TC32_BF16", kind=1,
+                              alpha=1.5, kscale=0, oracle_fmt=2),
+    "lu_e4m3_rl_n16384": dict(n=16384, nb=256, outer="TC32_E4M3", kind=1,
+                              alpha=1.5, kscale=0, oracle_fmt=3),
+}
+DEFAULT_WORKLOAD = "lu_tc32_rl_n16384"
+NVML_REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x10: "sync_boost",
+                0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+                0x80: "hw_power_brake_slowdown", 0x2: "applications_clocks_setting",
+                0x100: "display_clock_setting"}
+
+
+def lu_flops(n: int) -> float:
+    return 2.0 * n ** 3 / 3.0
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        d["source"] = "measured"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/<name>.json), if present."""
+    p = os.path.join(ROOT, "profiles", f"{name}.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+class ClockSampler:
+    """Samples SM clocks and clock-event reasons through NVML every 20 ms."""
+
+    def __init__(self, device_index: int):
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in NVML_REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t is not None:
+            self._t.join()
+        return False
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def cpu_baseline(wl: dict, budget_s: float = 12.0) -> dict:
+    """The CPU restatement of the reference algorithm (oracle, all host
+    threads) on a bounded sample of the same workload: the leading outer
+    steps of the same n x n factorization, run until the time budget is
+    spent.  TFLOP/s = (2n^3/3 - 2(n-k nb)^3/3) / time for k steps done."""
+    import oracle as O
+    n, nb = wl["n"], wl["nb"]
+    a = O.gen_matrix(n, seed=1, kind=wl["kind"], alpha=wl["alpha"], kscale=wl["kscale"])
+    t0 = time.perf_counter()
+    k = 0
+    nc = (n + nb - 1) // nb
+    while k < nc and time.perf_counter() - t0 < budget_s:
+        O.lu_rl_steps(a, nb, wl["oracle_fmt"], k, k + 1)
+        k += 1
+    dt = time.perf_counter() - t0
+    rest = max(0, n - k * nb)
+    flops = lu_flops(n) - lu_flops(rest)
+    return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"outer steps 0..{k - 1} of {nc} (nb={nb}) of the n={n} "
+                      f"factorization, {dt:.1f} s, {flops / 1e12:.2f} TFLOP"}
+
+
+def run_reference(args, wl) -> None:
+    """--impl reference: the reference algorithm as its CPU restatement on
+    the host cores (the reference itself has no CPU path), same workload,
+    each step a bounded sample (the first outer step of a fresh copy)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle as O
+    n, nb = wl["n"], wl["nb"]
+    base = O.gen_matrix(n, seed=1, kind=wl["kind"], alpha=wl["alpha"], kscale=wl["kscale"])
+    a = O.colmajor(n, n)
+    steps_done = 0
+    flops = lu_flops(n) - lu_flops(n - nb)
+    times = []
+    for i in range(args.warmup + args.steps):
+        np.copyto(a, base)
+        t0 = time.perf_counter()
+        O.lu_rl_steps(a, nb, wl["oracle_fmt"], 0, 1)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            steps_done += 1
+    total = sum(times)
+    value = steps_done * flops / total / 1e12
+    sample = (f"per step: outer step 0 (panel + trailing update, "
+              f"{flops / 1e9:.1f} GFLOP) of the n={n} factorization on a fresh copy")
+    line = {
+        "metric": "LU TFLOP/s (2n^3/3)", "value": value, "unit": "TFLOP/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / max(1, steps_done),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if wl["oracle_fmt"] == 0 else "f32 storage, rounded-operand update",
+        "data": "synthetic (seeded counter-based generator)",
+        "config": config_of(args, wl),
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": O.num_threads(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl) -> dict:
+    return {"workload": args.workload, "n": wl["n"], "nb": wl["nb"],
+            "variant": "right-looking", "inner_update": "FP32",
+            "outer_update": wl["outer"],
+            "matrix": f"R + D, R ~ {'N(0,1)/sqrt(n)' if wl['kind'] else 'U[-1,1)'}, "
+                      f"row dominance {wl['alpha']}",
+            "l2": "inputs larger than L2: a distinct 4n^2-byte matrix per step",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import remifa_b200 as rb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    n, nb = wl["n"], wl["nb"]
+    outer = getattr(rb.compute_type, wl["outer"])
+    nmat = args.warmup + args.steps
+    base = rb.gen_matrix(n, seed=1 + rank, kind=wl["kind"], alpha=wl["alpha"],
+                         kscale=wl["kscale"], device=dev)
+    mats = []
+    for _ in range(nmat):
+        m = rb.colmajor_empty(n, n, n, torch.float32, dev)
+        m.copy_(base)
+        mats.append(m)
+    ws = torch.empty(rb.workspace_size(n, nb=nb, outer=outer), dtype=torch.uint8, device=dev)
+    infos = torch.zeros(nmat, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for i in range(args.warmup):
+        rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1], workspace=ws)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with rb.profile() as prof:
+            t_start.record(stream)
+            for i in range(args.warmup, nmat):
+                rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1],
+                               workspace=ws)
+            t_end.record(stream)
+            torch.cuda.synchronize(dev)
+    ms = t_start.elapsed_time(t_end)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    bad = int((infos != 0).sum().item())
+    value = world * args.steps * lu_flops(n) / (ms / 1e3) / 1e12
+
+    # ---- end to end: pinned host matrix -> device -> factor -> host
+    # column-major pinned host buffers (same strides as the device matrix, so
+    # each transfer is one contiguous copy)
+    host_a = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+    host_a.copy_(base)
+    host_lu = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+    dA = mats[0]
+    e_ms = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dA.copy_(host_a, non_blocking=True)
+        rb.lu_nopiv_rl(dA, nb=nb, outer=outer, info=infos[0:1], workspace=ws)
+        host_lu.copy_(dA, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i > 0:  # first iteration warms the pinned paths
+            e_ms.append(e0.elapsed_time(e1))
+    e2e_ms = sum(e_ms) / len(e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * lu_flops(n) / (e2e_ms / 1e3) / 1e12
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    peaks = measured_peaks()
+    dom = "tc_update" if outer != rb.FP32 else "sgemm_update"
+    ent = prof.entries.get(dom, {})
+    roofline = None
+    if ent.get("launches"):
+        avg_ms = ent["total_ms"] / ent["launches"]
+        if dom == "tc_update":
+            achieved = ent["bytes"] / (ent["total_ms"] / 1e3) / 1e9
+            peak = peaks["hbm_gbs"]
+            tr = profiled_traffic(f"tc_update_{args.workload}")
+            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peaks["source"] + " hbm_gbs",
+                        "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+                        "algorithmic_bytes_per_launch": ent["bytes"] / ent["launches"],
+                        "avg_launch_ms": avg_ms, "launches": ent["launches"],
+                        "time_share": ent["total_ms"] / ms}
+        else:
+            achieved = ent["flops"] / (ent["total_ms"] / 1e3) / 1e12
+            roofline = {"kernel": dom, "bound": "fp32-simt", "achieved": achieved,
+                        "peak": None, "unit": "TFLOP/s", "frac": None,
+                        "note": "FP32 SIMT GEMM (no tensor cores on the FP32 plain path)",
+                        "traffic": None, "avg_launch_ms": avg_ms,
+                        "launches": ent["launches"],
+                        "time_share": ent["total_ms"] / ms}
+    line = {
+        "metric": "LU TFLOP/s (2n^3/3)",
+        "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if outer == rb.FP32 else
+                 f"f32 storage, {wl['outer']} update (fp32 accumulate)",
+        "data": "synthetic (seeded counter-based generator on the device)",
+        "config": config_of(args, wl),
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": 4 * n * n, "d2h_bytes_per_step": 4 * n * n,
+                "path": "lu_nopiv_rl_c via remifa_b200.lu_nopiv_rl, pinned host buffers"},
+        "gpu_launches": prof.launches,
+        "roofline": roofline,
+        "kernels": {k: {"launches": v["launches"], "ms": v["total_ms"]}
+                    for k, v in prof.entries.items()},
+        "clocks": clk.summary(),
+        "bad_info_steps": bad,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -171,6 +171,23 @@ LU_API lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
                           int64_t lda, uint64_t seed, int kind, double alpha,
                           int kscale, double gamma_bits);
 
+/* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
+typedef struct lu_profile_entry {
+  char name[32];     /* kernel class, e.g. "tc_update", "diag_factor" */
+  int64_t launches;  /* launches recorded */
+  double total_ms;   /* summed CUDA-event time on the launching stream */
+  double bytes;      /* summed algorithmic bytes (HBM-bound kernels) */
+  double flops;      /* summed algorithmic flops */
+} lu_profile_entry;
+
+/* Start recording CUDA events around each kernel class (clears old data). */
+LU_API void lu_profile_begin(void);
+/* Stop recording, wait for the recorded events and write up to max_entries
+ * aggregated entries; returns the number of kernel classes seen. */
+LU_API int lu_profile_end(lu_profile_entry* out, int max_entries);
+/* Number of kernels this library has launched in this process. */
+LU_API long long lu_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

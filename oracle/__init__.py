@@ -68,6 +68,8 @@ def lib():
                                        _i64, _f32p, _i64]
         L.orc_lu_rl_f32.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int,
                                     ctypes.c_int]
+        L.orc_lu_rl_f32_range.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int,
+                                          ctypes.c_int, _i64, _i64]
         L.orc_lu_f64.argtypes = [_i64, _f64p, _i64]
         L.orc_lu_solve_f64.argtypes = [_i64, _f64p, _i64, _f64p]
         L.orc_lu_solve_f32.argtypes = [_i64, _f32p, _i64, _f32p]
@@ -169,6 +171,13 @@ def lu_rl(a: np.ndarray, nb: int = 256, outer_fmt: int = 0, threads: int = 0) ->
     out[:, :] = a
     lib().orc_lu_rl_f32(a.shape[0], a.shape[1], nb, _p32(out), ld(out), outer_fmt, threads)
     return out
+
+
+def lu_rl_steps(a: np.ndarray, nb: int, outer_fmt: int, kk0: int, kk1: int,
+                threads: int = 0) -> None:
+    """In place: outer steps [kk0, kk1) of the restated RL factorization."""
+    lib().orc_lu_rl_f32_range(a.shape[0], a.shape[1], nb, _p32(a), ld(a), outer_fmt,
+                              threads, kk0, kk1)
 
 
 def lu_f64(a: np.ndarray) -> np.ndarray:

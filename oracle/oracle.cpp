@@ -316,12 +316,19 @@ void round_copy(int64_t rows, int64_t cols, const float* a, int64_t lda,
 // reference src/lu_nopiv.hxx:130-197
 void orc_lu_rl_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int outer_fmt, int threads) {
+  orc_lu_rl_f32_range(m, n, nb, a, lda, outer_fmt, threads, 0, -1);
+}
+
+void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
+                         int64_t lda, int outer_fmt, int threads, int64_t kk0,
+                         int64_t kk1) {
   const int saved = omp_get_max_threads();
   if (threads > 0) omp_set_num_threads(threads);
   const int64_t nc = (n - 1) / nb + 1;
+  if (kk1 < 0 || kk1 > nc) kk1 = nc;
   std::vector<float> lc, uc;
   std::vector<int> ls, us;
-  for (int64_t kk = 0; kk < nc; ++kk) {
+  for (int64_t kk = kk0; kk < kk1; ++kk) {
     const int64_t ofs = kk * nb;
     const int64_t ofst = (kk + 1) * nb;
     const int64_t in = std::min(n - ofs, nb);

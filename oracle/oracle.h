@@ -75,6 +75,11 @@ void orc_gemm_sub_f32(int64_t m, int64_t n, int64_t k, const float* a,
  *   thread count. */
 void orc_lu_rl_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int outer_fmt, int threads);
+/* Only outer steps [kk0, kk1) of the same factorization (kk1 < 0: to the
+ * end); running [0,k) then [k,end) equals one full call. */
+void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
+                         int64_t lda, int outer_fmt, int threads, int64_t kk0,
+                         int64_t kk1);
 
 /* ---- FP64 oracle ----------------------------------------------------- */
 void orc_lu_f64(int64_t n, double* a, int64_t lda);

@@ -38,6 +38,16 @@ class LuOpts(ctypes.Structure):
     ]
 
 
+class LuProfileEntry(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches", ctypes.c_int64),
+        ("total_ms", ctypes.c_double),
+        ("bytes", ctypes.c_double),
+        ("flops", ctypes.c_double),
+    ]
+
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _int = ctypes.c_int
@@ -63,6 +73,9 @@ SIGNATURES = {
                                 _i64, _vp, ctypes.c_size_t]),
     "lu_gen_matrix_c": (_int, [_vp, _i64, _vp, _i64, ctypes.c_uint64, _int,
                                ctypes.c_double, _int, ctypes.c_double]),
+    "lu_profile_begin": (None, []),
+    "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
+    "lu_launch_count": (ctypes.c_longlong, []),
 }
 
 _lib = None

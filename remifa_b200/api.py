@@ -204,3 +204,37 @@ def gen_matrix(n: int, seed: int, kind: int = 0, alpha: float = 2.0,
                                     float(alpha), int(kscale), float(gamma_bits))
     _lib.check(st, "lu_gen_matrix_c")
     return a
+
+
+class profile:
+    """Context manager recording per-kernel-class CUDA-event times inside
+    the library (on the stream each kernel is launched on).
+
+        with rb.profile() as prof:
+            rb.lu_nopiv_rl(a, outer=rb.TC32)
+        prof.entries["tc_update"]  -> dict(launches, total_ms, bytes, flops)
+    """
+
+    def __enter__(self):
+        self.entries = {}
+        self.launches0 = _lib.lib().lu_launch_count()
+        _lib.lib().lu_profile_begin()
+        return self
+
+    def __exit__(self, *exc):
+        L = _lib.lib()
+        buf = (_lib.LuProfileEntry * 64)()
+        k = L.lu_profile_end(buf, 64)
+        for i in range(min(k, 64)):
+            e = buf[i]
+            self.entries[e.name.decode()] = dict(launches=int(e.launches),
+                                                 total_ms=float(e.total_ms),
+                                                 bytes=float(e.bytes),
+                                                 flops=float(e.flops))
+        self.launches = L.lu_launch_count() - self.launches0
+        return False
+
+
+def launch_count() -> int:
+    """Kernels launched by liblu_b200.so in this process so far."""
+    return int(_lib.lib().lu_launch_count())

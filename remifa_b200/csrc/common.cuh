@@ -31,6 +31,7 @@ constexpr int kNoBadPivot = 0x7f7f7f7f;
       ::lub::record_cuda_error(_e, "kernel launch", __FILE__, __LINE__); \
       return LU_ERR_CUDA;                                               \
     }                                                                   \
+    ::lub::count_launch();                                              \
   } while (0)
 
 #define LUB_TRY(expr)                       \
@@ -41,6 +42,8 @@ constexpr int kNoBadPivot = 0x7f7f7f7f;
 
 void record_cuda_error(cudaError_t e, const char* what, const char* file,
                        int line);
+// Counts one kernel launch of this library (profile.cu).
+void count_launch();
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -49,6 +52,16 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 int sm_count();
 
 // ---- device helpers -------------------------------------------------------
+
+// Asynchronous 4-byte global -> shared copy (no register round trip, so a
+// thread can have hundreds in flight).  Complete with cp_async_wait_all().
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 // Record the 1-based global index of a zero / non-finite pivot.
 __device__ __forceinline__ void note_pivot(float d, int64_t col0,

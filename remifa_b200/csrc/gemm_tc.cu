@@ -1,0 +1,403 @@
+// Tensor-core Schur update on sm_100a: C (fp32, column-major) -= A * B with
+// A and B in fp16 / bf16 / e4m3, accumulated in fp32 in tensor memory.
+//
+// Replaces the reference's cublasGemmEx TC32 call for the trailing update
+// (src/gemm.cu:255-287 called from src/lu_nopiv.hxx:172-183).
+//
+// Operand layouts (both K-major, what the tensor core consumes directly):
+//   A : M x K, row-major        (row i at A + i*lda_p; the L21 copy)
+//   B : K x N, column-major     (column j at B + j*ldb_p; the U12 copy)
+// so a 128 x BK tile of A and a 256 x BK tile of B are each one TMA box of
+// 128-byte rows with the 128-byte swizzle.
+//
+// One persistent CTA per SM, 10 warps:
+//   warp 0      : TMA producer (4-stage ring of A/B tiles, mbarriers)
+//   warp 1      : TMEM allocator + single-thread tcgen05.mma issuer
+//                 (128 x 256 x 16 per instruction), commits to mbarriers
+//   warps 2..9  : epilogue, two warpgroups; each warp owns 32 rows (its TMEM
+//                 lane quarter) and 128 columns of the tile.  It reads the
+//                 accumulator with tcgen05.ld in 32 x 32 chunks, writes
+//                 scale * acc into a shared-memory staging tile and issues a
+//                 TMA reduce-add of that tile into C, so C is updated in L2
+//                 (one fp32 add, the same single rounding as C - acc) without
+//                 the SM ever loading C.  When C cannot be described by a
+//                 tensor map (unaligned), the epilogue loads and stores C with
+//                 ordinary coalesced accesses instead.
+// Two TMEM accumulators (2 x 256 columns) let the epilogue of tile i overlap
+// the MMAs of tile i+1.  Every mbarrier wait is bounded (sm100.cuh).
+#include "common.cuh"
+#include "kernels.cuh"
+#include "sm100.cuh"
+#include "tc_gemm.cuh"
+
+#include <cstring>
+#include <mutex>
+
+namespace lub {
+namespace {
+
+using namespace sm100;
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int kRowBytes = 128;                  // bytes of K per tile row
+constexpr int kStageA = BM * kRowBytes;         // 16 KB
+constexpr int kStageB = BN * kRowBytes;         // 32 KB
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 32 * (2 + kEpiWarps);  // 320
+constexpr int kTmemCols = 2 * BN;               // two accumulators
+constexpr int kEpiChunk = 32 * 32 * 4;          // one 32 x 32 fp32 staging tile
+
+template <int EPI> struct Cfg;
+template <> struct Cfg<0> {  // register epilogue
+  static constexpr int kStages = 4;
+  static constexpr size_t kEpiBytes = 0;
+};
+template <> struct Cfg<1> {  // TMA reduce-add epilogue, 2 staging tiles per warp
+  static constexpr int kStages = 3;
+  static constexpr size_t kEpiBytes = (size_t)kEpiWarps * 2 * kEpiChunk;
+};
+template <int EPI>
+constexpr size_t smem_bytes() {
+  return 1024 /*align slack*/ + (size_t)Cfg<EPI>::kStages * (kStageA + kStageB) +
+         Cfg<EPI>::kEpiBytes + 256;
+}
+
+struct TcParams {
+  float* C;
+  int64_t ldc;
+  int M, N, K;
+  int kb_count;        // number of BK blocks along K
+  int tiles_m, tiles_n;
+  const int* scale_a;  // per 128-row tile of A (log2), or null
+  const int* scale_b;  // per 128-column tile of B (log2), or null
+  float alpha;         // C += alpha * acc (alpha = -1 for the Schur update)
+  int* err;
+};
+
+// KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
+// EPI  0: C loaded/stored by the epilogue threads; 1: TMA reduce-add.
+template <int KIND, int EPI>
+__global__ void __launch_bounds__(kThreads, 1)
+tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
+                 const __grid_constant__ CUtensorMap tmap_b,
+                 const __grid_constant__ CUtensorMap tmap_c, TcParams p,
+                 uint32_t idesc) {
+  constexpr int kStages = Cfg<EPI>::kStages;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + kStages * kStageA;
+  uint8_t* sEpi = sB + kStages * kStageB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sEpi + Cfg<EPI>::kEpiBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* tfull = empty + kStages;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int num_tiles = p.tiles_m * p.tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], kEpiWarps);
+    }
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      prefetch_tmap(&tmap_a);
+      prefetch_tmap(&tmap_b);
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+        const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        for (int kb = 0; kb < p.kb_count; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty)) { ok = false; break; }
+          mbar_arrive_expect_tx(&full[s], kStageA + kStageB);
+          const int kx = kb * kRowBytes;  // element offset along K == bytes for 8-bit
+          const int kelem = KIND == 0 ? kb * (kRowBytes / 2) : kx;
+          tma_load_2d(sA + s * kStageA, &tmap_a, &full[s], kelem, tm * BM);
+          tma_load_2d(sB + s * kStageB, &tmap_b, &full[s], kelem, tn * BN);
+          if (++s == kStages) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int local = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+        const int acc = local & 1;
+        const uint32_t aph = (local >> 1) & 1;
+        if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + acc * BN;
+        for (int kb = 0; kb < p.kb_count; ++kb) {
+          if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * kStageA);
+          const uint32_t b0 = smem_u32(sB + s * kStageB);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {  // 4 MMAs of 32 bytes of K each
+            const uint64_t ad = sw128_kmajor_desc(a0 + k * 32);
+            const uint64_t bd = sw128_kmajor_desc(b0 + k * 32);
+            const uint32_t accum = (kb > 0 || k > 0) ? 1u : 0u;
+            if (KIND == 0) mma_f16(d_tmem, ad, bd, idesc, accum);
+            else mma_f8(d_tmem, ad, bd, idesc, accum);
+          }
+          mma_commit(&empty[s]);  // frees the stage when these MMAs finish
+          if (++s == kStages) { s = 0; ph ^= 1; }
+        }
+        if (ok) mma_commit(&tfull[acc]);
+      }
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int ew = warp - 2;             // 0..7
+    const int quarter = warp & 3;        // TMEM lane quarter this warp may read
+    const int half = ew / 4;             // columns [128*half, 128*half + 128)
+    const int row_in_tile = quarter * 32 + lane;
+    int local = 0;
+    bool ok = true;
+    if constexpr (EPI == 1) {
+      float* stage = reinterpret_cast<float*>(sEpi + (size_t)ew * 2 * kEpiChunk);
+      int issued = 0;  // reduces issued by this warp; buffer = issued & 1
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+        const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        const int acc = local & 1;
+        const uint32_t aph = (local >> 1) & 1;
+        const int col0 = tn * BN + half * 128;
+        float sa = 1.0f;
+        if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
+        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+          const int cc = col0 + c * 32;
+          float av[32];
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                                 (uint32_t)(acc * BN + half * 128 + c * 32);
+          tmem_ld32(taddr, av);
+          tmem_ld_wait();
+          if (c == 3) {  // accumulator fully read: hand it back to the MMA warp
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[acc]);
+          }
+          // whole 32 x 32 box outside C: nothing to add
+          if (cc >= p.N || tm * BM + quarter * 32 >= p.M) continue;
+          float s = p.alpha * sa;
+          if (p.scale_b) s = ldexpf(s, -p.scale_b[cc / 128]);
+          float* buf = stage + (issued & 1) * (kEpiChunk / 4);
+          // the reduce issued two commits ago (same buffer) must be done
+          // reading it; at most the latest one (other buffer) may remain
+          if (lane == 0) bulk_wait_group_read<1>();
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) buf[j * 32 + lane] = s * av[j];
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            tma_reduce_add_2d(&tmap_c, buf, tm * BM + quarter * 32, cc);
+            bulk_commit_group();
+          }
+          ++issued;
+        }
+      }
+      if (lane == 0) bulk_wait_group<0>();
+      __syncwarp();
+    } else {
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+        const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        const int acc = local & 1;
+        const uint32_t aph = (local >> 1) & 1;
+        const int64_t row = (int64_t)tm * BM + row_in_tile;
+        const bool row_ok = row < p.M;
+        const int col0 = tn * BN + half * 128;
+        float sa = 1.0f;
+        if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
+        const int64_t ldc = p.ldc;
+        float* cbase = p.C + row + (int64_t)col0 * ldc;
+        float cv[32];
+        // load the first chunk of C before waiting for the accumulator
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          cv[j] = (row_ok && col0 + j < p.N) ? cbase[j * ldc] : 0.0f;
+        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+          float* cp = cbase + (int64_t)(c * 32) * ldc;
+          const int cc = col0 + c * 32;
+          if (c > 0) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              cv[j] = (row_ok && cc + j < p.N) ? cp[j * ldc] : 0.0f;
+          }
+          float av[32];
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                                 (uint32_t)(acc * BN + half * 128 + c * 32);
+          tmem_ld32(taddr, av);
+          tmem_ld_wait();
+          float s = p.alpha * sa;
+          if (p.scale_b) s = ldexpf(s, -p.scale_b[cc / 128]);
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (row_ok && cc + j < p.N) cp[j * ldc] = __fmaf_rn(s, av[j], cv[j]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[acc]);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, kTmemCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side: tensor maps through the driver entry point (no -lcuda)
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
+                                   void*, const cuuint64_t*, const cuuint64_t*,
+                                   const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// rows x inner (inner contiguous, row stride ld elements), box box_rows x
+// (128 bytes of inner).
+// Column-major fp32 C (rows contiguous), 32 x 32 boxes, no swizzle.
+bool make_c_map(CUtensorMap* map, float* C, int64_t M, int64_t N, int64_t ldc) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)N};
+  cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool make_kmajor_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
+                     int esize, int64_t inner, int64_t rows, int64_t ld,
+                     int box_rows) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * esize)};
+  cuuint32_t box[2] = {(cuuint32_t)(kRowBytes / esize), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
+                           int64_t N, int64_t K, float alpha, const void* A,
+                           int64_t lda_p, const void* B, int64_t ldb_p, float* C,
+                           int64_t ldc, const int* scale_a, const int* scale_b,
+                           int* err, int max_ctas) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
+  if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
+  const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
+  if ((lda_p * esize) % 16 != 0 || (ldb_p * esize) % 16 != 0 ||
+      (uintptr_t)A % 16 != 0 || (uintptr_t)B % 16 != 0)
+    return LU_ERR_INVALID_ARG;
+  if (lda_p < K || ldb_p < K) return LU_ERR_INVALID_ARG;
+  CUtensorMapDataType dt = kind == TcOperand::F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                         : kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                   : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  CUtensorMap ma, mb;
+  if (!make_kmajor_map(&ma, A, dt, esize, K, M, lda_p, BM)) return LU_ERR_CUDA;
+  if (!make_kmajor_map(&mb, B, dt, esize, K, N, ldb_p, BN)) return LU_ERR_CUDA;
+
+  TcParams p;
+  p.C = C;
+  p.ldc = ldc;
+  p.M = (int)M;
+  p.N = (int)N;
+  p.K = (int)K;
+  p.kb_count = (int)ceil_div(K * esize, kRowBytes);
+  p.tiles_m = (int)ceil_div(M, BM);
+  p.tiles_n = (int)ceil_div(N, BN);
+  p.scale_a = scale_a;
+  p.scale_b = scale_b;
+  p.alpha = alpha;
+  p.err = err;
+  const int tiles = p.tiles_m * p.tiles_n;
+  const int grid = std::min(tiles, max_ctas > 0 ? max_ctas : sm_count());
+  // TMA reduce-add needs a 16-byte aligned C with a 16-byte multiple stride
+  CUtensorMap mc;
+  std::memset(&mc, 0, sizeof(mc));
+  const bool tma_c = ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) &&
+                     make_c_map(&mc, C, M, N, ldc);
+  const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
+  const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
+  if (kind == TcOperand::E4M3) {
+    if (tma_c) {
+      LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 1>, smem_bytes<1>()));
+      tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, mc, p, idesc);
+    } else {
+      LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 0>, smem_bytes<0>()));
+      tc_update_kernel<1, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, mc, p, idesc);
+    }
+  } else {
+    if (tma_c) {
+      LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 1>, smem_bytes<1>()));
+      tc_update_kernel<0, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, mc, p, idesc);
+    } else {
+      LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 0>, smem_bytes<0>()));
+      tc_update_kernel<0, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, mc, p, idesc);
+    }
+  }
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+}  // namespace lub

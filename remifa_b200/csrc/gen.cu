@@ -108,9 +108,11 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
                                            kscale, gamma_bits, rowsum);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
+    count_launch();
     gen_diag_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(
         n, a, lda, scale, alpha, kscale, gamma_bits, rowsum);
     e = cudaGetLastError();
+    if (e == cudaSuccess) count_launch();
   }
   cudaFreeAsync(rowsum, st);
   if (e != cudaSuccess) {

@@ -9,10 +9,10 @@ namespace lub {
 size_t diag_smem_bytes(int w);
 lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
                              int64_t col0, int* first_bad);
-lu_status launch_lpanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
-                        int64_t M, int w);
-lu_status launch_upanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
-                        int64_t N, int w);
+// L rows (M of them, below) and U columns (N, right) of the w x w factored
+// diagonal block dg, one launch.
+lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
+                         int64_t M, int64_t N);
 lu_status launch_ref_panel(cudaStream_t st, int64_t m, int n, const float* d,
                            int64_t ldd, float* l, int64_t ldl, float* u,
                            int64_t ldu, int* stat);
@@ -35,7 +35,8 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
 
 // misc.cu
 lu_status launch_fill_int(cudaStream_t st, int* p, int v, int64_t count);
-lu_status launch_finalize_info(cudaStream_t st, const int* first_bad, int* info);
+lu_status launch_finalize_info(cudaStream_t st, const int* first_bad,
+                               const int* err, int* info);
 
 // Set the dynamic shared-memory limit of `func` for the current device.
 cudaError_t set_smem_limit(const void* func, size_t bytes);

@@ -14,10 +14,12 @@ __global__ void fill_int_kernel(int* p, int v, int64_t count) {
   if (i < count) p[i] = v;
 }
 
-// LAPACK-style info: 0, or the 1-based column of the first bad pivot.
-__global__ void finalize_info_kernel(const int* first_bad, int* info) {
+// LAPACK-style info: 0, or the 1-based column of the first bad pivot;
+// -1 if a bounded device-side wait gave up (err non-zero).
+__global__ void finalize_info_kernel(const int* first_bad, const int* err,
+                                     int* info) {
   const int f = *first_bad;
-  *info = (f == kNoBadPivot) ? 0 : f;
+  *info = (err != nullptr && *err != 0) ? -1 : (f == kNoBadPivot) ? 0 : f;
 }
 
 std::mutex g_mu;
@@ -77,8 +79,8 @@ lu_status launch_fill_int(cudaStream_t st, int* p, int v, int64_t count) {
 }
 
 lu_status launch_finalize_info(cudaStream_t st, const int* first_bad,
-                               int* info) {
-  finalize_info_kernel<<<1, 1, 0, st>>>(first_bad, info);
+                               const int* err, int* info) {
+  finalize_info_kernel<<<1, 1, 0, st>>>(first_bad, err, info);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

@@ -53,21 +53,26 @@ __device__ __forceinline__ void factor_tile_warp(float (&v)[8], int tw,
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block: w x w (w <= 128) at a (lda), factored in place.
-// Shared: D[w x w] column-major with leading dimension LD = w | 1.
+// Diagonal block: w x w (w <= 128) at a (lda), factored in place by one CTA.
+// Shared: D (w x w, column-major, leading dimension LD = round4(w) + 4 so
+// 4-row groups are 16-byte aligned), plus the L and U strips of the current
+// tile (Ls[k][i], Us[k][j]) for vectorised rank-8 updates.
 __global__ void __launch_bounds__(kThreads)
 diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
                    int* first_bad) {
-  extern __shared__ float smem[];
-  const int LD = w | 1;
+  extern __shared__ __align__(16) float smem[];
+  const int LD = ((w + 3) / 4) * 4 + 4;
   float* D = smem;
-  float* inv = smem + (size_t)LD * w;
+  float* Ls = D + (size_t)LD * w;     // [8][128]
+  float* Us = Ls + 8 * 128;           // [8][128]
+  float* inv = Us + 8 * 128;          // [8]
   const int tid = threadIdx.x;
 
   for (int idx = tid; idx < w * w; idx += kThreads) {
     const int i = idx % w, j = idx / w;
-    D[i + j * LD] = a[i + (int64_t)j * lda];
+    cp_async4(&D[i + j * LD], &a[i + (int64_t)j * lda]);
   }
+  cp_async_wait_all();
   __syncthreads();
 
   const int nt = (w + 7) / 8;
@@ -91,10 +96,15 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     const int s = w - t0 - 8;  // trailing extent inside the block
     if (s <= 0) break;
     // Phase B: L rows below the tile (threads 0..127), U columns right of it
-    // (threads 128..255).
+    // (threads 128..255); results also go to the strip buffers.
     if (tid < 128) {
       if (tid < s) {
         const int i = t0 + 8 + tid;
+        float u[8][8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+          for (int c = k + 1; c < 8; ++c) u[k][c] = D[(t0 + k) + (t0 + c) * LD];
         float row[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) row[c] = D[i + (t0 + c) * LD];
@@ -102,34 +112,45 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
         for (int k = 0; k < 8; ++k) {
           row[k] = __fmul_rn(row[k], inv[k]);
 #pragma unroll
-          for (int c = k + 1; c < 8; ++c)
-            row[c] = __fmaf_rn(-row[k], D[(t0 + k) + (t0 + c) * LD], row[c]);
+          for (int c = k + 1; c < 8; ++c) row[c] = __fmaf_rn(-row[k], u[k][c], row[c]);
         }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) D[i + (t0 + c) * LD] = row[c];
+        for (int c = 0; c < 8; ++c) {
+          D[i + (t0 + c) * LD] = row[c];
+          Ls[c * 128 + (i - t0 - 8)] = row[c];
+        }
       }
     } else {
       const int q = tid - 128;
       if (q < s) {
         const int j = t0 + 8 + q;
+        float l[8][8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+          for (int r = k + 1; r < 8; ++r) l[r][k] = D[(t0 + r) + (t0 + k) * LD];
         float col[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) col[r] = D[(t0 + r) + j * LD];
 #pragma unroll
         for (int k = 0; k < 8; ++k)
 #pragma unroll
-          for (int r = k + 1; r < 8; ++r)
-            col[r] = __fmaf_rn(-D[(t0 + r) + (t0 + k) * LD], col[k], col[r]);
+          for (int r = k + 1; r < 8; ++r) col[r] = __fmaf_rn(-l[r][k], col[k], col[r]);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) D[(t0 + r) + j * LD] = col[r];
+        for (int r = 0; r < 8; ++r) {
+          D[(t0 + r) + j * LD] = col[r];
+          Us[r * 128 + q] = col[r];
+        }
       }
     }
     __syncthreads();
-    // Phase C: rank-8 update of the trailing s x s block, 4x4 per item.
+    // Phase C: rank-8 update of the trailing s x s block, 4 x 4 per item:
+    // acc = sum_k fma(L[i][t0+k], U[t0+k][j]) in k order, D[i][j] -= acc.
     const int nb4 = (s + 3) / 4;
+    const bool vec = (s % 4 == 0);
     for (int b = tid; b < nb4 * nb4; b += kThreads) {
-      const int i0 = t0 + 8 + 4 * (b % nb4);
-      const int j0 = t0 + 8 + 4 * (b / nb4);
+      const int li = 4 * (b % nb4), lj = 4 * (b / nb4);  // local to the block
+      const int i0 = t0 + 8 + li, j0 = t0 + 8 + lj;
       float acc[4][4];
 #pragma unroll
       for (int ii = 0; ii < 4; ++ii)
@@ -137,27 +158,37 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
         for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = 0.0f;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        float l[4], u[4];
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii)
-          l[ii] = (i0 + ii < w) ? D[(i0 + ii) + (t0 + k) * LD] : 0.0f;
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          u[jj] = (j0 + jj < w) ? D[(t0 + k) + (j0 + jj) * LD] : 0.0f;
+        const float4 l4 = *reinterpret_cast<const float4*>(&Ls[k * 128 + li]);
+        const float4 u4 = *reinterpret_cast<const float4*>(&Us[k * 128 + lj]);
+        const float l[4] = {l4.x, l4.y, l4.z, l4.w};
+        const float u[4] = {u4.x, u4.y, u4.z, u4.w};
 #pragma unroll
         for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj)
             acc[ii][jj] = __fmaf_rn(l[ii], u[jj], acc[ii][jj]);
       }
+      if (vec && (i0 % 4) == 0) {
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
+        for (int jj = 0; jj < 4; ++jj) {
+          float4* p = reinterpret_cast<float4*>(&D[i0 + (j0 + jj) * LD]);
+          float4 c4 = *p;
+          c4.x = __fsub_rn(c4.x, acc[0][jj]);
+          c4.y = __fsub_rn(c4.y, acc[1][jj]);
+          c4.z = __fsub_rn(c4.z, acc[2][jj]);
+          c4.w = __fsub_rn(c4.w, acc[3][jj]);
+          *p = c4;
+        }
+      } else {
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          if (i0 + ii < w && j0 + jj < w) {
-            float* p = &D[(i0 + ii) + (j0 + jj) * LD];
-            *p = __fsub_rn(*p, acc[ii][jj]);
-          }
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            if (i0 + ii < w && j0 + jj < w) {
+              float* p = &D[(i0 + ii) + (j0 + jj) * LD];
+              *p = __fsub_rn(*p, acc[ii][jj]);
+            }
+      }
     }
     __syncthreads();
   }
@@ -169,181 +200,160 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 }
 
 // ---------------------------------------------------------------------------
-// L panel: rows [0, M) of `a` (lda) with w columns, against the factored
-// diagonal block `dg` (lda), in place.
-__global__ void __launch_bounds__(kThreads)
-lpanel_kernel(float* __restrict__ a, int64_t lda, const float* __restrict__ dg,
-              int64_t M, int w) {
-  extern __shared__ float smem[];
-  constexpr int LDS = kStrip + 1;
-  float* S = smem;                       // kStrip x w, column-major, ld LDS
-  float* Ut = S + (size_t)LDS * w;       // 8 x w, row-major (Ut[k*w + c])
-  float* inv = Ut + 8 * w;               // 8
-  const int tid = threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.x * kStrip;
-  const int rows = (int)((M - r0) < kStrip ? (M - r0) : kStrip);
+// L and U panels of one sub-panel, one launch.  `dg` is the factored w x w
+// diagonal block (lda); M rows lie below it, N columns right of it.
+// Blocks [0, nL) each own kPanelT rows of L21 (one row per thread); blocks
+// [nL, ...) each own kPanelT columns of U12 (one column per thread).
+// A thread walks its row (column) tile by tile, left to right: it first
+// applies the rank-8 updates of all earlier tiles in order (acc over the 8
+// columns, one subtraction per tile -- the sequence the reference's K = 8
+// GEMMs produce), then the tile elimination of the panel kernel.  Rows and
+// columns are independent, so no block-wide synchronisation is needed after
+// the staging of the diagonal block.
+constexpr int kPanelT = 256;
 
-  for (int idx = tid; idx < kStrip * w; idx += kThreads) {
-    const int i = idx % kStrip, j = idx / kStrip;
-    S[i + j * LDS] = (i < rows) ? a[(r0 + i) + (int64_t)j * lda] : 0.0f;
+__global__ void __launch_bounds__(kPanelT)
+lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
+               int64_t N, int nL) {
+  extern __shared__ __align__(16) float smem[];
+  const int tid = threadIdx.x;
+  const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
+  const int nt = wp / 8;
+  // F[c*wp + r] = D[r][c]: the factored block, column-major with a padded
+  // (zero-filled) leading dimension so 4-element groups are 16-byte aligned.
+  // The L role reads its strict upper part (U), the U role its strict lower
+  // part (L); the diagonal gives 1/d.
+  float* F = smem;
+  float* inv = F + (size_t)wp * wp;  // wp
+  float* S = inv + wp;               // the strip
+  const bool is_l = (int)blockIdx.x < nL;
+
+  for (int idx = tid; idx < wp * wp; idx += kPanelT) {
+    const int r = idx % wp, c = idx / wp;
+    if (r < w && c < w) cp_async4(&F[idx], &dg[r + (int64_t)c * lda]);
+    else F[idx] = 0.0f;
   }
 
-  const int nt = (w + 7) / 8;
-  for (int t = 0; t < nt; ++t) {
-    const int t0 = 8 * t;
-    const int tw = min(8, w - t0);
-    __syncthreads();  // previous phase done with Ut / S
-    for (int idx = tid; idx < 8 * (w - t0); idx += kThreads) {
-      const int k = idx / (w - t0), c = t0 + idx % (w - t0);
-      Ut[k * w + c] = (k < tw) ? dg[(t0 + k) + (int64_t)c * lda] : 0.0f;
+  if (is_l) {
+    // strip: kPanelT rows x w columns, S[c*kPanelT + r]
+    const int64_t r0 = (int64_t)blockIdx.x * kPanelT;
+    float* A = dg + w;  // first row below the diagonal block
+    const int64_t row = r0 + tid;
+    for (int c = 0; c < w; ++c) {
+      if (row < M) cp_async4(&S[c * kPanelT + tid], &A[row + (int64_t)c * lda]);
+      else S[c * kPanelT + tid] = 0.0f;
     }
-    if (tid < 8) inv[tid] = (tid < tw) ? __fdiv_rn(1.0f, dg[(t0 + tid) + (int64_t)(t0 + tid) * lda]) : 0.0f;
+    cp_async_wait_all();
     __syncthreads();
-    // Phase A: eliminate the tile columns of each row.
-    if (tid < kStrip) {
-      float row[8];
+    for (int k = tid; k < wp; k += kPanelT)
+      inv[k] = (k < w) ? __fdiv_rn(1.0f, F[k * wp + k]) : 0.0f;
+    __syncthreads();
+    const int r = tid;
+    for (int T = 0; T < nt; ++T) {
+      const int tw = min(8, w - 8 * T);
+      float x[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) row[c] = (c < tw) ? S[tid + (t0 + c) * LDS] : 0.0f;
+      for (int j = 0; j < 8; ++j) x[j] = (j < tw) ? S[(8 * T + j) * kPanelT + r] : 0.0f;
+      for (int t = 0; t < T; ++t) {
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+        float l[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) l[k] = S[(8 * t + k) * kPanelT + r];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          // U[8t .. 8t+7][8T + j]: one column of F, 8 consecutive rows
+          const float4 u0 = *reinterpret_cast<const float4*>(&F[(8 * T + j) * wp + 8 * t]);
+          const float4 u1 = *reinterpret_cast<const float4*>(&F[(8 * T + j) * wp + 8 * t + 4]);
+          float a = acc[j];
+          a = __fmaf_rn(l[0], u0.x, a);
+          a = __fmaf_rn(l[1], u0.y, a);
+          a = __fmaf_rn(l[2], u0.z, a);
+          a = __fmaf_rn(l[3], u0.w, a);
+          a = __fmaf_rn(l[4], u1.x, a);
+          a = __fmaf_rn(l[5], u1.y, a);
+          a = __fmaf_rn(l[6], u1.z, a);
+          a = __fmaf_rn(l[7], u1.w, a);
+          acc[j] = a;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = __fsub_rn(x[j], acc[j]);
+      }
+      // tile elimination (src/lu_nopiv.cu:141-168): 1/d multiply, fused
+      // rank-1 updates inside the tile
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         if (k < tw) {
-          row[k] = __fmul_rn(row[k], inv[k]);
+          x[k] = __fmul_rn(x[k], inv[8 * T + k]);
 #pragma unroll
-          for (int c = k + 1; c < 8; ++c)
-            if (c < tw) row[c] = __fmaf_rn(-row[k], Ut[k * w + t0 + c], row[c]);
+          for (int j = k + 1; j < 8; ++j)
+            if (j < tw) x[j] = __fmaf_rn(-x[k], F[(8 * T + j) * wp + 8 * T + k], x[j]);
         }
       }
 #pragma unroll
-      for (int c = 0; c < 8; ++c)
-        if (c < tw) S[tid + (t0 + c) * LDS] = row[c];
+      for (int j = 0; j < 8; ++j)
+        if (j < tw) S[(8 * T + j) * kPanelT + r] = x[j];
     }
-    const int s = w - t0 - 8;
-    if (s <= 0) break;
+    for (int c = 0; c < w; ++c)
+      if (row < M) A[row + (int64_t)c * lda] = S[c * kPanelT + tid];
+  } else {
+    // strip: w rows x kPanelT columns, S[i*(kPanelT+1) + c]
+    constexpr int LS = kPanelT + 1;
+    const int64_t c0 = (int64_t)(blockIdx.x - nL) * kPanelT;
+    float* A = dg + (int64_t)w * lda;  // first column right of the block
+    for (int idx = tid; idx < w * kPanelT; idx += kPanelT) {
+      const int i = idx % w, cc = idx / w;
+      const int64_t col = c0 + cc;
+      if (col < N) cp_async4(&S[i * LS + cc], &A[i + col * lda]);
+      else S[i * LS + cc] = 0.0f;
+    }
+    cp_async_wait_all();
     __syncthreads();
-    // Phase B: rank-8 update of the trailing columns (4 rows x 4 cols/item).
-    const int ncb = (s + 3) / 4;
-    for (int b = tid; b < (kStrip / 4) * ncb; b += kThreads) {
-      const int i0 = 4 * (b % (kStrip / 4));
-      const int c0 = t0 + 8 + 4 * (b / (kStrip / 4));
-      float acc[4][4];
+    const int c = tid;
+    for (int T = 0; T < nt; ++T) {
+      const int tw = min(8, w - 8 * T);
+      float x[8];
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
+      for (int j = 0; j < 8; ++j) x[j] = (j < tw) ? S[(8 * T + j) * LS + c] : 0.0f;
+      for (int t = 0; t < T; ++t) {
+        float acc[8];
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = 0.0f;
+        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        float l[4], u[4];
+        for (int k = 0; k < 8; ++k) {
+          const float u = S[(8 * t + k) * LS + c];
+          const float4 l0 = *reinterpret_cast<const float4*>(&F[(8 * t + k) * wp + 8 * T]);
+          const float4 l1 = *reinterpret_cast<const float4*>(&F[(8 * t + k) * wp + 8 * T + 4]);
+          acc[0] = __fmaf_rn(l0.x, u, acc[0]);
+          acc[1] = __fmaf_rn(l0.y, u, acc[1]);
+          acc[2] = __fmaf_rn(l0.z, u, acc[2]);
+          acc[3] = __fmaf_rn(l0.w, u, acc[3]);
+          acc[4] = __fmaf_rn(l1.x, u, acc[4]);
+          acc[5] = __fmaf_rn(l1.y, u, acc[5]);
+          acc[6] = __fmaf_rn(l1.z, u, acc[6]);
+          acc[7] = __fmaf_rn(l1.w, u, acc[7]);
+        }
 #pragma unroll
-        for (int ii = 0; ii < 4; ++ii) l[ii] = S[(i0 + ii) + (t0 + k) * LDS];
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) u[jj] = (c0 + jj < w) ? Ut[k * w + c0 + jj] : 0.0f;
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            acc[ii][jj] = __fmaf_rn(l[ii], u[jj], acc[ii][jj]);
+        for (int j = 0; j < 8; ++j) x[j] = __fsub_rn(x[j], acc[j]);
       }
-#pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          if (c0 + jj < w) {
-            float* p = &S[(i0 + ii) + (c0 + jj) * LDS];
-            *p = __fsub_rn(*p, acc[ii][jj]);
-          }
-    }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < kStrip * w; idx += kThreads) {
-    const int i = idx % kStrip, j = idx / kStrip;
-    if (i < rows) a[(r0 + i) + (int64_t)j * lda] = S[i + j * LDS];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// U panel: w rows of the block row starting at `a` (lda), columns [0, N),
-// against the factored diagonal block `dg` (lda), in place.
-__global__ void __launch_bounds__(kThreads)
-upanel_kernel(float* __restrict__ a, int64_t lda, const float* __restrict__ dg,
-              int64_t N, int w) {
-  extern __shared__ float smem[];
-  const int LDS = w | 1;
-  float* S = smem;                    // w x kStrip, column-major, ld LDS
-  float* Lt = S + (size_t)LDS * kStrip;  // w x 8, Lt[r*8 + k]
-  const int tid = threadIdx.x;
-  const int64_t c0g = (int64_t)blockIdx.x * kStrip;
-  const int cols = (int)((N - c0g) < kStrip ? (N - c0g) : kStrip);
-
-  for (int idx = tid; idx < kStrip * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    S[i + j * LDS] = (j < cols) ? a[i + (c0g + j) * lda] : 0.0f;
-  }
-
-  const int nt = (w + 7) / 8;
-  for (int t = 0; t < nt; ++t) {
-    const int t0 = 8 * t;
-    const int tw = min(8, w - t0);
-    __syncthreads();
-    for (int idx = tid; idx < 8 * (w - t0); idx += kThreads) {
-      const int k = idx % 8, r = t0 + idx / 8;
-      Lt[r * 8 + k] = (k < tw) ? dg[r + (int64_t)(t0 + k) * lda] : 0.0f;
-    }
-    __syncthreads();
-    // Phase A: forward substitution with the unit-lower tile.
-    if (tid < kStrip) {
-      float col[8];
-#pragma unroll
-      for (int r = 0; r < 8; ++r) col[r] = (r < tw) ? S[(t0 + r) + tid * LDS] : 0.0f;
+      // forward substitution with the unit-lower tile (src/lu_nopiv.cu:304-316)
 #pragma unroll
       for (int k = 0; k < 8; ++k)
 #pragma unroll
-        for (int r = k + 1; r < 8; ++r)
-          if (k < tw && r < tw)
-            col[r] = __fmaf_rn(-Lt[(t0 + r) * 8 + k], col[k], col[r]);
+        for (int j = k + 1; j < 8; ++j)
+          if (k < tw && j < tw)
+            x[j] = __fmaf_rn(-F[(8 * T + k) * wp + 8 * T + j], x[k], x[j]);
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
-        if (r < tw) S[(t0 + r) + tid * LDS] = col[r];
+      for (int j = 0; j < 8; ++j)
+        if (j < tw) S[(8 * T + j) * LS + c] = x[j];
     }
-    const int s = w - t0 - 8;
-    if (s <= 0) break;
     __syncthreads();
-    // Phase B: rank-8 update of the remaining rows (4 rows x 4 cols/item).
-    const int nrb = (s + 3) / 4;
-    for (int b = tid; b < nrb * (kStrip / 4); b += kThreads) {
-      const int i0 = t0 + 8 + 4 * (b % nrb);
-      const int j0 = 4 * (b / nrb);
-      float acc[4][4];
-#pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = 0.0f;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        float l[4], u[4];
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii) l[ii] = (i0 + ii < w) ? Lt[(i0 + ii) * 8 + k] : 0.0f;
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) u[jj] = S[(t0 + k) + (j0 + jj) * LDS];
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            acc[ii][jj] = __fmaf_rn(l[ii], u[jj], acc[ii][jj]);
-      }
-#pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          if (i0 + ii < w) {
-            float* p = &S[(i0 + ii) + (j0 + jj) * LDS];
-            *p = __fsub_rn(*p, acc[ii][jj]);
-          }
+    for (int idx = tid; idx < w * kPanelT; idx += kPanelT) {
+      const int i = idx % w, cc = idx / w;
+      const int64_t col = c0 + cc;
+      if (col < N) A[i + col * lda] = S[i * LS + cc];
     }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < kStrip * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    if (j < cols) a[i + (c0g + j) * lda] = S[i + j * LDS];
   }
 }
 
@@ -416,7 +426,8 @@ ref_panel_kernel(int64_t m, int n, const float* __restrict__ d, int64_t ldd,
 // launchers
 
 size_t diag_smem_bytes(int w) {
-  return ((size_t)(w | 1) * w + 8) * sizeof(float);
+  const int LD = ((w + 3) / 4) * 4 + 4;
+  return ((size_t)LD * w + 2 * 8 * 128 + 8) * sizeof(float);
 }
 
 lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
@@ -429,26 +440,21 @@ lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
   return LU_SUCCESS;
 }
 
-lu_status launch_lpanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
-                        int64_t M, int w) {
-  if (M <= 0) return LU_SUCCESS;
-  if (w <= 0 || w > 256) return LU_ERR_INVALID_ARG;
-  const size_t sm = ((size_t)(kStrip + 1) * w + 8 * (size_t)w + 8) * sizeof(float);
-  LUB_CUDA_TRY(set_smem_limit((const void*)lpanel_kernel, sm));
-  const int64_t grid = ceil_div(M, kStrip);
-  lpanel_kernel<<<(unsigned)grid, kThreads, sm, st>>>(a, lda, dg, M, w);
-  LUB_LAUNCH_CHECK();
-  return LU_SUCCESS;
+static size_t lupanel_smem_bytes(int w) {
+  const size_t wp = (size_t)((w + 7) / 8) * 8;
+  const size_t strip = std::max<size_t>((size_t)kPanelT * wp, wp * (kPanelT + 1));
+  return (wp * wp + wp + strip) * sizeof(float);
 }
 
-lu_status launch_upanel(cudaStream_t st, float* a, int64_t lda, const float* dg,
-                        int64_t N, int w) {
-  if (N <= 0) return LU_SUCCESS;
-  if (w <= 0 || w > 256) return LU_ERR_INVALID_ARG;
-  const size_t sm = ((size_t)(w | 1) * kStrip + 8 * (size_t)w) * sizeof(float);
-  LUB_CUDA_TRY(set_smem_limit((const void*)upanel_kernel, sm));
-  const int64_t grid = ceil_div(N, kStrip);
-  upanel_kernel<<<(unsigned)grid, kThreads, sm, st>>>(a, lda, dg, N, w);
+lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
+                         int64_t M, int64_t N) {
+  if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
+  const int64_t nL = M > 0 ? ceil_div(M, kPanelT) : 0;
+  const int64_t nU = N > 0 ? ceil_div(N, kPanelT) : 0;
+  if (nL + nU == 0) return LU_SUCCESS;
+  const size_t sm = lupanel_smem_bytes(w);
+  LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));
+  lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

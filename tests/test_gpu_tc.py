@@ -1,0 +1,171 @@
+"""GPU tests of the tcgen05 Schur update and the mixed-precision RL path.
+
+The tensor core's internal accumulation order is not specified, so these
+tests use stated tolerances: the update must match an fp64 product of the
+operands rounded exactly as the oracle rounds them (fp16 / bf16 / e4m3 with
+power-of-two tile scales) to within 2 K u32 (|A||B|)_ij."""
+import ctypes
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import remifa_b200 as rb
+
+pytestmark = pytest.mark.gpu
+U32 = 2.0 ** -24
+REF_SO = os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref",
+                      "libremifa_ref.so")
+
+
+def to_dev(a, lda=None):
+    m, n = a.shape
+    t = rb.colmajor_empty(m, n, lda if lda is not None else max(m, 1), torch.float32)
+    t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+    return t
+
+
+def to_host(t):
+    return np.asfortranarray(t.cpu().numpy())
+
+
+def pow2_scale(amax):
+    """Largest s with amax * 2^s <= 448 (0 for an empty tile)."""
+    if not amax > 0:
+        return 0
+    s = int(math.floor(math.log2(448.0 / amax)))
+    while amax * 2.0 ** (s + 1) <= 448.0:
+        s += 1
+    while amax * 2.0 ** s > 448.0:
+        s -= 1
+    return s
+
+
+def rounded_operands(A, B, fmt):
+    """The operands exactly as the library's copies hold them, in fp64 and
+    with the tile scales divided out again."""
+    if fmt != O.FMT_E4M3:
+        return (O.round_fmt(A, fmt).astype(np.float64),
+                O.round_fmt(B, fmt).astype(np.float64))
+    M, K = A.shape
+    N = B.shape[1]
+    Ar = np.zeros((M, K))
+    Br = np.zeros((K, N))
+    for t in range(0, M, 128):
+        blk = A[t:t + 128, :]
+        s = pow2_scale(float(np.abs(blk).max()))
+        Ar[t:t + 128, :] = O.round_fmt(blk, fmt, s).astype(np.float64) * 2.0 ** -s
+    for t in range(0, N, 128):
+        blk = B[:, t:t + 128]
+        s = pow2_scale(float(np.abs(blk).max()))
+        Br[:, t:t + 128] = O.round_fmt(blk, fmt, s).astype(np.float64) * 2.0 ** -s
+    return Ar, Br
+
+
+KINDS = [(rb.compute_type.TC32, O.FMT_FP16), (rb.compute_type.TC32_BF16, O.FMT_BF16),
+         (rb.compute_type.TC32_E4M3, O.FMT_E4M3)]
+
+
+@pytest.mark.parametrize("compute,fmt", KINDS)
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 500, 256), (1000, 777, 200),
+                                   (2048, 1536, 1024), (5, 7, 3), (96, 40, 16)])
+@pytest.mark.parametrize("pad", [0, 3])  # pad 0 (ld % 4 == 0): TMA reduce epilogue
+def test_tc_update_matches_rounded_fp64(built, compute, fmt, M, N, K, pad):
+    rng = np.random.default_rng(M * 7 + N + K)
+    A = np.asfortranarray(rng.standard_normal((M, K)).astype(np.float32))
+    B = np.asfortranarray((rng.standard_normal((K, N)) * 3).astype(np.float32))
+    C = np.asfortranarray(rng.standard_normal((M, N)).astype(np.float32))
+    Ar, Br = rounded_operands(A, B, fmt)
+    want = C.astype(np.float64) - Ar @ Br
+    bound = 2 * K * U32 * (np.abs(Ar) @ np.abs(Br)) + 2 * U32 * np.abs(want) + 1e-30
+    ldc = ((M + 3) // 4) * 4 if pad == 0 else M + 3
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C, lda=ldc)
+    rb.gemmex(compute, -1.0, dA, dB, 1.0, dC)
+    torch.cuda.synchronize()
+    got = to_host(dC)
+    err = np.abs(got - want)
+    assert np.all(err <= bound), (err / bound).max()
+
+
+def test_tc_update_repeated_calls_consistent(built):
+    # same inputs twice -> same bits (the tile schedule is static)
+    rng = np.random.default_rng(0)
+    A = np.asfortranarray(rng.standard_normal((1024, 256)).astype(np.float32))
+    B = np.asfortranarray(rng.standard_normal((256, 1024)).astype(np.float32))
+    outs = []
+    for _ in range(2):
+        dC = to_dev(np.zeros((1024, 1024), np.float32))
+        rb.gemmex(rb.TC32, -1.0, to_dev(A), to_dev(B), 1.0, dC)
+        outs.append(to_host(dC))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("n,nb,compute,fmt", [(512, 128, rb.TC32, O.FMT_FP16),
+                                              (1000, 256, rb.TC32, O.FMT_FP16),
+                                              (768, 128, rb.compute_type.TC32_BF16, O.FMT_BF16),
+                                              (768, 128, rb.compute_type.TC32_E4M3, O.FMT_E4M3)])
+def test_lu_rl_mixed_vs_oracle(built, n, nb, compute, fmt):
+    a = O.gen_matrix(n, seed=n, kind=1, alpha=1.5)
+    want = O.lu_rl(a, nb=nb, outer_fmt=fmt)
+    da = to_dev(a)
+    info = rb.lu_nopiv_rl(da, nb=nb, outer=compute)
+    torch.cuda.synchronize()
+    got = to_host(da)
+    assert int(info.item()) == 0
+    # same algorithm, same rounded operands; only the accumulation order of
+    # the tensor core differs from the oracle's fma chain
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel < 64 * n * U32, rel
+    fe_g, fe_o = O.factor_error(a, got), O.factor_error(a, want)
+    assert fe_g <= 2 * fe_o + 1e-7 and fe_o <= 2 * fe_g + 1e-7
+
+
+def test_lu_rl_tc32_vs_reference_gpu(built):
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference library not built")
+    L = ctypes.CDLL(REF_SO)
+    vp, i64, i = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    L.ref_lu_nopiv_rl_f32.argtypes = [vp, i64, i64, i64, vp, i64, vp, i, i, vp, i64]
+    n, nb = 2048, 256
+    a = O.gen_diagdom(n, lda=n)
+    mine, theirs = to_dev(a), to_dev(a)
+    rb.lu_nopiv_rl(mine, nb=nb, outer=rb.TC32)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    cpy = torch.zeros((n, n), dtype=torch.float16, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.ref_lu_nopiv_rl_f32(st, n, n, nb, ctypes.c_void_p(theirs.data_ptr()), n,
+                                 ctypes.c_void_p(info.data_ptr()), 0, 1,
+                                 ctypes.c_void_p(cpy.data_ptr()), n) == 0
+    torch.cuda.synchronize()
+    lm, lr = to_host(mine), to_host(theirs)
+    rel = np.abs(lm - lr).max() / np.abs(lr).max()
+    assert rel < 1e-3, rel
+    x1 = np.ones(n, np.float32)
+    b = O.gen_rhs(a, x1)
+    e_m = O.nwerr(a, b, O.lu_solve_f32(lm, b))
+    e_r = O.nwerr(a, b, O.lu_solve_f32(lr, b))
+    c_m = O.cwerr(a, b, O.lu_solve_f32(lm, b), lm)
+    c_r = O.cwerr(a, b, O.lu_solve_f32(lr, b), lr)
+    assert e_m <= 4 * e_r and e_r <= 4 * e_m, (e_m, e_r)
+    assert c_m <= 4 * c_r and c_r <= 4 * c_m, (c_m, c_r)
+
+
+def test_lu_rl_tc32_large_backward_error(built):
+    """n = 8192 through the device generator: size-independent check of the
+    solve residual (fp64 on the host) against the FP16-update error level."""
+    n = 8192
+    da = rb.gen_matrix(n, seed=5, kind=1, alpha=1.5)
+    a = to_host(da)
+    info = rb.lu_nopiv_rl(da, nb=256, outer=rb.TC32)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    lu = to_host(da)
+    x = O.gen_vector(n, seed=7, kind=1)
+    b = np.array(a, np.float64) @ x
+    xh = O.lu_solve_f64(lu, b)
+    be = O.backward_error(a, b, xh)
+    assert be < 1e-4, be

@@ -196,7 +196,8 @@ def run_reference(args, wl) -> None:
 
 
 def config_of(args, wl) -> dict:
-    return {"workload": args.workload, "n": wl["n"], "nb": wl["nb"],
+    return {"workload": args.workload, "n": wl["n"], "nb": getattr(args, "nb", None) or wl["nb"],
+            "lookahead": not getattr(args, "no_lookahead", False),
             "variant": "right-looking", "inner_update": "FP32",
             "outer_update": wl["outer"],
             "matrix": f"R + D, R ~ {'N(0,1)/sqrt(n)' if wl['kind'] else 'U[-1,1)'}, "
@@ -214,6 +215,9 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-lookahead", action="store_true",
+                    help="factor each outer block strictly after the previous update")
+    ap.add_argument("--nb", type=int, default=None, help="override the outer block size")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -233,7 +237,8 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
 
-    n, nb = wl["n"], wl["nb"]
+    n, nb = wl["n"], (args.nb or wl["nb"])
+    la = not args.no_lookahead
     outer = getattr(rb.compute_type, wl["outer"])
     nmat = args.warmup + args.steps
     base = rb.gen_matrix(n, seed=1 + rank, kind=wl["kind"], alpha=wl["alpha"],
@@ -248,7 +253,8 @@ def main() -> None:
     stream = torch.cuda.current_stream(dev)
 
     for i in range(args.warmup):
-        rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1], workspace=ws)
+        rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1], workspace=ws,
+                       lookahead=la)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -260,7 +266,7 @@ def main() -> None:
             t_start.record(stream)
             for i in range(args.warmup, nmat):
                 rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1],
-                               workspace=ws)
+                               workspace=ws, lookahead=la)
             t_end.record(stream)
             torch.cuda.synchronize(dev)
     ms = t_start.elapsed_time(t_end)
@@ -288,7 +294,8 @@ def main() -> None:
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         dA.copy_(host_a, non_blocking=True)
-        rb.lu_nopiv_rl(dA, nb=nb, outer=outer, info=infos[0:1], workspace=ws)
+        rb.lu_nopiv_rl(dA, nb=nb, outer=outer, info=infos[0:1], workspace=ws,
+                       lookahead=la)
         host_lu.copy_(dA, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)

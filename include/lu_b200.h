@@ -171,6 +171,32 @@ LU_API lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
                           int64_t lda, uint64_t seed, int kind, double alpha,
                           int kscale, double gamma_bits);
 
+/* ---- solve and iterative refinement (new: the reference solves on the
+ * host with LAPACK getrs, tests/testing_lu_gpu.hxx:1309-1313) ------------ */
+
+/* op(A) X = B with the in-place factors of A (fp32, ldlu): trans = 0 solves
+ * L U X = B, trans = 1 solves (L U)^T X = B.  d_x (fp64, n x nrhs, ldx)
+ * holds B on entry and X on exit.  fp64 arithmetic throughout. */
+LU_API lu_status lu_solve_c(lu_stream_t stream, int64_t n, const float* d_lu,
+                            int64_t ldlu, double* d_x, int64_t ldx,
+                            int64_t nrhs, int trans);
+
+/* Bytes of device workspace lu_refine_c needs for size n. */
+LU_API lu_status lu_refine_workspace_size(int64_t n, size_t* bytes);
+
+/* FP64 iterative refinement of A x = b (A fp32, the original matrix; d_lu
+ * its factors, mixed precision allowed).  x0 = (LU)^-1 b; then repeatedly
+ * r = b - A x in fp64, berr = ||r||inf / (||A||inf ||x||inf + ||b||inf),
+ * stop when berr <= tol, else x += (LU)^-1 r, at most max_iter updates.
+ * Synchronises the stream once per iteration to read berr.  *iters and
+ * *berr (host pointers, may be NULL) receive the iteration count and the
+ * final backward error; returns LU_ERR_NOT_CONVERGED if tol was not met. */
+LU_API lu_status lu_refine_c(lu_stream_t stream, int64_t n, const float* d_a,
+                             int64_t lda, const float* d_lu, int64_t ldlu,
+                             const double* d_b, double* d_x, double tol,
+                             int max_iter, int* iters, double* berr,
+                             void* workspace, size_t ws_bytes);
+
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {
   char name[32];     /* kernel class, e.g. "tc_update", "diag_factor" */

@@ -6,15 +6,15 @@ include/lu_b200.h); this package is the thin Python host layer over it.
 """
 from . import _lib
 from .api import (FP16, FP32, TC16, TC32, align_lda, colmajor, colmajor_empty,
-                  compute_type, convert, gemmex, gen_matrix, launch_count, ld,
-                  lu_nopiv_ll, lu_nopiv_panel, lu_nopiv_rl, make_opts, profile,
-                  workspace_size)
+                  compute_type, convert, gemmex, gen_matrix, gesv_mixed,
+                  launch_count, ld, lu_nopiv_ll, lu_nopiv_panel, lu_nopiv_rl,
+                  lu_solve, make_opts, profile, refine, workspace_size)
 
 __all__ = [
     "FP16", "FP32", "TC16", "TC32", "align_lda", "colmajor", "colmajor_empty",
     "compute_type", "convert", "gemmex", "gen_matrix", "ld", "lu_nopiv_ll",
     "lu_nopiv_panel", "lu_nopiv_rl", "make_opts", "workspace_size", "profile",
-    "launch_count",
+    "launch_count", "lu_solve", "refine", "gesv_mixed",
 ]
 
 

@@ -238,3 +238,51 @@ class profile:
 def launch_count() -> int:
     """Kernels launched by liblu_b200.so in this process so far."""
     return int(_lib.lib().lu_launch_count())
+
+
+def lu_solve(lu: torch.Tensor, b: torch.Tensor, trans: bool = False,
+             stream=None) -> torch.Tensor:
+    """Solve op(A) X = B with the in-place factors `lu` (fp32, column-major)
+    of A; B is fp64 (n or n x nrhs, column-major) and is overwritten with X
+    (returned).  trans=True solves A^T X = B."""
+    n = lu.shape[0]
+    x = b if b.dim() == 2 else b.view(-1, 1)
+    if x.dtype != torch.float64:
+        raise ValueError("lu_solve: right-hand sides must be float64")
+    ldx = ld(x) if x.shape[1] > 1 else max(n, 1)
+    st = _lib.lib().lu_solve_c(_stream(stream), n, _ptr(lu), ld(lu), _ptr(x), ldx,
+                               x.shape[1], int(bool(trans)))
+    _lib.check(st, "lu_solve_c")
+    return b
+
+
+def refine(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
+           x: torch.Tensor | None = None, tol: float = 1e-14, max_iter: int = 30,
+           stream=None, raise_on_stall: bool = False):
+    """FP64 iterative refinement of A x = b with (possibly low-precision)
+    factors `lu` of the fp32 matrix `a`.  Returns (x, iterations, berr)
+    where berr = ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf)."""
+    n = a.shape[0]
+    if x is None:
+        x = torch.empty(n, dtype=torch.float64, device=a.device)
+    it = ctypes.c_int(0)
+    be = ctypes.c_double(0.0)
+    st = _lib.lib().lu_refine_c(_stream(stream), n, _ptr(a), ld(a), _ptr(lu), ld(lu),
+                                _ptr(b), _ptr(x), float(tol), int(max_iter),
+                                ctypes.byref(it), ctypes.byref(be), None, 0)
+    if st == _lib.ERR_NOT_CONVERGED and not raise_on_stall:
+        return x, it.value, be.value
+    _lib.check(st, "lu_refine_c")
+    return x, it.value, be.value
+
+
+def gesv_mixed(a: torch.Tensor, b: torch.Tensor, outer=TC32, nb: int = 256,
+               tol: float = 1e-14, max_iter: int = 30, lookahead: bool = True,
+               stream=None):
+    """Solve A x = b to an fp64-level backward error: factor a copy of the
+    fp32 matrix with the `outer` trailing-update precision, then refine in
+    fp64.  Returns (x, info, iterations, berr)."""
+    lu = colmajor(a)
+    info = lu_nopiv_rl(lu, nb=nb, outer=outer, lookahead=lookahead, stream=stream)
+    x, it, be = refine(a, lu, b, tol=tol, max_iter=max_iter, stream=stream)
+    return x, info, it, be

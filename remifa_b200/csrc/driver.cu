@@ -19,6 +19,8 @@
 #include "profile.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <unordered_map>
 
 namespace lub {
 
@@ -70,18 +72,17 @@ static TcWs tc_ws_layout(size_t base, int64_t M, int64_t N, int64_t K,
   return w;
 }
 
-// C (fp32) -= A * B through the tensor cores: pack A (column-major fp32,
-// lda) and B (column-major fp32, ldb) into the workspace, then update.
-static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
-                                int64_t N, int64_t K, float alpha,
-                                const float* a, int64_t lda, const float* b,
-                                int64_t ldb, float* c, int64_t ldc, char* ws,
-                                const TcWs& w, int* err) {
+// Pack A (M x K, column-major fp32, lda) into the row-major low-precision
+// copy and B (K x N, column-major fp32, ldb) into the column-major copy,
+// with per-tile scales for e4m3.
+static lu_status tc_pack(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                         int64_t K, const float* a, int64_t lda, const float* b,
+                         int64_t ldb, char* ws, const TcWs& w) {
   const int64_t ldk = (K + 15) / 16 * 16;
-  void* ap = ws + w.off_a;
-  void* bp = ws + w.off_b;
   int* sa = nullptr;
   int* sb = nullptr;
+  ProfScope ps("pack_operands", st,
+               (double)(M + N) * K * (4.0 + tc_operand_bytes(kind)));
   if (kind == TcOperand::E4M3) {
     sa = reinterpret_cast<int*>(ws + w.off_sa);
     sb = reinterpret_cast<int*>(ws + w.off_sb);
@@ -89,17 +90,78 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
     LUB_TRY(launch_scale_rowtiles(st, M, K, a, lda, sa, tmp));
     LUB_TRY(launch_scale_coltiles(st, K, N, b, ldb, sb, tmp));
   }
-  const double es = tc_operand_bytes(kind);
-  {
-    ProfScope ps("pack_operands", st, (double)(M + N) * K * (4.0 + es));
-    LUB_TRY(launch_pack_a(st, kind, M, K, a, lda, ap, ldk, sa));
-    LUB_TRY(launch_pack_b(st, kind, K, N, b, ldb, bp, ldk, sb));
+  LUB_TRY(launch_pack_a(st, kind, M, K, a, lda, ws + w.off_a, ldk, sa));
+  LUB_TRY(launch_pack_b(st, kind, K, N, b, ldb, ws + w.off_b, ldk, sb));
+  return LU_SUCCESS;
+}
+
+// C[M x N] -= Ap[r0 .., :] * Bp[:, c0 ..] from packed operands (r0, c0 are
+// row / column offsets into the packed copies; multiples of 128 when the
+// copies carry e4m3 tile scales).
+static lu_status tc_apply(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                          int64_t K, int64_t r0, int64_t c0, float* c,
+                          int64_t ldc, char* ws, const TcWs& w, int* err,
+                          int tiles_per_cta) {
+  if (M <= 0 || N <= 0) return LU_SUCCESS;
+  const int64_t ldk = (K + 15) / 16 * 16;
+  const int64_t es = tc_operand_bytes(kind);
+  const int* sa = nullptr;
+  const int* sb = nullptr;
+  if (kind == TcOperand::E4M3) {
+    if (r0 % 128 != 0 || c0 % 128 != 0) return LU_ERR_INVALID_ARG;
+    sa = reinterpret_cast<const int*>(ws + w.off_sa) + r0 / 128;
+    sb = reinterpret_cast<const int*>(ws + w.off_sb) + c0 / 128;
   }
   // algorithmic bytes: C read + written once (fp32), both operands read once
-  ProfScope ps("tc_update", st, 8.0 * M * N + es * (double)(M + N) * K,
+  ProfScope ps("tc_update", st, 8.0 * M * N + (double)es * (M + N) * K,
                2.0 * M * N * K);
-  return launch_tc_update(st, kind, M, N, K, alpha, ap, ldk, bp, ldk, c, ldc,
-                          sa, sb, err);
+  return launch_tc_update(st, kind, M, N, K, -1.0f, ws + w.off_a + r0 * ldk * es,
+                          ldk, ws + w.off_b + c0 * ldk * es, ldk, c, ldc, sa, sb,
+                          err, 0, tiles_per_cta);
+}
+
+// C (fp32) -= A * B through the tensor cores (pack, then update).
+static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
+                                int64_t N, int64_t K, float alpha,
+                                const float* a, int64_t lda, const float* b,
+                                int64_t ldb, float* c, int64_t ldc, char* ws,
+                                const TcWs& w, int* err) {
+  LUB_TRY(tc_pack(st, kind, M, N, K, a, lda, b, ldb, ws, w));
+  if (alpha == -1.0f) return tc_apply(st, kind, M, N, K, 0, 0, c, ldc, ws, w, err, 0);
+  const int64_t ldk = (K + 15) / 16 * 16;
+  const int* sa = kind == TcOperand::E4M3 ? reinterpret_cast<const int*>(ws + w.off_sa) : nullptr;
+  const int* sb = kind == TcOperand::E4M3 ? reinterpret_cast<const int*>(ws + w.off_sb) : nullptr;
+  return launch_tc_update(st, kind, M, N, K, alpha, ws + w.off_a, ldk,
+                          ws + w.off_b, ldk, c, ldc, sa, sb, err);
+}
+
+// Internal streams of one device: panel work runs at the highest priority,
+// the bulk of each trailing update at the lowest, ordered by two events.
+struct DevStreams {
+  cudaStream_t panel = nullptr, update = nullptr;
+  cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
+  cudaEvent_t packed = nullptr, updated = nullptr;
+};
+
+static lu_status dev_streams(DevStreams** out) {
+  static std::mutex mu;
+  static std::unordered_map<int, DevStreams> cache;
+  int dev = 0;
+  LUB_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(dev);
+  if (it == cache.end()) {
+    DevStreams d;
+    int least = 0, greatest = 0;
+    LUB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.panel, cudaStreamNonBlocking, greatest));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.update, cudaStreamNonBlocking, least));
+    for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated})
+      LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    it = cache.emplace(dev, d).first;
+  }
+  *out = &it->second;
+  return LU_SUCCESS;
 }
 
 lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
@@ -127,10 +189,12 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   p->off_status = off;  // [0] first bad pivot, [1] device wait error
   off += 256;
   if (is_tc(p->outer) && n > p->nb) {
+    // two operand buffers: with look-ahead, step k+1 packs while the bulk
+    // update of step k still reads step k's copies
     const int64_t t = n - p->nb;
     TcWs w = tc_ws_layout(off, t, t, p->nb, tc_kind(p->outer));
     p->off_lcopy = w.off_a;
-    off += w.bytes;
+    off += 2 * w.bytes;
   }
   p->ws_bytes = off;
   return LU_SUCCESS;
@@ -158,46 +222,116 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
       ProfScope ps("sgemm_chunk8", st, 0.0,
                    2.0 * w * ((double)(updm - p0 - w) * (in - p0 - w) +
                               (double)(in - p0 - w) * (updm - in)));
-      // rest of the outer block column: rows [p0+w, updm), cols [p0+w, in)
-      LUB_TRY(launch_sgemm_update(st, updm - (p0 + w), in - (p0 + w), w, -1.0f,
-                                  dg + w, lda, dg + (int64_t)w * lda, lda, 1.0f,
-                                  dg + w + (int64_t)w * lda, lda, true));
+      // rest of the outer block column: rows [p0+w, updm), cols [p0+w, in);
       // rest of the outer block row: rows [p0+w, in), cols [in, updm)
-      if (updm > in)
-        LUB_TRY(launch_sgemm_update(st, in - (p0 + w), updm - in, w, -1.0f,
-                                    dg + w, lda, blk + p0 + in * lda, lda, 1.0f,
-                                    blk + (p0 + w) + in * lda, lda, true));
+      LUB_TRY(launch_sgemm_chunk8_2(
+          st, updm - (p0 + w), in - (p0 + w), w, dg + w, lda, dg + (int64_t)w * lda,
+          lda, dg + w + (int64_t)w * lda, lda,
+          updm > in ? in - (p0 + w) : 0, updm - in, w, dg + w, lda,
+          blk + p0 + in * lda, lda, blk + (p0 + w) + in * lda, lda));
     }
   }
   return LU_SUCCESS;
 }
 
+// Trailing update of outer step (ofs) restricted to rows [r0, n) x columns
+// [c0, c0 + ncols): the block at (ofst + r0, ofst + c0).
+static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
+                              int64_t lda, int64_t ofs, int64_t r0, int64_t rows,
+                              int64_t c0, int64_t cols, char* ws, const TcWs& w,
+                              int* err, int tiles_per_cta) {
+  if (rows <= 0 || cols <= 0) return LU_SUCCESS;
+  const int64_t nb = p.nb, ofst = ofs + nb;
+  float* c = a + (ofst + r0) + (ofst + c0) * lda;
+  if (is_tc(p.outer))
+    return tc_apply(st, tc_kind(p.outer), rows, cols, nb, r0, c0, c, lda, ws, w,
+                    err, tiles_per_cta);
+  ProfScope ps("sgemm_update", st, 8.0 * rows * cols, 2.0 * rows * cols * (double)nb);
+  return launch_sgemm_update(st, rows, cols, nb, -1.0f, a + (ofst + r0) + ofs * lda,
+                             lda, a + ofs + (ofst + c0) * lda, lda, 1.0f, c, lda,
+                             false);
+}
+
+// Right-looking factorization.  Without look-ahead every outer step runs in
+// order on the caller's stream.  With look-ahead the trailing update of step
+// k is split into U1 (the next block column and block row, which the panel
+// of step k+1 needs) and U2 (everything else); the panel, the operand
+// packing and U1 run on a high-priority stream, U2 on a low-priority one, so
+// the panel of step k+1 overlaps U2 of step k.  Every element still receives
+// its updates in the same order, so results are identical either way.
 static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                            int64_t lda, char* ws, int* first_bad, int* err) {
   const int64_t n = p.n, nb = p.nb;
-  TcWs w;
-  if (is_tc(p.outer) && n > nb) w = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
-  for (int64_t ofs = 0; ofs < n; ofs += nb) {
+  const bool tc = is_tc(p.outer);
+  TcWs w[2];
+  if (tc && n > nb) {
+    w[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
+    w[1] = w[0];
+    const size_t shift = w[0].bytes;
+    w[1].off_a += shift; w[1].off_b += shift; w[1].off_sa += shift;
+    w[1].off_sb += shift; w[1].off_tmp += shift;
+  }
+  const bool la = p.lookahead && n > 2 * nb &&
+                  !(tc_kind(p.outer) == TcOperand::E4M3 && tc && nb % 128 != 0);
+  if (!la) {
+    for (int64_t ofs = 0; ofs < n; ofs += nb) {
+      const int64_t in = std::min(n - ofs, nb);
+      LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, first_bad));
+      const int64_t tn = n - (ofs + nb);
+      if (tn <= 0) continue;
+      if (tc)
+        LUB_TRY(tc_pack(st, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
+                        lda, a + ofs + (ofs + nb) * lda, lda, ws, w[0]));
+      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tn, 0, tn, ws, w[0], err, 0));
+    }
+    return LU_SUCCESS;
+  }
+  DevStreams* S = nullptr;
+  LUB_TRY(dev_streams(&S));
+  cudaStream_t sp = S->panel, su = S->update;
+  LUB_CUDA_TRY(cudaEventRecord(S->fork, st));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->fork, 0));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(su, S->fork, 0));
+  lu_status status = LU_SUCCESS;
+  int64_t step = 0;
+  for (int64_t ofs = 0; ofs < n && status == LU_SUCCESS; ofs += nb, ++step) {
     const int64_t in = std::min(n - ofs, nb);
-    const int64_t updm = n - ofs;
-    LUB_TRY(factor_block(p, st, a, lda, ofs, in, updm, first_bad));
-    const int64_t ofst = ofs + nb;
-    const int64_t tn = n - ofst;
+    status = factor_block(p, sp, a, lda, ofs, in, n - ofs, first_bad);
+    if (status != LU_SUCCESS) break;
+    const int64_t tn = n - (ofs + nb);
     if (tn <= 0) continue;
-    if (is_tc(p.outer)) {
-      // TC32 outer update (src/lu_nopiv.hxx:155-183): rounded copies of
-      // L21 and U12, fp32 accumulation, C -= acc in fp32.
-      LUB_TRY(tc_update_fp32(st, tc_kind(p.outer), tn, tn, nb, -1.0f,
-                             a + ofst + ofs * lda, lda, a + ofs + ofst * lda, lda,
-                             a + ofst + ofst * lda, lda, ws, w, err));
+    const TcWs& wk = w[step & 1];
+    if (tc) {
+      status = tc_pack(sp, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
+                       lda, a + ofs + (ofs + nb) * lda, lda, ws, wk);
+      if (status != LU_SUCCESS) break;
+    }
+    if (cudaEventRecord(S->packed, sp) != cudaSuccess) { status = LU_ERR_CUDA; break; }
+    // U1 after U2 of the previous step (same elements, earlier step first)
+    if (step > 0 && cudaStreamWaitEvent(sp, S->updated, 0) != cudaSuccess) {
+      status = LU_ERR_CUDA;
+      break;
+    }
+    const int64_t b = std::min(nb, tn);
+    status = outer_update(p, sp, a, lda, ofs, 0, tn, 0, b, ws, wk, err, 1);
+    if (status == LU_SUCCESS && tn > nb)
+      status = outer_update(p, sp, a, lda, ofs, 0, nb, nb, tn - nb, ws, wk, err, 1);
+    if (status != LU_SUCCESS) break;
+    if (tn > nb) {
+      if (cudaStreamWaitEvent(su, S->packed, 0) != cudaSuccess) { status = LU_ERR_CUDA; break; }
+      status = outer_update(p, su, a, lda, ofs, nb, tn - nb, nb, tn - nb, ws, wk, err, 8);
+      if (status != LU_SUCCESS) break;
+      if (cudaEventRecord(S->updated, su) != cudaSuccess) { status = LU_ERR_CUDA; break; }
     } else {
-      ProfScope ps("sgemm_update", st, 8.0 * tn * tn, 2.0 * tn * tn * (double)nb);
-      LUB_TRY(launch_sgemm_update(st, tn, tn, nb, -1.0f, a + ofst + ofs * lda,
-                                  lda, a + ofs + ofst * lda, lda, 1.0f,
-                                  a + ofst + ofst * lda, lda, false));
+      if (cudaEventRecord(S->updated, sp) != cudaSuccess) { status = LU_ERR_CUDA; break; }
     }
   }
-  return LU_SUCCESS;
+  // join (also on the error path, so the caller's stream stays ordered)
+  cudaEventRecord(S->join_p, sp);
+  cudaEventRecord(S->join_u, su);
+  cudaStreamWaitEvent(st, S->join_p, 0);
+  cudaStreamWaitEvent(st, S->join_u, 0);
+  return status;
 }
 
 lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,

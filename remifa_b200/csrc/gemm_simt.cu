@@ -161,7 +161,124 @@ sgemm_update_kernel(int64_t M, int64_t N, int64_t K, float alpha,
   }
 }
 
+// Rank-8-chunked update C -= A * B over up to two independent regions in one
+// launch (the rest of an outer block column and of its block row), 64 x 64
+// tiles, 4 x 4 outputs per thread: the skinny shapes of these updates
+// (K <= 128, one dimension 128 wide) need many small tiles to fill the GPU.
+struct ChunkRegion {
+  int64_t M, N, K;
+  const float* A; int64_t lda;
+  const float* B; int64_t ldb;
+  float* C; int64_t ldc;
+  int tiles_m, tiles;
+};
+
+constexpr int CB = 64;
+
+__global__ void __launch_bounds__(NT)
+sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
+  __shared__ __align__(16) float As[2][BK][CB];
+  __shared__ __align__(16) float Bs[2][BK][CB];
+  const bool second = (int)blockIdx.x >= r0.tiles;
+  const ChunkRegion& r = second ? r1 : r0;
+  const int t = second ? (int)blockIdx.x - r0.tiles : (int)blockIdx.x;
+  const int64_t m0 = (int64_t)(t % r.tiles_m) * CB;
+  const int64_t n0 = (int64_t)(t / r.tiles_m) * CB;
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  const int a_col = tid / 32, a_row = (tid % 32) * 2;  // A tile CB x BK
+  const int b_col = tid / 4, b_k = (tid % 4) * 2;      // B tile BK x CB
+
+  float ra[2], rb[2];
+  auto load_tiles = [&](int64_t k0) {
+    const int64_t ak = k0 + a_col;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      ra[i] = (ak < r.K && m0 + a_row + i < r.M) ? r.A[m0 + a_row + i + ak * r.lda] : 0.0f;
+    const int64_t bc = n0 + b_col;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      rb[i] = (bc < r.N && k0 + b_k + i < r.K) ? r.B[k0 + b_k + i + bc * r.ldb] : 0.0f;
+  };
+  auto store_tiles = [&](int buf) {
+    As[buf][a_col][a_row] = ra[0];
+    As[buf][a_col][a_row + 1] = ra[1];
+    Bs[buf][b_k][b_col] = rb[0];
+    Bs[buf][b_k + 1][b_col] = rb[1];
+  };
+
+  float cr[4][4], acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t row = m0 + tx * 4 + i, col = n0 + ty * 4 + j;
+      cr[i][j] = (row < r.M && col < r.N) ? r.C[row + col * r.ldc] : 0.0f;
+      acc[i][j] = 0.0f;
+    }
+  const int64_t nk = (r.K + BK - 1) / BK;
+  load_tiles(0);
+  store_tiles(0);
+  __syncthreads();
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int buf = (int)(kt & 1);
+    if (kt + 1 < nk) load_tiles((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      const float4 a4 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
+      const float4 b4 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+      const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+      const float b[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+    }
+    // one rank-8 chunk done: C -= acc (the reference's K = 8 GEMM)
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        cr[i][j] = __fsub_rn(cr[i][j], acc[i][j]);
+        acc[i][j] = 0.0f;
+      }
+    if (kt + 1 < nk) {
+      store_tiles(buf ^ 1);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t row = m0 + tx * 4 + i, col = n0 + ty * 4 + j;
+      if (row < r.M && col < r.N) r.C[row + col * r.ldc] = cr[i][j];
+    }
+}
+
 }  // namespace
+
+lu_status launch_sgemm_chunk8_2(cudaStream_t st, int64_t M0, int64_t N0,
+                                int64_t K0, const float* A0, int64_t lda0,
+                                const float* B0, int64_t ldb0, float* C0,
+                                int64_t ldc0, int64_t M1, int64_t N1, int64_t K1,
+                                const float* A1, int64_t lda1, const float* B1,
+                                int64_t ldb1, float* C1, int64_t ldc1) {
+  ChunkRegion r0{M0, N0, K0, A0, lda0, B0, ldb0, C0, ldc0, 0, 0};
+  ChunkRegion r1{M1, N1, K1, A1, lda1, B1, ldb1, C1, ldc1, 0, 0};
+  for (ChunkRegion* r : {&r0, &r1}) {
+    if (r->M > 0 && r->N > 0 && r->K > 0) {
+      r->tiles_m = (int)ceil_div(r->M, CB);
+      r->tiles = r->tiles_m * (int)ceil_div(r->N, CB);
+    }
+  }
+  const int64_t grid = (int64_t)r0.tiles + r1.tiles;
+  if (grid == 0) return LU_SUCCESS;
+  if (grid > INT32_MAX) return LU_ERR_INVALID_ARG;
+  sgemm_chunk8_kernel<<<(unsigned)grid, NT, 0, st>>>(r0, r1);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
 
 lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,
                               float alpha, const float* A, int64_t lda,

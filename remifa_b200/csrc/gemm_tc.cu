@@ -73,6 +73,8 @@ struct TcParams {
   const int* scale_b;  // per 128-column tile of B (log2), or null
   float alpha;         // C += alpha * acc (alpha = -1 for the Schur update)
   int* err;
+  int tiles_per_cta;   // 0: persistent (tile = blockIdx.x, += gridDim.x);
+                       // > 0: CTA b owns the consecutive tiles [b*T, b*T+T)
 };
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
@@ -99,6 +101,9 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   const int num_tiles = p.tiles_m * p.tiles_n;
+  const int t_begin = p.tiles_per_cta > 0 ? (int)blockIdx.x * p.tiles_per_cta : (int)blockIdx.x;
+  const int t_end = p.tiles_per_cta > 0 ? min(num_tiles, t_begin + p.tiles_per_cta) : num_tiles;
+  const int t_step = p.tiles_per_cta > 0 ? 1 : (int)gridDim.x;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -125,7 +130,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+      for (int tile = t_begin; tile < t_end && ok; tile += t_step) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         for (int kb = 0; kb < p.kb_count; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty)) { ok = false; break; }
@@ -145,7 +150,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       uint32_t ph = 0;
       int local = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+      for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
         if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty)) { ok = false; break; }
@@ -181,7 +186,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
     if constexpr (EPI == 1) {
       float* stage = reinterpret_cast<float*>(sEpi + (size_t)ew * 2 * kEpiChunk);
       int issued = 0;  // reduces issued by this warp; buffer = issued & 1
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+      for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
@@ -226,7 +231,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       if (lane == 0) bulk_wait_group<0>();
       __syncwarp();
     } else {
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++local) {
+      for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
@@ -342,7 +347,7 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
                            int64_t N, int64_t K, float alpha, const void* A,
                            int64_t lda_p, const void* B, int64_t ldb_p, float* C,
                            int64_t ldc, const int* scale_a, const int* scale_b,
-                           int* err, int max_ctas) {
+                           int* err, int max_ctas, int tiles_per_cta) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
   if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
   const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
@@ -370,8 +375,11 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
   p.scale_b = scale_b;
   p.alpha = alpha;
   p.err = err;
+  p.tiles_per_cta = tiles_per_cta;
   const int tiles = p.tiles_m * p.tiles_n;
-  const int grid = std::min(tiles, max_ctas > 0 ? max_ctas : sm_count());
+  const int grid = tiles_per_cta > 0
+                       ? (int)ceil_div(tiles, tiles_per_cta)
+                       : std::min(tiles, max_ctas > 0 ? max_ctas : sm_count());
   // TMA reduce-add needs a 16-byte aligned C with a 16-byte multiple stride
   CUtensorMap mc;
   std::memset(&mc, 0, sizeof(mc));

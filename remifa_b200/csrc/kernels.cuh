@@ -23,6 +23,15 @@ lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,
                               const float* B, int64_t ldb, float beta, float* C,
                               int64_t ldc, bool chunk8);
 
+// Two independent rank-8-chunked updates C -= A * B in one launch (either
+// region may be empty).
+lu_status launch_sgemm_chunk8_2(cudaStream_t st, int64_t M0, int64_t N0,
+                                int64_t K0, const float* A0, int64_t lda0,
+                                const float* B0, int64_t ldb0, float* C0,
+                                int64_t ldc0, int64_t M1, int64_t N1, int64_t K1,
+                                const float* A1, int64_t lda1, const float* B1,
+                                int64_t ldb1, float* C1, int64_t ldc1);
+
 // convert.cu
 lu_status launch_convert(cudaStream_t st, int64_t m, int64_t n, const void* a,
                          lu_dtype ta, int64_t lda, void* out, lu_dtype tout,

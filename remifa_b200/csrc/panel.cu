@@ -37,7 +37,7 @@ __device__ __forceinline__ void factor_tile_warp(float (&v)[8], int tw,
   for (int k = 0; k < 8; ++k) {
     if (k < tw) {
       const float d = __shfl_sync(mask, v[k], k);
-      const float iv = __fdiv_rn(1.0f, d);
+      const float iv = __frcp_rn(d);  // correctly rounded 1/d
       if (r == 0) {
         inv[k] = iv;
         note_pivot(d, col0 + k, first_bad);
@@ -50,6 +50,38 @@ __device__ __forceinline__ void factor_tile_warp(float (&v)[8], int tw,
       }
     }
   }
+}
+
+// The same tile factorization by a single thread, the tile held in
+// registers (T points at its top-left element in shared memory, ld LD).
+__device__ __forceinline__ void factor_tile_thread(float* T, int LD, int tw,
+                                                   float* inv, int64_t col0,
+                                                   int* first_bad) {
+  float v[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[r][c] = (r < tw && c < tw) ? T[r + c * LD] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k < tw) {
+      const float d = v[k][k];
+      note_pivot(d, col0 + k, first_bad);
+      const float iv = __frcp_rn(d);  // correctly rounded 1/d
+      inv[k] = iv;
+#pragma unroll
+      for (int r = k + 1; r < 8; ++r) v[r][k] = __fmul_rn(v[r][k], iv);
+#pragma unroll
+      for (int c = k + 1; c < 8; ++c)
+#pragma unroll
+        for (int r = k + 1; r < 8; ++r) v[r][c] = __fmaf_rn(-v[r][k], v[k][c], v[r][c]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (r < tw && c < tw) T[r + c * LD] = v[r][c];
 }
 
 // ---------------------------------------------------------------------------
@@ -79,19 +111,10 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
   for (int t = 0; t < nt; ++t) {
     const int t0 = 8 * t;
     const int tw = min(8, w - t0);
-    // Phase A: factor the tile (warp 0, lane = tile row).
-    if (tid < 32) {
-      float v[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-        v[c] = (tid < tw && c < tw) ? D[(t0 + tid) + (t0 + c) * LD] : 0.0f;
-      factor_tile_warp(v, tw, inv, col0 + t0, first_bad);
-      if (tid < tw) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < tw) D[(t0 + tid) + (t0 + c) * LD] = v[c];
-      }
-    }
+    // Phase A: one thread factors the 8 x 8 tile in registers
+    // (src/lu_nopiv.cu:123-171): 1/d, scale the column below, fused rank-1
+    // update of the rest of the tile.
+    if (tid == 0) factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
     __syncthreads();
     const int s = w - t0 - 8;  // trailing extent inside the block
     if (s <= 0) break;
@@ -202,15 +225,20 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 // ---------------------------------------------------------------------------
 // L and U panels of one sub-panel, one launch.  `dg` is the factored w x w
 // diagonal block (lda); M rows lie below it, N columns right of it.
-// Blocks [0, nL) each own kPanelT rows of L21 (one row per thread); blocks
-// [nL, ...) each own kPanelT columns of U12 (one column per thread).
-// A thread walks its row (column) tile by tile, left to right: it first
-// applies the rank-8 updates of all earlier tiles in order (acc over the 8
-// columns, one subtraction per tile -- the sequence the reference's K = 8
-// GEMMs produce), then the tile elimination of the panel kernel.  Rows and
-// columns are independent, so no block-wide synchronisation is needed after
-// the staging of the diagonal block.
+//
+// Eight threads (one group, lane & 7 = j) own one row of L21 (L blocks) or
+// one column of U12 (U blocks); a CTA of 256 threads owns 32 of them.  The
+// group walks its row (column) tile by tile, left to right.  For tile T,
+// thread j first applies the rank-8 updates of all earlier tiles to element
+// j of the tile, in order (acc = sum over the 8 columns of the earlier tile
+// with fused multiply-adds, then one subtraction per tile: the sequence the
+// reference's K = 8 GEMMs produce), then the group performs the tile
+// elimination of the panel kernel, passing the eliminated value of column k
+// to the others with a shuffle.  Rows (columns) are independent, so the
+// only synchronisation after staging is within the 8-lane group.
 constexpr int kPanelT = 256;
+constexpr int kGroup = 8;
+constexpr int kItems = kPanelT / kGroup;  // rows / columns per CTA
 
 __global__ void __launch_bounds__(kPanelT)
 lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
@@ -219,142 +247,131 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   const int tid = threadIdx.x;
   const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
   const int nt = wp / 8;
-  // F[c*wp + r] = D[r][c]: the factored block, column-major with a padded
-  // (zero-filled) leading dimension so 4-element groups are 16-byte aligned.
-  // The L role reads its strict upper part (U), the U role its strict lower
-  // part (L); the diagonal gives 1/d.
-  float* F = smem;
-  float* inv = F + (size_t)wp * wp;  // wp
-  float* S = inv + wp;               // the strip
+  const int ls = wp + 4;             // strip row stride (breaks bank aliasing)
+  const int lf = wp + 4;             // leading dimension of F, same reason
+  float* F = smem;                   // diagonal block, wp x wp, F[c*lf + r]
+  float* inv = F + (size_t)wp * lf;  // wp
+  float* S = inv + wp;               // kItems x ls
   const bool is_l = (int)blockIdx.x < nL;
+  const int j = tid & (kGroup - 1);
+  const int q = tid / kGroup;        // item of this group
+  const unsigned gmask = 0xffu << (tid & 24);  // the 8 lanes of the group
 
+  // Stage the factored diagonal block, column-major with a padded leading
+  // dimension (F[c*lf + r] = D[r][c]): U[8t..8t+7][c] is one aligned 8-float
+  // run, and the 8 columns a group reads at once fall in distinct banks.
   for (int idx = tid; idx < wp * wp; idx += kPanelT) {
     const int r = idx % wp, c = idx / wp;
-    if (r < w && c < w) cp_async4(&F[idx], &dg[r + (int64_t)c * lda]);
-    else F[idx] = 0.0f;
+    if (r < w && c < w) cp_async4(&F[c * lf + r], &dg[r + (int64_t)c * lda]);
+    else F[c * lf + r] = 0.0f;
+  }
+  int64_t item0;
+  float* A;
+  int64_t count;
+  if (is_l) {
+    item0 = (int64_t)blockIdx.x * kItems;
+    A = dg + w;                      // first row below the block
+    count = M;
+    // strip: S[q*ls + c] = A[row q, column c]; consecutive threads read
+    // consecutive rows of one column
+    for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
+      const int qq = idx % kItems, c = idx / kItems;
+      const int64_t row = item0 + qq;
+      if (row < M && c < w) cp_async4(&S[qq * ls + c], &A[row + (int64_t)c * lda]);
+      else S[qq * ls + c] = 0.0f;
+    }
+  } else {
+    item0 = (int64_t)(blockIdx.x - nL) * kItems;
+    A = dg + (int64_t)w * lda;       // first column right of the block
+    count = N;
+    // strip: S[q*ls + i] = A[row i, column q]; consecutive threads read
+    // consecutive rows of one column
+    for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
+      const int i = idx % wp, qq = idx / wp;
+      const int64_t col = item0 + qq;
+      if (col < N && i < w) cp_async4(&S[qq * ls + i], &A[i + col * lda]);
+      else S[qq * ls + i] = 0.0f;
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (is_l) {
+    for (int k = tid; k < wp; k += kPanelT)
+      inv[k] = (k < w) ? __frcp_rn(F[k * lf + k]) : 0.0f;
+    __syncthreads();
   }
 
+  const bool valid = item0 + q < count;
+  float* srow = S + q * ls;
+  for (int T = 0; T < nt; ++T) {
+    const int tw = min(8, w - 8 * T);
+    float x = srow[8 * T + j];
+    // updates of earlier tiles, in order
+    for (int t = 0; t < T; ++t) {
+      const float4 v0 = *reinterpret_cast<const float4*>(&srow[8 * t]);
+      const float4 v1 = *reinterpret_cast<const float4*>(&srow[8 * t + 4]);
+      float acc = 0.0f;
+      if (is_l) {
+        // U[8t+k][8T+j]: column 8T+j of F, rows 8t..8t+7
+        const float* fcol = &F[(8 * T + j) * lf + 8 * t];
+        const float4 f0 = *reinterpret_cast<const float4*>(fcol);
+        const float4 f1 = *reinterpret_cast<const float4*>(fcol + 4);
+        acc = __fmaf_rn(v0.x, f0.x, acc);
+        acc = __fmaf_rn(v0.y, f0.y, acc);
+        acc = __fmaf_rn(v0.z, f0.z, acc);
+        acc = __fmaf_rn(v0.w, f0.w, acc);
+        acc = __fmaf_rn(v1.x, f1.x, acc);
+        acc = __fmaf_rn(v1.y, f1.y, acc);
+        acc = __fmaf_rn(v1.z, f1.z, acc);
+        acc = __fmaf_rn(v1.w, f1.w, acc);
+      } else {
+        // L[8T+j][8t+k]: row 8T+j of F, columns 8t..8t+7 (the 8 lanes of a
+        // group read 8 consecutive words)
+        const float* frow = &F[(8 * t) * lf + 8 * T + j];
+        acc = __fmaf_rn(frow[0 * lf], v0.x, acc);
+        acc = __fmaf_rn(frow[1 * lf], v0.y, acc);
+        acc = __fmaf_rn(frow[2 * lf], v0.z, acc);
+        acc = __fmaf_rn(frow[3 * lf], v0.w, acc);
+        acc = __fmaf_rn(frow[4 * lf], v1.x, acc);
+        acc = __fmaf_rn(frow[5 * lf], v1.y, acc);
+        acc = __fmaf_rn(frow[6 * lf], v1.z, acc);
+        acc = __fmaf_rn(frow[7 * lf], v1.w, acc);
+      }
+      x = __fsub_rn(x, acc);
+    }
+    // tile elimination
+    if (is_l) {
+      // src/lu_nopiv.cu:141-168: x_k *= 1/d_k, then x_j -= x_k * U[k][j]
+      for (int k = 0; k < tw; ++k) {
+        if (j == k) x = __fmul_rn(x, inv[8 * T + k]);
+        const float xk = __shfl_sync(gmask, x, k, kGroup);
+        if (j > k && j < tw) x = __fmaf_rn(-xk, F[(8 * T + j) * lf + 8 * T + k], x);
+      }
+    } else {
+      // src/lu_nopiv.cu:304-316: x_j -= L[j][k] * x_k (unit diagonal)
+      for (int k = 0; k < tw; ++k) {
+        const float xk = __shfl_sync(gmask, x, k, kGroup);
+        if (j > k && j < tw) x = __fmaf_rn(-F[(8 * T + k) * lf + 8 * T + j], xk, x);
+      }
+    }
+    if (j < tw) srow[8 * T + j] = x;
+    __syncwarp(gmask);
+  }
+  __syncthreads();
   if (is_l) {
-    // strip: kPanelT rows x w columns, S[c*kPanelT + r]
-    const int64_t r0 = (int64_t)blockIdx.x * kPanelT;
-    float* A = dg + w;  // first row below the diagonal block
-    const int64_t row = r0 + tid;
-    for (int c = 0; c < w; ++c) {
-      if (row < M) cp_async4(&S[c * kPanelT + tid], &A[row + (int64_t)c * lda]);
-      else S[c * kPanelT + tid] = 0.0f;
+    for (int idx = tid; idx < kItems * w; idx += kPanelT) {
+      const int qq = idx % kItems, c = idx / kItems;
+      const int64_t row = item0 + qq;
+      if (row < M) A[row + (int64_t)c * lda] = S[qq * ls + c];
     }
-    cp_async_wait_all();
-    __syncthreads();
-    for (int k = tid; k < wp; k += kPanelT)
-      inv[k] = (k < w) ? __fdiv_rn(1.0f, F[k * wp + k]) : 0.0f;
-    __syncthreads();
-    const int r = tid;
-    for (int T = 0; T < nt; ++T) {
-      const int tw = min(8, w - 8 * T);
-      float x[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) x[j] = (j < tw) ? S[(8 * T + j) * kPanelT + r] : 0.0f;
-      for (int t = 0; t < T; ++t) {
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
-        float l[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) l[k] = S[(8 * t + k) * kPanelT + r];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          // U[8t .. 8t+7][8T + j]: one column of F, 8 consecutive rows
-          const float4 u0 = *reinterpret_cast<const float4*>(&F[(8 * T + j) * wp + 8 * t]);
-          const float4 u1 = *reinterpret_cast<const float4*>(&F[(8 * T + j) * wp + 8 * t + 4]);
-          float a = acc[j];
-          a = __fmaf_rn(l[0], u0.x, a);
-          a = __fmaf_rn(l[1], u0.y, a);
-          a = __fmaf_rn(l[2], u0.z, a);
-          a = __fmaf_rn(l[3], u0.w, a);
-          a = __fmaf_rn(l[4], u1.x, a);
-          a = __fmaf_rn(l[5], u1.y, a);
-          a = __fmaf_rn(l[6], u1.z, a);
-          a = __fmaf_rn(l[7], u1.w, a);
-          acc[j] = a;
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = __fsub_rn(x[j], acc[j]);
-      }
-      // tile elimination (src/lu_nopiv.cu:141-168): 1/d multiply, fused
-      // rank-1 updates inside the tile
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (k < tw) {
-          x[k] = __fmul_rn(x[k], inv[8 * T + k]);
-#pragma unroll
-          for (int j = k + 1; j < 8; ++j)
-            if (j < tw) x[j] = __fmaf_rn(-x[k], F[(8 * T + j) * wp + 8 * T + k], x[j]);
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (j < tw) S[(8 * T + j) * kPanelT + r] = x[j];
-    }
-    for (int c = 0; c < w; ++c)
-      if (row < M) A[row + (int64_t)c * lda] = S[c * kPanelT + tid];
   } else {
-    // strip: w rows x kPanelT columns, S[i*(kPanelT+1) + c]
-    constexpr int LS = kPanelT + 1;
-    const int64_t c0 = (int64_t)(blockIdx.x - nL) * kPanelT;
-    float* A = dg + (int64_t)w * lda;  // first column right of the block
-    for (int idx = tid; idx < w * kPanelT; idx += kPanelT) {
-      const int i = idx % w, cc = idx / w;
-      const int64_t col = c0 + cc;
-      if (col < N) cp_async4(&S[i * LS + cc], &A[i + col * lda]);
-      else S[i * LS + cc] = 0.0f;
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const int c = tid;
-    for (int T = 0; T < nt; ++T) {
-      const int tw = min(8, w - 8 * T);
-      float x[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) x[j] = (j < tw) ? S[(8 * T + j) * LS + c] : 0.0f;
-      for (int t = 0; t < T; ++t) {
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float u = S[(8 * t + k) * LS + c];
-          const float4 l0 = *reinterpret_cast<const float4*>(&F[(8 * t + k) * wp + 8 * T]);
-          const float4 l1 = *reinterpret_cast<const float4*>(&F[(8 * t + k) * wp + 8 * T + 4]);
-          acc[0] = __fmaf_rn(l0.x, u, acc[0]);
-          acc[1] = __fmaf_rn(l0.y, u, acc[1]);
-          acc[2] = __fmaf_rn(l0.z, u, acc[2]);
-          acc[3] = __fmaf_rn(l0.w, u, acc[3]);
-          acc[4] = __fmaf_rn(l1.x, u, acc[4]);
-          acc[5] = __fmaf_rn(l1.y, u, acc[5]);
-          acc[6] = __fmaf_rn(l1.z, u, acc[6]);
-          acc[7] = __fmaf_rn(l1.w, u, acc[7]);
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = __fsub_rn(x[j], acc[j]);
-      }
-      // forward substitution with the unit-lower tile (src/lu_nopiv.cu:304-316)
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-#pragma unroll
-        for (int j = k + 1; j < 8; ++j)
-          if (k < tw && j < tw)
-            x[j] = __fmaf_rn(-F[(8 * T + k) * wp + 8 * T + j], x[k], x[j]);
-#pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (j < tw) S[(8 * T + j) * LS + c] = x[j];
-    }
-    __syncthreads();
-    for (int idx = tid; idx < w * kPanelT; idx += kPanelT) {
-      const int i = idx % w, cc = idx / w;
-      const int64_t col = c0 + cc;
-      if (col < N) A[i + col * lda] = S[i * LS + cc];
+    for (int idx = tid; idx < kItems * w; idx += kPanelT) {
+      const int i = idx % w, qq = idx / w;
+      const int64_t col = item0 + qq;
+      if (col < N) A[i + col * lda] = S[qq * ls + i];
     }
   }
+  (void)valid;
 }
 
 // ---------------------------------------------------------------------------
@@ -442,15 +459,14 @@ lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
 
 static size_t lupanel_smem_bytes(int w) {
   const size_t wp = (size_t)((w + 7) / 8) * 8;
-  const size_t strip = std::max<size_t>((size_t)kPanelT * wp, wp * (kPanelT + 1));
-  return (wp * wp + wp + strip) * sizeof(float);
+  return (wp * (wp + 4) + wp + (size_t)kItems * (wp + 4)) * sizeof(float);
 }
 
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
                          int64_t M, int64_t N) {
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
-  const int64_t nL = M > 0 ? ceil_div(M, kPanelT) : 0;
-  const int64_t nU = N > 0 ? ceil_div(N, kPanelT) : 0;
+  const int64_t nL = M > 0 ? ceil_div(M, kItems) : 0;
+  const int64_t nU = N > 0 ? ceil_div(N, kItems) : 0;
   if (nL + nU == 0) return LU_SUCCESS;
   const size_t sm = lupanel_smem_bytes(w);
   LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));

@@ -1,0 +1,31 @@
+// Triangular solves and FP64 residuals (solve.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace lub {
+
+// op(T) X = X in place, T = the unit-lower L (upper = false) or the upper U
+// (upper = true) of the in-place factors lu (fp32, ld); op = T or T^T;
+// X fp64 n x nrhs (ldx).
+lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
+                      double* X, int64_t ldx, int64_t nrhs, bool upper,
+                      bool trans);
+
+// Workspace (bytes) of launch_residual / launch_norm_inf for size n.
+size_t residual_ws_bytes(int64_t n);
+
+// r = b - A x (fp64, deterministic order); maxes[0..2] receive the bit
+// patterns of max|r|, max|x|, max|b|.
+lu_status launch_residual(cudaStream_t st, int64_t n, const float* A,
+                          int64_t lda, const double* b, const double* x,
+                          double* r, void* ws, unsigned long long* maxes);
+
+// *out = bit pattern of ||A||_inf (max row sum of |a_ij|).
+lu_status launch_norm_inf(cudaStream_t st, int64_t n, const float* A,
+                          int64_t lda, void* ws, unsigned long long* out);
+
+// x += d
+lu_status launch_axpy(cudaStream_t st, int64_t n, const double* d, double* x);
+
+}  // namespace lub

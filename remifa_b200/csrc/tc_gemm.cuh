@@ -13,11 +13,14 @@ inline int tc_operand_bytes(TcOperand k) { return k == TcOperand::E4M3 ? 1 : 2; 
 // B column-major (ldb_p), both of type `kind`.  scale_a / scale_b (log2 per
 // 128-row tile of A / 128-column tile of B) are divided out of the product.
 // err: device int set non-zero if a bounded wait in the kernel gave up.
+// tiles_per_cta = 0 launches one persistent CTA per SM (max_ctas caps it);
+// > 0 gives every CTA that many consecutive 128 x 256 tiles, so SMs free up
+// while the update runs and concurrent (higher-priority) work can start.
 lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
                            int64_t N, int64_t K, float alpha, const void* A,
                            int64_t lda_p, const void* B, int64_t ldb_p, float* C,
                            int64_t ldc, const int* scale_a, const int* scale_b,
-                           int* err, int max_ctas = 0);
+                           int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
 // Largest power-of-two scale per 128-row tile of the fp32 column-major
 // src (M x K) / per 128-column tile of src (K x N) such that amax * 2^s <=

@@ -169,3 +169,19 @@ def test_lu_rl_tc32_large_backward_error(built):
     xh = O.lu_solve_f64(lu, b)
     be = O.backward_error(a, b, xh)
     assert be < 1e-4, be
+
+
+@pytest.mark.parametrize("compute", [rb.FP32, rb.TC32, rb.compute_type.TC32_BF16,
+                                     rb.compute_type.TC32_E4M3])
+@pytest.mark.parametrize("n,nb", [(1500, 256), (2048, 128), (777, 64)])
+def test_lookahead_is_bit_identical(built, compute, n, nb):
+    """The look-ahead schedule (panel k+1 concurrent with the bulk update of
+    step k on two streams) must not change any element's update order."""
+    if compute == rb.compute_type.TC32_E4M3 and nb % 128:
+        nb = 128
+    a = O.gen_matrix(n, seed=3, kind=1, alpha=1.5)
+    d1, d2 = to_dev(a), to_dev(a)
+    rb.lu_nopiv_rl(d1, nb=nb, outer=compute, lookahead=False)
+    rb.lu_nopiv_rl(d2, nb=nb, outer=compute, lookahead=True)
+    torch.cuda.synchronize()
+    assert torch.equal(d1, d2)

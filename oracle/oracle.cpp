@@ -369,6 +369,58 @@ void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
   omp_set_num_threads(saved);
 }
 
+// reference src/lu_nopiv_inner_ll.hxx:197-370 (T = P = F = float, ib = 8):
+// m rows, n = outer block width; l and u point at the outer block's
+// diagonal (the same matrix for W = fp32).
+static void inner_ll(int64_t m, int64_t n, float* a, int64_t lda) {
+  const int64_t ib = 8;
+  const int64_t inc = (n - 1) / ib + 1;
+  float d[64];
+  for (int64_t k = 0; k < inc; ++k) {
+    const int64_t iofs = k * ib;
+    const int64_t cblkm = m - iofs;
+    const int64_t cblkn = std::min(n - iofs, ib);
+    const int64_t iofst = (k + 1) * ib;
+    if (iofs > 0) {
+      // L inner panel (src/lu_nopiv_inner_ll.hxx:225-246)
+      orc_gemm_sub_f32(cblkm, cblkn, iofs, a + iofs, lda, a + iofs * lda, lda,
+                       a + iofs + iofs * lda, lda);
+      // U inner panel (src/lu_nopiv_inner_ll.hxx:249-300)
+      if (cblkm > cblkn)
+        orc_gemm_sub_f32(cblkn, cblkm - cblkn, iofs, a + iofs, lda,
+                         a + iofst * lda, lda, a + iofs + iofst * lda, lda);
+    }
+    for (int64_t c = 0; c < cblkn; ++c)
+      for (int64_t r = 0; r < cblkn; ++r) d[r + c * 8] = at(a, lda, iofs + r, iofs + c);
+    float* t = a + iofs + iofs * lda;
+    orc_panel_f32(cblkm, cblkn, d, 8, t, lda, t, lda);
+  }
+}
+
+// reference src/lu_nopiv_ll.hxx:208-575 for W = OP = OF = float, I = O = FP32
+// (the lu_nopiv_ll_f32 wrapper, src/lu_nopiv_ll.cxx:14-29)
+void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                   int threads) {
+  const int saved = omp_get_max_threads();
+  if (threads > 0) omp_set_num_threads(threads);
+  const int64_t nc = (n - 1) / nb + 1;
+  for (int64_t kk = 0; kk < nc; ++kk) {
+    const int64_t ofs = kk * nb;
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = m - ofs;
+    if (ofs > 0) {
+      // block column (src/lu_nopiv_ll.hxx:239-250) and block row (:311-339)
+      orc_gemm_sub_f32(updm, in, ofs, a + ofs, lda, a + ofs * lda, lda,
+                       a + ofs + ofs * lda, lda);
+      if (updm > in)
+        orc_gemm_sub_f32(in, updm - in, ofs, a + ofs, lda, a + (ofs + in) * lda,
+                         lda, a + ofs + (ofs + in) * lda, lda);
+    }
+    inner_ll(updm, in, a + ofs + ofs * lda, lda);
+  }
+  omp_set_num_threads(saved);
+}
+
 // ---------------------------------------------------------------- FP64
 
 void orc_lu_f64(int64_t n, double* a, int64_t lda) {

@@ -81,6 +81,13 @@ void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
                          int64_t lda, int outer_fmt, int threads, int64_t kk0,
                          int64_t kk1);
 
+/* remifa::lu_nopiv_ll (src/lu_nopiv_ll.hxx:41-582) with ib = 8 for W = fp32,
+ * I = O = FP32 (the lu_nopiv_ll_f32 wrapper): left-looking outer blocks
+ * (one K = ofs update of the block column and block row), left-looking
+ * inner tiles (one K = 8t update), then the panel kernel. */
+void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                   int threads);
+
 /* ---- FP64 oracle ----------------------------------------------------- */
 void orc_lu_f64(int64_t n, double* a, int64_t lda);
 /* solve with unit-lower L and upper U stored together (no pivots) */

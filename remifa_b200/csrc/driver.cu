@@ -173,10 +173,17 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   const int dw = o.diag_width == 0 ? 128 : o.diag_width;
   if (dw < 8 || dw > 128 || dw % 8 != 0) return LU_ERR_INVALID_ARG;
   if (dtype != LU_F32) return LU_ERR_UNSUPPORTED;
-  if (o.variant != LU_RIGHT_LOOKING) return LU_ERR_UNSUPPORTED;
+  if (o.variant != LU_RIGHT_LOOKING && o.variant != LU_LEFT_LOOKING)
+    return LU_ERR_INVALID_ARG;
   if (o.inner_update != LU_COMPUTE_FP32) return LU_ERR_UNSUPPORTED;
   if (o.outer_update != LU_COMPUTE_FP32 && !is_tc((lu_compute)o.outer_update))
     return LU_ERR_UNSUPPORTED;
+  if (o.variant == LU_LEFT_LOOKING) {
+    // one diagonal kernel covers the outer block; e4m3 tile scales would
+    // have to follow the growing K range of the left-looking products
+    if (o.nb > 128) return LU_ERR_UNSUPPORTED;
+    if (o.outer_update == LU_COMPUTE_TC32_E4M3) return LU_ERR_UNSUPPORTED;
+  }
   p->n = n;
   p->nb = o.nb;
   p->diag_w = (int)std::min<int64_t>(dw, o.nb);
@@ -188,6 +195,22 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   size_t off = 0;
   p->off_status = off;  // [0] first bad pivot, [1] device wait error
   off += 256;
+  if (p->variant == LU_LEFT_LOOKING) {
+    p->diag_w = (int)p->nb;
+    if (is_tc(p->outer) && n > p->nb) {
+      // low-precision copies of all factored L columns (row-major) and U
+      // rows (column-major), leading dimension round16(n)
+      const int64_t ldk = (n + 15) / 16 * 16;
+      const size_t es = (size_t)tc_operand_bytes(tc_kind(p->outer));
+      off = align_up(off, 1024);
+      p->off_lcopy = off;
+      off = align_up(off + (size_t)n * ldk * es, 1024);
+      p->off_ucopy = off;
+      off = align_up(off + (size_t)n * ldk * es, 1024);
+    }
+    p->ws_bytes = off;
+    return LU_SUCCESS;
+  }
   if (is_tc(p->outer) && n > p->nb) {
     // two operand buffers: with look-ahead, step k+1 packs while the bulk
     // update of step k still reads step k's copies
@@ -334,6 +357,70 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   return status;
 }
 
+// Left-looking (Crout) factorization, restating src/lu_nopiv_ll.hxx:208-575
+// with nb <= 128: per outer block, one K = ofs update of the block column and
+// the block row (FP32 SIMT, or tensor cores on the low-precision copies of
+// all earlier factors), then the Crout diagonal kernel and the left-looking
+// L/U panels.  The FP32 path applies every update in the reference's order.
+static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
+                           int64_t lda, char* ws, int* first_bad, int* err) {
+  const int64_t n = p.n, nb = p.nb;
+  const bool tc = is_tc(p.outer);
+  const TcOperand kind = tc_kind(p.outer);
+  const int64_t ldk = (n + 15) / 16 * 16;
+  const int64_t es = tc_operand_bytes(kind);
+  char* Lc = ws + p.off_lcopy;
+  char* Uc = ws + p.off_ucopy;
+  for (int64_t ofs = 0; ofs < n; ofs += nb) {
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = n - ofs;
+    float* blk = a + ofs + ofs * lda;
+    if (ofs > 0) {
+      if (tc) {
+        ProfScope ps("tc_update", st,
+                     8.0 * updm * in + 8.0 * in * (updm - in) + es * (double)ofs * (updm + in),
+                     2.0 * ofs * ((double)updm * in + (double)in * (updm - in)));
+        LUB_TRY(launch_tc_update(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es, ldk,
+                                 Uc + ofs * ldk * es, ldk, blk, lda, nullptr, nullptr, err));
+        if (updm > in)
+          LUB_TRY(launch_tc_update(st, kind, in, updm - in, ofs, -1.0f,
+                                   Lc + ofs * ldk * es, ldk, Uc + (ofs + in) * ldk * es,
+                                   ldk, blk + in * lda, lda, nullptr, nullptr, err));
+      } else {
+        ProfScope ps("sgemm_update", st, 0.0,
+                     2.0 * ofs * ((double)updm * in + (double)in * (updm - in)));
+        LUB_TRY(launch_sgemm_update(st, updm, in, ofs, -1.0f, a + ofs, lda,
+                                    a + ofs * lda, lda, 1.0f, blk, lda, false));
+        if (updm > in)
+          LUB_TRY(launch_sgemm_update(st, in, updm - in, ofs, -1.0f, a + ofs, lda,
+                                      a + (ofs + in) * lda, lda, 1.0f, blk + in * lda,
+                                      lda, false));
+      }
+    }
+    {
+      ProfScope ps("diag_factor", st, 8.0 * in * in, 2.0 * in * in * (double)in / 3.0);
+      LUB_TRY(launch_diag_crout(st, blk, lda, (int)in, ofs, first_bad));
+    }
+    const int64_t rest = updm - in;
+    if (rest > 0) {
+      {
+        ProfScope ps("lupanel", st, 16.0 * rest * in, 2.0 * rest * (double)in * in);
+        LUB_TRY(launch_lupanel(st, blk, lda, (int)in, rest, rest, true));
+      }
+      if (tc) {
+        ProfScope ps("pack_operands", st, 2.0 * rest * in * (4.0 + es));
+        // L21 rows [ofs+in, n) of the block's columns -> row-major copy;
+        // U12 columns [ofs+in, n) of the block's rows -> column-major copy
+        LUB_TRY(launch_pack_a(st, kind, rest, in, blk + in, lda,
+                              Lc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
+        LUB_TRY(launch_pack_b(st, kind, in, rest, blk + in * lda, lda,
+                              Uc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
+      }
+    }
+  }
+  return LU_SUCCESS;
+}
+
 lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
                     void* d_a, lu_dtype dtype_a, int64_t lda, int* d_info,
                     void* d_a_lowp, int64_t ld_lowp, void* workspace,
@@ -361,7 +448,9 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
   lu_status s = launch_fill_int(st, first_bad, kNoBadPivot, 1);
   if (s == LU_SUCCESS) s = launch_fill_int(st, err, 0, 1);
   if (s == LU_SUCCESS && n > 0)
-    s = rl_factor(p, st, static_cast<float*>(d_a), lda, wsb, first_bad, err);
+    s = p.variant == LU_LEFT_LOOKING
+            ? ll_factor(p, st, static_cast<float*>(d_a), lda, wsb, first_bad, err)
+            : rl_factor(p, st, static_cast<float*>(d_a), lda, wsb, first_bad, err);
   if (s == LU_SUCCESS) s = launch_finalize_info(st, first_bad, err, d_info);
   if (s == LU_SUCCESS && d_a_lowp != nullptr && n > 0)
     s = launch_convert(st, m, n, d_a, LU_F32, lda, d_a_lowp, LU_F16, ld_lowp, 0);

@@ -10,9 +10,12 @@ size_t diag_smem_bytes(int w);
 lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
                              int64_t col0, int* first_bad);
 // L rows (M of them, below) and U columns (N, right) of the w x w factored
-// diagonal block dg, one launch.
+// diagonal block dg, one launch.  left: left-looking (Crout) update order.
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
-                         int64_t M, int64_t N);
+                         int64_t M, int64_t N, bool left = false);
+// Left-looking (Crout) factorization of a w x w (w <= 128) diagonal block.
+lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
+                            int64_t col0, int* first_bad);
 lu_status launch_ref_panel(cudaStream_t st, int64_t m, int n, const float* d,
                            int64_t ldd, float* l, int64_t ldl, float* u,
                            int64_t ldu, int* stat);

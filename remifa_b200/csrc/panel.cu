@@ -223,6 +223,92 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 }
 
 // ---------------------------------------------------------------------------
+// Diagonal block of the left-looking (Crout) variant, w <= 128, one CTA.
+// Per tile T, in the reference's order (src/lu_nopiv_inner_ll.hxx:197-370):
+// the tile column (rows >= 8T) and the tile row (columns right of the tile)
+// receive one update summing all earlier columns of the block (acc over
+// k < 8T, subtracted once), then the tile is factored and the L rows and U
+// columns of the block are eliminated with it.
+__global__ void __launch_bounds__(kThreads)
+diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
+                  int* first_bad) {
+  extern __shared__ __align__(16) float smem[];
+  const int LD = ((w + 3) / 4) * 4 + 4;
+  float* D = smem;
+  float* inv = D + (size_t)LD * w;  // 8
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < w * w; idx += kThreads) {
+    const int i = idx % w, j = idx / w;
+    cp_async4(&D[i + j * LD], &a[i + (int64_t)j * lda]);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int nt = (w + 7) / 8;
+  for (int t = 0; t < nt; ++t) {
+    const int t0 = 8 * t;
+    const int tw = min(8, w - t0);
+    if (t0 > 0) {
+      // (a) tile column: rows [t0, w) x cols [t0, t0+tw); tile row: rows
+      // [t0, t0+tw) x cols [t0+tw, w)
+      const int ncol = (w - t0) * tw;
+      const int nrow = tw * (w - t0 - tw);
+      for (int e = tid; e < ncol + nrow; e += kThreads) {
+        int i, c;
+        if (e < ncol) { i = t0 + e % (w - t0); c = t0 + e / (w - t0); }
+        else { const int f = e - ncol; i = t0 + f % tw; c = t0 + tw + f / tw; }
+        float acc = 0.0f;
+        for (int k = 0; k < t0; ++k) acc = __fmaf_rn(D[i + k * LD], D[k + c * LD], acc);
+        D[i + c * LD] = __fsub_rn(D[i + c * LD], acc);
+      }
+      __syncthreads();
+    }
+    // (b) factor the tile
+    if (tid == 0) factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
+    __syncthreads();
+    const int s = w - t0 - tw;
+    if (s <= 0) break;
+    // (c) eliminate the block's L rows / U columns with the tile
+    if (tid < 128) {
+      if (tid < s) {
+        const int i = t0 + tw + tid;
+        float row[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) row[c] = D[i + (t0 + c) * LD];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          row[k] = __fmul_rn(row[k], inv[k]);
+#pragma unroll
+          for (int c = k + 1; c < 8; ++c)
+            row[c] = __fmaf_rn(-row[k], D[(t0 + k) + (t0 + c) * LD], row[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) D[i + (t0 + c) * LD] = row[c];
+      }
+    } else {
+      const int q = tid - 128;
+      if (q < s) {
+        const int j = t0 + tw + q;
+        float col[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) col[r] = D[(t0 + r) + j * LD];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+          for (int r = k + 1; r < 8; ++r)
+            col[r] = __fmaf_rn(-D[(t0 + r) + (t0 + k) * LD], col[k], col[r]);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) D[(t0 + r) + j * LD] = col[r];
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < w * w; idx += kThreads) {
+    const int i = idx % w, j = idx / w;
+    a[i + (int64_t)j * lda] = D[i + j * LD];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // L and U panels of one sub-panel, one launch.  `dg` is the factored w x w
 // diagonal block (lda); M rows lie below it, N columns right of it.
 //
@@ -242,7 +328,7 @@ constexpr int kItems = kPanelT / kGroup;  // rows / columns per CTA
 
 __global__ void __launch_bounds__(kPanelT)
 lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
-               int64_t N, int nL) {
+               int64_t N, int nL, bool left) {
   extern __shared__ __align__(16) float smem[];
   const int tid = threadIdx.x;
   const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
@@ -306,11 +392,15 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   for (int T = 0; T < nt; ++T) {
     const int tw = min(8, w - 8 * T);
     float x = srow[8 * T + j];
-    // updates of earlier tiles, in order
+    // updates of earlier tiles, in order.  Right-looking (the reference's
+    // lu_nopiv_inner_rl): one subtraction per earlier tile.  Left-looking
+    // (lu_nopiv_inner_ll, src/lu_nopiv_inner_ll.hxx:225-300): one sum over
+    // all earlier columns, subtracted once.
+    float accl = 0.0f;
     for (int t = 0; t < T; ++t) {
       const float4 v0 = *reinterpret_cast<const float4*>(&srow[8 * t]);
       const float4 v1 = *reinterpret_cast<const float4*>(&srow[8 * t + 4]);
-      float acc = 0.0f;
+      float acc = left ? accl : 0.0f;
       if (is_l) {
         // U[8t+k][8T+j]: column 8T+j of F, rows 8t..8t+7
         const float* fcol = &F[(8 * T + j) * lf + 8 * t];
@@ -337,8 +427,10 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
         acc = __fmaf_rn(frow[6 * lf], v1.z, acc);
         acc = __fmaf_rn(frow[7 * lf], v1.w, acc);
       }
-      x = __fsub_rn(x, acc);
+      if (left) accl = acc;
+      else x = __fsub_rn(x, acc);
     }
+    if (left && T > 0) x = __fsub_rn(x, accl);
     // tile elimination
     if (is_l) {
       // src/lu_nopiv.cu:141-168: x_k *= 1/d_k, then x_j -= x_k * U[k][j]
@@ -457,20 +549,32 @@ lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
   return LU_SUCCESS;
 }
 
+lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
+                            int64_t col0, int* first_bad) {
+  if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
+  const int LD = ((w + 3) / 4) * 4 + 4;
+  const size_t sm = ((size_t)LD * w + 8) * sizeof(float);
+  LUB_CUDA_TRY(set_smem_limit((const void*)diag_crout_kernel, sm));
+  diag_crout_kernel<<<1, kThreads, sm, st>>>(a, lda, w, col0, first_bad);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
 static size_t lupanel_smem_bytes(int w) {
   const size_t wp = (size_t)((w + 7) / 8) * 8;
   return (wp * (wp + 4) + wp + (size_t)kItems * (wp + 4)) * sizeof(float);
 }
 
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
-                         int64_t M, int64_t N) {
+                         int64_t M, int64_t N, bool left) {
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
   const int64_t nL = M > 0 ? ceil_div(M, kItems) : 0;
   const int64_t nU = N > 0 ? ceil_div(N, kItems) : 0;
   if (nL + nU == 0) return LU_SUCCESS;
   const size_t sm = lupanel_smem_bytes(w);
   LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));
-  lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL);
+  lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL,
+                                                           left);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

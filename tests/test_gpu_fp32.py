@@ -226,3 +226,65 @@ def test_workspace_caller_provided(built):
     np.testing.assert_array_equal(to_host(da), O.lu_rl(a, nb=128))
     with pytest.raises(RuntimeError):
         rb.lu_nopiv_rl(to_dev(a), nb=128, workspace=ws[:1])
+
+
+# ------------------------------------------------------------ left-looking
+
+LL_CASES = [(7, 8), (64, 64), (200, 64), (257, 128), (520, 64), (1024, 128), (777, 32)]
+
+
+@pytest.mark.parametrize("n,nb", LL_CASES)
+def test_lu_ll_fp32_bit_exact_vs_oracle(built, n, nb):
+    a = O.gen_matrix(n, seed=n + 3, kind=1, alpha=1.5, lda=n + 2)
+    want = O.lu_ll(a, nb=nb)
+    da = to_dev(a)
+    info = rb.lu_nopiv_ll(da, nb=nb)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(da), want)
+    assert int(info.item()) == 0
+
+
+def test_lu_ll_fp32_vs_reference_gpu(built):
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference library not built")
+    L = ctypes.CDLL(REF_SO)
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    L.ref_lu_nopiv_ll_f32.argtypes = [vp, i, i, i, vp, i, vp]
+    n, nb = 1024, 64
+    a = O.gen_diagdom(n, lda=n)
+    mine, theirs = to_dev(a), to_dev(a)
+    rb.lu_nopiv_ll(mine, nb=nb)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert L.ref_lu_nopiv_ll_f32(_st(), n, n, nb, ctypes.c_void_p(theirs.data_ptr()), n,
+                                 ctypes.c_void_p(info.data_ptr())) == 0
+    torch.cuda.synchronize()
+    lm, lr = to_host(mine), to_host(theirs)
+    assert np.abs(lm - lr).max() / np.abs(lr).max() <= 4 * n * 2.0 ** -24
+    b = O.gen_rhs(a, np.ones(n, np.float32))
+    e_m = O.nwerr(a, b, O.lu_solve_f32(lm, b))
+    e_r = O.nwerr(a, b, O.lu_solve_f32(lr, b))
+    assert e_m <= 4 * e_r and e_r <= 4 * e_m
+
+
+@pytest.mark.parametrize("compute", [rb.TC32, rb.compute_type.TC32_BF16])
+def test_lu_ll_tensor_core(built, compute):
+    n, nb = 1500, 128
+    a = O.gen_matrix(n, seed=5, kind=1, alpha=1.5)
+    da = to_dev(a)
+    info = rb.lu_nopiv_ll(da, nb=nb, outer=compute)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    got = to_host(da)
+    fe = O.factor_error(a, got)
+    assert fe < (2e-4 if compute == rb.TC32 else 2e-3), fe
+    # same algorithm in fp32: close to the FP32 Crout factors
+    want = O.lu_ll(a, nb=nb)
+    assert np.abs(got - want).max() / np.abs(want).max() < (1e-3 if compute == rb.TC32 else 1e-2)
+
+
+def test_lu_ll_limits(built):
+    a = to_dev(O.gen_matrix(300, seed=1, kind=0, alpha=2.0))
+    with pytest.raises(NotImplementedError):
+        rb.lu_nopiv_ll(a, nb=256)
+    with pytest.raises(NotImplementedError):
+        rb.lu_nopiv_ll(a, nb=128, outer=rb.compute_type.TC32_E4M3)

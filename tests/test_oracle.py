@@ -272,3 +272,27 @@ def test_golden_ref_rl_tc32():
     assert rel < 1e-4
     fe_ref, fe_orc = O.factor_error(a, np.asfortranarray(ref)), O.factor_error(a, lu)
     assert fe_orc <= 2 * fe_ref and fe_ref <= 2 * fe_orc
+
+
+@pytest.mark.parametrize("n,nb", [(7, 8), (64, 16), (200, 64), (257, 128)])
+def test_lu_ll_against_fp64(n, nb):
+    a = O.gen_matrix(n, seed=n + 1, kind=1, alpha=1.5)
+    lu = O.lu_ll(a, nb=nb)
+    assert O.factor_error(a, lu) <= 10 * n * U32
+    # same factorization as RL up to rounding
+    assert np.abs(lu - O.lu_rl(a, nb=nb)).max() <= 8 * n * U32 * np.abs(lu).max()
+
+
+def test_golden_ref_ll_f32():
+    g = _golden("ref_ll_f32_n256_nb64.npz")
+    a = np.asfortranarray(g["a_in"])
+    np.testing.assert_array_equal(a, O.gen_diagdom(256, lda=256))
+    lu = O.lu_ll(a, nb=64)
+    ref = g["lu"]
+    rel = np.abs(lu - ref).max() / np.abs(ref).max()
+    assert rel <= 4 * 256 * U32
+    x1 = np.ones(256, np.float32)
+    b = O.gen_rhs(a, x1)
+    e_ref = O.nwerr(a, b, O.lu_solve_f32(np.asfortranarray(ref), b))
+    e_orc = O.nwerr(a, b, O.lu_solve_f32(lu, b))
+    assert e_orc <= 4 * e_ref + 1e-12 and e_ref <= 4 * e_orc + 1e-12

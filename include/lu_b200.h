@@ -197,6 +197,35 @@ LU_API lu_status lu_refine_c(lu_stream_t stream, int64_t n, const float* d_a,
                              int max_iter, int* iters, double* berr,
                              void* workspace, size_t ws_bytes);
 
+/* Several right-hand sides (B, X fp64, n x nrhs) and the transposed system
+ * (trans = 1: A^T X = B, backward error with ||A||_1).  *iters / *berr
+ * receive the largest iteration count / backward error over the columns. */
+LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
+                                const float* d_a, int64_t lda, const float* d_lu,
+                                int64_t ldlu, const double* d_b, int64_t ldb,
+                                double* d_x, int64_t ldx, int trans, double tol,
+                                int max_iter, int* iters, double* berr,
+                                void* workspace, size_t ws_bytes);
+
+/* ---- adjoint of the solve (new) ---------------------------------------- */
+
+/* Backward pass of X = A^-1 B for a loss with gradient G = dL/dX, reusing
+ * the forward factors d_lu of A: on exit d_g holds dL/dB = A^-T G and, when
+ * d_da is not NULL, d_da = dL/dA = -(A^-T G) X^T (fp64 outer product stored
+ * fp32); d_x is the forward solution X (fp64, n x nrhs).
+ * d_a == NULL: A^-T G by two transposed triangular solves (U^T, then L^T).
+ * d_a != NULL (the fp32 matrix A): FP64 refinement of A^T dB = G to tol as in
+ * lu_refine_ex_c (trans = 1); LU_ERR_NOT_CONVERGED is returned after dA is
+ * still written.  Workspace: lu_adjoint_workspace_size, or NULL for
+ * stream-ordered allocation; unused without refinement. */
+LU_API lu_status lu_adjoint_workspace_size(int64_t n, int64_t nrhs, size_t* bytes);
+LU_API lu_status lu_adjoint_c(lu_stream_t stream, int64_t n, int64_t nrhs,
+                              const float* d_a, int64_t lda, const float* d_lu,
+                              int64_t ldlu, const double* d_x, int64_t ldx,
+                              double* d_g, int64_t ldg, float* d_da, int64_t ldda,
+                              double tol, int max_iter, int* iters, double* berr,
+                              void* workspace, size_t ws_bytes);
+
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {
   char name[32];     /* kernel class, e.g. "tc_update", "diag_factor" */

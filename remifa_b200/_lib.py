@@ -78,6 +78,13 @@ SIGNATURES = {
     "lu_refine_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_double,
                            _int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_double),
                            _vp, ctypes.c_size_t]),
+    "lu_refine_ex_c": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
+                              _i64, _int, ctypes.c_double, _int, ctypes.POINTER(_int),
+                              ctypes.POINTER(ctypes.c_double), _vp, ctypes.c_size_t]),
+    "lu_adjoint_workspace_size": (_int, [_i64, _i64, ctypes.POINTER(ctypes.c_size_t)]),
+    "lu_adjoint_c": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
+                            _vp, _i64, ctypes.c_double, _int, ctypes.POINTER(_int),
+                            ctypes.POINTER(ctypes.c_double), _vp, ctypes.c_size_t]),
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),

@@ -28,4 +28,14 @@ lu_status launch_norm_inf(cudaStream_t st, int64_t n, const float* A,
 // x += d
 lu_status launch_axpy(cudaStream_t st, int64_t n, const double* d, double* x);
 
+// adjoint.cu: dA = alpha * P Q^T (fp64 in, fp32 out); r = b - A^T x; ||A||_1
+lu_status launch_outer(cudaStream_t st, int64_t n, int64_t k, double alpha,
+                       const double* P, int64_t ldp, const double* Q, int64_t ldq,
+                       float* dA, int64_t ldda);
+lu_status launch_residual_t(cudaStream_t st, int64_t n, const float* A,
+                            int64_t lda, const double* b, const double* x,
+                            double* r, unsigned long long* maxes);
+lu_status launch_norm_one(cudaStream_t st, int64_t n, const float* A,
+                          int64_t lda, unsigned long long* out);
+
 }  // namespace lub

@@ -197,6 +197,20 @@ LU_API lu_status lu_refine_c(lu_stream_t stream, int64_t n, const float* d_a,
                              int max_iter, int* iters, double* berr,
                              void* workspace, size_t ws_bytes);
 
+/* lu_refine_c without any allocation (no counterpart in the reference): the
+ * scratch is one array compiled into the library (LU_REFINE_STATIC_SCRATCH_BYTES
+ * of device memory per device), so n <= LU_REFINE_STATIC_MAX_N, else
+ * LU_ERR_INVALID_ARG with nothing enqueued.  For callers that cannot hand
+ * over or allocate device memory.  The first call on a device looks the
+ * array up (cudaGetSymbolAddress) and should come before any stream capture;
+ * calls overlapping in time on one device share the array and race. */
+#define LU_REFINE_STATIC_MAX_N 4096
+#define LU_REFINE_STATIC_SCRATCH_BYTES 614400
+LU_API lu_status lu_refine_static_c(lu_stream_t stream, int64_t n, const float* d_a,
+                                    int64_t lda, const float* d_lu, int64_t ldlu,
+                                    const double* d_b, double* d_x, double tol,
+                                    int max_iter, int* iters, double* berr);
+
 /* Several right-hand sides (B, X fp64, n x nrhs) and the transposed system
  * (trans = 1: A^T X = B, backward error with ||A||_1).  *iters / *berr
  * receive the largest iteration count / backward error over the columns. */

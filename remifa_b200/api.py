@@ -286,3 +286,22 @@ def gesv_mixed(a: torch.Tensor, b: torch.Tensor, outer=TC32, nb: int = 256,
     info = lu_nopiv_rl(lu, nb=nb, outer=outer, lookahead=lookahead, stream=stream)
     x, it, be = refine(a, lu, b, tol=tol, max_iter=max_iter, stream=stream)
     return x, info, it, be
+
+
+def refine_static(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
+                  x: torch.Tensor, tol: float = 1e-14, max_iter: int = 30,
+                  stream=None):
+    """refine() without any device allocation (lu_refine_static_c): the
+    scratch is compiled into the library, so n <= 4096 and calls must not
+    overlap in time on one device.  x (fp64, n) receives the solution.
+    Returns (iterations, berr)."""
+    n = a.shape[0]
+    it = ctypes.c_int(0)
+    be = ctypes.c_double(0.0)
+    st = _lib.lib().lu_refine_static_c(_stream(stream), n, _ptr(a), ld(a), _ptr(lu),
+                                       ld(lu), _ptr(b), _ptr(x), float(tol),
+                                       int(max_iter), ctypes.byref(it),
+                                       ctypes.byref(be))
+    if st != _lib.ERR_NOT_CONVERGED:
+        _lib.check(st, "lu_refine_static_c")
+    return it.value, be.value

@@ -40,6 +40,8 @@ constexpr int kNoBadPivot = 0x7f7f7f7f;
     if (_s != LU_SUCCESS) return _s;        \
   } while (0)
 
+// Store a plain message for lu_last_error (this thread).
+void record_message(const char* msg);
 void record_cuda_error(cudaError_t e, const char* what, const char* file,
                        int line);
 // Counts one kernel launch of this library (profile.cu).

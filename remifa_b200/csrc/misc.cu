@@ -34,6 +34,11 @@ void record_cuda_error(cudaError_t e, const char* what, const char* file,
   if (std::getenv("LU_B200_VERBOSE")) std::fprintf(stderr, "[lu_b200] %s\n", g_last_error);
 }
 
+void record_message(const char* msg) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+  if (std::getenv("LU_B200_VERBOSE")) std::fprintf(stderr, "[lu_b200] %s\n", g_last_error);
+}
+
 const char* last_error_message() { return g_last_error; }
 
 int sm_count() {

@@ -240,6 +240,64 @@ LU_API lu_status lu_adjoint_c(lu_stream_t stream, int64_t n, int64_t nrhs,
                               double tol, int max_iter, int* iters, double* berr,
                               void* workspace, size_t ws_bytes);
 
+/* ---- batched factorization of many uneven matrices (new) -------------- */
+
+/* Many independent no-pivot LUs (fp32, column-major, in place, sizes 1 ..
+ * LU_BATCH_MAX_N) in one persistent launch.  A plan fixes the sizes and the
+ * per-size-bucket choice of block width (32 or 64) and outer-update
+ * precision (LU_COMPUTE_FP32 or LU_COMPUTE_TC32); executing it allocates
+ * nothing, so the launch can be captured in a CUDA graph (lu_batch_graph_*).
+ * Matrix i is factored exactly as lu_nopiv_rl_c with nb = its bucket's block
+ * width and inner updates FP32 would factor it.  Buckets: n < 32, [32, 64),
+ * [64, 128), [128, 256), [256, 512), 512. */
+#define LU_BATCH_MAX_N 512
+#define LU_BATCH_BUCKETS 6
+typedef struct lu_batch_tuning {
+  int32_t nb[LU_BATCH_BUCKETS];     /* 32 or 64 */
+  int32_t outer[LU_BATCH_BUCKETS];  /* LU_COMPUTE_FP32 or LU_COMPUTE_TC32 */
+} lu_batch_tuning;
+typedef struct lu_batch_plan_t* lu_batch_plan;
+typedef struct lu_batch_graph_t* lu_batch_graph;
+
+/* opts: inner_update FP32; outer_update FP32 or TC32 (every bucket's
+ * default); nb 0 (= 64), 32 or 64.  tuning (optional) overrides per bucket.
+ * h_n: host array of the batch sizes.  Allocates the plan's device arrays
+ * on the current device. */
+LU_API lu_status lu_batch_plan_create(const lu_opts* opts, int64_t batch,
+                                      const int32_t* h_n, const lu_batch_tuning* tuning,
+                                      lu_batch_plan* plan);
+LU_API void lu_batch_plan_destroy(lu_batch_plan plan);
+LU_API lu_status lu_batch_plan_tuning(lu_batch_plan plan, lu_batch_tuning* out);
+LU_API lu_status lu_batch_plan_set_tuning(lu_batch_plan plan, const lu_batch_tuning* t);
+
+/* Factor matrix i at d_ptrs[i] (device array of device pointers) with
+ * leading dimension d_lda[i] (device array; NULL: lda = n_i) in place;
+ * d_info[i] = 0, the 1-based column of the first zero / non-finite pivot,
+ * or -1 if a bounded device wait gave up.  Asynchronous on `stream`. */
+LU_API lu_status lu_batch_c(lu_batch_plan plan, lu_stream_t stream, float* const* d_ptrs,
+                            const int32_t* d_lda, int32_t* d_info);
+
+/* Project autotuner: for every size bucket present in the plan, times each
+ * block width (32, 64) at the plan's outer precision on up to 4 x SMs
+ * seeded matrices with that bucket's sizes (median of `reps` runs after a
+ * warm-up), keeps the fastest in the plan and returns the table in *out
+ * (may be NULL).  Allocates and synchronises: a setup-time call. */
+LU_API lu_status lu_batch_autotune(lu_batch_plan plan, lu_stream_t stream, int reps,
+                                   lu_batch_tuning* out);
+
+/* The same call captured once into a CUDA graph and replayed. */
+LU_API lu_status lu_batch_graph_create(lu_batch_plan plan, lu_stream_t stream,
+                                       float* const* d_ptrs, const int32_t* d_lda,
+                                       int32_t* d_info, lu_batch_graph* graph);
+LU_API lu_status lu_batch_graph_launch(lu_batch_graph graph, lu_stream_t stream);
+LU_API void lu_batch_graph_destroy(lu_batch_graph graph);
+
+/* Seeded generator for a batch: matrix i is lu_gen_matrix_c(n_i, seed + i,
+ * kind, alpha) (no scaling).  d_n, d_lda (NULL: lda = n): device arrays. */
+LU_API lu_status lu_gen_batch_c(lu_stream_t stream, int64_t batch, float* const* d_ptrs,
+                                const int32_t* d_n, const int32_t* d_lda, uint64_t seed,
+                                int kind, double alpha);
+
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {
   char name[32];     /* kernel class, e.g. "tc_update", "diag_factor" */

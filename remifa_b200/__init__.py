@@ -5,6 +5,7 @@ lives in liblu_b200.so (hand-written CUDA for sm_100a behind the C ABI in
 include/lu_b200.h); this package is the thin Python host layer over it.
 """
 from . import _lib
+from . import batch
 from .api import (FP16, FP32, TC16, TC32, align_lda, colmajor, colmajor_empty,
                   compute_type, convert, gemmex, gen_matrix, gesv_mixed,
                   launch_count, ld, lu_nopiv_ll, lu_nopiv_panel, lu_nopiv_rl,

@@ -48,6 +48,17 @@ class LuProfileEntry(ctypes.Structure):
     ]
 
 
+BATCH_MAX_N = 512
+BATCH_BUCKETS = 6
+
+
+class LuBatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("nb", ctypes.c_int32 * BATCH_BUCKETS),
+        ("outer", ctypes.c_int32 * BATCH_BUCKETS),
+    ]
+
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _int = ctypes.c_int
@@ -87,6 +98,18 @@ SIGNATURES = {
     "lu_adjoint_c": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
                             _vp, _i64, ctypes.c_double, _int, ctypes.POINTER(_int),
                             ctypes.POINTER(ctypes.c_double), _vp, ctypes.c_size_t]),
+    "lu_batch_plan_create": (_int, [ctypes.POINTER(LuOpts), _i64, _vp,
+                                    ctypes.POINTER(LuBatchTuning), ctypes.POINTER(_vp)]),
+    "lu_batch_plan_destroy": (None, [_vp]),
+    "lu_batch_plan_tuning": (_int, [_vp, ctypes.POINTER(LuBatchTuning)]),
+    "lu_batch_plan_set_tuning": (_int, [_vp, ctypes.POINTER(LuBatchTuning)]),
+    "lu_batch_c": (_int, [_vp, _vp, _vp, _vp, _vp]),
+    "lu_batch_autotune": (_int, [_vp, _vp, _int, ctypes.POINTER(LuBatchTuning)]),
+    "lu_batch_graph_create": (_int, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "lu_batch_graph_launch": (_int, [_vp, _vp]),
+    "lu_batch_graph_destroy": (None, [_vp]),
+    "lu_gen_batch_c": (_int, [_vp, _i64, _vp, _vp, _vp, ctypes.c_uint64, _int,
+                              ctypes.c_double]),
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),

@@ -80,6 +80,30 @@ __global__ void gen_diag_kernel(int64_t n, float* __restrict__ a, int64_t lda,
   a[i + i * lda] = ldexpf(ldexpf(d, kscale), row_shift(gamma_bits, i, n));
 }
 
+// One CTA per matrix of a batch (n <= 1024): thread per row.
+__global__ void __launch_bounds__(256)
+gen_batch_kernel(float* const* __restrict__ ptrs, const int32_t* __restrict__ ns,
+                 const int32_t* __restrict__ ldas, uint64_t seed, int kind,
+                 double alpha) {
+  const int mat = blockIdx.x;
+  const int64_t n = ns[mat];
+  const int64_t lda = ldas ? (int64_t)ldas[mat] : n;
+  float* a = ptrs[mat];
+  const uint64_t seedmix = mix64(seed + (uint64_t)mat);
+  const float scale =
+      kind == 0 ? 0x1p-23f : (float)(0x1p-21 / sqrt((double)n));
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    unsigned long long s = 0;
+    for (int64_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const int32_t q = sample_q(seedmix, (uint64_t)i, (uint64_t)j, kind);
+      s += (unsigned long long)(q < 0 ? -(int64_t)q : (int64_t)q);
+      a[i + j * lda] = __fmul_rn((float)q, scale);
+    }
+    a[i + i * lda] = __double2float_rn(__dmul_rn(__dmul_rn(alpha, (double)s), (double)scale));
+  }
+}
+
 uint64_t host_mix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -122,4 +146,23 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
   return LU_SUCCESS;
 }
 
+lu_status launch_gen_batch(cudaStream_t st, int64_t batch, float* const* ptrs,
+                           const int32_t* ns, const int32_t* ldas, uint64_t seed,
+                           int kind, double alpha) {
+  if (batch < 0 || (kind != 0 && kind != 1) || batch > INT32_MAX) return LU_ERR_INVALID_ARG;
+  if (batch == 0) return LU_SUCCESS;
+  if (!ptrs || !ns) return LU_ERR_INVALID_ARG;
+  gen_batch_kernel<<<(unsigned)batch, 256, 0, st>>>(ptrs, ns, ldas, seed, kind, alpha);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
 }  // namespace lub
+
+extern "C" LU_API lu_status lu_gen_batch_c(lu_stream_t stream, int64_t batch,
+                                           float* const* d_ptrs, const int32_t* d_n,
+                                           const int32_t* d_lda, uint64_t seed, int kind,
+                                           double alpha) {
+  return lub::launch_gen_batch((cudaStream_t)stream, batch, d_ptrs, d_n, d_lda, seed,
+                               kind, alpha);
+}

@@ -45,6 +45,10 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
                             uint64_t seed, int kind, double alpha, int kscale,
                             double gamma_bits);
 
+lu_status launch_gen_batch(cudaStream_t st, int64_t batch, float* const* ptrs,
+                           const int32_t* ns, const int32_t* ldas, uint64_t seed,
+                           int kind, double alpha);
+
 // misc.cu
 lu_status launch_fill_int(cudaStream_t st, int* p, int v, int64_t count);
 lu_status launch_finalize_info(cudaStream_t st, const int* first_bad,

@@ -59,8 +59,9 @@ constexpr int kAStage = kTileM * 128;   // fp16 K-major tile, 128-byte rows
 constexpr int kAOff = 0;                // 2 A stages (or one fp32 L tile)
 constexpr int kBOff = 2 * kAStage;      // B operand (fp16) or U (fp32)
 constexpr int kLOff = kBOff + 64 * 64 * 4;
-constexpr int kLDL = 72;                // L_kk leading dimension (skewed)
-constexpr int kCOff = kLOff + 64 * kLDL * 4;
+constexpr int kLDT = 68;                // L_kk, row-major, row stride
+constexpr int kUOff = kLOff + 64 * kLDT * 4;  // 2 x (8 x 64) substituted chunk rows
+constexpr int kCOff = kUOff + 2 * 8 * 64 * 4;
 constexpr int kTmemCols = 128;          // two 128 x 64 fp32 accumulators
 constexpr uint32_t kIdesc = make_idesc(0, 0, kTileM, 64);  // fp16, M128 N64
 
@@ -94,8 +95,12 @@ size_t smem_bytes_for(int nmax) {
   return 1024 + (size_t)kCOff + (size_t)ldc * 64 * 4 + sizeof(Misc) + 16;
 }
 
-// L_kk element (r, c), rows 32..63 skewed by four banks
-__device__ __forceinline__ int lidx(int r, int c) { return r + ((r >> 5) << 2) + c * kLDL; }
+__device__ __forceinline__ void load8(const float* p, float (&v)[8]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  const float4 b = *reinterpret_cast<const float4*>(p + 4);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
 
 // ---------------------------------------------------------------------------
 // Asynchronous copy of a rows x cols column-major block from global (ld gld)
@@ -126,57 +131,114 @@ __device__ __forceinline__ void async_block(const float* src, int64_t gld, int r
   cp_async_wait_all();
 }
 
+// Shared (ld sld) -> global (ld gld) copy of a rows x cols column-major block.
+__device__ __forceinline__ void store_block(float* dst, int64_t gld, int rows, int cols,
+                                            bool vec, const float* src, int sld) {
+  const int tid = threadIdx.x;
+  if (vec) {
+    const int r4 = rows >> 2;
+    for (int idx = tid; idx < r4 * cols; idx += kT) {
+      const int c = idx / r4, r = 4 * (idx - c * r4);
+      *reinterpret_cast<float4*>(dst + r + (int64_t)c * gld) =
+          *reinterpret_cast<const float4*>(src + r + c * sld);
+    }
+    const int rt = rows & 3;
+    for (int idx = tid; idx < rt * cols; idx += kT) {
+      const int c = idx / rt, r = 4 * r4 + (idx - c * rt);
+      dst[r + (int64_t)c * gld] = src[r + c * sld];
+    }
+  } else {
+    for (int idx = tid; idx < rows * cols; idx += kT) {
+      const int c = idx / rows, r = idx - c * rows;
+      dst[r + (int64_t)c * gld] = src[r + c * sld];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
-// U_kj = L_kk^-1 A_kj for rows [r0, r0 + NB) of the block column (wj
-// columns), in 8-row chunks: forward substitution inside the chunk, then a
-// rank-8 update of the later chunks.  Thread (column c, chunk s) holds the 8
-// values of its chunk; the chunk being substituted is passed on by shuffles
-// among the 8 lanes of its column.  Also writes the B operand.
-__device__ __forceinline__ void trsm_block(float* C, int ldc, const float* Lkk,
-                                           int r0, int NB, int wj, bool tc,
-                                           uint8_t* sB) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int s = lane & 7;
+// U_kj = L_kk^-1 A_kj for rows [r0, r0 + NB) of the block column (wj <= 64
+// columns), in 8-row chunks: forward substitution inside chunk q, then a
+// rank-8 update of the later chunks.  Warp s owns chunk s (8 rows) of
+// columns lane and lane + 32, so every L_kk read is a warp-wide broadcast;
+// the substituted chunk is handed to the other warps through shared memory
+// (double-buffered, one CTA barrier per chunk).  Also writes the B operand.
+// Lt: L_kk row-major (row stride kLDT).
+__device__ __forceinline__ void trsm_block(float* C, int ldc, const float* Lt,
+                                           float* ustage, int r0, int NB, int wj,
+                                           bool tc, uint8_t* sB) {
+  const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nch = NB >> 3;
-  const unsigned full = 0xffffffffu;
+  const bool mine = s < nch;
+  const bool a0 = mine && lane < wj, a1 = mine && lane + 32 < wj;
+  float v0[8], v1[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    v0[i] = a0 ? C[(r0 + 8 * s + i) + lane * ldc] : 0.0f;
+    v1[i] = a1 ? C[(r0 + 8 * s + i) + (lane + 32) * ldc] : 0.0f;
+  }
 #pragma unroll 1
-  for (int pass = 0; pass < 2; ++pass) {
-    const int c = warp * 4 + (lane >> 3) + 32 * pass;  // 0..63
-    const bool active = (c < wj) && (s < nch);
-    float v[8];
+  for (int q = 0; q < nch; ++q) {
+    float* us = ustage + (q & 1) * 512;
+    if (s == q) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = active ? C[(r0 + 8 * s + i) + c * ldc] : 0.0f;
-#pragma unroll 1
-    for (int q = 0; q < nch; ++q) {
-      if (active && s == q) {
+      for (int i = 1; i < 8; ++i) {
+        float l[8];
+        load8(Lt + (8 * q + i) * kLDT + 8 * q, l);
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk)
-#pragma unroll
-          for (int i = kk + 1; i < 8; ++i)
-            v[i] = __fmaf_rn(-Lkk[lidx(8 * q + i, 8 * q + kk)], v[kk], v[i]);
+        for (int kk = 0; kk < 8; ++kk) {
+          if (kk < i) {
+            v0[i] = __fmaf_rn(-l[kk], v0[kk], v0[i]);
+            v1[i] = __fmaf_rn(-l[kk], v1[kk], v1[i]);
+          }
+        }
       }
-      float u[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) u[i] = __shfl_sync(full, v[i], (lane & ~7) + q);
-      if (active && s > q) {
+      if (q + 1 < nch) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          float acc = 0.0f;
-#pragma unroll
-          for (int kk = 0; kk < 8; ++kk)
-            acc = __fmaf_rn(Lkk[lidx(8 * s + i, 8 * q + kk)], u[kk], acc);
-          v[i] = __fsub_rn(v[i], acc);
+          us[i * 64 + lane] = v0[i];
+          us[i * 64 + lane + 32] = v1[i];
         }
       }
     }
-    if (active) {
+    if (q + 1 == nch) break;
+    __syncthreads();
+    if (mine && s > q) {
+      float u0[8], u1[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) C[(r0 + 8 * s + i) + c * ldc] = v[i];
+      for (int kk = 0; kk < 8; ++kk) {
+        u0[kk] = us[kk * 64 + lane];
+        u1[kk] = us[kk * 64 + lane + 32];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        float l[8];
+        load8(Lt + (8 * s + i) * kLDT + 8 * q, l);
+        float acc0 = 0.0f, acc1 = 0.0f;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+          acc0 = __fmaf_rn(l[kk], u0[kk], acc0);
+          acc1 = __fmaf_rn(l[kk], u1[kk], acc1);
+        }
+        v0[i] = __fsub_rn(v0[i], acc0);
+        v1[i] = __fsub_rn(v1[i], acc1);
+      }
     }
-    if (tc) {
-      // B row c (N index), 16-byte chunk s (K = 8s .. 8s+7), 128-byte swizzle
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (a0) C[(r0 + 8 * s + i) + lane * ldc] = v0[i];
+    if (a1) C[(r0 + 8 * s + i) + (lane + 32) * ldc] = v1[i];
+  }
+  if (tc) {
+    // B row c (N index), 16-byte chunk s (K = 8s .. 8s+7), 128-byte swizzle
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      const bool act = h ? a1 : a0;
+      const float* v = h ? v1 : v0;
+      if (!mine) continue;
       uint4 pk = make_uint4(0, 0, 0, 0);
-      if (active) {
+      if (act) {
         __half2 h0 = __floats2half2_rn(v[0], v[1]);
         __half2 h1 = __floats2half2_rn(v[2], v[3]);
         __half2 h2 = __floats2half2_rn(v[4], v[5]);
@@ -187,128 +249,193 @@ __device__ __forceinline__ void trsm_block(float* C, int ldc, const float* Lkk,
         pk.w = *reinterpret_cast<uint32_t*>(&h3);
       }
       *reinterpret_cast<uint4*>(sB + c * 128 + ((s ^ (c & 7)) << 4)) = pk;
-    } else if (s < nch) {
-      float* Bf = reinterpret_cast<float*>(sB);  // U row-major [kk][64]
+    }
+  } else if (mine) {
+    float* Bf = reinterpret_cast<float*>(sB);  // U row-major [kk][64]
 #pragma unroll
-      for (int i = 0; i < 8; ++i) Bf[(8 * s + i) * 64 + c] = active ? v[i] : 0.0f;
+    for (int i = 0; i < 8; ++i) {
+      Bf[(8 * s + i) * 64 + lane] = a0 ? v0[i] : 0.0f;
+      Bf[(8 * s + i) * 64 + lane + 32] = a1 ? v1[i] : 0.0f;
     }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Inner elimination of the panel: rows [c0, n) of the block column, wj
-// columns (global column offset c0).
-__device__ __forceinline__ void panel_block(float* C, int ldc, int n, int c0,
-                                            int wj, Misc* ms) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int M = n - c0;
-  const unsigned full = 0xffffffffu;
-  const int nt = (wj + 7) >> 3;
-#pragma unroll 1
-  for (int t = 0; t < nt; ++t) {
-    const int t0 = 8 * t;
-    const int tw = min(8, wj - t0);
-    float* inv = ms->inv[t & 1];
-    if (warp == ((t0 >> 5) % kWarps)) {
-      // tile rows t0 .. t0+7 sit in lanes lb .. lb+7 of this warp
-      const int lb = t0 & 31;
-      const int rr = lane - lb;
-      const bool in_tile = rr >= 0 && rr < tw;
-      float* rowp = C + (c0 + t0 + rr);
-      float v[8];
+// columns (global column offset c0).  Row p (panel-local) belongs to thread
+// p mod 256.
+
+// Owner warp of tile t: one lane factors the 8x8 tile in registers (no
+// shuffles on the dependency chain), then the U strip (rows t0..t0+7,
+// columns t0+8 .. wj-1, one column per lane).
+__device__ __forceinline__ void tile_factor(float* C, int ldc, int c0, int t0,
+                                            int wj, float* inv, int* bad) {
+  const int lane = threadIdx.x & 31;
+  const int tw = min(8, wj - t0);
+  float* T = C + (c0 + t0);
+  if (lane == (t0 & 31)) {
+    float v[8][8];  // v[c][r]: tile column c
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] = (in_tile && c < tw) ? rowp[(t0 + c) * ldc] : 0.0f;
+    for (int c = 0; c < 8; ++c) {
+      if (c < tw) {
+        load8(T + (t0 + c) * ldc, v[c]);
+      } else {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (k < tw) {
-          const float d = __shfl_sync(full, v[k], lb + k);
-          const float iv = __frcp_rn(d);  // correctly rounded 1/d
-          if (lane == lb) {
-            inv[k] = iv;
-            note_pivot(d, c0 + t0 + k, &ms->bad);
-          }
-          if (in_tile && rr > k) v[k] = __fmul_rn(v[k], iv);
-#pragma unroll
-          for (int c = k + 1; c < 8; ++c) {
-            const float ukc = __shfl_sync(full, v[c], lb + k);
-            if (c < tw && in_tile && rr > k) v[c] = __fmaf_rn(-v[k], ukc, v[c]);
-          }
-        }
-      }
-      if (in_tile) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < tw) rowp[(t0 + c) * ldc] = v[c];
-      }
-      __syncwarp();
-      // U strip: rows t0..t0+7, columns t0+8 .. wj-1 (tw == 8 whenever any exist)
-      for (int c = t0 + 8 + lane; c < wj; c += 32) {
-        float* colp = C + (c0 + t0) + c * ldc;
-        float col[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) col[r] = colp[r];
-#pragma unroll
-        for (int kk = 0; kk < 8; ++kk)
-#pragma unroll
-          for (int r = kk + 1; r < 8; ++r)
-            col[r] = __fmaf_rn(-C[(c0 + t0 + r) + (t0 + kk) * ldc], col[kk], col[r]);
-#pragma unroll
-        for (int r = 0; r < 8; ++r) colp[r] = col[r];
+        for (int r = 0; r < 8; ++r) v[c][r] = 0.0f;
       }
     }
-    __syncthreads();
-    // rows below the tile: L elimination and rank-8 update of this thread's rows
-    if (tw == 8) {
-      const float* T = C + (c0 + t0);  // tile / U strip rows, column stride ldc
-      for (int p = tid; p < M; p += kT) {
-        if (p < t0 + 8) continue;
-        float* rowp = C + (c0 + p);
-        float rv[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) rv[c] = rowp[(t0 + c) * ldc];
+    for (int k = 0; k < 8; ++k) {
+      if (k < tw) {
+        const float d = v[k][k];
+        note_pivot(d, c0 + t0 + k, bad);
+        const float iv = __frcp_rn(d);  // correctly rounded 1/d
+        inv[k] = iv;
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-          rv[kk] = __fmul_rn(rv[kk], inv[kk]);
+        for (int r = k + 1; r < 8; ++r) v[k][r] = __fmul_rn(v[k][r], iv);
 #pragma unroll
-          for (int c = kk + 1; c < 8; ++c)
-            rv[c] = __fmaf_rn(-rv[kk], T[kk + (t0 + c) * ldc], rv[c]);
-        }
+        for (int c = k + 1; c < 8; ++c)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) rowp[(t0 + c) * ldc] = rv[c];
-#pragma unroll 2
-        for (int c = t0 + 8; c < wj; ++c) {
-          const float* uc = T + c * ldc;
-          float acc = 0.0f;
-#pragma unroll
-          for (int kk = 0; kk < 8; ++kk) acc = __fmaf_rn(rv[kk], uc[kk], acc);
-          rowp[c * ldc] = __fsub_rn(rowp[c * ldc], acc);
-        }
+          for (int r = k + 1; r < 8; ++r) v[c][r] = __fmaf_rn(-v[k][r], v[c][k], v[c][r]);
       }
-    } else {
-      // last, partial tile of the matrix: rows below exist only up to n
-      const float* T = C + (c0 + t0);
-      for (int p = tid; p < M; p += kT) {
-        if (p < t0 + 8) continue;
-        float* rowp = C + (c0 + p);
-        float rv[8];
+    }
+    // rows r >= tw of a partial tile lie below the matrix: never stored
 #pragma unroll
-        for (int c = 0; c < 8; ++c) rv[c] = c < tw ? rowp[(t0 + c) * ldc] : 0.0f;
+    for (int c = 0; c < 8; ++c) {
+      if (c < tw) {
+        if (tw == 8) {
+          *reinterpret_cast<float4*>(T + (t0 + c) * ldc) =
+              make_float4(v[c][0], v[c][1], v[c][2], v[c][3]);
+          *reinterpret_cast<float4*>(T + (t0 + c) * ldc + 4) =
+              make_float4(v[c][4], v[c][5], v[c][6], v[c][7]);
+        } else {
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-          if (kk < tw) {
-            rv[kk] = __fmul_rn(rv[kk], inv[kk]);
-#pragma unroll
-            for (int c = kk + 1; c < 8; ++c)
-              if (c < tw) rv[c] = __fmaf_rn(-rv[kk], T[kk + (t0 + c) * ldc], rv[c]);
-          }
+          for (int r = 0; r < 8; ++r)
+            if (r < tw) T[r + (t0 + c) * ldc] = v[c][r];
         }
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < tw) rowp[(t0 + c) * ldc] = rv[c];
       }
     }
   }
+  __syncwarp();
+  for (int c = t0 + 8 + lane; c < wj; c += 32) {
+    float col[8];
+    load8(T + c * ldc, col);
+#pragma unroll
+    for (int kk = 0; kk < 7; ++kk) {
+      float l[8];
+      load8(T + (t0 + kk) * ldc, l);  // tile column kk: l[r] = L[r][kk]
+#pragma unroll
+      for (int r = kk + 1; r < 8; ++r) col[r] = __fmaf_rn(-l[r], col[kk], col[r]);
+    }
+    *reinterpret_cast<float4*>(T + c * ldc) = make_float4(col[0], col[1], col[2], col[3]);
+    *reinterpret_cast<float4*>(T + c * ldc + 4) = make_float4(col[4], col[5], col[6], col[7]);
+  }
+}
+
+// Rows pa (and pb when TWO) below tile t (tw == 8): L elimination with the
+// tile's U part and 1/d, then the rank-8 update of columns t0+8 .. wj-1.  Two
+// rows share every shared-memory read of the tile and the U strip.
+template <bool TWO>
+__device__ __forceinline__ void row_update(float* C, int ldc, int c0, int t0, int wj,
+                                           int pa, int pb, const float* inv) {
+  float* ra_p = C + (c0 + pa);
+  float* rb_p = C + (c0 + pb);
+  const float* T = C + (c0 + t0);
+  float ra[8], rb[8], iv[8];
+  load8(inv, iv);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    ra[c] = ra_p[(t0 + c) * ldc];
+    rb[c] = TWO ? rb_p[(t0 + c) * ldc] : 0.0f;
+  }
+  // element c: fused updates with k = 0 .. c-1, then the 1/d multiply
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    float u[8];
+    load8(T + (t0 + c) * ldc, u);  // u[k] = U[k][c]
+#pragma unroll
+    for (int k = 0; k < c; ++k) {
+      ra[c] = __fmaf_rn(-ra[k], u[k], ra[c]);
+      if (TWO) rb[c] = __fmaf_rn(-rb[k], u[k], rb[c]);
+    }
+    ra[c] = __fmul_rn(ra[c], iv[c]);
+    if (TWO) rb[c] = __fmul_rn(rb[c], iv[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    ra_p[(t0 + c) * ldc] = ra[c];
+    if (TWO) rb_p[(t0 + c) * ldc] = rb[c];
+  }
+  int c = t0 + 8;
+#pragma unroll 1
+  for (; c + 4 <= wj; c += 4) {
+    float u[4][8], acca[4], accb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      load8(T + (c + j) * ldc, u[j]);
+      acca[j] = 0.0f;
+      accb[j] = 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acca[j] = __fmaf_rn(ra[k], u[j][k], acca[j]);
+        if (TWO) accb[j] = __fmaf_rn(rb[k], u[j][k], accb[j]);
+      }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      ra_p[(c + j) * ldc] = __fsub_rn(ra_p[(c + j) * ldc], acca[j]);
+      if (TWO) rb_p[(c + j) * ldc] = __fsub_rn(rb_p[(c + j) * ldc], accb[j]);
+    }
+  }
+  for (; c < wj; ++c) {
+    float u[8];
+    load8(T + c * ldc, u);
+    float acca = 0.0f, accb = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      acca = __fmaf_rn(ra[k], u[k], acca);
+      if (TWO) accb = __fmaf_rn(rb[k], u[k], accb);
+    }
+    ra_p[c * ldc] = __fsub_rn(ra_p[c * ldc], acca);
+    if (TWO) rb_p[c * ldc] = __fsub_rn(rb_p[c * ldc], accb);
+  }
+}
+
+// Rows of the panel are dealt to threads: row p < 256 to thread p, and row
+// 256 + j to thread 255 - j, so the warps that own the diagonal tiles (rows
+// below 64) take second rows last.
+__device__ __forceinline__ void panel_block(float* C, int ldc, int n, int c0,
+                                            int wj, Misc* ms) {
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int M = n - c0;
+  const int nt = (wj + 7) >> 3;
+  const int pa = tid, pb = kT + (kT - 1 - tid);
+  if (warp == 0) tile_factor(C, ldc, c0, 0, wj, ms->inv[0], &ms->bad);
   __syncthreads();
+#pragma unroll 1
+  for (int t = 0; t < nt; ++t) {
+    const int t0 = 8 * t;
+    const float* inv = ms->inv[t & 1];
+    // rows exist below tile t only when it is a full tile
+    const bool ha = pa >= t0 + 8 && pa < M;
+    const bool hb = pb < M;  // pb >= 256 > t0 + 8
+    const bool lookahead = t + 1 < nt && warp == (((t0 + 8) >> 5) % kWarps);
+    if (lookahead) {
+      // this warp owns tile t+1: update its first rows (which include the
+      // tile's) and factor the tile while the other warps finish chunk t
+      if (ha) row_update<false>(C, ldc, c0, t0, wj, pa, pa, inv);
+      tile_factor(C, ldc, c0, t0 + 8, wj, ms->inv[(t + 1) & 1], &ms->bad);
+      if (hb) row_update<false>(C, ldc, c0, t0, wj, pb, pb, inv);
+    } else if (ha && hb) {
+      row_update<true>(C, ldc, c0, t0, wj, pa, pb, inv);
+    } else if (ha || hb) {
+      const int p = ha ? pa : pb;
+      row_update<false>(C, ldc, c0, t0, wj, p, p, inv);
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -473,6 +600,7 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
   uint8_t* sA = sm + kAOff;
   uint8_t* sB = sm + kBOff;
   float* Lkk = reinterpret_cast<float*>(sm + kLOff);
+  float* ustage = reinterpret_cast<float*>(sm + kUOff);
   float* C = reinterpret_cast<float*>(sm + kCOff);
   Misc* ms = reinterpret_cast<Misc*>(sm + kCOff + (size_t)a.ldc * 64 * 4);
   const int tid = threadIdx.x;
@@ -520,10 +648,10 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
 #pragma unroll 1
       for (int k = 0; k < j; ++k) {
         const int r0 = k * NB;
-        async_block(A + r0 + (int64_t)r0 * lda, lda, NB, NB, vec,
-                    [&](int r, int c) { return &Lkk[lidx(r, c)]; });
+        async_block(A + r0 + (int64_t)r0 * lda, lda, NB, NB, false,
+                    [&](int r, int c) { return &Lkk[r * kLDT + c]; });
         __syncthreads();
-        trsm_block(C, ldc, Lkk, r0, NB, wj, tc, sB);
+        trsm_block(C, ldc, Lkk, ustage, r0, NB, wj, tc, sB);
         if (tc) fence_proxy_async_smem();
         __syncthreads();
         if (r0 + NB < n) {
@@ -534,10 +662,7 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
       }
       if (ms->abort) break;
       panel_block(C, ldc, n, c0, wj, ms);
-      for (int idx = tid; idx < n * wj; idx += kT) {
-        const int r = idx % n, c = idx / n;
-        A[r + (int64_t)(c0 + c) * lda] = C[r + c * ldc];
-      }
+      store_block(A + (int64_t)c0 * lda, lda, n, wj, vec, C, ldc);
       __syncthreads();
     }
     if (tid == 0)

@@ -25,7 +25,7 @@ _i64 = ctypes.c_int64
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
 
-FMT_FP32, FMT_FP16, FMT_BF16, FMT_E4M3 = 0, 1, 2, 3
+FMT_FP32, FMT_FP16, FMT_BF16, FMT_E4M3, FMT_SPLIT = 0, 1, 2, 3, 4
 
 
 def build(force: bool = False) -> None:

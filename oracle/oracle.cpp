@@ -311,6 +311,30 @@ void round_copy(int64_t rows, int64_t cols, const float* a, int64_t lda,
   }
 }
 
+// Split fp16 copies (hi and lo parts) with per-tile scales bound 32768.
+void split_copy(int64_t rows, int64_t cols, const float* a, int64_t lda, float* hi,
+                float* lo, int64_t ldo, bool by_rows, int64_t tile,
+                std::vector<int>& scales) {
+  const int64_t ntile = ((by_rows ? rows : cols) + tile - 1) / tile;
+  scales.assign(ntile, 0);
+  for (int64_t t = 0; t < ntile; ++t) {
+    int64_t r0 = by_rows ? t * tile : 0, r1 = by_rows ? std::min(rows, r0 + tile) : rows;
+    int64_t c0 = by_rows ? 0 : t * tile, c1 = by_rows ? cols : std::min(cols, c0 + tile);
+    float amax = 0.0f;
+    for (int64_t j = c0; j < c1; ++j)
+      for (int64_t i = r0; i < r1; ++i) amax = std::max(amax, std::fabs(at(a, lda, i, j)));
+    const int s = pow2_scale(amax, 32768.0);
+    scales[t] = s;
+    for (int64_t j = c0; j < c1; ++j)
+      for (int64_t i = r0; i < r1; ++i) {
+        const float x = std::ldexp(at(a, lda, i, j), s);
+        const float h = round_fmt(x, 1);
+        hi[i + j * ldo] = h;
+        lo[i + j * ldo] = round_fmt(x - h, 1);
+      }
+  }
+}
+
 }  // namespace
 
 // reference src/lu_nopiv.hxx:130-197
@@ -339,6 +363,34 @@ void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
     if (outer_fmt == 0) {
       orc_gemm_sub_f32(tm, tn, nb, a + ofst + ofs * lda, lda,
                        a + ofs + ofst * lda, lda, a + ofst + ofst * lda, lda);
+    } else if (outer_fmt == 4) {
+      // Split fp16 (new; no reference counterpart): per 128-row tile of L21
+      // / 128-column tile of U12 a power-of-two scale bringing the tile max
+      // under 32768, x * 2^s = hi + lo with hi = rn16(x * 2^s) and lo =
+      // rn16(x * 2^s - hi); the product is taken over the concatenated K
+      // segments [hi|hi|lo] x [hi;lo;hi] (all hi*hi terms, then hi*lo, then
+      // lo*hi) accumulated in fp32, then the two scales are removed.
+      const int64_t T = 128;
+      std::vector<float> lh((size_t)tm * nb), ll((size_t)tm * nb);
+      std::vector<float> uh((size_t)nb * tn), ul((size_t)nb * tn);
+      split_copy(tm, nb, a + ofst + ofs * lda, lda, lh.data(), ll.data(), tm, true, T, ls);
+      split_copy(nb, tn, a + ofs + ofst * lda, lda, uh.data(), ul.data(), nb, false, T, us);
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int64_t j = 0; j < tn; ++j) {
+        std::vector<float> acc(tm, 0.0f);
+        const float* seg_a[3] = {lh.data(), lh.data(), ll.data()};
+        const float* seg_b[3] = {uh.data(), ul.data(), uh.data()};
+        for (int sg = 0; sg < 3; ++sg)
+          for (int64_t t = 0; t < nb; ++t) {
+            const float bt = seg_b[sg][t + j * nb];
+            const float* ap = seg_a[sg] + t * tm;
+            for (int64_t i = 0; i < tm; ++i) acc[i] = std::fma(ap[i], bt, acc[i]);
+          }
+        const int su = us[j / T];
+        float* cp = a + ofst + (ofst + j) * lda;
+        for (int64_t i = 0; i < tm; ++i)
+          cp[i] = cp[i] - std::ldexp(acc[i], -(ls[i / T] + su));
+      }
     } else {
       // TC32 with W = fp32 (src/lu_nopiv.hxx:155-183): the update multiplies
       // low-precision copies of L21 and U12 with fp32 accumulation.  For e4m3

@@ -71,6 +71,8 @@ void orc_gemm_sub_f32(int64_t m, int64_t n, int64_t k, const float* a,
  *   outer_fmt 0: the outer Schur update in fp32 (I = O = FP32);
  *   outer_fmt 1/2/3: the outer update multiplies copies of L21 and U12
  *     rounded to fp16/bf16/e4m3 (TC32 with W = fp32), fp32 accumulation.
+ *   outer_fmt 4: split fp16 (new, no reference counterpart): scaled copies
+ *     x * 2^s = hi + lo, product hi*hi + hi*lo + lo*hi in fp32.
  *   threads <= 0 uses all OpenMP threads; the result does not depend on the
  *   thread count. */
 void orc_lu_rl_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,

@@ -40,13 +40,14 @@ lu_status check_device() {
 
 static bool is_tc(lu_compute c) {
   return c == LU_COMPUTE_TC32 || c == LU_COMPUTE_TC32_BF16 ||
-         c == LU_COMPUTE_TC32_E4M3;
+         c == LU_COMPUTE_TC32_E4M3 || c == LU_COMPUTE_TC32_SPLIT;
 }
 
 static TcOperand tc_kind(lu_compute c) {
   return c == LU_COMPUTE_TC32_BF16 ? TcOperand::BF16
        : c == LU_COMPUTE_TC32_E4M3 ? TcOperand::E4M3
-                                   : TcOperand::F16;
+       : c == LU_COMPUTE_TC32_SPLIT ? TcOperand::SPLIT16
+                                    : TcOperand::F16;
 }
 
 // Workspace for the low-precision operand copies of an M x K by K x N
@@ -60,7 +61,7 @@ static TcWs tc_ws_layout(size_t base, int64_t M, int64_t N, int64_t K,
                          TcOperand kind) {
   TcWs w;
   const size_t es = (size_t)tc_operand_bytes(kind);
-  const int64_t ldk = (K + 15) / 16 * 16;
+  const int64_t ldk = tc_packed_k(kind, K);
   size_t off = align_up(base, 1024);
   w.off_a = off;  off = align_up(off + (size_t)M * ldk * es, 1024);
   w.off_b = off;  off = align_up(off + (size_t)N * ldk * es, 1024);
@@ -78,17 +79,17 @@ static TcWs tc_ws_layout(size_t base, int64_t M, int64_t N, int64_t K,
 static lu_status tc_pack(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                          int64_t K, const float* a, int64_t lda, const float* b,
                          int64_t ldb, char* ws, const TcWs& w) {
-  const int64_t ldk = (K + 15) / 16 * 16;
+  const int64_t ldk = tc_packed_k(kind, K);
   int* sa = nullptr;
   int* sb = nullptr;
   ProfScope ps("pack_operands", st,
-               (double)(M + N) * K * (4.0 + tc_operand_bytes(kind)));
-  if (kind == TcOperand::E4M3) {
+               (double)(M + N) * (4.0 * K + (double)tc_operand_bytes(kind) * ldk));
+  if (tc_scaled(kind)) {
     sa = reinterpret_cast<int*>(ws + w.off_sa);
     sb = reinterpret_cast<int*>(ws + w.off_sb);
     int* tmp = reinterpret_cast<int*>(ws + w.off_tmp);
-    LUB_TRY(launch_scale_rowtiles(st, M, K, a, lda, sa, tmp));
-    LUB_TRY(launch_scale_coltiles(st, K, N, b, ldb, sb, tmp));
+    LUB_TRY(launch_scale_rowtiles(st, M, K, a, lda, sa, tmp, tc_scale_bound(kind)));
+    LUB_TRY(launch_scale_coltiles(st, K, N, b, ldb, sb, tmp, tc_scale_bound(kind)));
   }
   LUB_TRY(launch_pack_a(st, kind, M, K, a, lda, ws + w.off_a, ldk, sa));
   LUB_TRY(launch_pack_b(st, kind, K, N, b, ldb, ws + w.off_b, ldk, sb));
@@ -103,19 +104,21 @@ static lu_status tc_apply(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                           int64_t ldc, char* ws, const TcWs& w, int* err,
                           int tiles_per_cta) {
   if (M <= 0 || N <= 0) return LU_SUCCESS;
-  const int64_t ldk = (K + 15) / 16 * 16;
+  const int64_t ldk = tc_packed_k(kind, K);
   const int64_t es = tc_operand_bytes(kind);
   const int* sa = nullptr;
   const int* sb = nullptr;
-  if (kind == TcOperand::E4M3) {
+  if (tc_scaled(kind)) {
     if (r0 % 128 != 0 || c0 % 128 != 0) return LU_ERR_INVALID_ARG;
     sa = reinterpret_cast<const int*>(ws + w.off_sa) + r0 / 128;
     sb = reinterpret_cast<const int*>(ws + w.off_sb) + c0 / 128;
   }
+  // the split product runs over the three concatenated K segments
+  const int64_t kk = kind == TcOperand::SPLIT16 ? ldk : K;
   // algorithmic bytes: C read + written once (fp32), both operands read once
-  ProfScope ps("tc_update", st, 8.0 * M * N + (double)es * (M + N) * K,
-               2.0 * M * N * K);
-  return launch_tc_update(st, kind, M, N, K, -1.0f, ws + w.off_a + r0 * ldk * es,
+  ProfScope ps("tc_update", st, 8.0 * M * N + (double)es * (M + N) * kk,
+               2.0 * M * N * kk);
+  return launch_tc_update(st, kind, M, N, kk, -1.0f, ws + w.off_a + r0 * ldk * es,
                           ldk, ws + w.off_b + c0 * ldk * es, ldk, c, ldc, sa, sb,
                           err, 0, tiles_per_cta);
 }
@@ -128,11 +131,11 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
                                 const TcWs& w, int* err) {
   LUB_TRY(tc_pack(st, kind, M, N, K, a, lda, b, ldb, ws, w));
   if (alpha == -1.0f) return tc_apply(st, kind, M, N, K, 0, 0, c, ldc, ws, w, err, 0);
-  const int64_t ldk = (K + 15) / 16 * 16;
-  const int* sa = kind == TcOperand::E4M3 ? reinterpret_cast<const int*>(ws + w.off_sa) : nullptr;
-  const int* sb = kind == TcOperand::E4M3 ? reinterpret_cast<const int*>(ws + w.off_sb) : nullptr;
-  return launch_tc_update(st, kind, M, N, K, alpha, ws + w.off_a, ldk,
-                          ws + w.off_b, ldk, c, ldc, sa, sb, err);
+  const int64_t ldk = tc_packed_k(kind, K);
+  const int* sa = tc_scaled(kind) ? reinterpret_cast<const int*>(ws + w.off_sa) : nullptr;
+  const int* sb = tc_scaled(kind) ? reinterpret_cast<const int*>(ws + w.off_sb) : nullptr;
+  return launch_tc_update(st, kind, M, N, kind == TcOperand::SPLIT16 ? ldk : K, alpha,
+                          ws + w.off_a, ldk, ws + w.off_b, ldk, c, ldc, sa, sb, err);
 }
 
 // Internal streams of one device: panel work runs at the highest priority,
@@ -182,7 +185,8 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     // one diagonal kernel covers the outer block; e4m3 tile scales would
     // have to follow the growing K range of the left-looking products
     if (o.nb > 128) return LU_ERR_UNSUPPORTED;
-    if (o.outer_update == LU_COMPUTE_TC32_E4M3) return LU_ERR_UNSUPPORTED;
+    if (o.outer_update == LU_COMPUTE_TC32_E4M3 || o.outer_update == LU_COMPUTE_TC32_SPLIT)
+      return LU_ERR_UNSUPPORTED;
   }
   p->n = n;
   p->nb = o.nb;
@@ -295,7 +299,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     w[1].off_sb += shift; w[1].off_tmp += shift;
   }
   const bool la = p.lookahead && n > 2 * nb &&
-                  !(tc_kind(p.outer) == TcOperand::E4M3 && tc && nb % 128 != 0);
+                  !(tc && tc_scaled(tc_kind(p.outer)) && nb % 128 != 0);
   if (!la) {
     for (int64_t ofs = 0; ofs < n; ofs += nb) {
       const int64_t in = std::min(n - ofs, nb);

@@ -355,9 +355,10 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
       (uintptr_t)A % 16 != 0 || (uintptr_t)B % 16 != 0)
     return LU_ERR_INVALID_ARG;
   if (lda_p < K || ldb_p < K) return LU_ERR_INVALID_ARG;
-  CUtensorMapDataType dt = kind == TcOperand::F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                         : kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                   : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  // split copies are plain fp16 operands with a tripled K
+  CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                         : kind == TcOperand::E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   CUtensorMap ma, mb;
   if (!make_kmajor_map(&ma, A, dt, esize, K, M, lda_p, BM)) return LU_ERR_CUDA;
   if (!make_kmajor_map(&mb, B, dt, esize, K, N, ldb_p, BN)) return LU_ERR_CUDA;

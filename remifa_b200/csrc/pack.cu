@@ -6,7 +6,9 @@
 // here the L21 panel is transposed while it is converted (row-major copy)
 // and the U12 panel keeps its column-major layout with a compact leading
 // dimension.  e4m3 copies carry one power-of-two scale per 128-row /
-// 128-column tile, the largest that keeps the tile's max |x| <= 448.
+// 128-column tile, the largest that keeps the tile's max |x| <= 448; split
+// fp16 copies (hi + lo) the same with bound 32768, which keeps the lo parts
+// of all but the tile's tiniest entries normal fp16 numbers.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tc_gemm.cuh"
@@ -47,6 +49,59 @@ pack_a_kernel(int64_t M, int64_t K, const float* __restrict__ src, int64_t lds,
       if (scale) x = ldexpf(x, scale[gi / 128]);
       dst[gi * ldd + gk] = to_low<T>(x);
     }
+  }
+}
+
+// Split fp16: x = hi + lo with hi = rn(x), lo = rn(x - hi) (x - hi exact).
+__device__ __forceinline__ void split16(float x, __half& hi, __half& lo) {
+  hi = __float2half_rn(x);
+  lo = __float2half_rn(__fsub_rn(x, __half2float(hi)));
+}
+
+// A: row i = [hi | hi | lo], segment stride kp, zeros in [K, kp).
+__global__ void __launch_bounds__(256)
+pack_a_split_kernel(int64_t M, int64_t K, int64_t kp, const float* __restrict__ src,
+                    int64_t lds, __half* __restrict__ dst, int64_t ldd,
+                    const int* __restrict__ scale) {
+  __shared__ float tile[TA][TA + 1];  // [k][i]
+  const int64_t i0 = (int64_t)blockIdx.x * TA;
+  const int64_t k0 = (int64_t)blockIdx.y * TA;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < TA * TA; q += 256) {
+    const int i = q % TA, k = q / TA;
+    const int64_t gi = i0 + i, gk = k0 + k;
+    tile[k][i] = (gi < M && gk < K) ? src[gi + gk * lds] : 0.0f;
+  }
+  __syncthreads();
+  for (int q = tid; q < TA * TA; q += 256) {
+    const int k = q % TA, i = q / TA;
+    const int64_t gi = i0 + i, gk = k0 + k;
+    if (gi < M && gk < kp) {
+      __half hi, lo;
+      split16(ldexpf(tile[k][i], scale[gi / 128]), hi, lo);
+      __half* row = dst + gi * ldd;
+      row[gk] = hi;
+      row[kp + gk] = hi;
+      row[2 * kp + gk] = lo;
+    }
+  }
+}
+
+// B: column j = [hi ; lo ; hi], segment stride kp, zeros in [K, kp).
+__global__ void __launch_bounds__(256)
+pack_b_split_kernel(int64_t K, int64_t kp, int64_t N, const float* __restrict__ src,
+                    int64_t lds, __half* __restrict__ dst, int64_t ldd,
+                    const int* __restrict__ scale) {
+  const int64_t k = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (k >= kp) return;
+  for (int64_t j = blockIdx.y; j < N; j += gridDim.y) {
+    const float x = k < K ? ldexpf(src[k + j * lds], scale[j / 128]) : 0.0f;
+    __half hi, lo;
+    split16(x, hi, lo);
+    __half* col = dst + j * ldd;
+    col[k] = hi;
+    col[kp + k] = lo;
+    col[2 * kp + k] = hi;
   }
 }
 
@@ -102,20 +157,21 @@ amax_cols_kernel(int64_t K, int64_t N, const float* __restrict__ src,
   if (threadIdx.x == 0) atomicMax(&amax_bits[blockIdx.x], __float_as_int(red[0]));
 }
 
-// s = largest integer with amax * 2^s <= 448 (0 for an all-zero or
+// s = largest integer with amax * 2^s <= bound (0 for an all-zero or
 // non-finite tile).
 __global__ void amax_to_scale_kernel(int n, const int* __restrict__ amax_bits,
-                                     int* __restrict__ scale) {
+                                     int* __restrict__ scale, float bound) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float a = __int_as_float(amax_bits[t]);
   int s = 0;
   if (a > 0.0f && isfinite(a)) {
-    int e;
-    frexpf(a, &e);  // a in [2^(e-1), 2^e)
-    s = 8 - e;      // a * 2^(8-e) < 256 <= 448
-    while (ldexpf(a, s + 1) <= 448.0f) ++s;
-    while (ldexpf(a, s) > 448.0f) --s;
+    int e, eb;
+    frexpf(a, &e);      // a in [2^(e-1), 2^e)
+    frexpf(bound, &eb); // bound in [2^(eb-1), 2^eb)
+    s = eb - 1 - e;     // a * 2^s < 2^(eb-1) <= bound
+    while (ldexpf(a, s + 1) <= bound) ++s;
+    while (ldexpf(a, s) > bound) --s;
   }
   scale[t] = s;
 }
@@ -148,6 +204,14 @@ lu_status launch_pack_a(cudaStream_t st, TcOperand kind, int64_t M, int64_t K,
     case TcOperand::F16: return pack_a_typed<__half>(st, M, K, src, lds, dst, ldd, nullptr);
     case TcOperand::BF16: return pack_a_typed<__nv_bfloat16>(st, M, K, src, lds, dst, ldd, nullptr);
     case TcOperand::E4M3: return pack_a_typed<uint8_t>(st, M, K, src, lds, dst, ldd, scale);
+    case TcOperand::SPLIT16: {
+      const int64_t kp = (K + 15) / 16 * 16;
+      if (!scale || ldd < 3 * kp) return LU_ERR_INVALID_ARG;
+      dim3 grid((unsigned)ceil_div(M, TA), (unsigned)ceil_div(kp, TA));
+      pack_a_split_kernel<<<grid, 256, 0, st>>>(M, K, kp, src, lds, (__half*)dst, ldd, scale);
+      LUB_LAUNCH_CHECK();
+      return LU_SUCCESS;
+    }
   }
   return LU_ERR_INVALID_ARG;
 }
@@ -160,13 +224,21 @@ lu_status launch_pack_b(cudaStream_t st, TcOperand kind, int64_t K, int64_t N,
     case TcOperand::F16: return pack_b_typed<__half>(st, K, N, src, lds, dst, ldd, nullptr);
     case TcOperand::BF16: return pack_b_typed<__nv_bfloat16>(st, K, N, src, lds, dst, ldd, nullptr);
     case TcOperand::E4M3: return pack_b_typed<uint8_t>(st, K, N, src, lds, dst, ldd, scale);
+    case TcOperand::SPLIT16: {
+      const int64_t kp = (K + 15) / 16 * 16;
+      if (!scale || ldd < 3 * kp) return LU_ERR_INVALID_ARG;
+      dim3 grid((unsigned)ceil_div(kp, 256), (unsigned)std::min<int64_t>(N, 65535));
+      pack_b_split_kernel<<<grid, 256, 0, st>>>(K, kp, N, src, lds, (__half*)dst, ldd, scale);
+      LUB_LAUNCH_CHECK();
+      return LU_SUCCESS;
+    }
   }
   return LU_ERR_INVALID_ARG;
 }
 
 lu_status launch_scale_rowtiles(cudaStream_t st, int64_t M, int64_t K,
                                 const float* src, int64_t lds, int* scale,
-                                int* tmp) {
+                                int* tmp, float bound) {
   if (M <= 0) return LU_SUCCESS;
   const int64_t tiles = ceil_div(M, 128);
   LUB_CUDA_TRY(cudaMemsetAsync(tmp, 0, tiles * sizeof(int), st));
@@ -175,14 +247,15 @@ lu_status launch_scale_rowtiles(cudaStream_t st, int64_t M, int64_t K,
     amax_rows_kernel<<<grid, 256, 0, st>>>(M, K, src, lds, tmp);
     LUB_LAUNCH_CHECK();
   }
-  amax_to_scale_kernel<<<(unsigned)ceil_div(tiles, 256), 256, 0, st>>>((int)tiles, tmp, scale);
+  amax_to_scale_kernel<<<(unsigned)ceil_div(tiles, 256), 256, 0, st>>>((int)tiles, tmp, scale,
+                                                                      bound);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }
 
 lu_status launch_scale_coltiles(cudaStream_t st, int64_t K, int64_t N,
                                 const float* src, int64_t lds, int* scale,
-                                int* tmp) {
+                                int* tmp, float bound) {
   if (N <= 0) return LU_SUCCESS;
   const int64_t tiles = ceil_div(N, 128);
   LUB_CUDA_TRY(cudaMemsetAsync(tmp, 0, tiles * sizeof(int), st));
@@ -191,7 +264,8 @@ lu_status launch_scale_coltiles(cudaStream_t st, int64_t K, int64_t N,
     amax_cols_kernel<<<grid, 256, 0, st>>>(K, N, src, lds, tmp);
     LUB_LAUNCH_CHECK();
   }
-  amax_to_scale_kernel<<<(unsigned)ceil_div(tiles, 256), 256, 0, st>>>((int)tiles, tmp, scale);
+  amax_to_scale_kernel<<<(unsigned)ceil_div(tiles, 256), 256, 0, st>>>((int)tiles, tmp, scale,
+                                                                      bound);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

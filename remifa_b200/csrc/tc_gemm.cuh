@@ -5,9 +5,23 @@
 
 namespace lub {
 
-enum class TcOperand { F16 = 0, BF16 = 1, E4M3 = 2 };
+// SPLIT16: compensated fp16, x * 2^s = hi + lo (both fp16); the copies hold
+// three K segments, A: [hi | hi | lo], B: [hi ; lo ; hi], so one fp16 product
+// of the concatenated operands is hi*hi + hi*lo + lo*hi.
+enum class TcOperand { F16 = 0, BF16 = 1, E4M3 = 2, SPLIT16 = 3 };
 
 inline int tc_operand_bytes(TcOperand k) { return k == TcOperand::E4M3 ? 1 : 2; }
+
+// Kinds whose copies carry one power-of-two scale per 128-row / 128-column
+// tile, and the bound the scaled tile maximum is brought under.
+inline bool tc_scaled(TcOperand k) { return k == TcOperand::E4M3 || k == TcOperand::SPLIT16; }
+inline float tc_scale_bound(TcOperand k) { return k == TcOperand::E4M3 ? 448.0f : 32768.0f; }
+
+// Length of one packed row / column along K (segments padded to 16).
+inline int64_t tc_packed_k(TcOperand k, int64_t K) {
+  const int64_t kp = (K + 15) / 16 * 16;
+  return k == TcOperand::SPLIT16 ? 3 * kp : kp;
+}
 
 // C[M x N] (fp32, column-major, ldc) += alpha * A * B, A row-major (lda_p),
 // B column-major (ldb_p), both of type `kind`.  scale_a / scale_b (log2 per
@@ -24,15 +38,16 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
 
 // Largest power-of-two scale per 128-row tile of the fp32 column-major
 // src (M x K) / per 128-column tile of src (K x N) such that amax * 2^s <=
-// 448 (e4m3 max).  `tmp` needs one int per tile.
+// bound (448: e4m3 max; 32768 for split fp16).  `tmp` needs one int per tile.
 lu_status launch_scale_rowtiles(cudaStream_t st, int64_t M, int64_t K,
                                 const float* src, int64_t lds, int* scale,
-                                int* tmp);
+                                int* tmp, float bound = 448.0f);
 lu_status launch_scale_coltiles(cudaStream_t st, int64_t K, int64_t N,
                                 const float* src, int64_t lds, int* scale,
-                                int* tmp);
+                                int* tmp, float bound = 448.0f);
 
-// A operand: dst[i*ldd + k] = round(src[i + k*lds] * 2^scale[i/128]).
+// A operand: dst[i*ldd + k] = round(src[i + k*lds] * 2^scale[i/128])
+// (SPLIT16: the three segments, each round16(K) long, zero padded).
 lu_status launch_pack_a(cudaStream_t st, TcOperand kind, int64_t M, int64_t K,
                         const float* src, int64_t lds, void* dst, int64_t ldd,
                         const int* scale);

@@ -32,16 +32,37 @@ def to_host(t):
     return np.asfortranarray(t.cpu().numpy())
 
 
-def pow2_scale(amax):
-    """Largest s with amax * 2^s <= 448 (0 for an empty tile)."""
+def pow2_scale(amax, bound=448.0):
+    """Largest s with amax * 2^s <= bound (0 for an empty tile)."""
     if not amax > 0:
         return 0
-    s = int(math.floor(math.log2(448.0 / amax)))
-    while amax * 2.0 ** (s + 1) <= 448.0:
+    s = int(math.floor(math.log2(bound / amax)))
+    while amax * 2.0 ** (s + 1) <= bound:
         s += 1
-    while amax * 2.0 ** s > 448.0:
+    while amax * 2.0 ** s > bound:
         s -= 1
     return s
+
+
+def split_tiles(X, by_rows):
+    """Split fp16 copies of X as the library holds them: per 128-row (A) /
+    128-column (B) tile x * 2^s = hi + lo, returned in fp64 with the scale
+    divided out again."""
+    hi = np.zeros(X.shape)
+    lo = np.zeros(X.shape)
+    n = X.shape[0] if by_rows else X.shape[1]
+    for t in range(0, n, 128):
+        blk = X[t:t + 128, :] if by_rows else X[:, t:t + 128]
+        s = pow2_scale(float(np.abs(blk).max()), 32768.0)
+        xs = (blk.astype(np.float64) * 2.0 ** s).astype(np.float32)
+        h = O.round_fmt(xs, O.FMT_FP16)
+        l = O.round_fmt((xs - h).astype(np.float32), O.FMT_FP16)
+        hv, lv = h.astype(np.float64) * 2.0 ** -s, l.astype(np.float64) * 2.0 ** -s
+        if by_rows:
+            hi[t:t + 128, :], lo[t:t + 128, :] = hv, lv
+        else:
+            hi[:, t:t + 128], lo[:, t:t + 128] = hv, lv
+    return hi, lo
 
 
 def rounded_operands(A, B, fmt):
@@ -90,6 +111,35 @@ def test_tc_update_matches_rounded_fp64(built, compute, fmt, M, N, K, pad):
     assert np.all(err <= bound), (err / bound).max()
 
 
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 500, 256), (1000, 777, 200),
+                                   (2048, 1536, 1024), (5, 7, 3), (96, 40, 16)])
+@pytest.mark.parametrize("pad", [0, 3])
+def test_tc_split_update_matches_three_products(built, M, N, K, pad):
+    """Split fp16: C - (Ahi Bhi + Ahi Blo + Alo Bhi), fp32 accumulation over
+    the 3K concatenated terms; and within ~2^-20 K |A||B| of the fp32-operand
+    product, far below the plain fp16 update's 2^-11."""
+    rng = np.random.default_rng(M * 5 + N + K)
+    A = np.asfortranarray(rng.standard_normal((M, K)).astype(np.float32))
+    B = np.asfortranarray((rng.standard_normal((K, N)) * 3).astype(np.float32))
+    C = np.asfortranarray(rng.standard_normal((M, N)).astype(np.float32))
+    Ah, Al = split_tiles(A, True)
+    Bh, Bl = split_tiles(B, False)
+    prod = Ah @ Bh + Ah @ Bl + Al @ Bh
+    want = C.astype(np.float64) - prod
+    mag = np.abs(Ah) @ np.abs(Bh) + np.abs(Ah) @ np.abs(Bl) + np.abs(Al) @ np.abs(Bh)
+    bound = 2 * 3 * K * U32 * mag + 2 * U32 * np.abs(want) + 1e-30
+    ldc = ((M + 3) // 4) * 4 if pad == 0 else M + 3
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C, lda=ldc)
+    rb.gemmex(rb.compute_type.TC32_SPLIT, -1.0, dA, dB, 1.0, dC)
+    torch.cuda.synchronize()
+    got = to_host(dC)
+    err = np.abs(got - want)
+    assert np.all(err <= bound), (err / bound).max()
+    exact = C.astype(np.float64) - A.astype(np.float64) @ B.astype(np.float64)
+    absab = np.abs(A.astype(np.float64)) @ np.abs(B.astype(np.float64))
+    assert np.all(np.abs(got - exact) <= 2.0 ** -20 * K * absab + 4 * U32 * np.abs(exact))
+
+
 def test_tc_update_repeated_calls_consistent(built):
     # same inputs twice -> same bits (the tile schedule is static)
     rng = np.random.default_rng(0)
@@ -107,7 +157,9 @@ def test_tc_update_repeated_calls_consistent(built):
 @pytest.mark.parametrize("n,nb,compute,fmt", [(512, 128, rb.TC32, O.FMT_FP16),
                                               (1000, 256, rb.TC32, O.FMT_FP16),
                                               (768, 128, rb.compute_type.TC32_BF16, O.FMT_BF16),
-                                              (768, 128, rb.compute_type.TC32_E4M3, O.FMT_E4M3)])
+                                              (768, 128, rb.compute_type.TC32_E4M3, O.FMT_E4M3),
+                                              (768, 128, rb.compute_type.TC32_SPLIT, O.FMT_SPLIT),
+                                              (1000, 256, rb.compute_type.TC32_SPLIT, O.FMT_SPLIT)])
 def test_lu_rl_mixed_vs_oracle(built, n, nb, compute, fmt):
     a = O.gen_matrix(n, seed=n, kind=1, alpha=1.5)
     want = O.lu_rl(a, nb=nb, outer_fmt=fmt)

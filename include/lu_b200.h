@@ -292,6 +292,29 @@ LU_API lu_status lu_batch_graph_create(lu_batch_plan plan, lu_stream_t stream,
 LU_API lu_status lu_batch_graph_launch(lu_batch_graph graph, lu_stream_t stream);
 LU_API void lu_batch_graph_destroy(lu_batch_graph graph);
 
+/* Solve with the factors of every matrix of the plan: d_x[i] (device, fp64,
+ * n_i x nrhs, ld n_i) holds B_i on entry and X_i = op(A_i)^-1 B_i on exit
+ * (trans = 1: A_i^T).  fp32 factors d_lu[i] (ld d_ldlu[i], NULL: n_i), fp64
+ * arithmetic; with the original matrices d_a (ld d_lda, NULL: n_i) each
+ * column then gets refine_iters rounds of FP64 refinement.  One warp per
+ * (matrix, column), no allocation, asynchronous. */
+LU_API lu_status lu_batch_solve_c(lu_batch_plan plan, lu_stream_t stream,
+                                  const float* const* d_lu, const int32_t* d_ldlu,
+                                  const float* const* d_a, const int32_t* d_lda,
+                                  double* const* d_x, int32_t nrhs, int trans,
+                                  int refine_iters);
+
+/* Backward pass of X_i = A_i^-1 B_i for the whole batch: d_g[i] (dL/dX_i,
+ * fp64 n_i x nrhs) is overwritten with dL/dB_i = A_i^-T G_i (refined as in
+ * lu_batch_solve_c), and d_da[i] (fp32, ld d_ldda[i] or n_i; may be NULL)
+ * receives dL/dA_i = -(A_i^-T G_i) X_i^T.  d_x: the forward solutions. */
+LU_API lu_status lu_batch_adjoint_c(lu_batch_plan plan, lu_stream_t stream,
+                                    const float* const* d_lu, const int32_t* d_ldlu,
+                                    const float* const* d_a, const int32_t* d_lda,
+                                    double* const* d_x, double* const* d_g,
+                                    float* const* d_da, const int32_t* d_ldda,
+                                    int32_t nrhs, int refine_iters);
+
 /* Seeded generator for a batch: matrix i is lu_gen_matrix_c(n_i, seed + i,
  * kind, alpha) (no scaling).  d_n, d_lda (NULL: lda = n): device arrays. */
 LU_API lu_status lu_gen_batch_c(lu_stream_t stream, int64_t batch, float* const* d_ptrs,

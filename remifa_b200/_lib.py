@@ -108,6 +108,10 @@ SIGNATURES = {
     "lu_batch_graph_create": (_int, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "lu_batch_graph_launch": (_int, [_vp, _vp]),
     "lu_batch_graph_destroy": (None, [_vp]),
+    "lu_batch_solve_c": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int32, _int,
+                                _int]),
+    "lu_batch_adjoint_c": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                  ctypes.c_int32, _int]),
     "lu_gen_batch_c": (_int, [_vp, _i64, _vp, _vp, _vp, ctypes.c_uint64, _int,
                               ctypes.c_double]),
     "lu_profile_begin": (None, []),

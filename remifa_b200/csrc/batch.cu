@@ -718,6 +718,12 @@ struct lu_batch_plan_t {
   lu_opts opts{};
 };
 
+namespace lub {
+int64_t batch_plan_size(const lu_batch_plan_t* p) { return p->batch; }
+const int32_t* batch_plan_dev_n(const lu_batch_plan_t* p) { return p->d_n; }
+int batch_plan_nmax(const lu_batch_plan_t* p) { return p->nmax; }
+}  // namespace lub
+
 struct lu_batch_graph_t {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;

@@ -71,6 +71,7 @@ def lib():
         L.orc_lu_rl_f32_range.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int,
                                           ctypes.c_int, _i64, _i64]
         L.orc_lu_ll_f32.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int]
+        L.orc_lu_ll_f16.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int]
         L.orc_lu_f64.argtypes = [_i64, _f64p, _i64]
         L.orc_lu_solve_f64.argtypes = [_i64, _f64p, _i64, _f64p]
         L.orc_lu_solve_f32.argtypes = [_i64, _f32p, _i64, _f32p]
@@ -174,12 +175,16 @@ def lu_rl(a: np.ndarray, nb: int = 256, outer_fmt: int = 0, threads: int = 0) ->
     return out
 
 
-def lu_ll(a: np.ndarray, nb: int = 256, threads: int = 0) -> np.ndarray:
-    """Factor a copy of `a` with the restated reference left-looking algorithm."""
+def lu_ll(a: np.ndarray, nb: int = 256, threads: int = 0,
+          fp16_storage: bool = False) -> np.ndarray:
+    """Factor a copy of `a` with the restated reference left-looking
+    algorithm (fp16_storage: the fp16-matrix variant; `a` must then hold
+    fp16-representable values)."""
     lda = ld(a) if a.strides[0] == a.itemsize else a.shape[0]
     out = colmajor(a.shape[0], a.shape[1], lda)
     out[:, :] = a
-    lib().orc_lu_ll_f32(a.shape[0], a.shape[1], nb, _p32(out), ld(out), threads)
+    fn = lib().orc_lu_ll_f16 if fp16_storage else lib().orc_lu_ll_f32
+    fn(a.shape[0], a.shape[1], nb, _p32(out), ld(out), threads)
     return out
 
 

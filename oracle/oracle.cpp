@@ -473,6 +473,43 @@ void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
   omp_set_num_threads(saved);
 }
 
+// Left-looking factorization of an fp16 matrix (values held in fp32, every
+// one fp16-representable): reference src/lu_nopiv_ll.hxx:208-575 with
+// W = fp16, O = TC32 -- the K = ofs products of fp16 values accumulated in
+// fp32 and the updated block column / row rounded to fp16 once -- and the
+// inner Crout elimination in fp32 with its results rounded to fp16 (the
+// product library's fp16 variant; the reference's fp16 wrappers factor the
+// panel in fp16 arithmetic instead).
+void orc_lu_ll_f16(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                   int threads) {
+  const int saved = omp_get_max_threads();
+  if (threads > 0) omp_set_num_threads(threads);
+  auto round_block = [&](int64_t rows, int64_t cols, float* p) {
+    for (int64_t j = 0; j < cols; ++j)
+      for (int64_t i = 0; i < rows; ++i) p[i + j * lda] = round_fmt(p[i + j * lda], 1);
+  };
+  const int64_t nc = (n - 1) / nb + 1;
+  for (int64_t kk = 0; kk < nc; ++kk) {
+    const int64_t ofs = kk * nb;
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = m - ofs;
+    float* blk = a + ofs + ofs * lda;
+    if (ofs > 0) {
+      orc_gemm_sub_f32(updm, in, ofs, a + ofs, lda, a + ofs * lda, lda, blk, lda);
+      round_block(updm, in, blk);
+      if (updm > in) {
+        orc_gemm_sub_f32(in, updm - in, ofs, a + ofs, lda, a + (ofs + in) * lda, lda,
+                         blk + in * lda, lda);
+        round_block(in, updm - in, blk + in * lda);
+      }
+    }
+    inner_ll(updm, in, blk, lda);
+    round_block(updm, in, blk);
+    if (updm > in) round_block(in, updm - in, blk + in * lda);
+  }
+  omp_set_num_threads(saved);
+}
+
 // ---------------------------------------------------------------- FP64
 
 void orc_lu_f64(int64_t n, double* a, int64_t lda) {

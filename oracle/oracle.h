@@ -89,6 +89,11 @@ void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
  * inner tiles (one K = 8t update), then the panel kernel. */
 void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int threads);
+/* Left-looking factorization of an fp16 matrix held in fp32 (fp16-valued
+ * entries): fp16 products accumulated in fp32, updated block column / row
+ * rounded to fp16, the inner Crout elimination in fp32 rounded to fp16. */
+void orc_lu_ll_f16(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                   int threads);
 
 /* ---- FP64 oracle ----------------------------------------------------- */
 void orc_lu_f64(int64_t n, double* a, int64_t lda);

@@ -175,7 +175,11 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   if (o.nb < 8 || o.nb % 8 != 0 || o.nb > 4096) return LU_ERR_INVALID_ARG;
   const int dw = o.diag_width == 0 ? 128 : o.diag_width;
   if (dw < 8 || dw > 128 || dw % 8 != 0) return LU_ERR_INVALID_ARG;
-  if (dtype != LU_F32) return LU_ERR_UNSUPPORTED;
+  // fp16 storage: the left-looking variant with fp16 tensor-core updates
+  if (dtype == LU_F16 &&
+      !(o.variant == LU_LEFT_LOOKING && o.outer_update == LU_COMPUTE_TC32))
+    return LU_ERR_UNSUPPORTED;
+  if (dtype != LU_F32 && dtype != LU_F16) return LU_ERR_UNSUPPORTED;
   if (o.variant != LU_RIGHT_LOOKING && o.variant != LU_LEFT_LOOKING)
     return LU_ERR_INVALID_ARG;
   if (o.inner_update != LU_COMPUTE_FP32) return LU_ERR_UNSUPPORTED;
@@ -199,6 +203,18 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   size_t off = 0;
   p->off_status = off;  // [0] first bad pivot, [1] device wait error
   off += 256;
+  if (p->variant == LU_LEFT_LOOKING && dtype == LU_F16) {
+    p->diag_w = (int)p->nb;
+    const int64_t ldk = (n + 15) / 16 * 16;
+    p->ld_shadow = std::max<int64_t>(4, (n + 3) / 4 * 4);
+    off = align_up(off, 1024);
+    p->off_shadow = off;
+    off = align_up(off + (size_t)p->ld_shadow * n * 4, 1024);
+    p->off_lcopy = off;
+    off = align_up(off + (size_t)n * ldk * 2, 1024);
+    p->ws_bytes = off;
+    return LU_SUCCESS;
+  }
   if (p->variant == LU_LEFT_LOOKING) {
     p->diag_w = (int)p->nb;
     if (is_tc(p->outer) && n > p->nb) {
@@ -425,6 +441,65 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
   return LU_SUCCESS;
 }
 
+// Left-looking factorization of an fp16 matrix (the reference's W = fp16
+// wrappers, src/lu_nopiv_ll.hxx:646-790, with O = TC32).  Per outer block:
+// one K = ofs tensor-core update of the block column and the block row read
+// straight from the fp16 matrix (U, column-major = K-major) and from a
+// row-major fp16 copy of the factored L columns, the sum formed in fp32 and
+// stored back to fp16 once; then the block column and row are copied to
+// fp32, factored there by the Crout diagonal kernel and the left-looking
+// panels, and rounded back to fp16.  The reference's fp16 wrappers factor
+// the panel in fp16 or with fp16 tensor-core inner updates; here the inner
+// elimination always runs in fp32, so its results are at least as accurate.
+static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_t lda,
+                               char* ws, int* first_bad, int* err) {
+  const int64_t n = p.n, nb = p.nb;
+  const int64_t ldk = (n + 15) / 16 * 16;
+  char* Lc = ws + p.off_lcopy;
+  float* S = reinterpret_cast<float*>(ws + p.off_shadow);
+  const int64_t lds = p.ld_shadow;
+  for (int64_t ofs = 0; ofs < n; ofs += nb) {
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = n - ofs;
+    const int64_t rest = updm - in;
+    __half* blk = a + ofs + ofs * lda;
+    float* sblk = S + ofs + ofs * lds;
+    if (ofs > 0) {
+      ProfScope ps("tc_update", st,
+                   4.0 * updm * in + 4.0 * in * rest + 2.0 * (double)ofs * (updm + in),
+                   2.0 * ofs * ((double)updm * in + (double)in * rest));
+      LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                 Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
+                                 err));
+      if (rest > 0)
+        LUB_TRY(launch_tc_update_h(st, TcOperand::F16, in, rest, ofs, -1.0f,
+                                   Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
+                                   blk + in * lda, lda, err));
+    }
+    LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
+    if (rest > 0)
+      LUB_TRY(launch_convert(st, in, rest, blk + in * lda, LU_F16, lda, sblk + in * lds,
+                             LU_F32, lds, 0));
+    {
+      ProfScope ps("diag_factor", st, 8.0 * in * in, 2.0 * in * in * (double)in / 3.0);
+      LUB_TRY(launch_diag_crout(st, sblk, lds, (int)in, ofs, first_bad));
+    }
+    if (rest > 0) {
+      ProfScope ps("lupanel", st, 16.0 * rest * in, 2.0 * rest * (double)in * in);
+      LUB_TRY(launch_lupanel(st, sblk, lds, (int)in, rest, rest, true));
+    }
+    LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
+    if (rest > 0) {
+      LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,
+                             LU_F16, lda, 0));
+      // L rows [ofs+in, n) of the block's columns, rounded exactly as stored
+      LUB_TRY(launch_pack_a(st, TcOperand::F16, rest, in, sblk + in, lds,
+                            Lc + ((ofs + in) * ldk + ofs) * 2, ldk, nullptr));
+    }
+  }
+  return LU_SUCCESS;
+}
+
 lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
                     void* d_a, lu_dtype dtype_a, int64_t lda, int* d_info,
                     void* d_a_lowp, int64_t ld_lowp, void* workspace,
@@ -437,6 +512,10 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
     return LU_ERR_INVALID_ARG;
   Plan p;
   LUB_TRY(make_plan(o, m, n, dtype_a, &p));
+  // fp16 storage: the tensor cores read U straight from the matrix
+  if (dtype_a == LU_F16 && n > 0 &&
+      ((uintptr_t)d_a % 16 != 0 || lda % 8 != 0 || d_a_lowp != nullptr))
+    return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device());
   if (workspace != nullptr && ws_bytes < p.ws_bytes) return LU_ERR_WORKSPACE;
 
@@ -452,7 +531,9 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
   lu_status s = launch_fill_int(st, first_bad, kNoBadPivot, 1);
   if (s == LU_SUCCESS) s = launch_fill_int(st, err, 0, 1);
   if (s == LU_SUCCESS && n > 0)
-    s = p.variant == LU_LEFT_LOOKING
+    s = dtype_a == LU_F16
+            ? ll_factor_f16(p, st, static_cast<__half*>(d_a), lda, wsb, first_bad, err)
+        : p.variant == LU_LEFT_LOOKING
             ? ll_factor(p, st, static_cast<float*>(d_a), lda, wsb, first_bad, err)
             : rl_factor(p, st, static_cast<float*>(d_a), lda, wsb, first_bad, err);
   if (s == LU_SUCCESS) s = launch_finalize_info(st, first_bad, err, d_info);

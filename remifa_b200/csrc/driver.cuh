@@ -20,6 +20,8 @@ struct Plan {
   size_t off_lcopy = 0;     // low-precision L21 copy (row-major)
   size_t off_ucopy = 0;     // low-precision U12 copy (column-major)
   size_t off_scales = 0;    // int per-tile scales (fp8)
+  size_t off_shadow = 0;    // fp16 storage: fp32 copy of the current block
+  int64_t ld_shadow = 0;    //   column and row, where the panel is factored
   size_t lcopy_bytes = 0, ucopy_bytes = 0, scale_bytes = 0;
   size_t ws_bytes = 0;
 };

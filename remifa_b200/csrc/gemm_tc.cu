@@ -32,6 +32,7 @@
 
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 namespace lub {
 namespace {
@@ -53,6 +54,10 @@ template <> struct Cfg<0> {  // register epilogue
   static constexpr int kStages = 4;
   static constexpr size_t kEpiBytes = 0;
 };
+template <> struct Cfg<2> {  // register epilogue, fp16 C
+  static constexpr int kStages = 4;
+  static constexpr size_t kEpiBytes = 0;
+};
 template <> struct Cfg<1> {  // TMA reduce-add epilogue, 2 staging tiles per warp
   static constexpr int kStages = 3;
   static constexpr size_t kEpiBytes = (size_t)kEpiWarps * 2 * kEpiChunk;
@@ -62,6 +67,12 @@ constexpr size_t smem_bytes() {
   return 1024 /*align slack*/ + (size_t)Cfg<EPI>::kStages * (kStageA + kStageB) +
          Cfg<EPI>::kEpiBytes + 256;
 }
+
+__device__ __forceinline__ float to_f32(float x) { return x; }
+__device__ __forceinline__ float to_f32(__half x) { return __half2float(x); }
+template <typename T> __device__ __forceinline__ T from_f32(float x);
+template <> __device__ __forceinline__ float from_f32<float>(float x) { return x; }
+template <> __device__ __forceinline__ __half from_f32<__half>(float x) { return __float2half_rn(x); }
 
 struct TcParams {
   float* C;
@@ -78,7 +89,9 @@ struct TcParams {
 };
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
-// EPI  0: C loaded/stored by the epilogue threads; 1: TMA reduce-add.
+// EPI  0: C loaded/stored by the epilogue threads; 1: TMA reduce-add;
+//      2: as 0 with C stored in fp16 (C + alpha * acc in fp32, rounded once
+//         to fp16; p.C then points at __half).
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
@@ -231,6 +244,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       if (lane == 0) bulk_wait_group<0>();
       __syncwarp();
     } else {
+      using CT = typename std::conditional<EPI == 2, __half, float>::type;
       for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int acc = local & 1;
@@ -241,22 +255,22 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         float sa = 1.0f;
         if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
         const int64_t ldc = p.ldc;
-        float* cbase = p.C + row + (int64_t)col0 * ldc;
+        CT* cbase = reinterpret_cast<CT*>(p.C) + row + (int64_t)col0 * ldc;
         float cv[32];
         // load the first chunk of C before waiting for the accumulator
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-          cv[j] = (row_ok && col0 + j < p.N) ? cbase[j * ldc] : 0.0f;
+          cv[j] = (row_ok && col0 + j < p.N) ? to_f32(cbase[j * ldc]) : 0.0f;
         if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
         tc_fence_after();
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
-          float* cp = cbase + (int64_t)(c * 32) * ldc;
+          CT* cp = cbase + (int64_t)(c * 32) * ldc;
           const int cc = col0 + c * 32;
           if (c > 0) {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              cv[j] = (row_ok && cc + j < p.N) ? cp[j * ldc] : 0.0f;
+              cv[j] = (row_ok && cc + j < p.N) ? to_f32(cp[j * ldc]) : 0.0f;
           }
           float av[32];
           const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
@@ -267,7 +281,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
           if (p.scale_b) s = ldexpf(s, -p.scale_b[cc / 128]);
 #pragma unroll
           for (int j = 0; j < 32; ++j)
-            if (row_ok && cc + j < p.N) cp[j * ldc] = __fmaf_rn(s, av[j], cv[j]);
+            if (row_ok && cc + j < p.N) cp[j * ldc] = from_f32<CT>(__fmaf_rn(s, av[j], cv[j]));
         }
         tc_fence_before();
         __syncwarp();
@@ -343,11 +357,12 @@ bool make_kmajor_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
 
 }  // namespace
 
-lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
-                           int64_t N, int64_t K, float alpha, const void* A,
-                           int64_t lda_p, const void* B, int64_t ldb_p, float* C,
-                           int64_t ldc, const int* scale_a, const int* scale_b,
-                           int* err, int max_ctas, int tiles_per_cta) {
+namespace {
+lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                         int64_t K, float alpha, const void* A, int64_t lda_p,
+                         const void* B, int64_t ldb_p, void* C, bool c_half,
+                         int64_t ldc, const int* scale_a, const int* scale_b,
+                         int* err, int max_ctas, int tiles_per_cta) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
   if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
   const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
@@ -364,7 +379,7 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
   if (!make_kmajor_map(&mb, B, dt, esize, K, N, ldb_p, BN)) return LU_ERR_CUDA;
 
   TcParams p;
-  p.C = C;
+  p.C = static_cast<float*>(C);
   p.ldc = ldc;
   p.M = (int)M;
   p.N = (int)N;
@@ -384,11 +399,15 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
   // TMA reduce-add needs a 16-byte aligned C with a 16-byte multiple stride
   CUtensorMap mc;
   std::memset(&mc, 0, sizeof(mc));
-  const bool tma_c = ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) &&
-                     make_c_map(&mc, C, M, N, ldc);
+  const bool tma_c = !c_half && ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) &&
+                     make_c_map(&mc, static_cast<float*>(C), M, N, ldc);
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
-  if (kind == TcOperand::E4M3) {
+  if (c_half) {
+    if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+    LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 2>, smem_bytes<2>()));
+    tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(ma, mb, mc, p, idesc);
+  } else if (kind == TcOperand::E4M3) {
     if (tma_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 1>, smem_bytes<1>()));
       tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, mc, p, idesc);
@@ -407,6 +426,24 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
   }
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
+}
+}  // namespace
+
+lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
+                           int64_t N, int64_t K, float alpha, const void* A,
+                           int64_t lda_p, const void* B, int64_t ldb_p, float* C,
+                           int64_t ldc, const int* scale_a, const int* scale_b,
+                           int* err, int max_ctas, int tiles_per_cta) {
+  return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, false, ldc,
+                        scale_a, scale_b, err, max_ctas, tiles_per_cta);
+}
+
+lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                             int64_t K, float alpha, const void* A, int64_t lda_p,
+                             const void* B, int64_t ldb_p, __half* C, int64_t ldc,
+                             int* err) {
+  return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, true, ldc,
+                        nullptr, nullptr, err, 0, 0);
 }
 
 }  // namespace lub

@@ -36,6 +36,13 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
                            int64_t ldc, const int* scale_a, const int* scale_b,
                            int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
+// The same update with C stored in fp16 (C = rn16(C + alpha * acc), the sum
+// in fp32): the left-looking factorization of an fp16 matrix.
+lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                             int64_t K, float alpha, const void* A, int64_t lda_p,
+                             const void* B, int64_t ldb_p, __half* C, int64_t ldc,
+                             int* err);
+
 // Largest power-of-two scale per 128-row tile of the fp32 column-major
 // src (M x K) / per 128-column tile of src (K x N) such that amax * 2^s <=
 // bound (448: e4m3 max; 32768 for split fp16).  `tmp` needs one int per tile.

@@ -47,7 +47,11 @@ WORKLOADS = {
                               alpha=1.5, kscale=0, oracle_fmt=2),
     "lu_e4m3_rl_n16384": dict(n=16384, nb=256, outer="TC32_E4M3", kind=1,
                               alpha=1.5, kscale=0, oracle_fmt=3),
+    "lu_split_rl_n16384": dict(n=16384, nb=256, outer="TC32_SPLIT", kind=1,
+                               alpha=1.5, kscale=0, oracle_fmt=4),
 }
+# Workloads with their own step (see the run_* functions below).
+SPECIAL = ("batch_10000_n16_512", "ll_f16_n16384", "precision_n32768", "adjoint_n8192")
 DEFAULT_WORKLOAD = "lu_tc32_rl_n16384"
 NVML_REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x10: "sync_boost",
                 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
@@ -245,7 +249,8 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + list(SPECIAL))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -255,6 +260,9 @@ def main() -> None:
                     help="factor each outer block strictly after the previous update")
     ap.add_argument("--nb", type=int, default=None, help="override the outer block size")
     args = ap.parse_args()
+    if args.workload in SPECIAL:
+        run_special(args)
+        return
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
@@ -413,6 +421,324 @@ def main() -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# special workloads: one JSON line each, same keys as the main line
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _base_line(args, metric, value, unit, ms, higher=True, dtype="f32", config=None):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": higher, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype, "data": "synthetic (seeded counter-based generator on the device)",
+            "config": config or {"workload": args.workload}}
+
+
+def run_batch(args, torch, rb):
+    """10,000 independent factorizations, n_i = floor(16 * 32**u_i) (seed
+    11), A_i = R_i + D_i (R ~ U[-1,1), row dominance 1.5), fp32 storage,
+    fp16 tensor-core outer updates, one persistent launch replayed as a CUDA
+    graph; each step factors its own fresh copy of the batch (1.5 GB)."""
+    from remifa_b200.batch import BatchPlan, MatrixBatch, batch_sizes
+    import oracle as O
+    sizes = batch_sizes(10_000, seed=11)
+    src = MatrixBatch(sizes, align=4).generate(seed=11)
+    plan = BatchPlan(sizes, outer=rb.TC32)
+    tuning = plan.autotune(reps=3)
+    nrun = args.warmup + args.steps
+    copies = [src.like(src.data.clone()) for _ in range(nrun)]
+    info = torch.zeros(len(sizes), dtype=torch.int32, device=src.data.device)
+    graphs = [plan.graph(m, info) for m in copies]
+    stream = torch.cuda.current_stream()
+    for i in range(args.warmup):
+        graphs[i].launch(stream)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with rb.profile() as prof:
+            e0.record(stream)
+            for i in range(args.warmup, nrun):
+                graphs[i].launch(stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    bad = int((info != 0).sum())
+    flops = src.flops
+    value = len(sizes) / (ms / 1e3)
+    nbytes = float((sizes.astype("float64") * src.lda).sum() * 4)
+    # end to end: pinned host batch -> device, factor, factors -> host
+    host = torch.empty(src.data.numel(), dtype=torch.float32, pin_memory=True)
+    host.copy_(src.data)
+    back = torch.empty_like(host)
+    dev = copies[0]
+    e_ms = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        a0, a1 = _events(torch)
+        a0.record(stream)
+        dev.data.copy_(host, non_blocking=True)
+        plan(dev, info)
+        back.copy_(dev.data, non_blocking=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        if i:
+            e_ms.append(a0.elapsed_time(a1))
+    e2e_ms = sum(e_ms) / len(e_ms)
+    peaks = measured_peaks()
+    achieved = 2 * nbytes / (ms / 1e3) / 1e9
+    line = _base_line(args, "batched LU matrices/s (10,000 sizes 16..511)", value,
+                      "matrices/s", ms, dtype="f32 storage, fp16 tensor-core updates",
+                      config={"workload": args.workload, "batch": len(sizes),
+                              "sizes": "floor(16*32^u), u~U[0,1) seed 11",
+                              "matrix": "R + D, R ~ U[-1,1), row dominance 1.5",
+                              "tuning": tuning, "l2": "a distinct 1.5 GB copy per step",
+                              "launch": "one persistent kernel per step, CUDA graph"})
+    line.update({
+        "tflops": flops / (ms / 1e3) / 1e12,
+        "e2e": {"value": len(sizes) / (e2e_ms / 1e3), "unit": "matrices/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes,
+                "path": "lu_batch_c via BatchPlan, pinned host buffers"},
+        "gpu_launches": prof.launches,
+        "roofline": {"kernel": "batch_lu_kernel", "bound": "hbm",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "peak_source": peaks["source"] + " hbm_gbs",
+                     "algorithmic_bytes_per_launch": 2 * nbytes, "traffic": None},
+        "clocks": clk.summary(), "bad_info": bad,
+    })
+    # CPU baseline: the oracle's RL restatement per matrix on a sample
+    import numpy as np
+    idx = list(range(0, len(sizes), 50))
+    t0 = time.perf_counter()
+    fl = 0.0
+    for i in idx:
+        n = int(sizes[i])
+        a = O.gen_matrix(n, seed=11 + i, kind=0, alpha=1.5)
+        nb = tuning["nb"][rb.batch.bucket_of(n)]
+        O.lu_rl(a, nb=nb, outer_fmt=1, threads=1)
+        fl += lu_flops(n)
+    dt = time.perf_counter() - t0
+    line["cpu_baseline"] = {"value": len(idx) / dt, "unit": "matrices/s", "cores": 1,
+                            "kind": "port",
+                            "sample": f"{len(idx)} of the 10,000 matrices (every 50th), "
+                                      f"{dt:.1f} s, {fl / dt / 1e9:.1f} GFLOP/s"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ll16(args, torch, rb):
+    """Left-looking factorization of an n = 16384 fp16 matrix (fp16
+    storage, fp16 tensor-core updates, nb = 128), A = R + D with R ~
+    N(0,1)/sqrt(n), row dominance 1.5."""
+    n, nb = 16384, 128
+    base32 = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5)
+    base = rb.colmajor_empty(n, n, n, torch.float16)
+    base.copy_(base32)
+    del base32
+    nrun = args.warmup + args.steps
+    mats = [base.clone(memory_format=torch.preserve_format) for _ in range(nrun)]
+    mats = [m if m.stride(0) == 1 else rb.colmajor(m) for m in mats]
+    ws = torch.empty(rb.workspace_size(n, nb=nb, outer=rb.TC32, variant=1, dtype=torch.float16),
+                     dtype=torch.uint8, device=base.device)
+    infos = torch.zeros(nrun, dtype=torch.int32, device=base.device)
+    stream = torch.cuda.current_stream()
+    for i in range(args.warmup):
+        rb.lu_nopiv_ll(mats[i], nb=nb, outer=rb.TC32, info=infos[i:i + 1], workspace=ws)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with rb.profile() as prof:
+            e0.record(stream)
+            for i in range(args.warmup, nrun):
+                rb.lu_nopiv_ll(mats[i], nb=nb, outer=rb.TC32, info=infos[i:i + 1],
+                               workspace=ws)
+            e1.record(stream)
+            torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    host = torch.empty((n, n), dtype=torch.float16, pin_memory=True).t()
+    host.copy_(base)
+    back = torch.empty((n, n), dtype=torch.float16, pin_memory=True).t()
+    e_ms = []
+    for i in range(3):
+        torch.cuda.synchronize()
+        a0, a1 = _events(torch)
+        a0.record(stream)
+        mats[0].copy_(host, non_blocking=True)
+        rb.lu_nopiv_ll(mats[0], nb=nb, outer=rb.TC32, info=infos[0:1], workspace=ws)
+        back.copy_(mats[0], non_blocking=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        if i:
+            e_ms.append(a0.elapsed_time(a1))
+    e2e_ms = sum(e_ms) / len(e_ms)
+    line = _base_line(args, "LU TFLOP/s (2n^3/3)", lu_flops(n) / (ms / 1e3) / 1e12,
+                      "TFLOP/s", ms, dtype="f16 storage, fp16 tensor-core updates (fp32 accumulate)",
+                      config={"workload": args.workload, "n": n, "nb": nb,
+                              "variant": "left-looking", "storage": "fp16",
+                              "matrix": "R + D, R ~ N(0,1)/sqrt(n), row dominance 1.5",
+                              "l2": "a distinct 2n^2-byte matrix per step"})
+    line.update({
+        "e2e": {"value": lu_flops(n) / (e2e_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": 2 * n * n,
+                "d2h_bytes_per_step": 2 * n * n, "path": "lu_nopiv_ll_c, fp16 pinned host"},
+        "gpu_launches": prof.launches,
+        "kernels": {k: {"launches": v["launches"], "ms": v["total_ms"]}
+                    for k, v in prof.entries.items()},
+        "clocks": clk.summary(), "bad_info_steps": int((infos != 0).sum())})
+    print(json.dumps(line), flush=True)
+
+
+def _condest(torch, rb, a, lu, n, iters=4):
+    """Hager/Higham 1-norm estimate of ||A^-1||_1 with refined solves."""
+    dev = a.device
+    x = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
+    est = 0.0
+    from remifa_b200.autograd import refine_ex
+    for _ in range(iters):
+        y = torch.empty((n, 1), dtype=torch.float64, device=dev)
+        refine_ex(a, lu, x.view(-1, 1).contiguous(), y, trans=False, tol=1e-12, max_iter=20)
+        est = float(y.abs().sum())
+        xi = torch.sign(y).view(-1, 1).contiguous()
+        xi[xi == 0] = 1.0
+        z = torch.empty((n, 1), dtype=torch.float64, device=dev)
+        refine_ex(a, lu, xi, z, trans=True, tol=1e-12, max_iter=20)
+        j = int(z.abs().argmax())
+        if float(z.abs().max()) <= float((z.view(-1) * x).sum()):
+            break
+        x = torch.zeros(n, dtype=torch.float64, device=dev)
+        x[j] = 1.0
+    return est
+
+
+def run_precision(args, torch, rb):
+    """n = 32768: time to an fp64-level solution (backward error <= 1e-14)
+    of A x = b, b = A x_true (x_true ~ N(0,1), fp64), for each Schur-update
+    precision (bf16, e4m3 with per-tile 2^k scales, split fp16, fp16, fp32
+    plain) on row-scaled diagonally dominant matrices A = S (R + D) with
+    kappa tuned to ~1e2, 1e4, 1e6.  value = FP32-plain time / best
+    mixed-precision time at kappa ~1e2."""
+    import math
+    n, nb = 32768, 256
+    precs = ["TC32_BF16", "TC32_E4M3", "TC32_SPLIT", "TC32", "FP32"]
+    results = []
+    base0 = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5)
+    lu0 = rb.colmajor(base0)
+    rb.lu_nopiv_rl(lu0, nb=nb, outer=rb.compute_type.TC32_SPLIT)
+    an = float(base0.abs().sum(dim=0).max())
+    k0 = an * _condest(torch, rb, base0, lu0, n)
+    del base0, lu0
+    torch.cuda.empty_cache()
+    for target in (1e2, 1e4, 1e6):
+        gamma = max(0.0, math.log2(target / k0))
+        base = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5, gamma_bits=gamma)
+        lu = rb.colmajor(base)
+        rb.lu_nopiv_rl(lu, nb=nb, outer=rb.compute_type.TC32_SPLIT)
+        kappa = float(base.abs().sum(dim=0).max()) * _condest(torch, rb, base, lu, n)
+        del lu
+        torch.cuda.empty_cache()
+        row = {"kappa_target": target, "gamma_bits": gamma, "kappa1_est": kappa}
+        for pr in precs:
+            r = time_to_solution(rb, torch, base, n, nb, getattr(rb.compute_type, pr), True,
+                                 reps=2)
+            row[pr] = r
+            torch.cuda.empty_cache()
+        results.append(row)
+        del base
+        torch.cuda.empty_cache()
+    first = results[0]
+    mixed = min(first[p]["ms"] for p in precs[:-1] if first[p]["berr"] <= 1e-14)
+    line = _base_line(args, "time-to-solution speedup vs FP32 plain (berr <= 1e-14)",
+                      first["FP32"]["ms"] / mixed, "x", mixed,
+                      dtype="f32 storage; bf16 / e4m3 / split-fp16 / fp16 updates; fp64 IR",
+                      config={"workload": args.workload, "n": n, "nb": nb,
+                              "matrix": "S (R + D), R ~ N(0,1)/sqrt(n), row dominance 1.5, "
+                                        "S = diag(2^-round(gamma i/(n-1)))",
+                              "x_true": "N(0,1) seed 7, b = A x_true in fp64"})
+    line["results"] = results
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, torch, rb):
+    """Differentiable solve: n = 8192, 64 right-hand sides, fp16 tensor-core
+    factors, dominance 2, loss sum(W * X), forward (factor + refined solves)
+    and backward (refined transposed solves + outer product); plus the
+    batched backward over 1,024 matrices of sizes U[64, 256]."""
+    import numpy as np
+    from remifa_b200.autograd import lu_solve_autograd
+    from remifa_b200.batch import BatchPlan, MatrixBatch, RhsBatch, batched_lu_solve
+    n, k = 8192, 64
+    A0 = rb.gen_matrix(n, seed=2, kind=1, alpha=2.0)
+    g = torch.Generator(device=A0.device)
+    g.manual_seed(3)
+    B = torch.randn(n, k, dtype=torch.float64, device=A0.device, generator=g)
+    W = torch.randn(n, k, dtype=torch.float64, device=A0.device, generator=g)
+    fw, bw = [], []
+    for i in range(args.warmup + args.steps):
+        A = A0.clone().requires_grad_(True)
+        e0, e1 = _events(torch)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        X = lu_solve_autograd(A, B, outer=rb.TC32, nb=256, refine=True)
+        e1.record()
+        (X * W).sum().backward()
+        e2.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            fw.append(e0.elapsed_time(e1))
+            bw.append(e1.elapsed_time(e2))
+    rng = np.random.default_rng(12)
+    sizes = rng.integers(64, 257, size=1024).astype(np.int32)
+    layout = MatrixBatch(sizes, align=4).generate(seed=12, alpha=2.0)
+    plan = BatchPlan(sizes, outer=rb.TC32)
+    rhs = RhsBatch(sizes, 1)
+    b = torch.randn(rhs.data.numel(), dtype=torch.float64, device=A0.device, generator=g)
+    w = torch.randn(rhs.data.numel(), dtype=torch.float64, device=A0.device, generator=g)
+    bfw, bbw = [], []
+    for i in range(args.warmup + args.steps):
+        a = layout.data.clone().requires_grad_(True)
+        e0, e1 = _events(torch)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x = batched_lu_solve(a, b, layout, plan, refine_iters=4)
+        e1.record()
+        (x * w).sum().backward()
+        e2.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            bfw.append(e0.elapsed_time(e1))
+            bbw.append(e1.elapsed_time(e2))
+    med = statistics.median
+    line = _base_line(args, "differentiable solve forward+backward ms (n=8192, 64 rhs)",
+                      med(fw) + med(bw), "ms", med(fw) + med(bw), higher=False,
+                      dtype="f32 storage, fp16 tensor-core factors, fp64 refinement",
+                      config={"workload": args.workload, "n": n, "nrhs": k,
+                              "matrix": "R + D, R ~ N(0,1)/sqrt(n), row dominance 2",
+                              "loss": "sum(W * X), W ~ N(0,1)"})
+    line.update({"forward_ms": med(fw), "backward_ms": med(bw),
+                 "batched": {"matrices": 1024, "sizes": "U[64,256] seed 12",
+                             "forward_ms": med(bfw), "backward_ms": med(bbw),
+                             "refine_iters": 4}})
+    print(json.dumps(line), flush=True)
+
+
+def run_special(args) -> None:
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "unavailable": "the reference has no batched, fp16-left-looking "
+                                         "timing harness, refinement or adjoint for this "
+                                         "workload; see the cpu_baseline field of our line"}))
+        return
+    import torch
+    import remifa_b200 as rb
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    fn = {"batch_10000_n16_512": run_batch, "ll_f16_n16384": run_ll16,
+          "precision_n32768": run_precision, "adjoint_n8192": run_adjoint}[args.workload]
+    fn(args, torch, rb)
 
 
 if __name__ == "__main__":

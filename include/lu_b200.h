@@ -212,8 +212,12 @@ LU_API lu_status lu_refine_static_c(lu_stream_t stream, int64_t n, const float* 
                                     int max_iter, int* iters, double* berr);
 
 /* Several right-hand sides (B, X fp64, n x nrhs) and the transposed system
- * (trans = 1: A^T X = B, backward error with ||A||_1).  *iters / *berr
- * receive the largest iteration count / backward error over the columns. */
+ * (trans = 1: A^T X = B, backward error with ||A||_1).  All columns are
+ * refined together (one multi-column solve per iteration) until the largest
+ * backward error over the columns is <= tol; *iters / *berr receive the
+ * iteration count and that largest backward error.  Workspace:
+ * lu_refine_ex_workspace_size (or NULL for stream-ordered allocation). */
+LU_API lu_status lu_refine_ex_workspace_size(int64_t n, int64_t nrhs, size_t* bytes);
 LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
                                 const float* d_a, int64_t lda, const float* d_lu,
                                 int64_t ldlu, const double* d_b, int64_t ldb,

@@ -91,6 +91,7 @@ SIGNATURES = {
                            _vp, ctypes.c_size_t]),
     "lu_refine_static_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_double,
                                   _int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_double)]),
+    "lu_refine_ex_workspace_size": (_int, [_i64, _i64, ctypes.POINTER(ctypes.c_size_t)]),
     "lu_refine_ex_c": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
                               _i64, _int, ctypes.c_double, _int, ctypes.POINTER(_int),
                               ctypes.POINTER(ctypes.c_double), _vp, ctypes.c_size_t]),

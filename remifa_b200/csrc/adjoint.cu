@@ -143,7 +143,7 @@ extern "C" {
 LU_API lu_status lu_adjoint_workspace_size(int64_t n, int64_t nrhs, size_t* bytes) {
   if (n < 0 || nrhs < 0 || !bytes) return LU_ERR_INVALID_ARG;
   size_t rw = 0;
-  LUB_TRY(lu_refine_workspace_size(n, &rw));
+  LUB_TRY(lu_refine_ex_workspace_size(n, nrhs, &rw));
   *bytes = align_up((size_t)n * (size_t)nrhs * 8, 256) + rw;
   return LU_SUCCESS;
 }

@@ -13,8 +13,10 @@
 #include "solve.cuh"
 #include "lu_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 using namespace lub;
 
@@ -24,13 +26,16 @@ struct RefineWs {
   size_t off_r, off_d, off_p, off_max, bytes;
 };
 
-RefineWs refine_layout(int64_t n) {
+// Residuals and corrections of all nrhs columns, one set of chunk partial
+// sums (the columns' residuals run one after another), and per column the
+// three maxima of the backward error plus the matrix norm.
+RefineWs refine_layout(int64_t n, int64_t nrhs = 1) {
   RefineWs w;
   size_t off = 0;
-  w.off_r = off; off = align_up(off + (size_t)n * 8, 256);
-  w.off_d = off; off = align_up(off + (size_t)n * 8, 256);
+  w.off_r = off; off = align_up(off + (size_t)n * nrhs * 8, 256);
+  w.off_d = off; off = align_up(off + (size_t)n * nrhs * 8, 256);
   w.off_p = off; off = align_up(off + residual_ws_bytes(n), 256);
-  w.off_max = off; off += 256;
+  w.off_max = off; off = align_up(off + (size_t)(3 * nrhs + 1) * 8, 256);
   w.bytes = off;
   return w;
 }
@@ -83,62 +88,70 @@ LU_API lu_status lu_refine_workspace_size(int64_t n, size_t* bytes) {
 
 namespace {
 
-// One right-hand side; trans: refine A^T x = b.
-lu_status refine_one(lu_stream_t stream, int64_t n, const float* d_a,
-                     int64_t lda, const float* d_lu, int64_t ldlu,
-                     const double* d_b, double* d_x, int trans, double tol,
-                     int max_iter, char* wb, const RefineWs& w, int* iters,
-                     double* berr) {
+// All nrhs columns together; trans: refine A^T X = B.  Per iteration: the
+// fp64 residual of every column, one read-back of all backward errors, then
+// one multi-column triangular solve of the corrections.
+lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float* d_a,
+                       int64_t lda, const float* d_lu, int64_t ldlu, const double* d_b,
+                       int64_t ldb, double* d_x, int64_t ldx, int trans, double tol,
+                       int max_iter, char* wb, const RefineWs& w, int* iters,
+                       double* berr) {
   cudaStream_t st = (cudaStream_t)stream;
-  double* r = reinterpret_cast<double*>(wb + w.off_r);
-  double* d = reinterpret_cast<double*>(wb + w.off_d);
+  double* R = reinterpret_cast<double*>(wb + w.off_r);
+  double* D = reinterpret_cast<double*>(wb + w.off_d);
   void* P = wb + w.off_p;
   unsigned long long* mx = reinterpret_cast<unsigned long long*>(wb + w.off_max);
-  lu_status s = LU_SUCCESS;
+  unsigned long long* mnorm = mx + 3 * nrhs;
+  std::vector<unsigned long long> h((size_t)(3 * nrhs + 1));
   double e = INFINITY;
   int it = 0;
-  unsigned long long h[4] = {0, 0, 0, 0};
-  do {
-    s = trans ? launch_norm_one(st, n, d_a, lda, mx + 3)
-              : launch_norm_inf(st, n, d_a, lda, P, mx + 3);
-    if (s != LU_SUCCESS) break;
-    if (cudaMemcpyAsync(d_x, d_b, (size_t)n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
-      s = LU_ERR_CUDA;
-      break;
+  LUB_TRY(trans ? launch_norm_one(st, n, d_a, lda, mnorm)
+                : launch_norm_inf(st, n, d_a, lda, P, mnorm));
+  LUB_CUDA_TRY(cudaMemcpy2DAsync(d_x, (size_t)ldx * 8, d_b, (size_t)ldb * 8, (size_t)n * 8,
+                                 (size_t)nrhs, cudaMemcpyDeviceToDevice, st));
+  LUB_TRY(lu_solve_c(stream, n, d_lu, ldlu, d_x, ldx, nrhs, trans));
+  for (;;) {
+    for (int64_t c = 0; c < nrhs; ++c) {
+      const double* b = d_b + c * ldb;
+      const double* x = d_x + c * ldx;
+      LUB_TRY(trans ? launch_residual_t(st, n, d_a, lda, b, x, R + c * n, mx + 3 * c)
+                    : launch_residual(st, n, d_a, lda, b, x, R + c * n, P, mx + 3 * c));
     }
-    if ((s = lu_solve_c(stream, n, d_lu, ldlu, d_x, n, 1, trans)) != LU_SUCCESS) break;
-    for (;;) {
-      s = trans ? launch_residual_t(st, n, d_a, lda, d_b, d_x, r, mx)
-                : launch_residual(st, n, d_a, lda, d_b, d_x, r, P, mx);
-      if (s != LU_SUCCESS) break;
-      if (cudaMemcpyAsync(h, mx, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-          cudaStreamSynchronize(st) != cudaSuccess) {
-        s = LU_ERR_CUDA;
-        break;
-      }
-      const double rmax = bits_to_double(h[0]), xmax = bits_to_double(h[1]);
-      const double bmax = bits_to_double(h[2]), anorm = bits_to_double(h[3]);
+    LUB_CUDA_TRY(cudaMemcpyAsync(h.data(), mx, h.size() * 8, cudaMemcpyDeviceToHost, st));
+    LUB_CUDA_TRY(cudaStreamSynchronize(st));
+    const double anorm = bits_to_double(h[3 * nrhs]);
+    e = 0.0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+      const double rmax = bits_to_double(h[3 * c]), xmax = bits_to_double(h[3 * c + 1]);
+      const double bmax = bits_to_double(h[3 * c + 2]);
       const double den = anorm * xmax + bmax;
-      e = den > 0.0 ? rmax / den : (rmax > 0.0 ? INFINITY : 0.0);
-      if (std::isnan(e)) break;
-      if (e <= tol || it >= max_iter) break;
-      if (cudaMemcpyAsync(d, r, (size_t)n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
-        s = LU_ERR_CUDA;
+      const double ec = den > 0.0 ? rmax / den : (rmax > 0.0 ? INFINITY : 0.0);
+      if (std::isnan(ec)) {
+        e = ec;
         break;
       }
-      if ((s = lu_solve_c(stream, n, d_lu, ldlu, d, n, 1, trans)) != LU_SUCCESS) break;
-      if ((s = launch_axpy(st, n, d, d_x)) != LU_SUCCESS) break;
-      ++it;
+      e = std::max(e, ec);
     }
-  } while (false);
+    if (std::isnan(e) || e <= tol || it >= max_iter) break;
+    LUB_CUDA_TRY(cudaMemcpyAsync(D, R, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, st));
+    LUB_TRY(lu_solve_c(stream, n, d_lu, ldlu, D, n, nrhs, trans));
+    for (int64_t c = 0; c < nrhs; ++c) LUB_TRY(launch_axpy(st, n, D + c * n, d_x + c * ldx));
+    ++it;
+  }
   if (iters) *iters = it;
   if (berr) *berr = e;
-  return s;
+  return LU_SUCCESS;
 }
 
 }  // namespace
 
 extern "C" {
+
+LU_API lu_status lu_refine_ex_workspace_size(int64_t n, int64_t nrhs, size_t* bytes) {
+  if (n < 0 || nrhs < 0 || !bytes) return LU_ERR_INVALID_ARG;
+  *bytes = refine_layout(n, std::max<int64_t>(nrhs, 1)).bytes;
+  return LU_SUCCESS;
+}
 
 LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
                                 const float* d_a, int64_t lda, const float* d_lu,
@@ -156,7 +169,7 @@ LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
   if (n == 0 || nrhs == 0) return LU_SUCCESS;
   if (!d_a || !d_lu || !d_b || !d_x) return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device_local());
-  const RefineWs w = refine_layout(n);
+  const RefineWs w = refine_layout(n, nrhs);
   if (workspace && ws_bytes < w.bytes) return LU_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   void* ws = workspace;
@@ -165,21 +178,13 @@ LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
     if (cudaMallocAsync(&ws, w.bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
-  lu_status s = LU_SUCCESS;
-  int it_max = 0;
-  double e_max = 0.0;
-  for (int64_t c = 0; c < nrhs && s == LU_SUCCESS; ++c) {
-    int it = 0;
-    double e = 0.0;
-    s = refine_one(stream, n, d_a, lda, d_lu, ldlu, d_b + c * ldb, d_x + c * ldx,
-                   trans, tol, max_iter, static_cast<char*>(ws), w, &it, &e);
-    it_max = std::max(it_max, it);
-    e_max = std::isnan(e) ? e : std::max(e_max, e);
-  }
+  double e = 0.0;
+  const lu_status s = refine_multi(stream, n, nrhs, d_a, lda, d_lu, ldlu, d_b, ldb, d_x,
+                                   ldx, trans, tol, max_iter, static_cast<char*>(ws), w,
+                                   iters, &e);
   if (owned) cudaFreeAsync(ws, st);
-  if (iters) *iters = it_max;
-  if (berr) *berr = e_max;
-  if (s == LU_SUCCESS && !(e_max <= tol)) s = LU_ERR_NOT_CONVERGED;
+  if (berr) *berr = e;
+  if (s == LU_SUCCESS && !(e <= tol)) return LU_ERR_NOT_CONVERGED;
   return s;
 }
 

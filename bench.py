@@ -236,6 +236,7 @@ def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2):
 def config_of(args, wl) -> dict:
     return {"workload": args.workload, "n": wl["n"], "nb": getattr(args, "nb", None) or wl["nb"],
             "lookahead": not getattr(args, "no_lookahead", False),
+            "diag_width": getattr(args, "diag_width", 0) or 128,
             "variant": "right-looking", "inner_update": "FP32",
             "outer_update": wl["outer"],
             "matrix": f"R + D, R ~ {'N(0,1)/sqrt(n)' if wl['kind'] else 'U[-1,1)'}, "
@@ -259,6 +260,8 @@ def main() -> None:
     ap.add_argument("--no-lookahead", action="store_true",
                     help="factor each outer block strictly after the previous update")
     ap.add_argument("--nb", type=int, default=None, help="override the outer block size")
+    ap.add_argument("--diag-width", type=int, default=0,
+                    help="override the diagonal-block width of the panel (0: library default)")
     ap.add_argument("--batch-count", type=int, default=10_000,
                     help="batched workload: the first N sizes of the seeded draw "
                          "(smaller cases for profiling)")
@@ -301,7 +304,7 @@ def main() -> None:
 
     for i in range(args.warmup):
         rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1], workspace=ws,
-                       lookahead=la)
+                       lookahead=la, diag_width=args.diag_width)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -313,7 +316,7 @@ def main() -> None:
             t_start.record(stream)
             for i in range(args.warmup, nmat):
                 rb.lu_nopiv_rl(mats[i], nb=nb, outer=outer, info=infos[i:i + 1],
-                               workspace=ws, lookahead=la)
+                               workspace=ws, lookahead=la, diag_width=args.diag_width)
             t_end.record(stream)
             torch.cuda.synchronize(dev)
     ms = t_start.elapsed_time(t_end)
@@ -325,25 +328,25 @@ def main() -> None:
     bad = int((infos != 0).sum().item())
     value = world * args.steps * lu_flops(n) / (ms / 1e3) / 1e12
 
-    # ---- end to end: pinned host matrix -> device -> factor -> host
-    # column-major pinned host buffers (same strides as the device matrix, so
-    # each transfer is one contiguous copy)
+    # ---- end to end through lu_nopiv_rl_host_c: pinned host matrix in, the
+    # factors streamed back into it per outer step while the factorization
+    # runs; the host matrix is reset from a pinned source between steps
+    # (outside the timed region)
+    host_src = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+    host_src.copy_(base)
     host_a = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
-    host_a.copy_(base)
-    host_lu = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
     dA = mats[0]
     e_ms = []
     for i in range(args.e2e_steps + 1):
+        host_a.copy_(host_src)
         torch.cuda.synchronize(dev)
         if world > 1:
             dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        dA.copy_(host_a, non_blocking=True)
-        rb.lu_nopiv_rl(dA, nb=nb, outer=outer, info=infos[0:1], workspace=ws,
-                       lookahead=la)
-        host_lu.copy_(dA, non_blocking=True)
+        rb.lu_nopiv_rl_host(host_a, dA, nb=nb, outer=outer, info=infos[0:1], workspace=ws,
+                            lookahead=la, diag_width=args.diag_width)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         if i > 0:  # first iteration warms the pinned paths
@@ -397,7 +400,8 @@ def main() -> None:
         "config": config_of(args, wl),
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 4 * n * n, "d2h_bytes_per_step": 4 * n * n,
-                "path": "lu_nopiv_rl_c via remifa_b200.lu_nopiv_rl, pinned host buffers"},
+                "path": "lu_nopiv_rl_host_c via remifa_b200.lu_nopiv_rl_host: pinned host "
+                        "matrix in, factors streamed back per outer step"},
         "gpu_launches": prof.launches,
         "roofline": roofline,
         "kernels": {k: {"launches": v["launches"], "ms": v["total_ms"]}

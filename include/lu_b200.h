@@ -119,6 +119,19 @@ LU_API lu_status lu_nopiv_rl_c(const lu_opts* opts, lu_stream_t stream, int64_t 
                         int* d_info, void* d_a_lowp, int64_t ld_lowp,
                         void* workspace, size_t ws_bytes);
 
+/* The right-looking factorization of an fp32 matrix in host memory (new; the
+ * reference takes device pointers only).  h_a (n x n, lda) is copied into
+ * the device buffer d_a (ldda), factored there, and every outer step's block
+ * column and block row are copied back into h_a as soon as they are final,
+ * on an internal copy stream, so the device-to-host transfer of the factors
+ * overlaps the rest of the factorization.  h_a should be pinned host memory
+ * (cudaHostAlloc / cudaHostRegister) for the copies to run asynchronously.
+ * d_info as for lu_nopiv_rl_c.  Asynchronous: synchronise `stream` before
+ * reading h_a. */
+LU_API lu_status lu_nopiv_rl_host_c(const lu_opts* opts, lu_stream_t stream, int64_t n,
+                                    float* h_a, int64_t lda, float* d_a, int64_t ldda,
+                                    int* d_info, void* workspace, size_t ws_bytes);
+
 /* In-place no-pivot LU, left-looking (Crout).
  * Replaces remifa::lu_nopiv_ll<...> (src/lu_nopiv_ll.hxx:41-66) and its 30
  * wrappers lu_nopiv_ll_* (src/lu_nopiv_ll.hxx:586-793). Arguments as
@@ -324,6 +337,12 @@ LU_API lu_status lu_batch_adjoint_c(lu_batch_plan plan, lu_stream_t stream,
 LU_API lu_status lu_gen_batch_c(lu_stream_t stream, int64_t batch, float* const* d_ptrs,
                                 const int32_t* d_n, const int32_t* d_lda, uint64_t seed,
                                 int kind, double alpha);
+
+/* Self-check (no reference counterpart): counts, over all 2^32 float bit
+ * patterns, the inputs where the library's correctly rounded reciprocal
+ * (used for the 1/d of every pivot) differs from CUDA's __frcp_rn; writes
+ * the count to *d_bad (device).  Expected 0. */
+LU_API lu_status lu_selfcheck_rcp_c(lu_stream_t stream, unsigned long long* d_bad);
 
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {

@@ -73,6 +73,8 @@ SIGNATURES = {
                                  ctypes.POINTER(ctypes.c_size_t)]),
     "lu_nopiv_rl_c": (_int, [ctypes.POINTER(LuOpts), _vp, _i64, _i64, _vp, _int,
                              _i64, _vp, _vp, _i64, _vp, ctypes.c_size_t]),
+    "lu_nopiv_rl_host_c": (_int, [ctypes.POINTER(LuOpts), _vp, _i64, _vp, _i64, _vp, _i64,
+                                  _vp, _vp, ctypes.c_size_t]),
     "lu_nopiv_ll_c": (_int, [ctypes.POINTER(LuOpts), _vp, _i64, _i64, _vp, _int,
                              _i64, _vp, _vp, _i64, _vp, ctypes.c_size_t]),
     "lu_panel_c": (_int, [_vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _vp,
@@ -115,6 +117,7 @@ SIGNATURES = {
                                   ctypes.c_int32, _int]),
     "lu_gen_batch_c": (_int, [_vp, _i64, _vp, _vp, _vp, ctypes.c_uint64, _int,
                               ctypes.c_double]),
+    "lu_selfcheck_rcp_c": (_int, [_vp, _vp]),
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),

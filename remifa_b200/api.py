@@ -142,6 +142,32 @@ def lu_nopiv_rl(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
                    a_cpy, info, lookahead, diag_width, workspace, stream)
 
 
+def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=FP32,
+                     outer=FP32, info: torch.Tensor | None = None, lookahead: bool = True,
+                     diag_width: int = 0, workspace: torch.Tensor | None = None,
+                     stream=None) -> torch.Tensor:
+    """Factor the column-major fp32 matrix in (pinned) host memory `h_a` in
+    place, using the device matrix `d_a` (same shape) as the working copy;
+    the factors stream back to `h_a` block by block while the factorization
+    runs (lu_nopiv_rl_host_c).  Returns the device info tensor."""
+    if h_a.is_cuda or not d_a.is_cuda:
+        raise ValueError("lu_nopiv_rl_host: h_a must be a host tensor, d_a a CUDA tensor")
+    if h_a.dtype != torch.float32 or d_a.dtype != torch.float32 or h_a.shape != d_a.shape:
+        raise ValueError("lu_nopiv_rl_host: float32 matrices of the same shape expected")
+    n = h_a.shape[0]
+    if info is None:
+        info = torch.zeros(1, dtype=torch.int32, device=d_a.device)
+    o = make_opts(nb, inner, outer, lookahead, diag_width, _lib.RIGHT_LOOKING)
+    ws_ptr, ws_bytes = None, 0
+    if workspace is not None:
+        ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
+    st = _lib.lib().lu_nopiv_rl_host_c(ctypes.byref(o), _stream(stream), n, _ptr(h_a),
+                                       ld(h_a), _ptr(d_a), ld(d_a), _ptr(info), ws_ptr,
+                                       ws_bytes)
+    _lib.check(st, "lu_nopiv_rl_host_c")
+    return info
+
+
 def lu_nopiv_ll(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
                 a_cpy: torch.Tensor | None = None, info: torch.Tensor | None = None,
                 lookahead: bool = True, diag_width: int = 0,

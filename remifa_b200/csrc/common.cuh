@@ -70,6 +70,28 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
+// Correctly rounded 1/d (IEEE round to nearest even).  For normal d with
+// 2^-125 < |d| < 2^125: the hardware approximation rcp.approx.ftz.f32 refined
+// by Newton-Raphson steps in fused multiply-adds, e = 1 - d y (exact when y
+// is within an ulp), y' = y + e y -- the FMA reciprocal iteration published
+// by Markstein ("Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  Two steps leave an
+// error far below the distance from 1/d to the nearest rounding boundary.
+// Other inputs (zero, subnormal, huge, inf, nan) take __frcp_rn.  Checked
+// against __frcp_rn for every float bit pattern (lu_selfcheck_rcp_c).
+__device__ __forceinline__ float rcp_rn(float d) {
+  const float a = fabsf(d);
+  if (a > 0x1p-125f && a < 0x1p125f) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+    float e = __fmaf_rn(-d, y, 1.0f);
+    y = __fmaf_rn(e, y, y);
+    e = __fmaf_rn(-d, y, 1.0f);
+    return __fmaf_rn(e, y, y);
+  }
+  return __frcp_rn(d);
+}
+
 // Record the 1-based global index of a zero / non-finite pivot.
 __device__ __forceinline__ void note_pivot(float d, int64_t col0,
                                            int* first_bad) {

@@ -141,9 +141,11 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
 // Internal streams of one device: panel work runs at the highest priority,
 // the bulk of each trailing update at the lowest, ordered by two events.
 struct DevStreams {
-  cudaStream_t panel = nullptr, update = nullptr;
+  cudaStream_t panel = nullptr, update = nullptr, copy = nullptr;
+  cudaEvent_t panel_done = nullptr, copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
+  cudaEvent_t done_with[2] = {nullptr, nullptr};  // U2 finished reading buffer b
 };
 
 static lu_status dev_streams(DevStreams** out) {
@@ -159,7 +161,9 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.panel, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.update, cudaStreamNonBlocking, least));
-    for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated})
+    LUB_CUDA_TRY(cudaStreamCreateWithFlags(&d.copy, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
+                           &d.done_with[0], &d.done_with[1], &d.panel_done, &d.copied})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
@@ -298,12 +302,25 @@ static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
 // Right-looking factorization.  Without look-ahead every outer step runs in
 // order on the caller's stream.  With look-ahead the trailing update of step
 // k is split into U1 (the next block column and block row, which the panel
-// of step k+1 needs) and U2 (everything else); the panel, the operand
-// packing and U1 run on a high-priority stream, U2 on a low-priority one, so
-// the panel of step k+1 overlaps U2 of step k.  Every element still receives
-// its updates in the same order, so results are identical either way.
+// of step k+1 needs), U2a (the block column and row after that, which U1 of
+// step k+1 updates next) and U2b (everything else).  The panel, the operand
+// packing and U1 run on a high-priority stream, U2a and U2b on a
+// low-priority one; U1 of step k+1 waits only for U2a of step k, so the
+// bulk U2b of step k overlaps the panels of steps k+1 and k+2.  The packed
+// operands are double-buffered: packing step k+2 waits until U2 of step k
+// has finished reading the same buffer.  Every element still receives its
+// updates in the same order, so results are identical either way.
+// Destination of the finished factors in host memory (lu_nopiv_rl_host_c):
+// each outer step's block column and block row are copied back on the
+// internal copy stream as soon as the step's panel is done.
+struct HostSink {
+  float* h = nullptr;
+  int64_t ldh = 0;
+};
+
 static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
-                           int64_t lda, char* ws, int* first_bad, int* err) {
+                           int64_t lda, char* ws, int* first_bad, int* err,
+                           const HostSink* sink = nullptr) {
   const int64_t n = p.n, nb = p.nb;
   const bool tc = is_tc(p.outer);
   TcWs w[2];
@@ -327,6 +344,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                         lda, a + ofs + (ofs + nb) * lda, lda, ws, w[0]));
       LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tn, 0, tn, ws, w[0], err, 0));
     }
+    if (sink)
+      LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h, (size_t)sink->ldh * 4, a, (size_t)lda * 4,
+                                     (size_t)n * 4, (size_t)n, cudaMemcpyDeviceToHost, st));
     return LU_SUCCESS;
   }
   DevStreams* S = nullptr;
@@ -337,36 +357,71 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   LUB_CUDA_TRY(cudaStreamWaitEvent(su, S->fork, 0));
   lu_status status = LU_SUCCESS;
   int64_t step = 0;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && status == LU_SUCCESS) status = LU_ERR_CUDA;
+    return status == LU_SUCCESS;
+  };
   for (int64_t ofs = 0; ofs < n && status == LU_SUCCESS; ofs += nb, ++step) {
     const int64_t in = std::min(n - ofs, nb);
     status = factor_block(p, sp, a, lda, ofs, in, n - ofs, first_bad);
     if (status != LU_SUCCESS) break;
+    if (sink) {
+      // block column (rows [ofs, n)) and block row (columns [ofs+in, n)) of
+      // this step are final: copy them back while the factorization goes on
+      if (!ok(cudaEventRecord(S->panel_done, sp)) ||
+          !ok(cudaStreamWaitEvent(S->copy, S->panel_done, 0)))
+        break;
+      const float* da = a + ofs + ofs * lda;
+      float* ha = sink->h + ofs + ofs * sink->ldh;
+      if (!ok(cudaMemcpy2DAsync(ha, (size_t)sink->ldh * 4, da, (size_t)lda * 4,
+                                (size_t)(n - ofs) * 4, (size_t)in,
+                                cudaMemcpyDeviceToHost, S->copy)))
+        break;
+      if (n - ofs - in > 0 &&
+          !ok(cudaMemcpy2DAsync(ha + in * sink->ldh, (size_t)sink->ldh * 4, da + in * lda,
+                                (size_t)lda * 4, (size_t)in * 4, (size_t)(n - ofs - in),
+                                cudaMemcpyDeviceToHost, S->copy)))
+        break;
+    }
     const int64_t tn = n - (ofs + nb);
     if (tn <= 0) continue;
-    const TcWs& wk = w[step & 1];
+    const int buf = (int)(step & 1);
+    const TcWs& wk = w[buf];
     if (tc) {
+      // U2 of step k-2 read this buffer
+      if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
       status = tc_pack(sp, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
                        lda, a + ofs + (ofs + nb) * lda, lda, ws, wk);
       if (status != LU_SUCCESS) break;
     }
-    if (cudaEventRecord(S->packed, sp) != cudaSuccess) { status = LU_ERR_CUDA; break; }
-    // U1 after U2 of the previous step (same elements, earlier step first)
-    if (step > 0 && cudaStreamWaitEvent(sp, S->updated, 0) != cudaSuccess) {
-      status = LU_ERR_CUDA;
-      break;
-    }
+    if (!ok(cudaEventRecord(S->packed, sp))) break;
+    // U1 after U2a of the previous step (same elements, earlier step first)
+    if (step > 0 && !ok(cudaStreamWaitEvent(sp, S->updated, 0))) break;
     const int64_t b = std::min(nb, tn);
     status = outer_update(p, sp, a, lda, ofs, 0, tn, 0, b, ws, wk, err, 1);
     if (status == LU_SUCCESS && tn > nb)
       status = outer_update(p, sp, a, lda, ofs, 0, nb, nb, tn - nb, ws, wk, err, 1);
     if (status != LU_SUCCESS) break;
     if (tn > nb) {
-      if (cudaStreamWaitEvent(su, S->packed, 0) != cudaSuccess) { status = LU_ERR_CUDA; break; }
-      status = outer_update(p, su, a, lda, ofs, nb, tn - nb, nb, tn - nb, ws, wk, err, 8);
+      if (!ok(cudaStreamWaitEvent(su, S->packed, 0))) break;
+      // U2a: block column and row k+2 (rows / columns [nb, 2nb) of the trailing part)
+      const int64_t b2 = std::min(nb, tn - nb);
+      status = outer_update(p, su, a, lda, ofs, nb, tn - nb, nb, b2, ws, wk, err, 8);
+      if (status == LU_SUCCESS && tn > 2 * nb)
+        status = outer_update(p, su, a, lda, ofs, nb, b2, 2 * nb, tn - 2 * nb, ws, wk,
+                              err, 8);
       if (status != LU_SUCCESS) break;
-      if (cudaEventRecord(S->updated, su) != cudaSuccess) { status = LU_ERR_CUDA; break; }
+      if (!ok(cudaEventRecord(S->updated, su))) break;
+      // U2b: the rest
+      if (tn > 2 * nb) {
+        status = outer_update(p, su, a, lda, ofs, 2 * nb, tn - 2 * nb, 2 * nb,
+                              tn - 2 * nb, ws, wk, err, 8);
+        if (status != LU_SUCCESS) break;
+      }
+      if (!ok(cudaEventRecord(S->done_with[buf], su))) break;
     } else {
-      if (cudaEventRecord(S->updated, sp) != cudaSuccess) { status = LU_ERR_CUDA; break; }
+      if (!ok(cudaEventRecord(S->updated, sp))) break;
+      if (!ok(cudaEventRecord(S->done_with[buf], sp))) break;
     }
   }
   // join (also on the error path, so the caller's stream stays ordered)
@@ -374,6 +429,10 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   cudaEventRecord(S->join_u, su);
   cudaStreamWaitEvent(st, S->join_p, 0);
   cudaStreamWaitEvent(st, S->join_u, 0);
+  if (sink) {
+    cudaEventRecord(S->copied, S->copy);
+    cudaStreamWaitEvent(st, S->copied, 0);
+  }
   return status;
 }
 
@@ -539,6 +598,41 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
   if (s == LU_SUCCESS) s = launch_finalize_info(st, first_bad, err, d_info);
   if (s == LU_SUCCESS && d_a_lowp != nullptr && n > 0)
     s = launch_convert(st, m, n, d_a, LU_F32, lda, d_a_lowp, LU_F16, ld_lowp, 0);
+  if (owned) cudaFreeAsync(ws, st);
+  return s;
+}
+
+lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_a,
+                         int64_t lda, float* d_a, int64_t ldda, int* d_info,
+                         void* workspace, size_t ws_bytes) {
+  if (n < 0 || lda < std::max<int64_t>(1, n) || ldda < std::max<int64_t>(1, n))
+    return LU_ERR_INVALID_ARG;
+  if (d_info == nullptr) return LU_ERR_INVALID_ARG;
+  if (n > 0 && (h_a == nullptr || d_a == nullptr)) return LU_ERR_INVALID_ARG;
+  if (o.variant != LU_RIGHT_LOOKING) return LU_ERR_UNSUPPORTED;
+  Plan p;
+  LUB_TRY(make_plan(o, n, n, LU_F32, &p));
+  LUB_TRY(check_device());
+  if (workspace != nullptr && ws_bytes < p.ws_bytes) return LU_ERR_WORKSPACE;
+  if (n > 0)
+    LUB_CUDA_TRY(cudaMemcpy2DAsync(d_a, (size_t)ldda * 4, h_a, (size_t)lda * 4,
+                                   (size_t)n * 4, (size_t)n, cudaMemcpyHostToDevice, st));
+  void* ws = workspace;
+  bool owned = false;
+  if (ws == nullptr) {
+    if (cudaMallocAsync(&ws, p.ws_bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
+    owned = true;
+  }
+  char* wsb = static_cast<char*>(ws);
+  int* first_bad = reinterpret_cast<int*>(wsb + p.off_status);
+  int* err = first_bad + 1;
+  lu_status s = launch_fill_int(st, first_bad, kNoBadPivot, 1);
+  if (s == LU_SUCCESS) s = launch_fill_int(st, err, 0, 1);
+  HostSink sink;
+  sink.h = h_a;
+  sink.ldh = lda;
+  if (s == LU_SUCCESS && n > 0) s = rl_factor(p, st, d_a, ldda, wsb, first_bad, err, &sink);
+  if (s == LU_SUCCESS) s = launch_finalize_info(st, first_bad, err, d_info);
   if (owned) cudaFreeAsync(ws, st);
   return s;
 }

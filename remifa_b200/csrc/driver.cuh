@@ -33,6 +33,9 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
                     void* d_a, lu_dtype dtype_a, int64_t lda, int* d_info,
                     void* d_a_lowp, int64_t ld_lowp, void* workspace,
                     size_t ws_bytes);
+lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_a,
+                         int64_t lda, float* d_a, int64_t ldda, int* d_info,
+                         void* workspace, size_t ws_bytes);
 lu_status gemm_update(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
                       int64_t k, double alpha, const float* a, int64_t lda,
                       const float* b, int64_t ldb, double beta, float* c,

@@ -73,6 +73,16 @@ lu_status lu_nopiv_rl_c(const lu_opts* opts, lu_stream_t stream, int64_t m,
                    d_a_lowp, ld_lowp, workspace, ws_bytes);
 }
 
+lu_status lu_nopiv_rl_host_c(const lu_opts* opts, lu_stream_t stream, int64_t n,
+                             float* h_a, int64_t lda, float* d_a, int64_t ldda,
+                             int* d_info, void* workspace, size_t ws_bytes) {
+  lu_opts o;
+  if (opts) o = *opts; else lu_opts_default(&o);
+  o.variant = LU_RIGHT_LOOKING;
+  return factorize_host(o, (cudaStream_t)stream, n, h_a, lda, d_a, ldda, d_info,
+                        workspace, ws_bytes);
+}
+
 lu_status lu_nopiv_ll_c(const lu_opts* opts, lu_stream_t stream, int64_t m,
                         int64_t n, void* d_a, lu_dtype dtype_a, int64_t lda,
                         int* d_info, void* d_a_lowp, int64_t ld_lowp,

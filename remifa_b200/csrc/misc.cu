@@ -90,4 +90,32 @@ lu_status launch_finalize_info(cudaStream_t st, const int* first_bad,
   return LU_SUCCESS;
 }
 
+namespace {
+
+// Counts the float bit patterns whose rcp_rn differs from __frcp_rn (NaN
+// results compare equal when both are NaN).  Grid-stride over [lo, hi).
+__global__ void rcp_check_kernel(uint64_t lo, uint64_t hi,
+                                 unsigned long long* __restrict__ bad) {
+  unsigned long long local = 0;
+  for (uint64_t i = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const float d = __uint_as_float((uint32_t)i);
+    const float a = rcp_rn(d), b = __frcp_rn(d);
+    const bool same = (__float_as_uint(a) == __float_as_uint(b)) || (isnan(a) && isnan(b));
+    local += same ? 0ull : 1ull;
+  }
+  if (local) atomicAdd(bad, local);
+}
+
+}  // namespace
+
 }  // namespace lub
+
+extern "C" LU_API lu_status lu_selfcheck_rcp_c(lu_stream_t stream, unsigned long long* d_bad) {
+  if (!d_bad) return LU_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  LUB_CUDA_TRY(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st));
+  lub::rcp_check_kernel<<<148 * 16, 256, 0, st>>>(0ull, 1ull << 32, d_bad);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}

@@ -37,7 +37,7 @@ __device__ __forceinline__ void factor_tile_warp(float (&v)[8], int tw,
   for (int k = 0; k < 8; ++k) {
     if (k < tw) {
       const float d = __shfl_sync(mask, v[k], k);
-      const float iv = __frcp_rn(d);  // correctly rounded 1/d
+      const float iv = rcp_rn(d);  // correctly rounded 1/d
       if (r == 0) {
         inv[k] = iv;
         note_pivot(d, col0 + k, first_bad);
@@ -67,7 +67,7 @@ __device__ __forceinline__ void factor_tile_thread(float* T, int LD, int tw,
     if (k < tw) {
       const float d = v[k][k];
       note_pivot(d, col0 + k, first_bad);
-      const float iv = __frcp_rn(d);  // correctly rounded 1/d
+      const float iv = rcp_rn(d);  // correctly rounded 1/d
       inv[k] = iv;
 #pragma unroll
       for (int r = k + 1; r < 8; ++r) v[r][k] = __fmul_rn(v[r][k], iv);
@@ -310,21 +310,136 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 
 // ---------------------------------------------------------------------------
 // L and U panels of one sub-panel, one launch.  `dg` is the factored w x w
-// diagonal block (lda); M rows lie below it, N columns right of it.
-//
-// Eight threads (one group, lane & 7 = j) own one row of L21 (L blocks) or
-// one column of U12 (U blocks); a CTA of 256 threads owns 32 of them.  The
-// group walks its row (column) tile by tile, left to right.  For tile T,
-// thread j first applies the rank-8 updates of all earlier tiles to element
-// j of the tile, in order (acc = sum over the 8 columns of the earlier tile
-// with fused multiply-adds, then one subtraction per tile: the sequence the
-// reference's K = 8 GEMMs produce), then the group performs the tile
-// elimination of the panel kernel, passing the eliminated value of column k
-// to the others with a shuffle.  Rows (columns) are independent, so the
-// only synchronisation after staging is within the 8-lane group.
+// diagonal block (lda); M rows lie below it (L21), N columns right of it
+// (U12).  A CTA owns kItems rows of L21 or columns of U12 ("items"), each
+// item's w values held contiguously in shared memory (S[item][pos]), and
+// walks the 8-wide tiles T left to right:
+//   (a) one thread per item eliminates tile T of its item: L rows
+//       x_k *= 1/d_k, x_j -= x_k U[k][j] (src/lu_nopiv.cu:141-168); U
+//       columns x_j -= L[j][k] x_k (src/lu_nopiv.cu:304-316);
+//   (b) all threads apply the rank-8 update of tile T to the item positions
+//       right of it, acc = sum_k fma(x_k, F_k) over the tile's 8 columns
+//       then one subtraction -- the reference's K = 8 GEMMs -- in register
+//       micro-tiles of 4 items x 8 positions (256 FMAs per 24 vector loads).
+// Each element receives the reference's operations in the reference's
+// order.  Left-looking mode (src/lu_nopiv_inner_ll.hxx:225-300) keeps one
+// running sum per element across the earlier tiles (ACC) and subtracts it
+// once, just before the element's tile is eliminated.
 constexpr int kPanelT = 256;
-constexpr int kGroup = 8;
-constexpr int kItems = kPanelT / kGroup;  // rows / columns per CTA
+constexpr int kItems = 64;                 // rows / columns per CTA
+constexpr int kMicroI = 4, kMicroP = 8;    // register micro-tile
+
+__device__ __forceinline__ void ld8(const float* p, float (&v)[8]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  const float4 b = *reinterpret_cast<const float4*>(p + 4);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void st8(float* p, const float (&v)[8]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  *reinterpret_cast<float4*>(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
+}
+
+// F[pos * lf + k]: the factor values that multiply item value k for
+// position pos -- U[k][pos] (L blocks, F column-major) or L[pos][k] (U
+// blocks, F row-major) -- so the 8 values of one tile are two float4.
+template <bool IS_L, bool LEFT>
+__device__ __forceinline__ void lupanel_strip(const float* F, int lf, const float* inv,
+                                              float* S, int ls, float* ACC, int w) {
+  constexpr int nitems = kItems;
+  const int tid = threadIdx.x;
+  const int nt = (w + 7) / 8;
+  for (int T = 0; T < nt; ++T) {
+    const int t0 = 8 * T;
+    const int tw = min(8, w - t0);
+    // (a) tile elimination, one thread per item
+    if (tid < nitems) {
+      float* xr = S + tid * ls + t0;
+      float x[8];
+      ld8(xr, x);
+      if (LEFT && T > 0) {
+        float acc[8];
+        ld8(ACC + tid * ls + t0, acc);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = __fsub_rn(x[c], acc[c]);
+      }
+      if (tw == 8) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          float f[8];
+          ld8(F + (t0 + c) * lf + t0, f);  // f[k] = U[k][c] (L) / L[c][k] (U)
+          if (IS_L) {
+#pragma unroll
+            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
+            x[c] = __fmul_rn(x[c], inv[t0 + c]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
+          }
+        }
+      } else {
+        for (int c = 0; c < tw; ++c) {
+          const float* f = F + (t0 + c) * lf + t0;
+          if (IS_L) {
+            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
+            x[c] = __fmul_rn(x[c], inv[t0 + c]);
+          } else {
+            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
+          }
+        }
+      }
+      st8(xr, x);
+    }
+    __syncthreads();
+    // (b) rank-8 update of positions [t0 + 8, w); thread m takes items
+    // ig, ig + 16, ig + 32, ig + 48 (ig = m % 16: consecutive lanes hit
+    // distinct banks) and 8 consecutive positions
+    const int p0 = t0 + 8;
+    if (p0 < w) {
+      constexpr int kIG = kItems / kMicroI;  // 16 item groups
+      const int npos = (w - p0 + kMicroP - 1) / kMicroP;
+      for (int m = tid; m < npos * kIG; m += kPanelT) {
+        const int ig = m % kIG, pp = p0 + (m / kIG) * kMicroP;
+        float xv[kMicroI][8];
+#pragma unroll
+        for (int a = 0; a < kMicroI; ++a) ld8(S + (ig + a * kIG) * ls + t0, xv[a]);
+        float acc[kMicroI][kMicroP];
+#pragma unroll
+        for (int a = 0; a < kMicroI; ++a) {
+          if (LEFT) {
+            ld8(ACC + (ig + a * kIG) * ls + pp, acc[a]);
+          } else {
+#pragma unroll
+            for (int b = 0; b < kMicroP; ++b) acc[a][b] = 0.0f;
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < kMicroP; ++b) {
+          float f[8];
+          ld8(F + (pp + b) * lf + t0, f);
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+#pragma unroll
+            for (int a = 0; a < kMicroI; ++a) acc[a][b] = __fmaf_rn(xv[a][k], f[k], acc[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < kMicroI; ++a) {
+          float* row = (LEFT ? ACC : S) + (ig + a * kIG) * ls + pp;
+          if (LEFT) {
+            st8(row, acc[a]);
+          } else {
+            float c[8];
+            ld8(row, c);
+#pragma unroll
+            for (int b = 0; b < kMicroP; ++b) c[b] = __fsub_rn(c[b], acc[a][b]);
+            st8(row, c);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
 
 __global__ void __launch_bounds__(kPanelT)
 lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
@@ -332,33 +447,30 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   extern __shared__ __align__(16) float smem[];
   const int tid = threadIdx.x;
   const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
-  const int nt = wp / 8;
-  const int ls = wp + 4;             // strip row stride (breaks bank aliasing)
+  const int ls = wp + 4;             // item stride (breaks bank aliasing)
   const int lf = wp + 4;             // leading dimension of F, same reason
-  float* F = smem;                   // diagonal block, wp x wp, F[c*lf + r]
+  float* F = smem;                   // diagonal block, wp x wp
   float* inv = F + (size_t)wp * lf;  // wp
   float* S = inv + wp;               // kItems x ls
+  float* ACC = S + (size_t)kItems * ls;  // left-looking running sums
   const bool is_l = (int)blockIdx.x < nL;
-  const int j = tid & (kGroup - 1);
-  const int q = tid / kGroup;        // item of this group
-  const unsigned gmask = 0xffu << (tid & 24);  // the 8 lanes of the group
 
-  // Stage the factored diagonal block, column-major with a padded leading
-  // dimension (F[c*lf + r] = D[r][c]): U[8t..8t+7][c] is one aligned 8-float
-  // run, and the 8 columns a group reads at once fall in distinct banks.
+  // Stage the factored diagonal block: column-major (F[c*lf + r]) for L
+  // blocks, row-major (F[r*lf + c]) for U blocks.
   for (int idx = tid; idx < wp * wp; idx += kPanelT) {
     const int r = idx % wp, c = idx / wp;
-    if (r < w && c < w) cp_async4(&F[c * lf + r], &dg[r + (int64_t)c * lda]);
-    else F[c * lf + r] = 0.0f;
+    float* dst = is_l ? &F[c * lf + r] : &F[r * lf + c];
+    if (r < w && c < w) cp_async4(dst, &dg[r + (int64_t)c * lda]);
+    else *dst = 0.0f;
   }
   int64_t item0;
   float* A;
-  int64_t count;
+  int nitems;
   if (is_l) {
     item0 = (int64_t)blockIdx.x * kItems;
     A = dg + w;                      // first row below the block
-    count = M;
-    // strip: S[q*ls + c] = A[row q, column c]; consecutive threads read
+    nitems = (int)std::min<int64_t>(kItems, M - item0);
+    // S[q*ls + c] = A[row q, column c]; consecutive threads read
     // consecutive rows of one column
     for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
       const int qq = idx % kItems, c = idx / kItems;
@@ -369,8 +481,8 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   } else {
     item0 = (int64_t)(blockIdx.x - nL) * kItems;
     A = dg + (int64_t)w * lda;       // first column right of the block
-    count = N;
-    // strip: S[q*ls + i] = A[row i, column q]; consecutive threads read
+    nitems = (int)std::min<int64_t>(kItems, N - item0);
+    // S[q*ls + i] = A[row i, column q]; consecutive threads read
     // consecutive rows of one column
     for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
       const int i = idx % wp, qq = idx / wp;
@@ -379,77 +491,20 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
       else S[qq * ls + i] = 0.0f;
     }
   }
+  if (left)
+    for (int idx = tid; idx < kItems * ls; idx += kPanelT) ACC[idx] = 0.0f;
   cp_async_wait_all();
   __syncthreads();
   if (is_l) {
     for (int k = tid; k < wp; k += kPanelT)
-      inv[k] = (k < w) ? __frcp_rn(F[k * lf + k]) : 0.0f;
+      inv[k] = (k < w) ? rcp_rn(F[k * lf + k]) : 0.0f;
     __syncthreads();
+    if (left) lupanel_strip<true, true>(F, lf, inv, S, ls, ACC, w);
+    else lupanel_strip<true, false>(F, lf, inv, S, ls, ACC, w);
+  } else {
+    if (left) lupanel_strip<false, true>(F, lf, inv, S, ls, ACC, w);
+    else lupanel_strip<false, false>(F, lf, inv, S, ls, ACC, w);
   }
-
-  const bool valid = item0 + q < count;
-  float* srow = S + q * ls;
-  for (int T = 0; T < nt; ++T) {
-    const int tw = min(8, w - 8 * T);
-    float x = srow[8 * T + j];
-    // updates of earlier tiles, in order.  Right-looking (the reference's
-    // lu_nopiv_inner_rl): one subtraction per earlier tile.  Left-looking
-    // (lu_nopiv_inner_ll, src/lu_nopiv_inner_ll.hxx:225-300): one sum over
-    // all earlier columns, subtracted once.
-    float accl = 0.0f;
-    for (int t = 0; t < T; ++t) {
-      const float4 v0 = *reinterpret_cast<const float4*>(&srow[8 * t]);
-      const float4 v1 = *reinterpret_cast<const float4*>(&srow[8 * t + 4]);
-      float acc = left ? accl : 0.0f;
-      if (is_l) {
-        // U[8t+k][8T+j]: column 8T+j of F, rows 8t..8t+7
-        const float* fcol = &F[(8 * T + j) * lf + 8 * t];
-        const float4 f0 = *reinterpret_cast<const float4*>(fcol);
-        const float4 f1 = *reinterpret_cast<const float4*>(fcol + 4);
-        acc = __fmaf_rn(v0.x, f0.x, acc);
-        acc = __fmaf_rn(v0.y, f0.y, acc);
-        acc = __fmaf_rn(v0.z, f0.z, acc);
-        acc = __fmaf_rn(v0.w, f0.w, acc);
-        acc = __fmaf_rn(v1.x, f1.x, acc);
-        acc = __fmaf_rn(v1.y, f1.y, acc);
-        acc = __fmaf_rn(v1.z, f1.z, acc);
-        acc = __fmaf_rn(v1.w, f1.w, acc);
-      } else {
-        // L[8T+j][8t+k]: row 8T+j of F, columns 8t..8t+7 (the 8 lanes of a
-        // group read 8 consecutive words)
-        const float* frow = &F[(8 * t) * lf + 8 * T + j];
-        acc = __fmaf_rn(frow[0 * lf], v0.x, acc);
-        acc = __fmaf_rn(frow[1 * lf], v0.y, acc);
-        acc = __fmaf_rn(frow[2 * lf], v0.z, acc);
-        acc = __fmaf_rn(frow[3 * lf], v0.w, acc);
-        acc = __fmaf_rn(frow[4 * lf], v1.x, acc);
-        acc = __fmaf_rn(frow[5 * lf], v1.y, acc);
-        acc = __fmaf_rn(frow[6 * lf], v1.z, acc);
-        acc = __fmaf_rn(frow[7 * lf], v1.w, acc);
-      }
-      if (left) accl = acc;
-      else x = __fsub_rn(x, acc);
-    }
-    if (left && T > 0) x = __fsub_rn(x, accl);
-    // tile elimination
-    if (is_l) {
-      // src/lu_nopiv.cu:141-168: x_k *= 1/d_k, then x_j -= x_k * U[k][j]
-      for (int k = 0; k < tw; ++k) {
-        if (j == k) x = __fmul_rn(x, inv[8 * T + k]);
-        const float xk = __shfl_sync(gmask, x, k, kGroup);
-        if (j > k && j < tw) x = __fmaf_rn(-xk, F[(8 * T + j) * lf + 8 * T + k], x);
-      }
-    } else {
-      // src/lu_nopiv.cu:304-316: x_j -= L[j][k] * x_k (unit diagonal)
-      for (int k = 0; k < tw; ++k) {
-        const float xk = __shfl_sync(gmask, x, k, kGroup);
-        if (j > k && j < tw) x = __fmaf_rn(-F[(8 * T + k) * lf + 8 * T + j], xk, x);
-      }
-    }
-    if (j < tw) srow[8 * T + j] = x;
-    __syncwarp(gmask);
-  }
-  __syncthreads();
   if (is_l) {
     for (int idx = tid; idx < kItems * w; idx += kPanelT) {
       const int qq = idx % kItems, c = idx / kItems;
@@ -463,7 +518,7 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
       if (col < N) A[i + col * lda] = S[qq * ls + i];
     }
   }
-  (void)valid;
+  (void)nitems;
 }
 
 // ---------------------------------------------------------------------------
@@ -560,9 +615,9 @@ lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
   return LU_SUCCESS;
 }
 
-static size_t lupanel_smem_bytes(int w) {
+static size_t lupanel_smem_bytes(int w, bool left) {
   const size_t wp = (size_t)((w + 7) / 8) * 8;
-  return (wp * (wp + 4) + wp + (size_t)kItems * (wp + 4)) * sizeof(float);
+  return (wp * (wp + 4) + wp + (size_t)(left ? 2 : 1) * kItems * (wp + 4)) * sizeof(float);
 }
 
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
@@ -571,7 +626,7 @@ lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
   const int64_t nL = M > 0 ? ceil_div(M, kItems) : 0;
   const int64_t nU = N > 0 ? ceil_div(N, kItems) : 0;
   if (nL + nU == 0) return LU_SUCCESS;
-  const size_t sm = lupanel_smem_bytes(w);
+  const size_t sm = lupanel_smem_bytes(w, left);
   LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));
   lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL,
                                                            left);

@@ -288,3 +288,19 @@ def test_lu_ll_limits(built):
         rb.lu_nopiv_ll(a, nb=256)
     with pytest.raises(NotImplementedError):
         rb.lu_nopiv_ll(a, nb=128, outer=rb.compute_type.TC32_E4M3)
+
+
+@pytest.mark.parametrize("n,outer", [(300, rb.FP32), (2048, rb.FP32), (2048, rb.TC32)])
+def test_host_entry_matches_device_entry(built, n, outer):
+    """lu_nopiv_rl_host_c (host matrix in, factors streamed back per outer
+    step) gives exactly the device entry point's factors."""
+    a = O.gen_matrix(n, seed=n + 3, kind=1, alpha=1.5)
+    d = rb.colmajor(torch.from_numpy(a).cuda())
+    rb.lu_nopiv_rl(d, nb=256, outer=outer)
+    h = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+    h.copy_(torch.from_numpy(a))
+    work = rb.colmajor_empty(n, n, n, torch.float32)
+    info = rb.lu_nopiv_rl_host(h, work, nb=256, outer=outer)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    assert np.array_equal(h.numpy(), d.cpu().numpy())

@@ -141,7 +141,8 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
 // Internal streams of one device: panel work runs at the highest priority,
 // the bulk of each trailing update at the lowest, ordered by two events.
 struct DevStreams {
-  cudaStream_t panel = nullptr, update = nullptr, copy = nullptr;
+  cudaStream_t panel = nullptr, update = nullptr, copy = nullptr, side = nullptr;
+  cudaEvent_t diag_done = nullptr, small_done = nullptr, big_done = nullptr;
   cudaEvent_t panel_done = nullptr, copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
@@ -162,8 +163,10 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.panel, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.update, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithFlags(&d.copy, cudaStreamNonBlocking));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
-                           &d.done_with[0], &d.done_with[1], &d.panel_done, &d.copied})
+                           &d.done_with[0], &d.done_with[1], &d.panel_done, &d.copied,
+                           &d.diag_done, &d.small_done, &d.big_done})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
@@ -281,6 +284,69 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
   return LU_SUCCESS;
 }
 
+// The same factorization of the outer block for the look-ahead schedule,
+// when it holds exactly two diagonal sub-blocks (in == 2 w): after the
+// first diagonal block, only what the second one needs stays on the panel
+// stream st -- the first w L rows and U columns of the sub-panel and their
+// rank-w update of the second diagonal block -- while the rest of the
+// sub-panel and of its update run on the side stream ss and overlap the
+// second diagonal factorization.  Every element receives the same
+// operations in the same order as in factor_block.
+static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* S,
+                                    float* a, int64_t lda, int64_t ofs, int64_t in,
+                                    int64_t updm, int* first_bad) {
+  const int w = p.diag_w;
+  if (in != 2 * w || updm <= in)
+    return factor_block(p, st, a, lda, ofs, in, updm, first_bad);
+  cudaStream_t ss = S->side;
+  float* blk = a + ofs + ofs * lda;
+  const int64_t big = updm - 2 * w;  // L rows / U columns beyond the outer block
+  {
+    ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * w / 3.0);
+    LUB_TRY(launch_diag_factor(st, blk, lda, w, ofs, first_bad));
+  }
+  LUB_CUDA_TRY(cudaEventRecord(S->diag_done, st));
+  {
+    ProfScope ps("lupanel", st, 2.0 * 8.0 * w * w, 2.0 * 2 * w * (double)w * w);
+    LUB_TRY(launch_lupanel(st, blk, lda, w, w, w, false, 0, 0));
+  }
+  LUB_CUDA_TRY(cudaEventRecord(S->small_done, st));
+  // side stream: the rest of the first sub-panel and of its update
+  LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->diag_done, 0));
+  {
+    ProfScope ps("lupanel", ss, 2.0 * 8.0 * big * w, 2.0 * 2 * big * (double)w * w);
+    LUB_TRY(launch_lupanel(ss, blk, lda, w, big, big, false, w, w));
+  }
+  LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->small_done, 0));
+  {
+    ProfScope ps("sgemm_chunk8", ss, 0.0, 2.0 * w * 2.0 * (double)big * w);
+    // rows [2w, updm) x columns [w, 2w), and rows [w, 2w) x columns [2w, updm)
+    LUB_TRY(launch_sgemm_chunk8_2(ss, big, w, w, blk + 2 * w, lda, blk + (int64_t)w * lda, lda,
+                                  blk + 2 * w + (int64_t)w * lda, lda, w, big, w, blk + w, lda,
+                                  blk + 2 * (int64_t)w * lda, lda,
+                                  blk + w + 2 * (int64_t)w * lda, lda));
+  }
+  LUB_CUDA_TRY(cudaEventRecord(S->big_done, ss));
+  // panel stream: the second diagonal block as soon as its own update is in
+  {
+    ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * (double)w * w * w);
+    LUB_TRY(launch_sgemm_chunk8_2(st, w, w, w, blk + w, lda, blk + (int64_t)w * lda, lda,
+                                  blk + w + (int64_t)w * lda, lda, 0, 0, 0, nullptr, lda,
+                                  nullptr, lda, nullptr, lda));
+  }
+  float* dg1 = blk + w + (int64_t)w * lda;
+  {
+    ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * w / 3.0);
+    LUB_TRY(launch_diag_factor(st, dg1, lda, w, ofs + w, first_bad));
+  }
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->big_done, 0));
+  {
+    ProfScope ps("lupanel", st, 2.0 * 8.0 * big * w, 2.0 * 2 * big * (double)w * w);
+    LUB_TRY(launch_lupanel(st, dg1, lda, w, big, big));
+  }
+  return LU_SUCCESS;
+}
+
 // Trailing update of outer step (ofs) restricted to rows [r0, n) x columns
 // [c0, c0 + ncols): the block at (ofst + r0, ofst + c0).
 static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
@@ -363,7 +429,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   };
   for (int64_t ofs = 0; ofs < n && status == LU_SUCCESS; ofs += nb, ++step) {
     const int64_t in = std::min(n - ofs, nb);
-    status = factor_block(p, sp, a, lda, ofs, in, n - ofs, first_bad);
+    status = factor_block_split(p, sp, S, a, lda, ofs, in, n - ofs, first_bad);
     if (status != LU_SUCCESS) break;
     if (sink) {
       // block column (rows [ofs, n)) and block row (columns [ofs+in, n)) of

@@ -11,8 +11,11 @@ lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
                              int64_t col0, int* first_bad);
 // L rows (M of them, below) and U columns (N, right) of the w x w factored
 // diagonal block dg, one launch.  left: left-looking (Crout) update order.
+// offL / offU: the first L row / U column handled is that many rows below /
+// columns right of the block's edge.
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
-                         int64_t M, int64_t N, bool left = false);
+                         int64_t M, int64_t N, bool left = false, int64_t offL = 0,
+                         int64_t offU = 0);
 // Left-looking (Crout) factorization of a w x w (w <= 128) diagonal block.
 lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
                             int64_t col0, int* first_bad);

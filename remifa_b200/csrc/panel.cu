@@ -443,7 +443,7 @@ __device__ __forceinline__ void lupanel_strip(const float* F, int lf, const floa
 
 __global__ void __launch_bounds__(kPanelT)
 lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
-               int64_t N, int nL, bool left) {
+               int64_t N, int nL, bool left, int64_t offL, int64_t offU) {
   extern __shared__ __align__(16) float smem[];
   const int tid = threadIdx.x;
   const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
@@ -468,7 +468,7 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   int nitems;
   if (is_l) {
     item0 = (int64_t)blockIdx.x * kItems;
-    A = dg + w;                      // first row below the block
+    A = dg + w + offL;               // first row of this launch's L rows
     nitems = (int)std::min<int64_t>(kItems, M - item0);
     // S[q*ls + c] = A[row q, column c]; consecutive threads read
     // consecutive rows of one column
@@ -480,7 +480,7 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
     }
   } else {
     item0 = (int64_t)(blockIdx.x - nL) * kItems;
-    A = dg + (int64_t)w * lda;       // first column right of the block
+    A = dg + (w + offU) * lda;       // first column of this launch's U columns
     nitems = (int)std::min<int64_t>(kItems, N - item0);
     // S[q*ls + i] = A[row i, column q]; consecutive threads read
     // consecutive rows of one column
@@ -621,7 +621,7 @@ static size_t lupanel_smem_bytes(int w, bool left) {
 }
 
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
-                         int64_t M, int64_t N, bool left) {
+                         int64_t M, int64_t N, bool left, int64_t offL, int64_t offU) {
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
   const int64_t nL = M > 0 ? ceil_div(M, kItems) : 0;
   const int64_t nU = N > 0 ? ceil_div(N, kItems) : 0;
@@ -629,7 +629,7 @@ lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
   const size_t sm = lupanel_smem_bytes(w, left);
   LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));
   lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL,
-                                                           left);
+                                                           left, offL, offU);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

@@ -92,6 +92,63 @@ __device__ __forceinline__ float rcp_rn(float d) {
   return __frcp_rn(d);
 }
 
+// rcp_rn without the range test, for callers that check the range of the
+// pivots afterwards (2^-125 < |d| < 2^125) and redo the work otherwise.
+__device__ __forceinline__ float rcp_rn_unchecked(float d) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+  float e = __fmaf_rn(-d, y, 1.0f);
+  y = __fmaf_rn(e, y, y);
+  e = __fmaf_rn(-d, y, 1.0f);
+  return __fmaf_rn(e, y, y);
+}
+
+// Factor a full 8x8 tile (column-major at T, leading dimension LD, 16-byte
+// aligned columns) in registers with the reference's operation order:
+// 1/d, the column below scaled, fused a - l*u for the rest
+// (src/lu_nopiv.cu:123-171).  The pivot chain carries no branch: the
+// pivots are range-checked afterwards, and if any lies outside
+// (2^-125, 2^125) -- zero, subnormal, huge or non-finite -- nothing is
+// written and false is returned, so the caller can redo the tile on the
+// exact slow path (which also reports the bad pivot).
+__device__ __forceinline__ bool factor_tile8_fast(float* T, int LD, float* inv) {
+  float v[8][8];  // v[c][r]: tile column c
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const float4 a = *reinterpret_cast<const float4*>(T + c * LD);
+    const float4 b = *reinterpret_cast<const float4*>(T + c * LD + 4);
+    v[c][0] = a.x; v[c][1] = a.y; v[c][2] = a.z; v[c][3] = a.w;
+    v[c][4] = b.x; v[c][5] = b.y; v[c][6] = b.z; v[c][7] = b.w;
+  }
+  float dk[8], ivk[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    dk[k] = v[k][k];
+    ivk[k] = rcp_rn_unchecked(dk[k]);
+#pragma unroll
+    for (int r = k + 1; r < 8; ++r) v[k][r] = __fmul_rn(v[k][r], ivk[k]);
+#pragma unroll
+    for (int c = k + 1; c < 8; ++c)
+#pragma unroll
+      for (int r = k + 1; r < 8; ++r) v[c][r] = __fmaf_rn(-v[k][r], v[c][k], v[c][r]);
+  }
+  bool safe = true;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float a = fabsf(dk[k]);
+    safe = safe && a > 0x1p-125f && a < 0x1p125f;
+  }
+  if (!safe) return false;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) inv[k] = ivk[k];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    *reinterpret_cast<float4*>(T + c * LD) = make_float4(v[c][0], v[c][1], v[c][2], v[c][3]);
+    *reinterpret_cast<float4*>(T + c * LD + 4) = make_float4(v[c][4], v[c][5], v[c][6], v[c][7]);
+  }
+  return true;
+}
+
 // Record the 1-based global index of a zero / non-finite pivot.
 __device__ __forceinline__ void note_pivot(float d, int64_t col0,
                                            int* first_bad) {

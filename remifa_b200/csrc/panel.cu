@@ -108,14 +108,18 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
   __syncthreads();
 
   const int nt = (w + 7) / 8;
+  // Phase A of tile 0: one thread factors the 8 x 8 tile in registers
+  // (src/lu_nopiv.cu:123-171): 1/d, scale the column below, fused rank-1
+  // update of the rest of the tile.  Later tiles are factored during the
+  // previous tile's Phase C (look-ahead, below).
+  if (tid == 0) {
+    const int tw0 = min(8, w);
+    if (!(tw0 == 8 && factor_tile8_fast(D, LD, inv)))
+      factor_tile_thread(D, LD, tw0, inv, col0, first_bad);
+  }
+  __syncthreads();
   for (int t = 0; t < nt; ++t) {
     const int t0 = 8 * t;
-    const int tw = min(8, w - t0);
-    // Phase A: one thread factors the 8 x 8 tile in registers
-    // (src/lu_nopiv.cu:123-171): 1/d, scale the column below, fused rank-1
-    // update of the rest of the tile.
-    if (tid == 0) factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
-    __syncthreads();
     const int s = w - t0 - 8;  // trailing extent inside the block
     if (s <= 0) break;
     // Phase B: L rows below the tile (threads 0..127), U columns right of it
@@ -169,10 +173,31 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     __syncthreads();
     // Phase C: rank-8 update of the trailing s x s block, 4 x 4 per item:
     // acc = sum_k fma(L[i][t0+k], U[t0+k][j]) in k order, D[i][j] -= acc.
+    // Look-ahead: warp 0 updates the next tile's 8 x 8 block (two elements
+    // per lane) and its lane 0 factors it, while warps 1.. update the rest.
+    const int t1w = min(8, s);  // width of tile t+1
+    if (tid < 32) {
+      float* T1 = D + (t0 + 8) + (t0 + 8) * LD;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = tid + 32 * h, i = e & 7, j = e >> 3;
+        if (i < t1w && j < t1w) {
+          float acc = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc = __fmaf_rn(Ls[k * 128 + i], Us[k * 128 + j], acc);
+          T1[i + j * LD] = __fsub_rn(T1[i + j * LD], acc);
+        }
+      }
+      __syncwarp();
+      if (tid == 0 && !(t1w == 8 && factor_tile8_fast(T1, LD, inv)))
+        factor_tile_thread(T1, LD, t1w, inv, col0 + t0 + 8, first_bad);
+    }
     const int nb4 = (s + 3) / 4;
     const bool vec = (s % 4 == 0);
-    for (int b = tid; b < nb4 * nb4; b += kThreads) {
+    for (int b = tid - 32; b < nb4 * nb4; b += kThreads - 32) {
+      if (b < 0) break;
       const int li = 4 * (b % nb4), lj = 4 * (b / nb4);  // local to the block
+      if (li < 8 && lj < 8) continue;  // the next tile: thread 0
       const int i0 = t0 + 8 + li, j0 = t0 + 8 + lj;
       float acc[4][4];
 #pragma unroll

@@ -32,7 +32,8 @@ __device__ __forceinline__ void tile_factor(float* C, int ldc, int c0, int t0,
   const int lane = threadIdx.x & 31;
   const int tw = min(8, wj - t0);
   float* T = C + (c0 + t0);
-  if (lane == (t0 & 31)) {
+  if (lane == (t0 & 31) && !(tw == 8 && factor_tile8_fast(T + t0 * ldc, ldc, inv))) {
+    // partial tile, or a pivot outside the fast range: the exact path
     float v[8][8];  // v[c][r]: tile column c
 #pragma unroll
     for (int c = 0; c < 8; ++c) {

@@ -359,6 +359,15 @@ LU_API void lu_profile_begin(void);
  * aggregated entries; returns the number of kernel classes seen. */
 LU_API int lu_profile_end(lu_profile_entry* out, int max_entries);
 /* Number of kernels this library has launched in this process. */
+/* Per-launch timeline of the last profiled region (after lu_profile_end):
+ * kernel class, stream (numbered in order of first use) and start / end in
+ * ms from the first recorded launch.  Returns the number of launches. */
+typedef struct lu_trace_entry {
+  char name[32];
+  int32_t stream;
+  double start_ms, end_ms;
+} lu_trace_entry;
+LU_API int lu_profile_trace(lu_trace_entry* out, int max_entries);
 LU_API long long lu_launch_count(void);
 
 #ifdef __cplusplus

@@ -59,6 +59,15 @@ class LuBatchTuning(ctypes.Structure):
     ]
 
 
+class LuTraceEntry(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("stream", ctypes.c_int32),
+        ("start_ms", ctypes.c_double),
+        ("end_ms", ctypes.c_double),
+    ]
+
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _int = ctypes.c_int
@@ -121,6 +130,7 @@ SIGNATURES = {
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),
+    "lu_profile_trace": (_int, [ctypes.POINTER(LuTraceEntry), _int]),
 }
 
 _lib = None

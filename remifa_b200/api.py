@@ -260,6 +260,16 @@ class profile:
         self.launches = L.lu_launch_count() - self.launches0
         return False
 
+    def trace(self) -> list:
+        """Per-launch timeline: dicts (name, stream, start_ms, end_ms)."""
+        L = _lib.lib()
+        k = L.lu_profile_trace(None, 0)
+        buf = (_lib.LuTraceEntry * max(k, 1))()
+        k = L.lu_profile_trace(buf, k)
+        return [dict(name=buf[i].name.decode(), stream=int(buf[i].stream),
+                     start_ms=float(buf[i].start_ms), end_ms=float(buf[i].end_ms))
+                for i in range(k)]
+
 
 def launch_count() -> int:
     """Kernels launched by liblu_b200.so in this process so far."""

@@ -96,6 +96,26 @@ static lu_status tc_pack(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   return LU_SUCCESS;
 }
 
+// Rows [r0, r1) of the L21 copy and columns [c0, c1) of the U12 copy only
+// (kinds without tile scales), at their places in the packed buffers.
+static lu_status tc_pack_range(cudaStream_t st, TcOperand kind, int64_t r0, int64_t r1,
+                               int64_t c0, int64_t c1, int64_t K, const float* a,
+                               int64_t lda, const float* b, int64_t ldb, char* ws,
+                               const TcWs& w) {
+  if (tc_scaled(kind)) return LU_ERR_UNSUPPORTED;
+  const int64_t ldk = tc_packed_k(kind, K);
+  const int64_t es = tc_operand_bytes(kind);
+  ProfScope ps("pack_operands", st,
+               (double)((r1 - r0) + (c1 - c0)) * (4.0 * K + (double)es * ldk));
+  if (r1 > r0)
+    LUB_TRY(launch_pack_a(st, kind, r1 - r0, K, a + r0, lda, ws + w.off_a + r0 * ldk * es,
+                          ldk, nullptr));
+  if (c1 > c0)
+    LUB_TRY(launch_pack_b(st, kind, K, c1 - c0, b + c0 * ldb, ldb,
+                          ws + w.off_b + c0 * ldk * es, ldk, nullptr));
+  return LU_SUCCESS;
+}
+
 // C[M x N] -= Ap[r0 .., :] * Bp[:, c0 ..] from packed operands (r0, c0 are
 // row / column offsets into the packed copies; multiples of 128 when the
 // copies carry e4m3 tile scales).
@@ -143,6 +163,8 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
 struct DevStreams {
   cudaStream_t panel = nullptr, update = nullptr, copy = nullptr, side = nullptr;
   cudaEvent_t diag_done = nullptr, small_done = nullptr, big_done = nullptr;
+  cudaEvent_t diag1_done = nullptr, lbig_done = nullptr, psmall_done = nullptr;
+  cudaEvent_t u1_done = nullptr, join_s = nullptr, spack_done = nullptr;
   cudaEvent_t panel_done = nullptr, copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
@@ -166,7 +188,9 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
                            &d.done_with[0], &d.done_with[1], &d.panel_done, &d.copied,
-                           &d.diag_done, &d.small_done, &d.big_done})
+                           &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
+                           &d.lbig_done, &d.psmall_done, &d.u1_done, &d.join_s,
+                           &d.spack_done})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
@@ -394,13 +418,13 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                            const HostSink* sink = nullptr) {
   const int64_t n = p.n, nb = p.nb;
   const bool tc = is_tc(p.outer);
-  TcWs w[2];
+  TcWs w2[2];
   if (tc && n > nb) {
-    w[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
-    w[1] = w[0];
-    const size_t shift = w[0].bytes;
-    w[1].off_a += shift; w[1].off_b += shift; w[1].off_sa += shift;
-    w[1].off_sb += shift; w[1].off_tmp += shift;
+    w2[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
+    w2[1] = w2[0];
+    const size_t shift = w2[0].bytes;
+    w2[1].off_a += shift; w2[1].off_b += shift; w2[1].off_sa += shift;
+    w2[1].off_sb += shift; w2[1].off_tmp += shift;
   }
   const bool la = p.lookahead && n > 2 * nb &&
                   !(tc && tc_scaled(tc_kind(p.outer)) && nb % 128 != 0);
@@ -412,8 +436,8 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       if (tn <= 0) continue;
       if (tc)
         LUB_TRY(tc_pack(st, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
-                        lda, a + ofs + (ofs + nb) * lda, lda, ws, w[0]));
-      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tn, 0, tn, ws, w[0], err, 0));
+                        lda, a + ofs + (ofs + nb) * lda, lda, ws, w2[0]));
+      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tn, 0, tn, ws, w2[0], err, 0));
     }
     if (sink)
       LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h, (size_t)sink->ldh * 4, a, (size_t)lda * 4,
@@ -432,47 +456,187 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     if (e != cudaSuccess && status == LU_SUCCESS) status = LU_ERR_CUDA;
     return status == LU_SUCCESS;
   };
+  cudaStream_t ss = S->side;
+  LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->fork, 0));
+  const int w = p.diag_w;
+  const TcOperand kind = tc_kind(p.outer);
+  // A step takes the deep schedule when its outer block holds two diagonal
+  // blocks and at least two of them remain beyond it (see below).
+  auto deep_step = [&](int64_t o) {
+    const int64_t in_ = std::min(n - o, nb), tn_ = n - (o + nb);
+    return in_ == 2 * w && tn_ >= 2 * w && !(tc && tc_scaled(kind));
+  };
+  bool pre = false;       // this step's first diagonal block is already queued
+  bool prev_deep = false; // the previous step ran the deep schedule
+  auto sink_copy = [&](int64_t ofs, int64_t in) {
+    const float* da = a + ofs + ofs * lda;
+    float* ha = sink->h + ofs + ofs * sink->ldh;
+    if (!ok(cudaMemcpy2DAsync(ha, (size_t)sink->ldh * 4, da, (size_t)lda * 4,
+                              (size_t)(n - ofs) * 4, (size_t)in, cudaMemcpyDeviceToHost,
+                              S->copy)))
+      return false;
+    if (n - ofs - in > 0 &&
+        !ok(cudaMemcpy2DAsync(ha + in * sink->ldh, (size_t)sink->ldh * 4, da + in * lda,
+                              (size_t)lda * 4, (size_t)in * 4, (size_t)(n - ofs - in),
+                              cudaMemcpyDeviceToHost, S->copy)))
+      return false;
+    return true;
+  };
   for (int64_t ofs = 0; ofs < n && status == LU_SUCCESS; ofs += nb, ++step) {
     const int64_t in = std::min(n - ofs, nb);
-    status = factor_block_split(p, sp, S, a, lda, ofs, in, n - ofs, first_bad);
-    if (status != LU_SUCCESS) break;
-    if (sink) {
-      // block column (rows [ofs, n)) and block row (columns [ofs+in, n)) of
-      // this step are final: copy them back while the factorization goes on
-      if (!ok(cudaEventRecord(S->panel_done, sp)) ||
-          !ok(cudaStreamWaitEvent(S->copy, S->panel_done, 0)))
-        break;
-      const float* da = a + ofs + ofs * lda;
-      float* ha = sink->h + ofs + ofs * sink->ldh;
-      if (!ok(cudaMemcpy2DAsync(ha, (size_t)sink->ldh * 4, da, (size_t)lda * 4,
-                                (size_t)(n - ofs) * 4, (size_t)in,
-                                cudaMemcpyDeviceToHost, S->copy)))
-        break;
-      if (n - ofs - in > 0 &&
-          !ok(cudaMemcpy2DAsync(ha + in * sink->ldh, (size_t)sink->ldh * 4, da + in * lda,
-                                (size_t)lda * 4, (size_t)in * 4, (size_t)(n - ofs - in),
-                                cudaMemcpyDeviceToHost, S->copy)))
-        break;
-    }
+    const int64_t updm = n - ofs;
     const int64_t tn = n - (ofs + nb);
-    if (tn <= 0) continue;
     const int buf = (int)(step & 1);
-    const TcWs& wk = w[buf];
-    if (tc) {
-      // U2 of step k-2 read this buffer
-      if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
-      status = tc_pack(sp, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
-                       lda, a + ofs + (ofs + nb) * lda, lda, ws, wk);
+    const TcWs& wk = w2[buf];
+    // the previous step's update of this block column / row ran partly on
+    // the side stream: a deep step only touches the diagonal square on the
+    // panel stream and everything else on the side stream after it, any
+    // other step waits for the side stream first
+    if (prev_deep && !deep_step(ofs) && !ok(cudaStreamWaitEvent(sp, S->u1_done, 0))) break;
+    if (deep_step(ofs)) {
+      // Deep schedule.  Panel stream sp: first diagonal block, the first w
+      // L rows / U columns of its sub-panel and their update of the second
+      // diagonal block, the second diagonal block, the first w L rows / U
+      // columns of the second sub-panel; then the first w x w block of the
+      // next outer block gets this step's update and is factored at once.
+      // Side stream ss: the rest of both sub-panels and of the first one's
+      // update, the rest of the operand packing and of the next block
+      // column / row update (U1).  Low-priority stream su: U2 as before.
+      float* blk = a + ofs + ofs * lda;
+      float* dg1 = blk + w + (int64_t)w * lda;
+      const int64_t big = updm - 2 * w;
+      if (!pre) {
+        ProfScope ps("diag_factor", sp, 8.0 * w * w, 2.0 * w * w * w / 3.0);
+        if ((status = launch_diag_factor(sp, blk, lda, w, ofs, first_bad)) != LU_SUCCESS) break;
+        if (!ok(cudaEventRecord(S->diag_done, sp))) break;
+      }
+      {
+        ProfScope ps("lupanel", sp, 16.0 * w * w, 4.0 * (double)w * w * w);
+        if ((status = launch_lupanel(sp, blk, lda, w, w, w, false, 0, 0)) != LU_SUCCESS) break;
+      }
+      if (!ok(cudaEventRecord(S->small_done, sp))) break;
+      if (!ok(cudaStreamWaitEvent(ss, S->diag_done, 0))) break;
+      {
+        ProfScope ps("lupanel", ss, 16.0 * big * w, 4.0 * big * (double)w * w);
+        if ((status = launch_lupanel(ss, blk, lda, w, big, big, false, w, w)) != LU_SUCCESS)
+          break;
+      }
+      if (!ok(cudaStreamWaitEvent(ss, S->small_done, 0))) break;
+      {
+        ProfScope ps("sgemm_chunk8", ss, 0.0, 4.0 * (double)big * w * w);
+        status = launch_sgemm_chunk8_2(ss, big, w, w, blk + 2 * w, lda, blk + (int64_t)w * lda,
+                                       lda, blk + 2 * w + (int64_t)w * lda, lda, w, big, w,
+                                       blk + w, lda, blk + 2 * (int64_t)w * lda, lda,
+                                       blk + w + 2 * (int64_t)w * lda, lda);
+        if (status != LU_SUCCESS) break;
+      }
+      if (!ok(cudaEventRecord(S->big_done, ss))) break;
+      {
+        ProfScope ps("sgemm_chunk8", sp, 0.0, 2.0 * (double)w * w * w);
+        status = launch_sgemm_chunk8_2(sp, w, w, w, blk + w, lda, blk + (int64_t)w * lda, lda,
+                                       dg1, lda, 0, 0, 0, nullptr, lda, nullptr, lda, nullptr,
+                                       lda);
+        if (status != LU_SUCCESS) break;
+      }
+      {
+        ProfScope ps("diag_factor", sp, 8.0 * w * w, 2.0 * w * w * w / 3.0);
+        if ((status = launch_diag_factor(sp, dg1, lda, w, ofs + w, first_bad)) != LU_SUCCESS)
+          break;
+      }
+      if (!ok(cudaEventRecord(S->diag1_done, sp))) break;
+      if (!ok(cudaStreamWaitEvent(sp, S->big_done, 0))) break;
+      {
+        ProfScope ps("lupanel", sp, 16.0 * w * w, 4.0 * (double)w * w * w);
+        if ((status = launch_lupanel(sp, dg1, lda, w, w, w, false, 0, 0)) != LU_SUCCESS) break;
+      }
+      if (!ok(cudaEventRecord(S->psmall_done, sp))) break;
+      if (!ok(cudaStreamWaitEvent(ss, S->diag1_done, 0))) break;
+      {
+        ProfScope ps("lupanel", ss, 16.0 * (big - w) * w, 4.0 * (big - w) * (double)w * w);
+        if ((status = launch_lupanel(ss, dg1, lda, w, big - w, big - w, false, w, w)) !=
+            LU_SUCCESS)
+          break;
+      }
+      if (!ok(cudaEventRecord(S->lbig_done, ss))) break;
+      if (sink) {
+        if (!ok(cudaStreamWaitEvent(S->copy, S->psmall_done, 0)) ||
+            !ok(cudaStreamWaitEvent(S->copy, S->lbig_done, 0)) || !sink_copy(ofs, in))
+          break;
+      }
+      // L21 rows / U12 columns relative to the trailing part (ofs + nb)
+      const float* L21 = a + (ofs + nb) + ofs * lda;
+      const float* U12 = a + ofs + (ofs + nb) * lda;
+      // the nb x nb diagonal square of the next outer block: its update by
+      // this step stays on the panel stream, so the next step's panel never
+      // waits for the side stream's share of U1
+      const int64_t sq = std::min(nb, tn);
+      if (tc) {
+        if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
+        if ((status = tc_pack_range(sp, kind, 0, sq, 0, sq, nb, L21, lda, U12, lda, ws, wk)) !=
+            LU_SUCCESS)
+          break;
+      }
+      // the rest of U1 on the side stream reads these packed rows / columns
+      // (or, on the FP32 path, the second sub-panel's first L rows / U columns)
+      if (!ok(cudaEventRecord(S->spack_done, sp))) break;
+      if (step > 0 && !ok(cudaStreamWaitEvent(sp, S->updated, 0))) break;
+      if ((status = outer_update(p, sp, a, lda, ofs, 0, sq, 0, sq, ws, wk, err, 1)) !=
+          LU_SUCCESS)
+        break;
+      pre = deep_step(ofs + nb);
+      if (pre) {
+        ProfScope ps("diag_factor", sp, 8.0 * w * w, 2.0 * w * w * w / 3.0);
+        float* nblk = a + (ofs + nb) + (ofs + nb) * lda;
+        if ((status = launch_diag_factor(sp, nblk, lda, w, ofs + nb, first_bad)) != LU_SUCCESS)
+          break;
+        if (!ok(cudaEventRecord(S->diag_done, sp))) break;
+      }
+      // side stream: the rest of the packing and of U1
+      if (tc) {
+        if (step >= 2 && !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))) break;
+        if ((status = tc_pack_range(ss, kind, sq, tn, sq, tn, nb, L21, lda, U12, lda, ws,
+                                    wk)) != LU_SUCCESS)
+          break;
+      }
+      if (!ok(cudaEventRecord(S->packed, ss))) break;
+      if (!ok(cudaStreamWaitEvent(ss, S->spack_done, 0))) break;
+      if (step > 0 && !ok(cudaStreamWaitEvent(ss, S->updated, 0))) break;
+      // U1 minus the square: block column below it, block row right of it
+      status = outer_update(p, ss, a, lda, ofs, sq, tn - sq, 0, sq, ws, wk, err, 1);
+      if (status == LU_SUCCESS)
+        status = outer_update(p, ss, a, lda, ofs, 0, sq, sq, tn - sq, ws, wk, err, 1);
+      if (status != LU_SUCCESS) break;
+      if (!ok(cudaEventRecord(S->u1_done, ss))) break;
+      prev_deep = true;
+    } else {
+      status = factor_block_split(p, sp, S, a, lda, ofs, in, updm, first_bad);
+      if (status != LU_SUCCESS) break;
+      if (sink) {
+        // block column (rows [ofs, n)) and block row (columns [ofs+in, n)) of
+        // this step are final: copy them back while the factorization goes on
+        if (!ok(cudaEventRecord(S->panel_done, sp)) ||
+            !ok(cudaStreamWaitEvent(S->copy, S->panel_done, 0)) || !sink_copy(ofs, in))
+          break;
+      }
+      prev_deep = false;
+      pre = false;
+      if (tn <= 0) continue;
+      if (tc) {
+        // U2 of step k-2 read this buffer
+        if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
+        status = tc_pack(sp, kind, tn, tn, nb, a + (ofs + nb) + ofs * lda, lda,
+                         a + ofs + (ofs + nb) * lda, lda, ws, wk);
+        if (status != LU_SUCCESS) break;
+      }
+      if (!ok(cudaEventRecord(S->packed, sp))) break;
+      // U1 after U2a of the previous step (same elements, earlier step first)
+      if (step > 0 && !ok(cudaStreamWaitEvent(sp, S->updated, 0))) break;
+      const int64_t b = std::min(nb, tn);
+      status = outer_update(p, sp, a, lda, ofs, 0, tn, 0, b, ws, wk, err, 1);
+      if (status == LU_SUCCESS && tn > nb)
+        status = outer_update(p, sp, a, lda, ofs, 0, nb, nb, tn - nb, ws, wk, err, 1);
       if (status != LU_SUCCESS) break;
     }
-    if (!ok(cudaEventRecord(S->packed, sp))) break;
-    // U1 after U2a of the previous step (same elements, earlier step first)
-    if (step > 0 && !ok(cudaStreamWaitEvent(sp, S->updated, 0))) break;
-    const int64_t b = std::min(nb, tn);
-    status = outer_update(p, sp, a, lda, ofs, 0, tn, 0, b, ws, wk, err, 1);
-    if (status == LU_SUCCESS && tn > nb)
-      status = outer_update(p, sp, a, lda, ofs, 0, nb, nb, tn - nb, ws, wk, err, 1);
-    if (status != LU_SUCCESS) break;
     if (tn > nb) {
       if (!ok(cudaStreamWaitEvent(su, S->packed, 0))) break;
       // U2a: block column and row k+2 (rows / columns [nb, 2nb) of the trailing part)
@@ -490,16 +654,19 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
         if (status != LU_SUCCESS) break;
       }
       if (!ok(cudaEventRecord(S->done_with[buf], su))) break;
-    } else {
-      if (!ok(cudaEventRecord(S->updated, sp))) break;
-      if (!ok(cudaEventRecord(S->done_with[buf], sp))) break;
+    } else if (tn > 0) {
+      cudaStream_t last = prev_deep ? ss : sp;
+      if (!ok(cudaEventRecord(S->updated, last))) break;
+      if (!ok(cudaEventRecord(S->done_with[buf], last))) break;
     }
   }
   // join (also on the error path, so the caller's stream stays ordered)
   cudaEventRecord(S->join_p, sp);
   cudaEventRecord(S->join_u, su);
+  cudaEventRecord(S->join_s, S->side);
   cudaStreamWaitEvent(st, S->join_p, 0);
   cudaStreamWaitEvent(st, S->join_u, 0);
+  cudaStreamWaitEvent(st, S->join_s, 0);
   if (sink) {
     cudaEventRecord(S->copied, S->copy);
     cudaStreamWaitEvent(st, S->copied, 0);

@@ -20,6 +20,7 @@ struct Rec {
   const char* name;
   cudaEvent_t a, b;
   double bytes, flops;
+  cudaStream_t st;
 };
 
 std::atomic<long long> g_launches{0};
@@ -48,7 +49,7 @@ ProfScope::ProfScope(const char* name, cudaStream_t st, double bytes,
     : st_(st), idx_(-1) {
   if (!g_on.load(std::memory_order_relaxed)) return;
   std::lock_guard<std::mutex> lk(g_mu);
-  Rec r{name, get_event(), get_event(), bytes, flops};
+  Rec r{name, get_event(), get_event(), bytes, flops, st};
   cudaEventRecord(r.a, st);
   g_recs.push_back(r);
   idx_ = (int)g_recs.size() - 1;
@@ -94,6 +95,32 @@ LU_API int lu_profile_end(lu_profile_entry* out, int max_entries) {
   int k = 0;
   for (auto& kv : agg) {
     if (out && k < max_entries) out[k] = kv.second;
+    ++k;
+  }
+  return k;
+}
+
+LU_API int lu_profile_trace(lu_trace_entry* out, int max_entries) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_recs.empty()) return 0;
+  std::map<cudaStream_t, int> ids;
+  int k = 0;
+  for (auto& r : g_recs) {
+    if (g_on.load()) break;  // only after lu_profile_end
+    if (out && k < max_entries) {
+      lu_trace_entry& e = out[k];
+      std::memset(&e, 0, sizeof(e));
+      std::strncpy(e.name, r.name, sizeof(e.name) - 1);
+      auto it = ids.find(r.st);
+      if (it == ids.end()) it = ids.emplace(r.st, (int)ids.size()).first;
+      e.stream = it->second;
+      float t0 = 0.0f, t1 = 0.0f;
+      cudaEventSynchronize(r.b);
+      if (cudaEventElapsedTime(&t0, g_recs[0].a, r.a) != cudaSuccess) t0 = 0.0f;
+      if (cudaEventElapsedTime(&t1, g_recs[0].a, r.b) != cudaSuccess) t1 = 0.0f;
+      e.start_ms = t0;
+      e.end_ms = t1;
+    }
     ++k;
   }
   return k;

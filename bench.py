@@ -374,13 +374,20 @@ def main() -> None:
             achieved = ent["bytes"] / (ent["total_ms"] / 1e3) / 1e9
             peak = peaks["hbm_gbs"]
             tr = profiled_traffic(f"tc_update_{args.workload}")
+            alg = ent["bytes"] / ent["launches"]
+            # DRAM traffic of one captured launch over its algorithmic bytes,
+            # applied to the average launch (traffic grows with the C term)
+            traffic = tr["traffic_over_algorithmic"] * alg if tr else None
             roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved,
                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "peak_source": peaks["source"] + " hbm_gbs",
-                        "traffic": tr.get("dram_bytes_per_launch") if tr else None,
-                        "algorithmic_bytes_per_launch": ent["bytes"] / ent["launches"],
+                        "traffic": traffic,
+                        "traffic_source": ("ncu dram bytes of one launch "
+                                           f"(profiles/tc_update_{args.workload}.json) "
+                                           "scaled to the average launch") if tr else None,
+                        "algorithmic_bytes_per_launch": alg,
                         "avg_launch_ms": avg_ms, "launches": ent["launches"],
-                        "time_share": ent["total_ms"] / ms}
+                        "event_time_over_wall": ent["total_ms"] / ms}
         else:
             achieved = ent["flops"] / (ent["total_ms"] / 1e3) / 1e12
             roofline = {"kernel": dom, "bound": "fp32-simt", "achieved": achieved,
@@ -388,7 +395,7 @@ def main() -> None:
                         "note": "FP32 SIMT GEMM (no tensor cores on the FP32 plain path)",
                         "traffic": None, "avg_launch_ms": avg_ms,
                         "launches": ent["launches"],
-                        "time_share": ent["total_ms"] / ms}
+                        "event_time_over_wall": ent["total_ms"] / ms}
     line = {
         "metric": "LU TFLOP/s (2n^3/3)",
         "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,

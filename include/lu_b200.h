@@ -189,7 +189,10 @@ LU_API lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
 
 /* op(A) X = B with the in-place factors of A (fp32, ldlu): trans = 0 solves
  * L U X = B, trans = 1 solves (L U)^T X = B.  d_x (fp64, n x nrhs, ldx)
- * holds B on entry and X on exit.  fp64 arithmetic throughout. */
+ * holds B on entry and X on exit.  fp64 arithmetic throughout.  One launch
+ * per triangle; a few counter words come from cudaMallocAsync on the
+ * stream (lu_refine_c and lu_refine_static_c take them from their own
+ * scratch instead). */
 LU_API lu_status lu_solve_c(lu_stream_t stream, int64_t n, const float* d_lu,
                             int64_t ldlu, double* d_x, int64_t ldx,
                             int64_t nrhs, int trans);

@@ -23,12 +23,13 @@ using namespace lub;
 namespace {
 
 struct RefineWs {
-  size_t off_r, off_d, off_p, off_max, bytes;
+  size_t off_r, off_d, off_p, off_max, off_sync, bytes;
 };
 
 // Residuals and corrections of all nrhs columns, one set of chunk partial
 // sums (the columns' residuals run one after another), and per column the
-// three maxima of the backward error plus the matrix norm.
+// three maxima of the backward error plus the matrix norm; the counters of
+// the triangular solves.
 RefineWs refine_layout(int64_t n, int64_t nrhs = 1) {
   RefineWs w;
   size_t off = 0;
@@ -36,6 +37,7 @@ RefineWs refine_layout(int64_t n, int64_t nrhs = 1) {
   w.off_d = off; off = align_up(off + (size_t)n * nrhs * 8, 256);
   w.off_p = off; off = align_up(off + residual_ws_bytes(n), 256);
   w.off_max = off; off = align_up(off + (size_t)(3 * nrhs + 1) * 8, 256);
+  w.off_sync = off; off = align_up(off + trsm_sync_bytes(nrhs), 256);
   w.bytes = off;
   return w;
 }
@@ -69,13 +71,12 @@ LU_API lu_status lu_solve_c(lu_stream_t stream, int64_t n, const float* d_lu,
   if (!d_lu || !d_x) return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device_local());
   cudaStream_t st = (cudaStream_t)stream;
-  if (!trans) {  // L U x = b: L y = b, then U x = y
-    LUB_TRY(launch_trsm(st, n, d_lu, ldlu, d_x, ldx, nrhs, false, false));
-    return launch_trsm(st, n, d_lu, ldlu, d_x, ldx, nrhs, true, false);
-  }
-  // (L U)^T x = U^T L^T x = b: U^T y = b, then L^T x = y
-  LUB_TRY(launch_trsm(st, n, d_lu, ldlu, d_x, ldx, nrhs, true, true));
-  return launch_trsm(st, n, d_lu, ldlu, d_x, ldx, nrhs, false, true);
+  // the solve's few counter words come from the stream-ordered allocator
+  void* sync = nullptr;
+  if (cudaMallocAsync(&sync, trsm_sync_bytes(nrhs), st) != cudaSuccess) return LU_ERR_ALLOC;
+  const lu_status s = launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync);
+  cudaFreeAsync(sync, st);
+  return s;
 }
 
 LU_API lu_status lu_refine_workspace_size(int64_t n, size_t* bytes) {
@@ -109,7 +110,8 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
                 : launch_norm_inf(st, n, d_a, lda, P, mnorm));
   LUB_CUDA_TRY(cudaMemcpy2DAsync(d_x, (size_t)ldx * 8, d_b, (size_t)ldb * 8, (size_t)n * 8,
                                  (size_t)nrhs, cudaMemcpyDeviceToDevice, st));
-  LUB_TRY(lu_solve_c(stream, n, d_lu, ldlu, d_x, ldx, nrhs, trans));
+  void* sync = wb + w.off_sync;
+  LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync));
   for (;;) {
     for (int64_t c = 0; c < nrhs; ++c) {
       const double* b = d_b + c * ldb;
@@ -134,7 +136,7 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
     }
     if (std::isnan(e) || e <= tol || it >= max_iter) break;
     LUB_CUDA_TRY(cudaMemcpyAsync(D, R, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, st));
-    LUB_TRY(lu_solve_c(stream, n, d_lu, ldlu, D, n, nrhs, trans));
+    LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, D, n, nrhs, trans != 0, sync));
     for (int64_t c = 0; c < nrhs; ++c) LUB_TRY(launch_axpy(st, n, D + c * n, d_x + c * ldx));
     ++it;
   }

@@ -7,10 +7,16 @@ namespace lub {
 
 // op(T) X = X in place, T = the unit-lower L (upper = false) or the upper U
 // (upper = true) of the in-place factors lu (fp32, ld); op = T or T^T;
-// X fp64 n x nrhs (ldx).
+// X fp64 n x nrhs (ldx).  One launch; sync = trsm_sync_bytes(nrhs) bytes of
+// device memory (cleared on the stream before the launch), not shared with
+// a solve in flight on another stream.
+size_t trsm_sync_bytes(int64_t nrhs);
 lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                       double* X, int64_t ldx, int64_t nrhs, bool upper,
-                      bool trans);
+                      bool trans, void* sync);
+// X <- (L U)^-1 X (trans: (L U)^-T X): two launch_trsm.
+lu_status launch_lu_solve(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
+                          double* X, int64_t ldx, int64_t nrhs, bool trans, void* sync);
 
 // Workspace (bytes) of launch_residual / launch_norm_inf for size n.
 size_t residual_ws_bytes(int64_t n);

@@ -95,3 +95,54 @@ def test_refine_reports_non_convergence(built):
     assert it == 0 and be > 1e-14
     with pytest.raises(rb._lib.LuError):
         rb.refine(da, lu, b, tol=1e-14, max_iter=0, raise_on_stall=True)
+
+
+@pytest.mark.parametrize("n,nrhs,lda_pad,x_off", [
+    (64, 1, 0, 0), (65, 3, 1, 1), (127, 9, 3, 0), (500, 17, 1, 1), (1027, 2, 0, 1),
+    (2111, 4, 2, 1), (3000, 1, 0, 0)])
+def test_solve_layouts_and_groups(built, n, nrhs, lda_pad, x_off):
+    """Ragged row blocks, right-hand-side groups of 1/2/4/8 with a partial last
+    group, a leading dimension that is not a multiple of 4 (4-byte tile copies)
+    and right-hand sides that start off a 16-byte boundary with an odd leading
+    dimension (solution blocks read without cp.async)."""
+    a, dlu0, lu = factors(n, seed=n)
+    dlu = rb.colmajor_empty(n, n, n + lda_pad, torch.float32)
+    dlu.copy_(dlu0)
+    L = np.tril(lu.astype(np.float64), -1) + np.eye(n)
+    U = np.triu(lu.astype(np.float64))
+    rng = np.random.default_rng(n + nrhs)
+    B = rng.standard_normal((n, nrhs))
+    for trans in (False, True):
+        M = (L @ U).T if trans else L @ U
+        want = np.linalg.solve(M, B)
+        buf = rb.colmajor_empty(n + x_off, nrhs, n + x_off + (1 if x_off else 0),
+                                torch.float64)
+        X = buf[x_off:, :]
+        X.copy_(torch.from_numpy(B))
+        rb.lu_solve(dlu, X, trans=trans)
+        got = X.cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max(), (trans, n, nrhs)
+
+
+def test_solve_large_single_rhs(built):
+    """n = 8192: 128 row blocks, most of them streaming a backlog of tiles."""
+    from scipy.linalg import solve_triangular
+    n = 8192
+    a = O.gen_matrix(n, seed=5, kind=1, alpha=1.5)
+    da = to_dev(a)
+    rb.lu_nopiv_rl(da, nb=256, outer=rb.TC32)
+    torch.cuda.synchronize()
+    lu = np.asfortranarray(da.cpu().numpy())
+    f = lu.astype(np.float64)
+    rng = np.random.default_rng(3)
+    b = rng.standard_normal(n)
+    for trans in (False, True):
+        if trans:
+            want = solve_triangular(f, b, lower=False, trans="T")
+            want = solve_triangular(f, want, lower=True, unit_diagonal=True, trans="T")
+        else:
+            want = O.lu_solve_f64(lu, b)
+        x = torch.from_numpy(b.copy()).cuda()
+        rb.lu_solve(da, x, trans=trans)
+        got = x.cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-11 * np.abs(want).max(), trans

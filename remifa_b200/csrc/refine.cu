@@ -71,11 +71,14 @@ LU_API lu_status lu_solve_c(lu_stream_t stream, int64_t n, const float* d_lu,
   if (!d_lu || !d_x) return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device_local());
   cudaStream_t st = (cudaStream_t)stream;
-  // the solve's few counter words come from the stream-ordered allocator
-  void* sync = nullptr;
-  if (cudaMallocAsync(&sync, trsm_sync_bytes(nrhs), st) != cudaSuccess) return LU_ERR_ALLOC;
-  const lu_status s = launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync);
-  cudaFreeAsync(sync, st);
+  // the solve's counter words and right-hand-side copy come from the
+  // stream-ordered allocator
+  void* ws = nullptr;
+  if (cudaMallocAsync(&ws, trsm_ws_bytes(n, nrhs), st) != cudaSuccess) return LU_ERR_ALLOC;
+  const lu_status s = launch_lu_solve(
+      st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, static_cast<unsigned*>(ws),
+      reinterpret_cast<double*>(static_cast<char*>(ws) + trsm_sync_bytes(nrhs)));
+  cudaFreeAsync(ws, st);
   return s;
 }
 
@@ -110,8 +113,10 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
                 : launch_norm_inf(st, n, d_a, lda, P, mnorm));
   LUB_CUDA_TRY(cudaMemcpy2DAsync(d_x, (size_t)ldx * 8, d_b, (size_t)ldb * 8, (size_t)n * 8,
                                  (size_t)nrhs, cudaMemcpyDeviceToDevice, st));
-  void* sync = wb + w.off_sync;
-  LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync));
+  // the solves copy their right-hand sides into R (free until the next
+  // residual) and count tickets in the sync words
+  unsigned* sync = reinterpret_cast<unsigned*>(wb + w.off_sync);
+  LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync, R));
   for (;;) {
     for (int64_t c = 0; c < nrhs; ++c) {
       const double* b = d_b + c * ldb;
@@ -136,7 +141,7 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
     }
     if (std::isnan(e) || e <= tol || it >= max_iter) break;
     LUB_CUDA_TRY(cudaMemcpyAsync(D, R, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, st));
-    LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, D, n, nrhs, trans != 0, sync));
+    LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, D, n, nrhs, trans != 0, sync, R));
     for (int64_t c = 0; c < nrhs; ++c) LUB_TRY(launch_axpy(st, n, D + c * n, d_x + c * ldx));
     ++it;
   }

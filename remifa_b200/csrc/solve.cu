@@ -10,23 +10,21 @@
 // factorization error -- what iterative refinement in fp64 needs.
 //
 // op(T) X = B, T = L (unit lower) or U (upper), op = identity or transpose,
-// runs as ONE launch per triangle (trsv_kernel): a CTA per (row block of 64
-// rows, group of up to 8 right-hand sides).  CTAs draw tickets in solve
-// order (an atomic counter), so a CTA only ever waits for CTAs that are
-// already running: no deadlock whatever the residency.  Row block t
-// streams the 64 x 64 tiles op(T)[t, q] of the blocks solved before it
-// through a cp.async ring in shared memory, consuming each as soon as that
-// block's solution is published (a per-group counter of finished blocks,
-// release / acquire at GPU scope) and accumulating per lane in fp64; tiles
-// are fetched ahead of the solve front, so the factor streams at memory
-// speed while the front advances.  The diagonal block is inverted (fp64
-// substitution, off the critical path while the CTA waits) and applied as
-// a 64 x 64 product, so the step that hands the solution from block to
-// block is one tile product, one shuffle reduction and one small product.
-// Every wait is bounded (a few seconds of %globaltimer); on expiry the CTA
-// raises the abort word, every later CTA stops waiting, and the rows of the
-// CTAs that gave up are written as NaN, so a failed solve never looks like
-// a result.
+// runs as one launch per triangle (trsv_kernel) after a copy kernel that
+// moves B aside and marks every entry of X pending (a signalling-NaN
+// pattern no arithmetic produces).  A CTA per (row block of 64 rows, group
+// of up to 8 right-hand sides); CTAs draw tickets in solve order (an atomic
+// counter), so a CTA only ever waits for CTAs already running: no deadlock
+// whatever the residency.  Each warp of a CTA owns 8 rows of the block and
+// streams its share of the tiles op(T)[t, q] of the blocks solved earlier
+// through its own cp.async ring, reading the solution entries it needs
+// straight from X (relaxed loads at GPU scope, re-read while pending; the
+// solution IS the flag, so publishing a block costs one store, no fence and
+// no counter).  The diagonal block is inverted in fp64 and the last tile is
+// folded into W = Dinv op(T)[t, t-1] while the CTA waits, so the hand-over
+// from block t-1 to block t is, per warp and without a CTA barrier:
+// x_t = Dinv (b - sum_{q<t-1} op(T)[t,q] x_q) - W x_{t-1}, i.e. 16 fma per
+// lane and one shuffle reduction after x_{t-1} lands.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "solve.cuh"
@@ -39,43 +37,25 @@ constexpr int kT = 256;    // threads per CTA of the residual kernels
 namespace trsv {
 
 constexpr int BS = 64;                 // rows of a row block = columns of a tile
-constexpr int kThreads = 256;          // 8 warps; warp w owns rows 8w .. 8w+7
-constexpr int S = 4;                   // ring stages
-constexpr int kSyncHeader = 4;         // ticket, abort, timeouts, spare
+constexpr int kThreads = 256;          // 8 warps
 constexpr unsigned long long kWaitNs = 4000000000ull;  // bound of one wait
-
-__host__ __device__ constexpr size_t smem_bytes(int nr) {
-  return (size_t)S * BS * BS * 4          // fp32 tiles
-         + (size_t)S * nr * BS * 8        // fp64 solution blocks of the tiles
-         + (size_t)BS * BS * 8            // inverse of the diagonal block
-         + (size_t)nr * BS * 8            // right-hand side / y
-         + (size_t)4 * nr * BS * 8        // partial sums of the final product
-         + 64;                            // control words
-}
 
 struct Args {
   const float* lu;
   int64_t ld;
-  double* X;
+  double* X;        // solutions, written in place
   int64_t ldx;
+  const double* B;  // right-hand sides (n x nrhs, ld n) of the warp kernel
   int64_t n;
   int64_t nrhs;
   int nblk;
   int ngroups;
-  int forward;   // op(T) lower: L or U^T
-  int unit;      // unit diagonal: L or L^T
-  int xvec;      // X 16-byte aligned with even ldx: solution blocks by cp.async
+  int forward;      // op(T) lower: L or U^T
+  int unit;         // unit diagonal: L or L^T
+  int xvec;         // X 16-byte aligned with even ldx (group kernel: cp.async)
   unsigned* sync;
 };
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -100,19 +80,17 @@ __device__ __forceinline__ void cp_wait() {
 
 __device__ __forceinline__ int imin64(int64_t a, int b) { return a < b ? (int)a : b; }
 
-// Shared-memory layout of a 64 x 64 tile of op(T) (rows r, columns k).
-// Not transposed: column k of op(T) is column k0+k of the factor, contiguous
-// in r; stored by 16-byte chunks (4 rows) with chunk index q ^ (k & 7), so
-// that 8 lanes reading chunk q of 8 consecutive columns hit 8 different
-// bank groups.  Transposed: row r of op(T) is contiguous in k; stored
-// row-major, lanes read consecutive k.
+// Shared layout of a full 64 x 64 tile of op(T) (rows r, columns k).  Not
+// transposed: column k contiguous in r, by 16-byte chunks with chunk index
+// (r/4) ^ (k & 7) (8 lanes reading one chunk of 8 consecutive columns hit 8
+// bank groups).  Transposed: row-major.
 template <bool TRANS>
 __device__ __forceinline__ int tile_index(int r, int k) {
   return TRANS ? r * BS + k : k * BS + 4 * ((r >> 2) ^ (k & 7)) + (r & 3);
 }
 
-// Issue the copy of tile op(T)[rows r0.., cols k0..] (rw x kw valid, the
-// rest zero) into dst.
+// Copy of the full tile op(T)[rows r0.., cols k0..] (rw x kw valid, the rest
+// zero), all threads of the CTA.
 template <bool TRANS, bool V16>
 __device__ __forceinline__ void load_tile(float* dst, const Args& a, int64_t r0, int rw,
                                           int64_t k0, int kw) {
@@ -121,9 +99,9 @@ __device__ __forceinline__ void load_tile(float* dst, const Args& a, int64_t r0,
 #pragma unroll
     for (int m = 0; m < BS * BS / 4 / kThreads; ++m) {
       const int c = tid + m * kThreads;
-      const int outer = c >> 4, q = c & 15;   // outer: k (or r), q: chunk of 4
-      int64_t mcol, mrow;                     // memory column, first memory row
-      int valid;                              // valid elements of the chunk
+      const int outer = c >> 4, q = c & 15;
+      int64_t mcol, mrow;
+      int valid;
       if (!TRANS) {
         mcol = k0 + outer; mrow = r0 + 4 * q;
         valid = outer < kw ? min(4, max(0, rw - 4 * q)) : 0;
@@ -153,8 +131,8 @@ __device__ __forceinline__ void load_tile(float* dst, const Args& a, int64_t r0,
   }
 }
 
-// Issue the copy of the diagonal block as plain fp32: memory column c,
-// memory row r of the block at c * 64 + r (the rest zero).
+// Copy of the diagonal block as plain fp32: memory column c, memory row r of
+// the block at c * 64 + r (the rest zero), all threads of the CTA.
 template <bool V16>
 __device__ __forceinline__ void load_diag(float* dst, const Args& a, int64_t r0, int rw) {
   const int tid = threadIdx.x;
@@ -179,9 +157,487 @@ __device__ __forceinline__ void load_diag(float* dst, const Args& a, int64_t r0,
   }
 }
 
+// Inverse of the diagonal block of op(T) (fp32 in Dsrc as load_diag left it)
+// by fp64 substitution with the reciprocals of the diagonal: column j by
+// lanes 4j .. 4j+3, part p holding rows 4s + p.  Written row-major into
+// Dinv[r * 64 + j] (the same space as Dsrc; a barrier separates the reads
+// from the writes).  Rows and columns past rw are the identity.  All threads.
+template <bool TRANS>
+__device__ __forceinline__ void invert_diag(const float* Dsrc, double* Dinv, double* rdiag,
+                                            int rw, bool fwd, bool unit) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  auto D = [&](int r, int k) -> double {
+    return (double)(TRANS ? Dsrc[r * BS + k] : Dsrc[k * BS + r]);
+  };
+  if (tid < BS) rdiag[tid] = (unit || tid >= rw) ? 1.0 : 1.0 / D(tid, tid);
+  __syncthreads();
+  const int j = tid >> 2, p = tid & 3;
+  double z[16];
+#pragma unroll
+  for (int s = 0; s < 16; ++s) z[s] = (4 * s + p == j) ? 1.0 : 0.0;
+  if (fwd) {
+#pragma unroll
+    for (int k = 0; k < BS; ++k) {
+      const bool live = k >= j;
+      if (live && p == (k & 3)) z[k >> 2] *= rdiag[k];
+      const double zk = __shfl_sync(0xffffffffu, z[k >> 2], (lane & ~3) | (k & 3));
+      if (live) {
+#pragma unroll
+        for (int s = 0; s < 16; ++s)
+          if (4 * s + p > k) z[s] = fma(-D(4 * s + p, k), zk, z[s]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = BS - 1; k >= 0; --k) {
+      const bool live = k <= j;
+      if (live && p == (k & 3)) z[k >> 2] *= rdiag[k];
+      const double zk = __shfl_sync(0xffffffffu, z[k >> 2], (lane & ~3) | (k & 3));
+      if (live) {
+#pragma unroll
+        for (int s = 0; s < 16; ++s)
+          if (4 * s + p < k) z[s] = fma(-D(4 * s + p, k), zk, z[s]);
+      }
+    }
+  }
+  __syncthreads();  // every read of the fp32 block precedes the overwrite
+#pragma unroll
+  for (int s = 0; s < 16; ++s) Dinv[(4 * s + p) * BS + j] = z[s];
+  __syncthreads();
+}
+
+// Sum over the 32 lanes of each of 8 per-lane partial rows: three halving
+// exchanges, then two full steps.  Lanes 4i .. 4i+3 end with row i.
+__device__ __forceinline__ double row_reduce(double (&v)[8], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double send = b4 ? v[i] : v[i + 4];
+    const double keep = b4 ? v[i + 4] : v[i];
+    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double send = b3 ? v[i] : v[i + 2];
+    const double keep = b3 ? v[i + 2] : v[i];
+    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  double s;
+  {
+    const double send = b2 ? v[0] : v[1];
+    const double keep = b2 ? v[1] : v[0];
+    s = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  return s;
+}
+
+// ======================================================================
+// Warp kernel (groups of 1 or 2 right-hand sides).  X is marked pending by
+// trsv_prepare_kernel; a solution entry is published by one store and read
+// by relaxed loads at GPU scope, re-read while pending -- the solution is
+// its own flag.
+// ======================================================================
+
+constexpr int S = 3;                   // stages of each warp's tile ring
+constexpr int kWarpTile = 8 * BS;      // floats of a warp's share of a tile
+// Marks a solution entry not yet published: a signalling-NaN payload that no
+// arithmetic produces (published NaNs are stored as the canonical quiet NaN).
+constexpr unsigned long long kPending = 0x7ff4dead5e1f5e1full;
+constexpr unsigned long long kQuietNaN = 0x7ff8000000000000ull;
+
+__host__ __device__ constexpr size_t warp_smem_bytes(int nr) {
+  return (size_t)S * 8 * kWarpTile * 4    // per-warp tile rings (fp32)
+         + (size_t)BS * BS * 8            // inverse of the diagonal block (fp64)
+         + (size_t)BS * BS * 4            // tile of the previous block (fp32)
+         + (size_t)8 * nr * BS * 8        // per-warp partial sums
+         + (size_t)BS * 8                 // reciprocals of the diagonal
+         + 64;                            // control words
+}
+
+__device__ __forceinline__ double ld_poll(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ void st_publish(double* p, double x) {
+  unsigned long long v = (unsigned long long)__double_as_longlong(x);
+  if ((v & 0x7ff0000000000000ull) == 0x7ff0000000000000ull && (v & 0xfffffffffffffull))
+    v = kQuietNaN;
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ bool pending(double x) {
+  return (unsigned long long)__double_as_longlong(x) == kPending;
+}
+
+// A warp's share of a tile.  Transposed (row share): rows 8w .. 8w+7 of the
+// block, row-major [i][k] (each row of op(T) is 256 contiguous bytes of one
+// factor column).  Not transposed (column share): columns 8w .. 8w+7 of the
+// tile, [j][r] (each column 256 contiguous bytes).  Copied by the warp's
+// own lanes.
+template <bool TRANS, bool V16>
+__device__ __forceinline__ void load_warp_tile(float* dst, const Args& a, int64_t r0, int rw,
+                                               int64_t k0, int kw, int w, int lane) {
+  const int b = 8 * w;
+  if (V16) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int c = lane + 32 * m;
+      const int o = c >> 4, q = c & 15;
+      int valid;
+      const float* src;
+      if (!TRANS) {
+        valid = b + o < kw ? min(4, max(0, rw - 4 * q)) : 0;
+        src = valid ? a.lu + (r0 + 4 * q) + (k0 + b + o) * a.ld : a.lu;
+      } else {
+        valid = b + o < rw ? min(4, max(0, kw - 4 * q)) : 0;
+        src = valid ? a.lu + (k0 + 4 * q) + (r0 + b + o) * a.ld : a.lu;
+      }
+      cp16z(dst + o * BS + 4 * q, src, valid * 4);
+    }
+  } else {
+#pragma unroll 4
+    for (int m = 0; m < 16; ++m) {
+      const int e = lane + 32 * m;
+      const int o = e >> 6, i = e & 63;
+      bool ok;
+      const float* src;
+      if (!TRANS) {
+        ok = b + o < kw && i < rw;
+        src = ok ? a.lu + (r0 + i) + (k0 + b + o) * a.ld : a.lu;
+      } else {
+        ok = b + o < rw && i < kw;
+        src = ok ? a.lu + (k0 + i) + (r0 + b + o) * a.ld : a.lu;
+      }
+      cp4z(dst + o * BS + i, src, ok ? 4 : 0);
+    }
+  }
+}
+
+// Solution entries of tile columns kb + h*ks (h < NX) of the group's
+// columns (0 outside the matrix), as loaded -- possibly still pending.
+template <int NX, int NR>
+__device__ __forceinline__ void fetch_x(double (&x)[NX][NR], const Args& a, int64_t k0, int kw,
+                                        int64_t c0, int nc, int kb, int ks) {
+#pragma unroll
+  for (int h = 0; h < NX; ++h)
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      const int k = kb + h * ks;
+      x[h][c] = (k < kw && c < nc) ? ld_poll(a.X + (k0 + k) + (c0 + c) * a.ldx) : 0.0;
+    }
+}
+// Re-read the entries still pending until the whole warp has them.
+// Bounded: after kWaitNs the pending entries become NaN and the count of
+// expired waits is raised; every other wait of the solve then gives up at
+// once, so a lost block costs one bound, not one per block, and its NaN
+// propagates to every later block (a failed solve never looks like a
+// result).
+template <int NX, int NR>
+__device__ __forceinline__ void settle_x(double (&x)[NX][NR], const Args& a, int64_t k0,
+                                         int64_t c0, int kb, int ks, int lane) {
+  bool ok = true;
+#pragma unroll
+  for (int h = 0; h < NX; ++h)
+#pragma unroll
+    for (int c = 0; c < NR; ++c) ok &= !pending(x[h][c]);
+  if (__all_sync(0xffffffffu, ok)) return;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    ok = true;
+#pragma unroll
+    for (int h = 0; h < NX; ++h)
+#pragma unroll
+      for (int c = 0; c < NR; ++c)
+        if (pending(x[h][c])) {
+          x[h][c] = ld_poll(a.X + (k0 + kb + h * ks) + (c0 + c) * a.ldx);
+          ok &= !pending(x[h][c]);
+        }
+    if (__all_sync(0xffffffffu, ok)) return;
+    const bool expired = global_ns() - t0 > kWaitNs;
+    if (__any_sync(0xffffffffu, expired || *(volatile unsigned*)(a.sync + 1) != 0u)) {
+#pragma unroll
+      for (int h = 0; h < NX; ++h)
+#pragma unroll
+        for (int c = 0; c < NR; ++c)
+          if (pending(x[h][c])) x[h][c] = __longlong_as_double((long long)kQuietNaN);
+      if (lane == 0 && expired) atomicAdd(a.sync + 1, 1u);
+      return;
+    }
+  }
+}
+
+// One CTA per (row block, group): warps stream their shares of the tiles
+// of all blocks but the previous one without CTA barriers; one barrier
+// combines the partial sums into c = Dinv y; the hand-over x = c - W x_prev
+// runs per warp (W = Dinv op(T)[block, previous block] in registers: rows
+// 8 warp + i, columns lane and lane + 32).
+template <bool TRANS, int NR, bool V16>
+__global__ void __launch_bounds__(kThreads, 2)
+trsv_kernel(Args a) {
+  constexpr int PD = NR == 1 ? 3 : 2;     // tiles whose solution entries are fetched ahead
+  constexpr int NX = TRANS ? 2 : 1;       // solution entries per lane per tile
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* ring = reinterpret_cast<float*>(smem);
+  double* Dinv = reinterpret_cast<double*>(smem + (size_t)S * 8 * kWarpTile * 4);
+  float* Tw = reinterpret_cast<float*>(Dinv + BS * BS);
+  double* part = reinterpret_cast<double*>(Tw + BS * BS);
+  double* rdiag = part + 8 * NR * BS;
+  int* ctrl = reinterpret_cast<int*>(rdiag + BS);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) ctrl[0] = (int)atomicAdd(a.sync, 1u);
+  __syncthreads();
+  const int ticket = ctrl[0];
+  const int t = ticket / a.ngroups, g = ticket - t * a.ngroups;
+  const bool fwd = a.forward != 0;
+  const int64_t r0 = (int64_t)(fwd ? t : a.nblk - 1 - t) * BS;
+  const int rw = imin64(a.n - r0, BS);
+  const int64_t c0 = (int64_t)g * NR;
+  const int nc = imin64(a.nrhs - c0, NR);
+  auto tile_k0 = [&](int q) -> int64_t { return (int64_t)(fwd ? q : a.nblk - 1 - q) * BS; };
+  auto tile_kw = [&](int q) -> int { return imin64(a.n - tile_k0(q), BS); };
+  const int nbulk = t > 1 ? t - 1 : 0;  // tiles before the previous block's
+  // tile columns whose solution entries this lane reads in the bulk phase
+  const int kb = TRANS ? lane : 8 * warp + (lane & 7);
+  const int ks = TRANS ? 32 : 0;
+
+  // ---- set-up copies: diagonal block, previous block's tile, ring prologue
+  float* Dsrc = reinterpret_cast<float*>(Dinv);
+  load_diag<V16>(Dsrc, a, r0, rw);
+  if (t >= 1) load_tile<TRANS, V16>(Tw, a, r0, rw, tile_k0(t - 1), tile_kw(t - 1));
+  cp_commit();
+  float* wring = ring + warp * S * kWarpTile;
+  auto issue = [&](int q) {
+    if (q < nbulk)
+      load_warp_tile<TRANS, V16>(wring + (q % S) * kWarpTile, a, r0, rw, tile_k0(q),
+                                 tile_kw(q), warp, lane);
+    cp_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < S - 1; ++q) issue(q);
+  double xq[PD][NX][NR];
+#pragma unroll
+  for (int d = 0; d < PD; ++d)
+    if (d < nbulk) fetch_x<NX, NR>(xq[d], a, tile_k0(d), tile_kw(d), c0, nc, kb, ks);
+  // right-hand sides of rows lane and lane + 32
+  double bm[2][NR];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      const int r = lane + 32 * h;
+      bm[h][c] = (r < rw && c < nc) ? a.B[(r0 + r) + (c0 + c) * a.n] : 0.0;
+    }
+
+  cp_wait<S - 1>();
+  __syncthreads();
+  invert_diag<TRANS>(Dsrc, Dinv, rdiag, rw, fwd, a.unit != 0);
+
+  // ---- W = Dinv * op(T)[block, previous block] ----
+  double W[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) W[i][0] = W[i][1] = 0.0;
+  if (t >= 1) {
+#pragma unroll 2
+    for (int m4 = 0; m4 < BS / 4; ++m4) {
+      float tk[2][4];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = lane + 32 * h;
+        if (!TRANS) {
+          const float4 u = *reinterpret_cast<const float4*>(Tw + tile_index<false>(4 * m4, k));
+          tk[h][0] = u.x; tk[h][1] = u.y; tk[h][2] = u.z; tk[h][3] = u.w;
+        } else {
+#pragma unroll
+          for (int mm = 0; mm < 4; ++mm) tk[h][mm] = Tw[tile_index<true>(4 * m4 + mm, k)];
+        }
+      }
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const double d = Dinv[(8 * warp + i) * BS + 4 * m4 + mm];
+          W[i][0] = fma(d, (double)tk[0][mm], W[i][0]);
+          W[i][1] = fma(d, (double)tk[1][mm], W[i][1]);
+        }
+    }
+  }
+
+  // ---- bulk: the tiles before the previous block's, per warp.
+  // Transposed: rows 8 warp + i, per-lane partials over columns lane and
+  // lane + 32.  Not transposed: columns 8 warp + j, per-lane partials of
+  // rows lane and lane + 32 (the solution entry of column j broadcast from
+  // lane j). ----
+  constexpr int NA = TRANS ? 8 : 2;
+  double acc[NA][NR];
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int c = 0; c < NR; ++c) acc[i][c] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < nbulk; ++q) {
+    double x[NX][NR];
+#pragma unroll
+    for (int h = 0; h < NX; ++h)
+#pragma unroll
+      for (int c = 0; c < NR; ++c) x[h][c] = xq[0][h][c];
+#pragma unroll
+    for (int d = 0; d + 1 < PD; ++d)
+#pragma unroll
+      for (int h = 0; h < NX; ++h)
+#pragma unroll
+        for (int c = 0; c < NR; ++c) xq[d][h][c] = xq[d + 1][h][c];
+    if (q + PD < nbulk)
+      fetch_x<NX, NR>(xq[PD - 1], a, tile_k0(q + PD), tile_kw(q + PD), c0, nc, kb, ks);
+    settle_x<NX, NR>(x, a, tile_k0(q), c0, kb, ks, lane);
+    cp_wait<S - 2>();
+    __syncwarp();
+    issue(q + S - 1);
+    const float* Ts = wring + (q % S) * kWarpTile;
+    if (TRANS) {
+#pragma unroll
+      for (int h = 0; h < NX; ++h) {
+        const int k = lane + 32 * h;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const double tv = (double)Ts[i * BS + k];
+#pragma unroll
+          for (int c = 0; c < NR; ++c) acc[i][c] = fma(tv, x[h][c], acc[i][c]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        double xj[NR];
+#pragma unroll
+        for (int c = 0; c < NR; ++c) xj[c] = __shfl_sync(0xffffffffu, x[0][c], j);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double tv = (double)Ts[j * BS + lane + 32 * h];
+#pragma unroll
+          for (int c = 0; c < NR; ++c) acc[h][c] = fma(tv, xj[c], acc[h][c]);
+        }
+      }
+    }
+  }
+  cp_wait<0>();
+
+  // the previous block's solution: fetched now, waited for after c
+  double xf[2][NR];
+  if (t >= 1) fetch_x<2, NR>(xf, a, tile_k0(t - 1), tile_kw(t - 1), c0, nc, lane, 32);
+
+  // ---- partial sums of the warps -> y = b - sum -> c = Dinv y ----
+  if (TRANS) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      double v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = acc[i][c];
+      const double s = row_reduce(v, lane);
+      if ((lane & 3) == 0) part[c * BS + 8 * warp + (lane >> 2)] = s;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < NR; ++c)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) part[(warp * NR + c) * BS + lane + 32 * h] = acc[h][c];
+  }
+  __syncthreads();
+  double cv[NR];
+#pragma unroll
+  for (int c = 0; c < NR; ++c) {
+    double y[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int m = lane + 32 * h;
+      double s;
+      if (TRANS) {
+        s = part[c * BS + m];
+      } else {
+        s = part[c * BS + m];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) s += part[(w * NR + c) * BS + m];
+      }
+      y[h] = bm[h][c] - s;
+    }
+    double v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      v[i] = fma(Dinv[(8 * warp + i) * BS + lane + 32], y[1],
+                 Dinv[(8 * warp + i) * BS + lane] * y[0]);
+    cv[c] = row_reduce(v, lane);
+  }
+
+  // ---- hand-over: x = c - W x_prev once the previous block is out ----
+  if (t >= 1) {
+    settle_x<2, NR>(xf, a, tile_k0(t - 1), c0, lane, 32, lane);
+#pragma unroll
+    for (int c = 0; c < NR; ++c) {
+      double v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = fma(W[i][1], xf[1][c], W[i][0] * xf[0][c]);
+      cv[c] -= row_reduce(v, lane);
+    }
+  }
+  const int ri = 8 * warp + (lane >> 2);
+  if ((lane & 3) == 0 && ri < rw) {
+#pragma unroll
+    for (int c = 0; c < NR; ++c)
+      if (c < nc) st_publish(a.X + (r0 + ri) + (c0 + c) * a.ldx, cv[c]);
+  }
+}
+
+// B <- X and X <- pending, for the rows and columns of the solve; the first
+// thread also clears the ticket counter and the expired-wait count.
+__global__ void trsv_prepare_kernel(int64_t n, int64_t nrhs, double* __restrict__ X,
+                                    int64_t ldx, double* __restrict__ B,
+                                    unsigned* __restrict__ sync) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e == 0) {
+    sync[0] = 0;
+    sync[1] = 0;
+  }
+  if (e >= n * nrhs) return;
+  const int64_t c = e / n, i = e - c * n;
+  double* p = X + i + c * ldx;
+  B[e] = *p;
+  *p = __longlong_as_double((long long)kPending);
+}
+
+// ======================================================================
+// Group kernel (groups of 4 or 8 right-hand sides).  Row blocks publish
+// through a per-group counter of finished blocks (release / acquire at GPU
+// scope); the solution blocks of finished blocks are staged through the
+// CTA's cp.async ring together with the tiles, so a CTA that starts behind
+// the solve front streams its backlog at memory speed.
+// ======================================================================
+
+constexpr int kGS = 4;                 // ring stages of the group kernel
+constexpr int kSyncHeader = 4;         // ticket, abort, expired waits, spare
+
+__host__ __device__ constexpr size_t group_smem_bytes(int nr) {
+  return (size_t)kGS * BS * BS * 4        // fp32 tiles
+         + (size_t)kGS * nr * BS * 8      // fp64 solution blocks of the tiles
+         + (size_t)BS * BS * 8            // inverse of the diagonal block
+         + (size_t)nr * BS * 8            // right-hand side / y
+         + (size_t)BS * 8                 // reciprocals of the diagonal
+         + 64;                            // control words
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Solution block of a tile: rows k0 .. k0+kw of the group's columns, the
 // rest zero.  Async form: 16-byte copies through L2 (the block was written
-// by another SM; L1 is bypassed).  Sync form: plain L2 loads.
+// by another SM; L1 is bypassed).  Sync form: L2 loads.
 template <int NR>
 __device__ __forceinline__ void load_x_async(double* dst, const Args& a, int64_t k0, int kw,
                                              int64_t c0, int nc) {
@@ -202,15 +658,15 @@ __device__ __forceinline__ void load_x_sync(double* dst, const Args& a, int64_t 
 }
 
 template <bool TRANS, int NR, bool V16>
-__global__ void __launch_bounds__(kThreads, NR >= 8 ? 1 : 2)
-trsv_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, 1)
+trsv_group_kernel(Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* Tr = reinterpret_cast<float*>(smem);
-  double* Xr = reinterpret_cast<double*>(smem + (size_t)S * BS * BS * 4);
-  double* Dinv = Xr + S * NR * BS;
+  double* Xr = reinterpret_cast<double*>(smem + (size_t)kGS * BS * BS * 4);
+  double* Dinv = Xr + kGS * NR * BS;
   double* ybuf = Dinv + BS * BS;
-  double* red = ybuf + NR * BS;
-  int* ctrl = reinterpret_cast<int*>(red + 4 * NR * BS);  // ticket, avail[2], abort
+  double* rdiag = ybuf + NR * BS;
+  int* ctrl = reinterpret_cast<int*>(rdiag + BS);  // ticket, avail[2], give-up
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned* abort_word = a.sync + 1;
@@ -229,8 +685,6 @@ trsv_kernel(Args a) {
   const int64_t c0 = (int64_t)g * NR;
   const int nc = imin64(a.nrhs - c0, NR);
   unsigned* done = a.sync + kSyncHeader + g;
-
-  // column offset / width of the tile at solve position q
   auto tile_k0 = [&](int q) -> int64_t { return (int64_t)(fwd ? q : a.nblk - 1 - q) * BS; };
   auto tile_kw = [&](int q) -> int { return imin64(a.n - tile_k0(q), BS); };
 
@@ -239,7 +693,6 @@ trsv_kernel(Args a) {
     const int c = e / BS, r = e % BS;
     ybuf[e] = (c < nc && r < rw) ? a.X[(r0 + r) + (c0 + c) * a.ldx] : 0.0;
   }
-  // diagonal block (fp32, in the inverse's space), then the ring prologue
   float* Dsrc = reinterpret_cast<float*>(Dinv);
   load_diag<V16>(Dsrc, a, r0, rw);
   cp_commit();
@@ -247,7 +700,7 @@ trsv_kernel(Args a) {
   unsigned xbits = 0;
   auto issue = [&](int q) {
     if (q < t) {
-      const int st = q % S;
+      const int st = q % kGS;
       const int64_t k0 = tile_k0(q);
       const int kw = tile_kw(q);
       load_tile<TRANS, V16>(Tr + st * BS * BS, a, r0, rw, k0, kw);
@@ -261,55 +714,14 @@ trsv_kernel(Args a) {
     cp_commit();
   };
 #pragma unroll 1
-  for (int q = 0; q < S - 1; ++q) issue(q);
+  for (int q = 0; q < kGS - 1; ++q) issue(q);
 
-  // ---- inverse of the diagonal block: fp64 substitution, column j by the
-  // four lanes 4j .. 4j+3, lane part p holding rows 4s + p ----
-  cp_wait<S - 1>();
+  cp_wait<kGS - 1>();
   __syncthreads();
-  if (rw < BS && tid >= rw && tid < BS) Dsrc[tid * BS + tid] = 1.0f;  // identity padding
-  __syncthreads();
-  {
-    const int j = tid >> 2, p = tid & 3;
-    // element (r, k) of op(T): memory row r, column k (or the transpose)
-    auto D = [&](int r, int k) -> double {
-      return (double)(TRANS ? Dsrc[r * BS + k] : Dsrc[k * BS + r]);
-    };
-    double z[16];
-#pragma unroll
-    for (int s = 0; s < 16; ++s) z[s] = (4 * s + p == j) ? 1.0 : 0.0;
-    const bool unit = a.unit != 0;
-    if (fwd) {
-#pragma unroll
-      for (int k = 0; k < BS; ++k) {
-        const bool live = k >= j;
-        if (live && !unit && p == (k & 3)) z[k >> 2] = z[k >> 2] / D(k, k);
-        const double zk = __shfl_sync(0xffffffffu, z[k >> 2], (lane & ~3) | (k & 3));
-        if (live) {
-#pragma unroll
-          for (int s = 0; s < 16; ++s)
-            if (4 * s + p > k) z[s] = fma(-D(4 * s + p, k), zk, z[s]);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = BS - 1; k >= 0; --k) {
-        const bool live = k <= j;
-        if (live && !unit && p == (k & 3)) z[k >> 2] = z[k >> 2] / D(k, k);
-        const double zk = __shfl_sync(0xffffffffu, z[k >> 2], (lane & ~3) | (k & 3));
-        if (live) {
-#pragma unroll
-          for (int s = 0; s < 16; ++s)
-            if (4 * s + p < k) z[s] = fma(-D(4 * s + p, k), zk, z[s]);
-        }
-      }
-    }
-    __syncthreads();  // every read of the fp32 block precedes the overwrite
-#pragma unroll
-    for (int s = 0; s < 16; ++s) Dinv[j * BS + 4 * s + p] = z[s];
-  }
+  invert_diag<TRANS>(Dsrc, Dinv, rdiag, rw, fwd, a.unit != 0);
 
-  // ---- stream the tiles of the blocks solved before this one ----
+  // ---- all tiles of the blocks solved before this one; warp w rows
+  // 8w .. 8w+7, per-lane partials over columns lane and lane + 32 ----
   double acc[8][NR];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
@@ -344,12 +756,12 @@ trsv_kernel(Args a) {
       ++refresh;
       if (ctrl[3]) { aborted = true; break; }
     }
-    const int st = q % S;
-    cp_wait<S - 2>();
+    const int st = q % kGS;
+    cp_wait<kGS - 2>();
     if (!((xbits >> st) & 1u))
       load_x_sync<NR>(Xr + st * NR * BS, a, tile_k0(q), tile_kw(q), c0, nc);
     __syncthreads();
-    issue(q + S - 1);
+    issue(q + kGS - 1);
     const float* Ts = Tr + st * BS * BS;
     const double* xs = Xr + st * NR * BS;
 #pragma unroll
@@ -379,64 +791,31 @@ trsv_kernel(Args a) {
     for (int e = tid; e < NR * BS; e += kThreads) {
       const int c = e / BS, r = e % BS;
       if (c < nc && r < rw)
-        a.X[(r0 + r) + (c0 + c) * a.ldx] = __longlong_as_double(0x7ff8000000000000ll);
+        a.X[(r0 + r) + (c0 + c) * a.ldx] = __longlong_as_double((long long)kQuietNaN);
     }
     return;
   }
 
-  // ---- y = b - sum: each row reduced over the 32 lanes (three halving
-  // exchanges, then two full steps); lane 4i ends with row 8 warp + i ----
+  // ---- y = b - sum, then x = Dinv y (rows 8 warp + i, lanes over j) ----
 #pragma unroll
   for (int c = 0; c < NR; ++c) {
     double v[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = acc[i][c];
-    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const double send = b4 ? v[i] : v[i + 4];
-      const double keep = b4 ? v[i + 4] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const double send = b3 ? v[i] : v[i + 2];
-      const double keep = b3 ? v[i + 2] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    {
-      const double send = b2 ? v[0] : v[1];
-      const double keep = b2 ? v[1] : v[0];
-      v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-    if ((lane & 3) == 0) ybuf[c * BS + 8 * warp + (lane >> 2)] -= v[0];
+    const double s = row_reduce(v, lane);
+    if ((lane & 3) == 0) ybuf[c * BS + 8 * warp + (lane >> 2)] -= s;
   }
   __syncthreads();
-
-  // ---- x = Dinv y: row r = tid & 63, quarter p of the columns ----
-  {
-    const int r = tid & 63, p = tid >> 6;
-    double part[NR];
+  const int ri = 8 * warp + (lane >> 2);
 #pragma unroll
-    for (int c = 0; c < NR; ++c) part[c] = 0.0;
+  for (int c = 0; c < NR; ++c) {
+    double v[8];
 #pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-      const int j = 16 * p + jj;
-      const double d = Dinv[j * BS + r];
-#pragma unroll
-      for (int c = 0; c < NR; ++c) part[c] = fma(d, ybuf[c * BS + j], part[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < NR; ++c) red[(p * NR + c) * BS + r] = part[c];
-  }
-  __syncthreads();
-  for (int e = tid; e < NR * BS; e += kThreads) {
-    const int c = e / BS, r = e % BS;
-    const double x = ((red[(0 * NR + c) * BS + r] + red[(1 * NR + c) * BS + r]) +
-                      red[(2 * NR + c) * BS + r]) + red[(3 * NR + c) * BS + r];
-    if (c < nc && r < rw) a.X[(r0 + r) + (c0 + c) * a.ldx] = x;
+    for (int i = 0; i < 8; ++i)
+      v[i] = fma(Dinv[(8 * warp + i) * BS + lane + 32], ybuf[c * BS + lane + 32],
+                 Dinv[(8 * warp + i) * BS + lane] * ybuf[c * BS + lane]);
+    const double x = row_reduce(v, lane);
+    if ((lane & 3) == 0 && ri < rw && c < nc) a.X[(r0 + ri) + (c0 + c) * a.ldx] = x;
   }
   __syncthreads();
   if (tid == 0) st_release(done, (unsigned)(t + 1));
@@ -446,8 +825,15 @@ int group_width(int64_t nrhs) { return nrhs >= 8 ? 8 : nrhs >= 4 ? 4 : nrhs >= 2
 
 template <bool TRANS, int NR, bool V16>
 lu_status launch_one(cudaStream_t st, const Args& a) {
-  const size_t smem = smem_bytes(NR);
-  auto fn = trsv_kernel<TRANS, NR, V16>;
+  size_t smem;
+  void (*fn)(Args);
+  if constexpr (NR <= 2) {
+    smem = warp_smem_bytes(NR);
+    fn = trsv_kernel<TRANS, NR, V16>;
+  } else {
+    smem = group_smem_bytes(NR);
+    fn = trsv_group_kernel<TRANS, NR, V16>;
+  }
   LUB_CUDA_TRY(set_smem_limit((const void*)fn, smem));
   fn<<<(unsigned)((int64_t)a.nblk * a.ngroups), kThreads, smem, st>>>(a);
   LUB_LAUNCH_CHECK();
@@ -550,32 +936,45 @@ __global__ void axpy_kernel(int64_t n, const double* __restrict__ d,
 }  // namespace
 
 size_t trsm_sync_bytes(int64_t nrhs) {
-  const int64_t groups = ceil_div(nrhs < 1 ? 1 : nrhs, trsv::group_width(nrhs));
+  const int64_t groups = ceil_div(nrhs < 1 ? 1 : nrhs, 4);
   return align_up((size_t)(trsv::kSyncHeader + groups) * 4, 256);
+}
+
+size_t trsm_ws_bytes(int64_t n, int64_t nrhs) {
+  return trsm_sync_bytes(nrhs) +
+         align_up((size_t)(n < 0 ? 0 : n) * (size_t)(nrhs < 0 ? 0 : nrhs) * 8, 256);
 }
 
 lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                       double* X, int64_t ldx, int64_t nrhs, bool upper,
-                      bool trans, void* sync) {
+                      bool trans, unsigned* sync, double* B) {
   if (n <= 0 || nrhs <= 0) return LU_SUCCESS;
-  if (!sync) return LU_ERR_INVALID_ARG;
+  if (!sync || !B) return LU_ERR_INVALID_ARG;
   const int nr = trsv::group_width(nrhs);
+  if (ceil_div(n, trsv::BS) * ceil_div(nrhs, nr) > 0x7fffffffll) return LU_ERR_INVALID_ARG;
   trsv::Args a;
   a.lu = lu;
   a.ld = ld;
   a.X = X;
   a.ldx = ldx;
+  a.B = B;
   a.n = n;
   a.nrhs = nrhs;
-  if (ceil_div(n, trsv::BS) * ceil_div(nrhs, nr) > 0x7fffffffll) return LU_ERR_INVALID_ARG;
   a.nblk = (int)ceil_div(n, trsv::BS);
   a.ngroups = (int)ceil_div(nrhs, nr);
   // op(T) is lower (forward substitution) for L and for U^T
   a.forward = upper == trans;
   a.unit = !upper;
   a.xvec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && (ldx % 2 == 0);
-  a.sync = static_cast<unsigned*>(sync);
-  LUB_CUDA_TRY(cudaMemsetAsync(sync, 0, (size_t)(trsv::kSyncHeader + a.ngroups) * 4, st));
+  a.sync = sync;
+  if (nr <= 2) {
+    const int64_t elems = n * nrhs;
+    trsv::trsv_prepare_kernel<<<(unsigned)ceil_div(elems, 256), 256, 0, st>>>(n, nrhs, X, ldx,
+                                                                            B, sync);
+    LUB_LAUNCH_CHECK();
+  } else {
+    LUB_CUDA_TRY(cudaMemsetAsync(sync, 0, (size_t)(trsv::kSyncHeader + a.ngroups) * 4, st));
+  }
   const bool v16 = ((reinterpret_cast<uintptr_t>(lu) & 15) == 0) && (ld % 4 == 0);
   if (trans)
     return v16 ? trsv::launch_nr<true, true>(st, a, nr) : trsv::launch_nr<true, false>(st, a, nr);
@@ -583,14 +982,15 @@ lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
 }
 
 lu_status launch_lu_solve(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
-                          double* X, int64_t ldx, int64_t nrhs, bool trans, void* sync) {
+                          double* X, int64_t ldx, int64_t nrhs, bool trans, unsigned* sync,
+                          double* B) {
   if (!trans) {  // L U x = b: L y = b, then U x = y
-    LUB_TRY(launch_trsm(st, n, lu, ld, X, ldx, nrhs, false, false, sync));
-    return launch_trsm(st, n, lu, ld, X, ldx, nrhs, true, false, sync);
+    LUB_TRY(launch_trsm(st, n, lu, ld, X, ldx, nrhs, false, false, sync, B));
+    return launch_trsm(st, n, lu, ld, X, ldx, nrhs, true, false, sync, B);
   }
   // (L U)^T x = U^T L^T x = b: U^T y = b, then L^T x = y
-  LUB_TRY(launch_trsm(st, n, lu, ld, X, ldx, nrhs, true, true, sync));
-  return launch_trsm(st, n, lu, ld, X, ldx, nrhs, false, true, sync);
+  LUB_TRY(launch_trsm(st, n, lu, ld, X, ldx, nrhs, true, true, sync, B));
+  return launch_trsm(st, n, lu, ld, X, ldx, nrhs, false, true, sync, B);
 }
 
 size_t residual_ws_bytes(int64_t n) {

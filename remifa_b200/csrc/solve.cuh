@@ -7,16 +7,19 @@ namespace lub {
 
 // op(T) X = X in place, T = the unit-lower L (upper = false) or the upper U
 // (upper = true) of the in-place factors lu (fp32, ld); op = T or T^T;
-// X fp64 n x nrhs (ldx).  One launch; sync = trsm_sync_bytes(nrhs) bytes of
-// device memory (cleared on the stream before the launch), not shared with
-// a solve in flight on another stream.
+// X fp64 n x nrhs (ldx).  One solve launch per triangle (plus a copy kernel
+// that moves X into B, n x nrhs with ld n, for groups of 1-2 columns).
+// sync: trsm_sync_bytes(nrhs) bytes of device memory.  sync and B are not
+// shared with a solve in flight on another stream.  trsm_ws_bytes = both.
 size_t trsm_sync_bytes(int64_t nrhs);
+size_t trsm_ws_bytes(int64_t n, int64_t nrhs);
 lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                       double* X, int64_t ldx, int64_t nrhs, bool upper,
-                      bool trans, void* sync);
+                      bool trans, unsigned* sync, double* B);
 // X <- (L U)^-1 X (trans: (L U)^-T X): two launch_trsm.
 lu_status launch_lu_solve(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
-                          double* X, int64_t ldx, int64_t nrhs, bool trans, void* sync);
+                          double* X, int64_t ldx, int64_t nrhs, bool trans, unsigned* sync,
+                          double* B);
 
 // Workspace (bytes) of launch_residual / launch_norm_inf for size n.
 size_t residual_ws_bytes(int64_t n);

@@ -176,6 +176,26 @@ def test_lu_rl_mixed_vs_oracle(built, n, nb, compute, fmt):
     assert fe_g <= 2 * fe_o + 1e-7 and fe_o <= 2 * fe_g + 1e-7
 
 
+@pytest.mark.parametrize("alpha", [1.05, 4.0])
+@pytest.mark.parametrize("kscale", [0, 8])
+def test_lu_rl_tc32_dominance_and_scale_grid(built, alpha, kscale):
+    """The n = 16384 mixed-precision workload's matrix family at a size the
+    oracle finishes quickly: row dominance 1.05 / 4 and entries scaled by
+    2^0 / 2^8 (fp16 operand range)."""
+    n, nb = 1024, 256
+    a = O.gen_matrix(n, seed=17, kind=1, alpha=alpha, kscale=kscale)
+    want = O.lu_rl(a, nb=nb, outer_fmt=O.FMT_FP16)
+    da = to_dev(a)
+    info = rb.lu_nopiv_rl(da, nb=nb, outer=rb.TC32)
+    torch.cuda.synchronize()
+    got = to_host(da)
+    assert int(info.item()) == 0
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel < 64 * n * U32, rel
+    fe_g, fe_o = O.factor_error(a, got), O.factor_error(a, want)
+    assert fe_g <= 2 * fe_o + 1e-7 and fe_o <= 2 * fe_g + 1e-7
+
+
 def test_lu_rl_tc32_vs_reference_gpu(built):
     if not os.path.exists(REF_SO):
         pytest.skip("reference library not built")

@@ -328,10 +328,11 @@ def main() -> None:
     bad = int((infos != 0).sum().item())
     value = world * args.steps * lu_flops(n) / (ms / 1e3) / 1e12
 
-    # ---- end to end through lu_nopiv_rl_host_c: pinned host matrix in, the
-    # factors streamed back into it per outer step while the factorization
-    # runs; the host matrix is reset from a pinned source between steps
-    # (outside the timed region)
+    # ---- end to end through lu_nopiv_rl_host_c: the pinned host matrix goes
+    # in by column chunks while the device factors the chunks already in, and
+    # each finished block column goes back while the factorization runs; the
+    # host matrix is reset from a pinned source between steps (outside the
+    # timed region)
     host_src = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
     host_src.copy_(base)
     host_a = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
@@ -408,7 +409,8 @@ def main() -> None:
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 4 * n * n, "d2h_bytes_per_step": 4 * n * n,
                 "path": "lu_nopiv_rl_host_c via remifa_b200.lu_nopiv_rl_host: pinned host "
-                        "matrix in, factors streamed back per outer step"},
+                        "matrix in by column chunks overlapping the factorization, finished "
+                        "block columns streamed back"},
         "gpu_launches": prof.launches,
         "roofline": roofline,
         "kernels": {k: {"launches": v["launches"], "ms": v["total_ms"]}

@@ -121,13 +121,17 @@ LU_API lu_status lu_nopiv_rl_c(const lu_opts* opts, lu_stream_t stream, int64_t 
 
 /* The right-looking factorization of an fp32 matrix in host memory (new; the
  * reference takes device pointers only).  h_a (n x n, lda) is copied into
- * the device buffer d_a (ldda), factored there, and every outer step's block
- * column and block row are copied back into h_a as soon as they are final,
- * on an internal copy stream, so the device-to-host transfer of the factors
- * overlaps the rest of the factorization.  h_a should be pinned host memory
- * (cudaHostAlloc / cudaHostRegister) for the copies to run asynchronously.
- * d_info as for lu_nopiv_rl_c.  Asynchronous: synchronise `stream` before
- * reading h_a. */
+ * the device buffer d_a (ldda) by column chunks of whole outer blocks on an
+ * internal copy stream; each chunk, once in, receives the outer steps of the
+ * earlier chunks (beside the factorization of the previous chunk), then its
+ * own steps, each of which sends its finished block column back into h_a on
+ * a second internal copy stream -- so both transfers overlap the
+ * factorization.  The factors are bit-identical to lu_nopiv_rl_c's.  With
+ * look-ahead and tensor-core updates one extra operand buffer (the size of
+ * one packed L21 / U12 pair) is taken from cudaMallocAsync on `stream`
+ * besides the workspace.  h_a should be pinned host memory (cudaHostAlloc /
+ * cudaHostRegister) for the copies to run asynchronously.  d_info as for
+ * lu_nopiv_rl_c.  Asynchronous: synchronise `stream` before reading h_a. */
 LU_API lu_status lu_nopiv_rl_host_c(const lu_opts* opts, lu_stream_t stream, int64_t n,
                                     float* h_a, int64_t lda, float* d_a, int64_t ldda,
                                     int* d_info, void* workspace, size_t ws_bytes);

@@ -147,9 +147,11 @@ def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=
                      diag_width: int = 0, workspace: torch.Tensor | None = None,
                      stream=None) -> torch.Tensor:
     """Factor the column-major fp32 matrix in (pinned) host memory `h_a` in
-    place, using the device matrix `d_a` (same shape) as the working copy;
-    the factors stream back to `h_a` block by block while the factorization
-    runs (lu_nopiv_rl_host_c).  Returns the device info tensor."""
+    place, using the device matrix `d_a` (same shape) as the working copy.
+    The matrix goes in by column chunks while the device works on the chunks
+    already in, and each chunk's factors go back as soon as they are final
+    (lu_nopiv_rl_host_c); the factors equal lu_nopiv_rl's bit for bit.
+    Returns the device info tensor."""
     if h_a.is_cuda or not d_a.is_cuda:
         raise ValueError("lu_nopiv_rl_host: h_a must be a host tensor, d_a a CUDA tensor")
     if h_a.dtype != torch.float32 or d_a.dtype != torch.float32 or h_a.shape != d_a.shape:

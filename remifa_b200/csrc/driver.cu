@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <mutex>
 #include <unordered_map>
+#include <vector>
 
 namespace lub {
 
@@ -96,23 +97,36 @@ static lu_status tc_pack(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   return LU_SUCCESS;
 }
 
-// Rows [r0, r1) of the L21 copy and columns [c0, c1) of the U12 copy only
-// (kinds without tile scales), at their places in the packed buffers.
+// Rows [r0, r1) of the L21 copy and columns [c0, c1) of the U12 copy only,
+// at their places in the packed buffers (for kinds with tile scales r0 and
+// c0 are multiples of 128, so the ranges cover whole scale tiles of the
+// full copies and their scales land in the same slots).
 static lu_status tc_pack_range(cudaStream_t st, TcOperand kind, int64_t r0, int64_t r1,
                                int64_t c0, int64_t c1, int64_t K, const float* a,
                                int64_t lda, const float* b, int64_t ldb, char* ws,
                                const TcWs& w) {
-  if (tc_scaled(kind)) return LU_ERR_UNSUPPORTED;
+  const bool scaled = tc_scaled(kind);
+  if (scaled && (r0 % 128 != 0 || c0 % 128 != 0)) return LU_ERR_UNSUPPORTED;
   const int64_t ldk = tc_packed_k(kind, K);
   const int64_t es = tc_operand_bytes(kind);
   ProfScope ps("pack_operands", st,
                (double)((r1 - r0) + (c1 - c0)) * (4.0 * K + (double)es * ldk));
-  if (r1 > r0)
+  int* tmp = reinterpret_cast<int*>(ws + w.off_tmp);
+  if (r1 > r0) {
+    int* sa = scaled ? reinterpret_cast<int*>(ws + w.off_sa) + r0 / 128 : nullptr;
+    if (scaled)
+      LUB_TRY(launch_scale_rowtiles(st, r1 - r0, K, a + r0, lda, sa, tmp, tc_scale_bound(kind)));
     LUB_TRY(launch_pack_a(st, kind, r1 - r0, K, a + r0, lda, ws + w.off_a + r0 * ldk * es,
-                          ldk, nullptr));
-  if (c1 > c0)
+                          ldk, sa));
+  }
+  if (c1 > c0) {
+    int* sb = scaled ? reinterpret_cast<int*>(ws + w.off_sb) + c0 / 128 : nullptr;
+    if (scaled)
+      LUB_TRY(launch_scale_coltiles(st, K, c1 - c0, b + c0 * ldb, ldb, sb, tmp,
+                                    tc_scale_bound(kind)));
     LUB_TRY(launch_pack_b(st, kind, K, c1 - c0, b + c0 * ldb, ldb,
-                          ws + w.off_b + c0 * ldk * es, ldk, nullptr));
+                          ws + w.off_b + c0 * ldk * es, ldk, sb));
+  }
   return LU_SUCCESS;
 }
 
@@ -160,12 +174,22 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
 
 // Internal streams of one device: panel work runs at the highest priority,
 // the bulk of each trailing update at the lowest, ordered by two events.
+constexpr int kMaxChunks = 16;  // column chunks of the host-memory entry
+
 struct DevStreams {
   cudaStream_t panel = nullptr, update = nullptr, copy = nullptr, side = nullptr;
+  cudaStream_t copy_out = nullptr;  // device-to-host, concurrent with `copy`
+  cudaStream_t catchup = nullptr;   // the host entry's catch_up of arrived chunks
+  cudaEvent_t cu_done = nullptr;
+  // per outer step of the host entry: the step's block column is final
+  // once what was queued on the panel (p) and side (s) streams has run
+  std::vector<cudaEvent_t> step_p, step_s;
+  cudaEvent_t chunk_in[kMaxChunks] = {};
+  cudaEvent_t out_done = nullptr;
   cudaEvent_t diag_done = nullptr, small_done = nullptr, big_done = nullptr;
-  cudaEvent_t diag1_done = nullptr, lbig_done = nullptr, psmall_done = nullptr;
+  cudaEvent_t diag1_done = nullptr;
   cudaEvent_t u1_done = nullptr, join_s = nullptr, spack_done = nullptr;
-  cudaEvent_t panel_done = nullptr, copied = nullptr;
+  cudaEvent_t copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
   cudaEvent_t done_with[2] = {nullptr, nullptr};  // U2 finished reading buffer b
@@ -185,16 +209,37 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.panel, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.update, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithFlags(&d.copy, cudaStreamNonBlocking));
+    LUB_CUDA_TRY(cudaStreamCreateWithFlags(&d.copy_out, cudaStreamNonBlocking));
+    for (int q = 0; q < kMaxChunks; ++q) {
+      LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.chunk_in[q], cudaEventDisableTiming));
+    }
+    LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.out_done, cudaEventDisableTiming));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup, cudaStreamNonBlocking, least));
+    LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
-                           &d.done_with[0], &d.done_with[1], &d.panel_done, &d.copied,
+                           &d.done_with[0], &d.done_with[1], &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
-                           &d.lbig_done, &d.psmall_done, &d.u1_done, &d.join_s,
+                           &d.u1_done, &d.join_s,
                            &d.spack_done})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
   *out = &it->second;
+  return LU_SUCCESS;
+}
+
+// At least `steps` per-step events in S (created on first need).
+static lu_status step_events(DevStreams* S, int64_t steps) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  while ((int64_t)S->step_p.size() < steps) {
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    LUB_CUDA_TRY(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+    LUB_CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+    S->step_p.push_back(e1);
+    S->step_s.push_back(e2);
+  }
   return LU_SUCCESS;
 }
 
@@ -275,10 +320,11 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
 }
 
 // Factor the outer block column/row starting at (ofs, ofs): width `in`,
-// `updm` rows (and columns) remaining.
+// L rows [ofs, ofs + updm) and U columns [ofs, ofs + updc) (updc = updm for
+// a whole factorization; fewer columns when only a column range is present).
 static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
                               int64_t lda, int64_t ofs, int64_t in,
-                              int64_t updm, int* first_bad) {
+                              int64_t updm, int64_t updc, int* first_bad) {
   float* blk = a + ofs + ofs * lda;
   for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
     const int w = (int)std::min<int64_t>(in - p0, p.diag_w);
@@ -287,21 +333,22 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
       ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * w / 3.0);
       LUB_TRY(launch_diag_factor(st, dg, lda, w, ofs + p0, first_bad));
     }
-    const int64_t rest = updm - (p0 + w);
-    if (rest > 0) {
-      ProfScope ps("lupanel", st, 2.0 * 8.0 * rest * w, 2.0 * rest * (double)w * w);
-      LUB_TRY(launch_lupanel(st, dg, lda, w, rest, rest));
+    const int64_t rest = updm - (p0 + w), restc = updc - (p0 + w);
+    if (rest > 0 || restc > 0) {
+      ProfScope ps("lupanel", st, 8.0 * (rest + restc) * w,
+                   (double)(rest + restc) * (double)w * w);
+      LUB_TRY(launch_lupanel(st, dg, lda, w, rest, restc));
     }
     if (p0 + w < in) {
       ProfScope ps("sgemm_chunk8", st, 0.0,
                    2.0 * w * ((double)(updm - p0 - w) * (in - p0 - w) +
-                              (double)(in - p0 - w) * (updm - in)));
+                              (double)(in - p0 - w) * (updc - in)));
       // rest of the outer block column: rows [p0+w, updm), cols [p0+w, in);
-      // rest of the outer block row: rows [p0+w, in), cols [in, updm)
+      // rest of the outer block row: rows [p0+w, in), cols [in, updc)
       LUB_TRY(launch_sgemm_chunk8_2(
           st, updm - (p0 + w), in - (p0 + w), w, dg + w, lda, dg + (int64_t)w * lda,
           lda, dg + w + (int64_t)w * lda, lda,
-          updm > in ? in - (p0 + w) : 0, updm - in, w, dg + w, lda,
+          updc > in ? in - (p0 + w) : 0, updc - in, w, dg + w, lda,
           blk + p0 + in * lda, lda, blk + (p0 + w) + in * lda, lda));
     }
   }
@@ -318,13 +365,14 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
 // operations in the same order as in factor_block.
 static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* S,
                                     float* a, int64_t lda, int64_t ofs, int64_t in,
-                                    int64_t updm, int* first_bad) {
+                                    int64_t updm, int64_t updc, int* first_bad) {
   const int w = p.diag_w;
   if (in != 2 * w || updm <= in)
-    return factor_block(p, st, a, lda, ofs, in, updm, first_bad);
+    return factor_block(p, st, a, lda, ofs, in, updm, updc, first_bad);
   cudaStream_t ss = S->side;
   float* blk = a + ofs + ofs * lda;
-  const int64_t big = updm - 2 * w;  // L rows / U columns beyond the outer block
+  const int64_t big = updm - 2 * w;   // L rows beyond the outer block
+  const int64_t bigc = updc - 2 * w;  // U columns beyond the outer block
   {
     ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * w / 3.0);
     LUB_TRY(launch_diag_factor(st, blk, lda, w, ofs, first_bad));
@@ -338,15 +386,15 @@ static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* 
   // side stream: the rest of the first sub-panel and of its update
   LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->diag_done, 0));
   {
-    ProfScope ps("lupanel", ss, 2.0 * 8.0 * big * w, 2.0 * 2 * big * (double)w * w);
-    LUB_TRY(launch_lupanel(ss, blk, lda, w, big, big, false, w, w));
+    ProfScope ps("lupanel", ss, 8.0 * (big + bigc) * w, (double)(big + bigc) * (double)w * w);
+    LUB_TRY(launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w));
   }
   LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->small_done, 0));
   {
-    ProfScope ps("sgemm_chunk8", ss, 0.0, 2.0 * w * 2.0 * (double)big * w);
-    // rows [2w, updm) x columns [w, 2w), and rows [w, 2w) x columns [2w, updm)
+    ProfScope ps("sgemm_chunk8", ss, 0.0, 2.0 * w * (double)(big + bigc) * w);
+    // rows [2w, updm) x columns [w, 2w), and rows [w, 2w) x columns [2w, updc)
     LUB_TRY(launch_sgemm_chunk8_2(ss, big, w, w, blk + 2 * w, lda, blk + (int64_t)w * lda, lda,
-                                  blk + 2 * w + (int64_t)w * lda, lda, w, big, w, blk + w, lda,
+                                  blk + 2 * w + (int64_t)w * lda, lda, w, bigc, w, blk + w, lda,
                                   blk + 2 * (int64_t)w * lda, lda,
                                   blk + w + 2 * (int64_t)w * lda, lda));
   }
@@ -365,8 +413,8 @@ static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* 
   }
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->big_done, 0));
   {
-    ProfScope ps("lupanel", st, 2.0 * 8.0 * big * w, 2.0 * 2 * big * (double)w * w);
-    LUB_TRY(launch_lupanel(st, dg1, lda, w, big, big));
+    ProfScope ps("lupanel", st, 8.0 * (big + bigc) * w, (double)(big + bigc) * (double)w * w);
+    LUB_TRY(launch_lupanel(st, dg1, lda, w, big, bigc));
   }
   return LU_SUCCESS;
 }
@@ -394,29 +442,37 @@ static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
 // (measured on B200 at n = 16384: 2 tiles 133 TF/s, 8 tiles 124, 16 tiles 122).
 constexpr int kU2Tiles = 2;
 
-// Right-looking factorization.  Without look-ahead every outer step runs in
-// order on the caller's stream.  With look-ahead the trailing update of step
-// k is split into U1 (the next block column and block row, which the panel
-// of step k+1 needs), U2a (the block column and row after that, which U1 of
-// step k+1 updates next) and U2b (everything else).  The panel, the operand
-// packing and U1 run on a high-priority stream, U2a and U2b on a
-// low-priority one; U1 of step k+1 waits only for U2a of step k, so the
-// bulk U2b of step k overlaps the panels of steps k+1 and k+2.  The packed
-// operands are double-buffered: packing step k+2 waits until U2 of step k
-// has finished reading the same buffer.  Every element still receives its
-// updates in the same order, so results are identical either way.
-// Destination of the finished factors in host memory (lu_nopiv_rl_host_c):
-// each outer step's block column and block row are copied back on the
-// internal copy stream as soon as the step's panel is done.
-struct HostSink {
+// Right-looking factorization of the steps whose outer block starts in
+// [col_begin, col_end), restricted to the columns [0, col_end) (rows always
+// run to n): col_begin = 0, col_end = n is the whole factorization; the
+// host-memory entry factors one arrived column range at a time (after
+// catch_up gave it the earlier steps).  Without look-ahead every outer step
+// runs in order on the caller's stream.  With look-ahead the trailing
+// update of step k is split into U1 (the next block column and block row,
+// which the panel of step k+1 needs), U2a (the block column and row after
+// that, which U1 of step k+1 updates next) and U2b (everything else).  The
+// panel, the operand packing and U1 run on a high-priority stream, U2a and
+// U2b on a low-priority one; U1 of step k+1 waits only for U2a of step k,
+// so the bulk U2b of step k overlaps the panels of steps k+1 and k+2.  The
+// packed operands are double-buffered: packing step k+2 waits until U2 of
+// step k has finished reading the same buffer.  Every element still
+// receives its updates in the same order, so results are identical either
+// way.
+// Where rl_factor sends each finished block column (host-memory entry):
+// after a step's panel, rows [0, n) of its block column are final; they go
+// to h (ldh) on the copy stream `out`.
+struct ColumnSink {
   float* h = nullptr;
   int64_t ldh = 0;
+  cudaStream_t out = nullptr;
 };
 
 static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                            int64_t lda, char* ws, int* first_bad, int* err,
-                           const HostSink* sink = nullptr) {
+                           int64_t col_begin = 0, int64_t col_end = -1,
+                           const ColumnSink* sink = nullptr) {
   const int64_t n = p.n, nb = p.nb;
+  if (col_end < 0) col_end = n;
   const bool tc = is_tc(p.outer);
   TcWs w2[2];
   if (tc && n > nb) {
@@ -429,23 +485,25 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const bool la = p.lookahead && n > 2 * nb &&
                   !(tc && tc_scaled(tc_kind(p.outer)) && nb % 128 != 0);
   if (!la) {
-    for (int64_t ofs = 0; ofs < n; ofs += nb) {
+    for (int64_t ofs = col_begin; ofs < col_end; ofs += nb) {
       const int64_t in = std::min(n - ofs, nb);
-      LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, first_bad));
-      const int64_t tn = n - (ofs + nb);
-      if (tn <= 0) continue;
+      LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, col_end - ofs, first_bad));
+      if (sink)
+        LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h + ofs * sink->ldh, (size_t)sink->ldh * 4,
+                                       a + ofs * lda, (size_t)lda * 4, (size_t)n * 4,
+                                       (size_t)in, cudaMemcpyDeviceToHost, st));
+      const int64_t tr = n - (ofs + nb), tcn = col_end - (ofs + nb);
+      if (tr <= 0 || tcn <= 0) continue;
       if (tc)
-        LUB_TRY(tc_pack(st, tc_kind(p.outer), tn, tn, nb, a + (ofs + nb) + ofs * lda,
+        LUB_TRY(tc_pack(st, tc_kind(p.outer), tr, tcn, nb, a + (ofs + nb) + ofs * lda,
                         lda, a + ofs + (ofs + nb) * lda, lda, ws, w2[0]));
-      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tn, 0, tn, ws, w2[0], err, 0));
+      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tr, 0, tcn, ws, w2[0], err, 0));
     }
-    if (sink)
-      LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h, (size_t)sink->ldh * 4, a, (size_t)lda * 4,
-                                     (size_t)n * 4, (size_t)n, cudaMemcpyDeviceToHost, st));
     return LU_SUCCESS;
   }
   DevStreams* S = nullptr;
   LUB_TRY(dev_streams(&S));
+  if (sink) LUB_TRY(step_events(S, ceil_div(n, nb)));
   cudaStream_t sp = S->panel, su = S->update;
   LUB_CUDA_TRY(cudaEventRecord(S->fork, st));
   LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->fork, 0));
@@ -461,31 +519,31 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const int w = p.diag_w;
   const TcOperand kind = tc_kind(p.outer);
   // A step takes the deep schedule when its outer block holds two diagonal
-  // blocks and at least two of them remain beyond it (see below).
+  // blocks and at least two of them remain beyond it, in rows and columns.
   auto deep_step = [&](int64_t o) {
-    const int64_t in_ = std::min(n - o, nb), tn_ = n - (o + nb);
-    return in_ == 2 * w && tn_ >= 2 * w && !(tc && tc_scaled(kind));
+    const int64_t in_ = std::min(n - o, nb), tr_ = n - (o + nb), tc_ = col_end - (o + nb);
+    return o < col_end && in_ == 2 * w && tr_ >= 2 * w && tc_ >= 2 * w &&
+           !(tc && tc_scaled(kind));
   };
   bool pre = false;       // this step's first diagonal block is already queued
   bool prev_deep = false; // the previous step ran the deep schedule
-  auto sink_copy = [&](int64_t ofs, int64_t in) {
-    const float* da = a + ofs + ofs * lda;
-    float* ha = sink->h + ofs + ofs * sink->ldh;
-    if (!ok(cudaMemcpy2DAsync(ha, (size_t)sink->ldh * 4, da, (size_t)lda * 4,
-                              (size_t)(n - ofs) * 4, (size_t)in, cudaMemcpyDeviceToHost,
-                              S->copy)))
+  // block column [ofs, ofs + in) is final once the panel work queued so far
+  // on sp (and, with `side`, on ss) has run
+  auto sink_column = [&](int64_t ofs, int64_t in, bool side) {
+    const int64_t t = ofs / nb;
+    cudaEvent_t ep = S->step_p[t], es = S->step_s[t];
+    if (!ok(cudaEventRecord(ep, sp)) || !ok(cudaEventRecord(es, side ? ss : sp)) ||
+        !ok(cudaStreamWaitEvent(sink->out, ep, 0)) || !ok(cudaStreamWaitEvent(sink->out, es, 0)))
       return false;
-    if (n - ofs - in > 0 &&
-        !ok(cudaMemcpy2DAsync(ha + in * sink->ldh, (size_t)sink->ldh * 4, da + in * lda,
-                              (size_t)lda * 4, (size_t)in * 4, (size_t)(n - ofs - in),
-                              cudaMemcpyDeviceToHost, S->copy)))
-      return false;
-    return true;
+    return ok(cudaMemcpy2DAsync(sink->h + ofs * sink->ldh, (size_t)sink->ldh * 4, a + ofs * lda,
+                                (size_t)lda * 4, (size_t)n * 4, (size_t)in,
+                                cudaMemcpyDeviceToHost, sink->out));
   };
-  for (int64_t ofs = 0; ofs < n && status == LU_SUCCESS; ofs += nb, ++step) {
+  for (int64_t ofs = col_begin; ofs < col_end && status == LU_SUCCESS; ofs += nb, ++step) {
     const int64_t in = std::min(n - ofs, nb);
-    const int64_t updm = n - ofs;
-    const int64_t tn = n - (ofs + nb);
+    const int64_t updm = n - ofs, updc = col_end - ofs;
+    const int64_t tr = n - (ofs + nb);        // trailing rows
+    const int64_t tcn = col_end - (ofs + nb); // trailing columns
     const int buf = (int)(step & 1);
     const TcWs& wk = w2[buf];
     // the previous step's update of this block column / row ran partly on
@@ -496,36 +554,37 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     if (deep_step(ofs)) {
       // Deep schedule.  Panel stream sp: first diagonal block, the first w
       // L rows / U columns of its sub-panel and their update of the second
-      // diagonal block, the second diagonal block, the first w L rows / U
-      // columns of the second sub-panel; then the first w x w block of the
-      // next outer block gets this step's update and is factored at once.
+      // diagonal block, the second diagonal block, the first nb L rows / U
+      // columns of the second sub-panel; then the nb x nb diagonal square of
+      // the next outer block gets this step's update and its first w x w
+      // block is factored at once.
       // Side stream ss: the rest of both sub-panels and of the first one's
       // update, the rest of the operand packing and of the next block
       // column / row update (U1).  Low-priority stream su: U2 as before.
       float* blk = a + ofs + ofs * lda;
       float* dg1 = blk + w + (int64_t)w * lda;
-      const int64_t big = updm - 2 * w;
+      const int64_t big = updm - 2 * w, bigc = updc - 2 * w;
       if (!pre) {
         ProfScope ps("diag_factor", sp, 8.0 * w * w, 2.0 * w * w * w / 3.0);
         if ((status = launch_diag_factor(sp, blk, lda, w, ofs, first_bad)) != LU_SUCCESS) break;
         if (!ok(cudaEventRecord(S->diag_done, sp))) break;
       }
       {
-        ProfScope ps("lupanel", sp, 16.0 * w * w, 4.0 * (double)w * w * w);
+        ProfScope ps("lupanel", sp, 16.0 * w * w, 2.0 * (double)w * w * w);
         if ((status = launch_lupanel(sp, blk, lda, w, w, w, false, 0, 0)) != LU_SUCCESS) break;
       }
       if (!ok(cudaEventRecord(S->small_done, sp))) break;
       if (!ok(cudaStreamWaitEvent(ss, S->diag_done, 0))) break;
       {
-        ProfScope ps("lupanel", ss, 16.0 * big * w, 4.0 * big * (double)w * w);
-        if ((status = launch_lupanel(ss, blk, lda, w, big, big, false, w, w)) != LU_SUCCESS)
+        ProfScope ps("lupanel", ss, 8.0 * (big + bigc) * w, (double)(big + bigc) * w * w);
+        if ((status = launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w)) != LU_SUCCESS)
           break;
       }
       if (!ok(cudaStreamWaitEvent(ss, S->small_done, 0))) break;
       {
-        ProfScope ps("sgemm_chunk8", ss, 0.0, 4.0 * (double)big * w * w);
+        ProfScope ps("sgemm_chunk8", ss, 0.0, 2.0 * (double)(big + bigc) * w * w);
         status = launch_sgemm_chunk8_2(ss, big, w, w, blk + 2 * w, lda, blk + (int64_t)w * lda,
-                                       lda, blk + 2 * w + (int64_t)w * lda, lda, w, big, w,
+                                       lda, blk + 2 * w + (int64_t)w * lda, lda, w, bigc, w,
                                        blk + w, lda, blk + 2 * (int64_t)w * lda, lda,
                                        blk + w + 2 * (int64_t)w * lda, lda);
         if (status != LU_SUCCESS) break;
@@ -545,31 +604,30 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       }
       if (!ok(cudaEventRecord(S->diag1_done, sp))) break;
       if (!ok(cudaStreamWaitEvent(sp, S->big_done, 0))) break;
+      // the nb x nb diagonal square of the next outer block: its update by
+      // this step stays on the panel stream, so the next step's panel never
+      // waits for the side stream's share of U1.  That update reads the
+      // first sq rows of L21 and columns of U12, so the second sub-panel's
+      // share of them is eliminated here too; the side stream takes the rest.
+      const int64_t sq = std::min(nb, tcn);
+      const int64_t mh = std::min(sq, big), nh = std::min(sq, bigc);
       {
-        ProfScope ps("lupanel", sp, 16.0 * w * w, 4.0 * (double)w * w * w);
-        if ((status = launch_lupanel(sp, dg1, lda, w, w, w, false, 0, 0)) != LU_SUCCESS) break;
+        ProfScope ps("lupanel", sp, 8.0 * (mh + nh) * w, (double)(mh + nh) * w * w);
+        if ((status = launch_lupanel(sp, dg1, lda, w, mh, nh, false, 0, 0)) != LU_SUCCESS)
+          break;
       }
-      if (!ok(cudaEventRecord(S->psmall_done, sp))) break;
       if (!ok(cudaStreamWaitEvent(ss, S->diag1_done, 0))) break;
       {
-        ProfScope ps("lupanel", ss, 16.0 * (big - w) * w, 4.0 * (big - w) * (double)w * w);
-        if ((status = launch_lupanel(ss, dg1, lda, w, big - w, big - w, false, w, w)) !=
+        ProfScope ps("lupanel", ss, 8.0 * (big - mh + bigc - nh) * w,
+                     (double)(big - mh + bigc - nh) * w * w);
+        if ((status = launch_lupanel(ss, dg1, lda, w, big - mh, bigc - nh, false, mh, nh)) !=
             LU_SUCCESS)
           break;
       }
-      if (!ok(cudaEventRecord(S->lbig_done, ss))) break;
-      if (sink) {
-        if (!ok(cudaStreamWaitEvent(S->copy, S->psmall_done, 0)) ||
-            !ok(cudaStreamWaitEvent(S->copy, S->lbig_done, 0)) || !sink_copy(ofs, in))
-          break;
-      }
+      if (sink && !sink_column(ofs, in, true)) break;
       // L21 rows / U12 columns relative to the trailing part (ofs + nb)
       const float* L21 = a + (ofs + nb) + ofs * lda;
       const float* U12 = a + ofs + (ofs + nb) * lda;
-      // the nb x nb diagonal square of the next outer block: its update by
-      // this step stays on the panel stream, so the next step's panel never
-      // waits for the side stream's share of U1
-      const int64_t sq = std::min(nb, tn);
       if (tc) {
         if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
         if ((status = tc_pack_range(sp, kind, 0, sq, 0, sq, nb, L21, lda, U12, lda, ws, wk)) !=
@@ -594,7 +652,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       // side stream: the rest of the packing and of U1
       if (tc) {
         if (step >= 2 && !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))) break;
-        if ((status = tc_pack_range(ss, kind, sq, tn, sq, tn, nb, L21, lda, U12, lda, ws,
+        if ((status = tc_pack_range(ss, kind, sq, tr, sq, tcn, nb, L21, lda, U12, lda, ws,
                                     wk)) != LU_SUCCESS)
           break;
       }
@@ -602,59 +660,55 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       if (!ok(cudaStreamWaitEvent(ss, S->spack_done, 0))) break;
       if (step > 0 && !ok(cudaStreamWaitEvent(ss, S->updated, 0))) break;
       // U1 minus the square: block column below it, block row right of it
-      status = outer_update(p, ss, a, lda, ofs, sq, tn - sq, 0, sq, ws, wk, err, 1);
+      status = outer_update(p, ss, a, lda, ofs, sq, tr - sq, 0, sq, ws, wk, err, 1);
       if (status == LU_SUCCESS)
-        status = outer_update(p, ss, a, lda, ofs, 0, sq, sq, tn - sq, ws, wk, err, 1);
+        status = outer_update(p, ss, a, lda, ofs, 0, sq, sq, tcn - sq, ws, wk, err, 1);
       if (status != LU_SUCCESS) break;
       if (!ok(cudaEventRecord(S->u1_done, ss))) break;
       prev_deep = true;
     } else {
-      status = factor_block_split(p, sp, S, a, lda, ofs, in, updm, first_bad);
+      status = factor_block_split(p, sp, S, a, lda, ofs, in, updm, updc, first_bad);
       if (status != LU_SUCCESS) break;
-      if (sink) {
-        // block column (rows [ofs, n)) and block row (columns [ofs+in, n)) of
-        // this step are final: copy them back while the factorization goes on
-        if (!ok(cudaEventRecord(S->panel_done, sp)) ||
-            !ok(cudaStreamWaitEvent(S->copy, S->panel_done, 0)) || !sink_copy(ofs, in))
-          break;
-      }
+      // factor_block_split ends on sp after the side stream's share
+      if (sink && !sink_column(ofs, in, false)) break;
       prev_deep = false;
       pre = false;
-      if (tn <= 0) continue;
+      if (tr <= 0 || tcn <= 0) continue;
       if (tc) {
         // U2 of step k-2 read this buffer
         if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
-        status = tc_pack(sp, kind, tn, tn, nb, a + (ofs + nb) + ofs * lda, lda,
+        status = tc_pack(sp, kind, tr, tcn, nb, a + (ofs + nb) + ofs * lda, lda,
                          a + ofs + (ofs + nb) * lda, lda, ws, wk);
         if (status != LU_SUCCESS) break;
       }
       if (!ok(cudaEventRecord(S->packed, sp))) break;
       // U1 after U2a of the previous step (same elements, earlier step first)
       if (step > 0 && !ok(cudaStreamWaitEvent(sp, S->updated, 0))) break;
-      const int64_t b = std::min(nb, tn);
-      status = outer_update(p, sp, a, lda, ofs, 0, tn, 0, b, ws, wk, err, 1);
-      if (status == LU_SUCCESS && tn > nb)
-        status = outer_update(p, sp, a, lda, ofs, 0, nb, nb, tn - nb, ws, wk, err, 1);
+      const int64_t b = std::min(nb, tcn);
+      status = outer_update(p, sp, a, lda, ofs, 0, tr, 0, b, ws, wk, err, 1);
+      if (status == LU_SUCCESS && tcn > nb)
+        status = outer_update(p, sp, a, lda, ofs, 0, std::min(nb, tr), nb, tcn - nb, ws, wk,
+                              err, 1);
       if (status != LU_SUCCESS) break;
     }
-    if (tn > nb) {
+    if (tr > nb && tcn > nb) {
       if (!ok(cudaStreamWaitEvent(su, S->packed, 0))) break;
       // U2a: block column and row k+2 (rows / columns [nb, 2nb) of the trailing part)
-      const int64_t b2 = std::min(nb, tn - nb);
-      status = outer_update(p, su, a, lda, ofs, nb, tn - nb, nb, b2, ws, wk, err, kU2Tiles);
-      if (status == LU_SUCCESS && tn > 2 * nb)
-        status = outer_update(p, su, a, lda, ofs, nb, b2, 2 * nb, tn - 2 * nb, ws, wk,
+      const int64_t b2c = std::min(nb, tcn - nb), b2r = std::min(nb, tr - nb);
+      status = outer_update(p, su, a, lda, ofs, nb, tr - nb, nb, b2c, ws, wk, err, kU2Tiles);
+      if (status == LU_SUCCESS && tcn > 2 * nb)
+        status = outer_update(p, su, a, lda, ofs, nb, b2r, 2 * nb, tcn - 2 * nb, ws, wk,
                               err, kU2Tiles);
       if (status != LU_SUCCESS) break;
       if (!ok(cudaEventRecord(S->updated, su))) break;
       // U2b: the rest
-      if (tn > 2 * nb) {
-        status = outer_update(p, su, a, lda, ofs, 2 * nb, tn - 2 * nb, 2 * nb,
-                              tn - 2 * nb, ws, wk, err, kU2Tiles);
+      if (tr > 2 * nb && tcn > 2 * nb) {
+        status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
+                              tcn - 2 * nb, ws, wk, err, kU2Tiles);
         if (status != LU_SUCCESS) break;
       }
       if (!ok(cudaEventRecord(S->done_with[buf], su))) break;
-    } else if (tn > 0) {
+    } else if (tr > 0 && tcn > 0) {
       cudaStream_t last = prev_deep ? ss : sp;
       if (!ok(cudaEventRecord(S->updated, last))) break;
       if (!ok(cudaEventRecord(S->done_with[buf], last))) break;
@@ -667,11 +721,56 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   cudaStreamWaitEvent(st, S->join_p, 0);
   cudaStreamWaitEvent(st, S->join_u, 0);
   cudaStreamWaitEvent(st, S->join_s, 0);
-  if (sink) {
-    cudaEventRecord(S->copied, S->copy);
-    cudaStreamWaitEvent(st, S->copied, 0);
-  }
   return status;
+}
+
+// Give the columns [c0, c1) (all rows) the outer steps whose blocks start
+// before c0, in step order: per step the U part of its panel -- the
+// unit-lower solves with the outer block's diagonal sub-blocks and the
+// rank-w update between them, exactly as factor_block applies them to a
+// column right of the block -- then its trailing update.  Every element
+// receives the same operations in the same order as when rl_factor runs
+// over the whole matrix, so the factors are bit-identical.
+// With S given, step t waits for S->step_p / step_s[t] first (the step's
+// block column final), so the catch-up of an arrived chunk can run beside
+// the factorization of the chunk before it.
+static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda, char* ws,
+                          const TcWs& wk, int* err, int64_t c0, int64_t c1,
+                          const DevStreams* S = nullptr) {
+  const int64_t n = p.n, nb = p.nb, nc = c1 - c0;
+  const bool tc = is_tc(p.outer);
+  const TcOperand kind = tc_kind(p.outer);
+  for (int64_t ofs = 0; ofs < c0; ofs += nb) {
+    if (S) {
+      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[ofs / nb], 0));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[ofs / nb], 0));
+    }
+    const int64_t in = std::min(n - ofs, nb);
+    float* blk = a + ofs + ofs * lda;
+    for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
+      const int w = (int)std::min<int64_t>(in - p0, p.diag_w);
+      float* dg = blk + p0 + p0 * lda;
+      {
+        ProfScope ps("lupanel", st, 8.0 * nc * w, (double)nc * w * w);
+        LUB_TRY(launch_lupanel(st, dg, lda, w, 0, nc, false, 0, c0 - (ofs + p0 + w)));
+      }
+      if (p0 + w < in) {
+        ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * w * (double)(in - p0 - w) * nc);
+        LUB_TRY(launch_sgemm_chunk8_2(st, 0, 0, 0, nullptr, lda, nullptr, lda, nullptr, lda,
+                                      in - (p0 + w), nc, w, dg + w, lda,
+                                      blk + p0 + (c0 - ofs) * lda, lda,
+                                      blk + (p0 + w) + (c0 - ofs) * lda, lda));
+      }
+    }
+    const int64_t tr = n - (ofs + nb);
+    if (tr <= 0) continue;
+    const int64_t cr = c0 - (ofs + nb);  // column offset in the trailing part
+    if (tc)
+      LUB_TRY(tc_pack_range(st, kind, 0, tr, cr, cr + nc, nb, a + (ofs + nb) + ofs * lda, lda,
+                            a + ofs + (ofs + nb) * lda, lda, ws, wk));
+    LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tr, cr, nc, ws, wk, err, 0));
+  }
+  return LU_SUCCESS;
 }
 
 // Left-looking (Crout) factorization, restating src/lu_nopiv_ll.hxx:208-575
@@ -840,6 +939,14 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
   return s;
 }
 
+// Host-memory entry.  The matrix goes in by column chunks of whole outer
+// blocks on one copy stream while the device works: each chunk, once in,
+// receives the steps of the earlier chunks (catch_up, beside the
+// factorization of the previous chunk), then its own steps run (rl_factor
+// restricted to it), each sending its finished block column back on a
+// second copy stream while the factorization goes on.
+// Every element receives the same operations in the same order as in the
+// device-memory entry, so the factors are bit-identical to it.
 lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_a,
                          int64_t lda, float* d_a, int64_t ldda, int* d_info,
                          void* workspace, size_t ws_bytes) {
@@ -852,9 +959,6 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
   LUB_TRY(make_plan(o, n, n, LU_F32, &p));
   LUB_TRY(check_device());
   if (workspace != nullptr && ws_bytes < p.ws_bytes) return LU_ERR_WORKSPACE;
-  if (n > 0)
-    LUB_CUDA_TRY(cudaMemcpy2DAsync(d_a, (size_t)ldda * 4, h_a, (size_t)lda * 4,
-                                   (size_t)n * 4, (size_t)n, cudaMemcpyHostToDevice, st));
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {
@@ -866,10 +970,89 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
   int* err = first_bad + 1;
   lu_status s = launch_fill_int(st, first_bad, kNoBadPivot, 1);
   if (s == LU_SUCCESS) s = launch_fill_int(st, err, 0, 1);
-  HostSink sink;
-  sink.h = h_a;
-  sink.ldh = lda;
-  if (s == LU_SUCCESS && n > 0) s = rl_factor(p, st, d_a, ldda, wsb, first_bad, err, &sink);
+  const int64_t nb = p.nb;
+  const bool tc = is_tc(p.outer);
+  const TcOperand kind = tc_kind(p.outer);
+  const int64_t nblk = ceil_div(std::max<int64_t>(n, 1), nb);
+  // four chunks of whole outer blocks (B200 at n = 16384: 4 chunks 40 ms,
+  // 2 or 3 chunks 41-42 ms, 8 chunks 46 ms, one 47 ms)
+  const int64_t cw = ceil_div(nblk, 4) * nb;
+  const bool chunked = n > 2 * nb && !(tc && tc_scaled(kind) && nb % 128 != 0) &&
+                       ceil_div(n, cw) <= kMaxChunks;
+  auto h2d = [&](cudaStream_t sm, int64_t c0, int64_t c1) {
+    return cudaMemcpy2DAsync(d_a + c0 * ldda, (size_t)ldda * 4, h_a + c0 * lda,
+                             (size_t)lda * 4, (size_t)n * 4, (size_t)(c1 - c0),
+                             cudaMemcpyHostToDevice, sm);
+  };
+  auto d2h = [&](cudaStream_t sm, int64_t c0, int64_t c1) {
+    return cudaMemcpy2DAsync(h_a + c0 * lda, (size_t)lda * 4, d_a + c0 * ldda,
+                             (size_t)ldda * 4, (size_t)n * 4, (size_t)(c1 - c0),
+                             cudaMemcpyDeviceToHost, sm);
+  };
+  if (s == LU_SUCCESS && n > 0 && !chunked) {
+    if (h2d(st, 0, n) != cudaSuccess) s = LU_ERR_CUDA;
+    if (s == LU_SUCCESS) s = rl_factor(p, st, d_a, ldda, wsb, first_bad, err);
+    if (s == LU_SUCCESS && d2h(st, 0, n) != cudaSuccess) s = LU_ERR_CUDA;
+  } else if (s == LU_SUCCESS && n > 0) {
+    DevStreams* S = nullptr;
+    s = dev_streams(&S);
+    TcWs wk;
+    if (tc) wk = tc_ws_layout(256, n - nb, n - nb, nb, kind);
+    cudaStream_t ci = S ? S->copy : nullptr, co = S ? S->copy_out : nullptr;
+    ColumnSink sink;
+    sink.h = h_a;
+    sink.ldh = lda;
+    sink.out = co;
+    auto ok = [&](cudaError_t e) {
+      if (e != cudaSuccess && s == LU_SUCCESS) s = LU_ERR_CUDA;
+      return s == LU_SUCCESS;
+    };
+    // Under look-ahead rl_factor marks each step's finished block column
+    // with an event, and the catch-up of an arrived chunk runs on its own
+    // stream beside the factorization of the chunk before it (with its own
+    // operand buffer); otherwise the catch-up runs in order on the stream.
+    const bool la = p.lookahead && n > 2 * nb && !(tc && tc_scaled(kind) && nb % 128 != 0);
+    cudaStream_t cu = la && S ? S->catchup : st;
+    TcWs wcu = wk;
+    char* cubuf = wsb;
+    void* cu_alloc = nullptr;
+    if (s == LU_SUCCESS && la && tc) {
+      wcu = tc_ws_layout(0, n - nb, n - nb, nb, kind);
+      if (cudaMallocAsync(&cu_alloc, wcu.bytes, st) != cudaSuccess) s = LU_ERR_ALLOC;
+      cubuf = static_cast<char*>(cu_alloc);
+    }
+    if (s == LU_SUCCESS && ok(cudaEventRecord(S->fork, st)) &&
+        ok(cudaStreamWaitEvent(ci, S->fork, 0)) && ok(cudaStreamWaitEvent(co, S->fork, 0)) &&
+        (!la || ok(cudaStreamWaitEvent(cu, S->fork, 0)))) {
+      int q = 0;
+      for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q)
+        if (ok(h2d(ci, c0, std::min(n, c0 + cw)))) ok(cudaEventRecord(S->chunk_in[q], ci));
+      q = 0;
+      for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
+        const int64_t c1 = std::min(n, c0 + cw);
+        if (!ok(cudaStreamWaitEvent(cu, S->chunk_in[q], 0))) break;
+        if (q > 0) {
+          s = catch_up(p, cu, d_a, ldda, cubuf, wcu, err, c0, c1, la ? S : nullptr);
+          if (s != LU_SUCCESS) break;
+        }
+        if (la && (!ok(cudaEventRecord(S->cu_done, cu)) ||
+                   !ok(cudaStreamWaitEvent(st, S->cu_done, 0))))
+          break;
+        if ((s = rl_factor(p, st, d_a, ldda, wsb, first_bad, err, c0, c1, &sink)) != LU_SUCCESS)
+          break;
+      }
+      // join the side streams (also on the error path)
+      if (la) {
+        cudaEventRecord(S->cu_done, cu);
+        cudaStreamWaitEvent(st, S->cu_done, 0);
+      }
+      cudaEventRecord(S->out_done, co);
+      cudaStreamWaitEvent(st, S->out_done, 0);
+      cudaEventRecord(S->copied, ci);
+      cudaStreamWaitEvent(st, S->copied, 0);
+    }
+    if (cu_alloc) cudaFreeAsync(cu_alloc, st);
+  }
   if (s == LU_SUCCESS) s = launch_finalize_info(st, first_bad, err, d_info);
   if (owned) cudaFreeAsync(ws, st);
   return s;

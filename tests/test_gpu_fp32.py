@@ -290,17 +290,28 @@ def test_lu_ll_limits(built):
         rb.lu_nopiv_ll(a, nb=128, outer=rb.compute_type.TC32_E4M3)
 
 
-@pytest.mark.parametrize("n,outer", [(300, rb.FP32), (2048, rb.FP32), (2048, rb.TC32)])
-def test_host_entry_matches_device_entry(built, n, outer):
-    """lu_nopiv_rl_host_c (host matrix in, factors streamed back per outer
-    step) gives exactly the device entry point's factors."""
+@pytest.mark.parametrize("n,nb,outer,la,pad", [
+    (300, 256, rb.FP32, True, 0),                          # too small to chunk
+    (2048, 256, rb.FP32, True, 0),                         # 8 chunks of one block
+    (2048, 256, rb.TC32, True, 0),
+    (2048, 256, rb.TC32, False, 0),                        # no look-ahead
+    (2600, 256, rb.FP32, True, 3),                         # ragged last block, padded lda
+    (4000, 256, rb.TC32, True, 0),                         # 2-block chunks, ragged end
+    (3000, 128, rb.compute_type.TC32_BF16, True, 1),
+    (4096, 256, rb.compute_type.TC32_E4M3, True, 0),       # tile scales per chunk range
+    (4096, 256, rb.compute_type.TC32_SPLIT, True, 0),
+    (8192, 256, rb.TC32, True, 0)])                        # 4-block chunks: deep steps inside
+def test_host_entry_matches_device_entry(built, n, nb, outer, la, pad):
+    """lu_nopiv_rl_host_c (host matrix in by column chunks, each chunk caught
+    up with the earlier steps, factored and sent back while later chunks
+    compute) gives exactly the device entry point's factors."""
     a = O.gen_matrix(n, seed=n + 3, kind=1, alpha=1.5)
-    d = rb.colmajor(torch.from_numpy(a).cuda())
-    rb.lu_nopiv_rl(d, nb=256, outer=outer)
-    h = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+    d = rb.colmajor(torch.from_numpy(a).cuda(), lda=n + pad)
+    rb.lu_nopiv_rl(d, nb=nb, outer=outer, lookahead=la)
+    h = torch.empty((n, n + pad), dtype=torch.float32, pin_memory=True).t()[:n, :]
     h.copy_(torch.from_numpy(a))
-    work = rb.colmajor_empty(n, n, n, torch.float32)
-    info = rb.lu_nopiv_rl_host(h, work, nb=256, outer=outer)
+    work = rb.colmajor_empty(n, n, n + 2 * pad, torch.float32)
+    info = rb.lu_nopiv_rl_host(h, work, nb=nb, outer=outer, lookahead=la)
     torch.cuda.synchronize()
     assert int(info.item()) == 0
     assert np.array_equal(h.numpy(), d.cpu().numpy())

@@ -118,11 +118,13 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
   unsigned* sync = reinterpret_cast<unsigned*>(wb + w.off_sync);
   LUB_TRY(launch_lu_solve(st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, sync, R));
   for (;;) {
-    for (int64_t c = 0; c < nrhs; ++c) {
-      const double* b = d_b + c * ldb;
-      const double* x = d_x + c * ldx;
-      LUB_TRY(trans ? launch_residual_t(st, n, d_a, lda, b, x, R + c * n, mx + 3 * c)
-                    : launch_residual(st, n, d_a, lda, b, x, R + c * n, P, mx + 3 * c));
+    if (nrhs > 1) {
+      // all columns in one pass over A
+      LUB_TRY(launch_residual_multi(st, n, nrhs, d_a, lda, d_b, ldb, d_x, ldx, R, n,
+                                    trans != 0, mx));
+    } else {
+      LUB_TRY(trans ? launch_residual_t(st, n, d_a, lda, d_b, d_x, R, mx)
+                    : launch_residual(st, n, d_a, lda, d_b, d_x, R, P, mx));
     }
     LUB_CUDA_TRY(cudaMemcpyAsync(h.data(), mx, h.size() * 8, cudaMemcpyDeviceToHost, st));
     LUB_CUDA_TRY(cudaStreamSynchronize(st));

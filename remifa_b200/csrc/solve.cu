@@ -933,6 +933,141 @@ __global__ void axpy_kernel(int64_t n, const double* __restrict__ d,
   if (i < n) x[i] += d[i];
 }
 
+
+// ---- residuals of several right-hand sides: R = B - op(A) X, columns in
+// groups of kRG, A read once per group (fp64 arithmetic, each sum in a fixed
+// order, so the result does not depend on scheduling).  maxes[3c .. 3c+2]
+// receive max |r|, |x|, |b| of column c.
+constexpr int kRG = 8;    // right-hand sides per group
+constexpr int kRK = 64;   // rows of X staged per step (not transposed)
+
+__device__ __forceinline__ void atomic_max_abs(unsigned long long* p, double v) {
+  atomicMax(p, (unsigned long long)__double_as_longlong(fabs(v)));
+}
+
+// Not transposed: thread per row i, sums over k in order.
+__global__ void __launch_bounds__(kT)
+residual_multi_kernel(int64_t n, int64_t nrhs, const float* __restrict__ A, int64_t lda,
+                      const double* __restrict__ B, int64_t ldb,
+                      const double* __restrict__ X, int64_t ldx, double* __restrict__ R,
+                      int64_t ldr, unsigned long long* __restrict__ maxes) {
+  __shared__ double xs[kRK][kRG];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int64_t i = (int64_t)blockIdx.x * kT + tid;
+  const int64_t c0 = (int64_t)blockIdx.y * kRG;
+  const int nc = (int)((nrhs - c0) < kRG ? (nrhs - c0) : kRG);
+  double acc[kRG];
+#pragma unroll
+  for (int c = 0; c < kRG; ++c) acc[c] = 0.0;
+  const float* row = A + (i < n ? i : 0);
+  for (int64_t k0 = 0; k0 < n; k0 += kRK) {
+    const int kw = (int)((n - k0) < kRK ? (n - k0) : kRK);
+    for (int e = tid; e < kRK * kRG; e += kT) {
+      const int c = e / kRK, kk = e % kRK;
+      xs[kk][c] = (kk < kw && c < nc) ? X[(k0 + kk) + (c0 + c) * ldx] : 0.0;
+    }
+    __syncthreads();
+    if (i < n) {
+      if (kw == kRK) {
+#pragma unroll 8
+        for (int kk = 0; kk < kRK; ++kk) {
+          const double a = (double)row[(k0 + kk) * lda];
+#pragma unroll
+          for (int c = 0; c < kRG; ++c) acc[c] = fma(a, xs[kk][c], acc[c]);
+        }
+      } else {
+        for (int kk = 0; kk < kw; ++kk) {
+          const double a = (double)row[(k0 + kk) * lda];
+#pragma unroll
+          for (int c = 0; c < kRG; ++c) acc[c] = fma(a, xs[kk][c], acc[c]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < kRG; ++c) {
+    double r = 0.0, x = 0.0, b = 0.0;
+    if (i < n && c < nc) {
+      b = B[i + (c0 + c) * ldb];
+      x = X[i + (c0 + c) * ldx];
+      r = b - acc[c];
+      R[i + (c0 + c) * ldr] = r;
+    }
+    double m[3] = {fabs(r), fabs(x), fabs(b)};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m[q] = fmax(m[q], __shfl_xor_sync(0xffffffffu, m[q], o));
+      if (lane == 0 && c < nc) atomic_max_abs(&maxes[3 * (c0 + c) + q], m[q]);
+    }
+  }
+}
+
+// Transposed: r_j = b_j - sum_i A[i, j] x_i.  Warp w of a CTA owns columns
+// j0 + 4w .. j0 + 4w + 3 of A; lanes run over i (coalesced), each lane sums
+// its rows in order, then a halving exchange over the 32 lanes leaves the
+// (column, right-hand side) pair 4-column x 8-rhs index `lane` in lane.
+constexpr int kTJ = 4;                 // columns of A per warp
+constexpr int kTI = 256;               // rows of X staged per step
+__global__ void __launch_bounds__(kT)
+residual_multi_t_kernel(int64_t n, int64_t nrhs, const float* __restrict__ A, int64_t lda,
+                        const double* __restrict__ B, int64_t ldb,
+                        const double* __restrict__ X, int64_t ldx, double* __restrict__ R,
+                        int64_t ldr, unsigned long long* __restrict__ maxes) {
+  __shared__ double xs[kRG][kTI];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t jb = (int64_t)blockIdx.x * (kT / 32) * kTJ + warp * kTJ;
+  const int64_t c0 = (int64_t)blockIdx.y * kRG;
+  const int nc = (int)((nrhs - c0) < kRG ? (nrhs - c0) : kRG);
+  double v[kTJ * kRG];
+#pragma unroll
+  for (int q = 0; q < kTJ * kRG; ++q) v[q] = 0.0;
+  for (int64_t i0 = 0; i0 < n; i0 += kTI) {
+    const int iw = (int)((n - i0) < kTI ? (n - i0) : kTI);
+    for (int e = tid; e < kTI * kRG; e += kT) {
+      const int c = e / kTI, ii = e % kTI;
+      xs[c][ii] = (ii < iw && c < nc) ? X[(i0 + ii) + (c0 + c) * ldx] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < kTJ; ++jj) {
+      const int64_t j = jb + jj;
+      if (j < n) {
+        const float* col = A + j * lda + i0;
+        for (int ii = lane; ii < iw; ii += 32) {
+          const double a = (double)col[ii];
+#pragma unroll
+          for (int c = 0; c < kRG; ++c) v[jj * kRG + c] = fma(a, xs[c][ii], v[jj * kRG + c]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // halving exchange: after the step with offset s, slot q holds index
+  // q + (bits of lane above s) -- finally slot 0 holds index `lane`
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool up = lane & s;
+#pragma unroll
+    for (int q = 0; q < s; ++q) {
+      const double send = up ? v[q] : v[q + s];
+      const double keep = up ? v[q + s] : v[q];
+      v[q] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  const int jj = lane / kRG, c = lane % kRG;
+  const int64_t j = jb + jj;
+  if (j < n && c < nc) {
+    const double b = B[j + (c0 + c) * ldb];
+    const double x = X[j + (c0 + c) * ldx];
+    const double r = b - v[0];
+    R[j + (c0 + c) * ldr] = r;
+    atomic_max_abs(&maxes[3 * (c0 + c)], r);
+    atomic_max_abs(&maxes[3 * (c0 + c) + 1], x);
+    atomic_max_abs(&maxes[3 * (c0 + c) + 2], b);
+  }
+}
 }  // namespace
 
 size_t trsm_sync_bytes(int64_t nrhs) {
@@ -1020,6 +1155,25 @@ lu_status launch_norm_inf(cudaStream_t st, int64_t n, const float* A,
   rowsum_partial_kernel<<<g, kT, 0, st>>>(n, A, lda, P);
   LUB_LAUNCH_CHECK();
   rowsum_final_kernel<<<(unsigned)ceil_div(n, kT), kT, 0, st>>>(n, nch, P, out);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+lu_status launch_residual_multi(cudaStream_t st, int64_t n, int64_t nrhs, const float* A,
+                                int64_t lda, const double* B, int64_t ldb, const double* X,
+                                int64_t ldx, double* R, int64_t ldr, bool trans,
+                                unsigned long long* maxes) {
+  if (n <= 0 || nrhs <= 0) return LU_SUCCESS;
+  LUB_CUDA_TRY(cudaMemsetAsync(maxes, 0, (size_t)3 * nrhs * sizeof(unsigned long long), st));
+  const int64_t groups = ceil_div(nrhs, kRG);
+  if (groups > 65535) return LU_ERR_INVALID_ARG;
+  if (!trans) {
+    dim3 g((unsigned)ceil_div(n, kT), (unsigned)groups);
+    residual_multi_kernel<<<g, kT, 0, st>>>(n, nrhs, A, lda, B, ldb, X, ldx, R, ldr, maxes);
+  } else {
+    dim3 g((unsigned)ceil_div(n, (kT / 32) * kTJ), (unsigned)groups);
+    residual_multi_t_kernel<<<g, kT, 0, st>>>(n, nrhs, A, lda, B, ldb, X, ldx, R, ldr, maxes);
+  }
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

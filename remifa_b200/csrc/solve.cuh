@@ -34,6 +34,14 @@ lu_status launch_residual(cudaStream_t st, int64_t n, const float* A,
 lu_status launch_norm_inf(cudaStream_t st, int64_t n, const float* A,
                           int64_t lda, void* ws, unsigned long long* out);
 
+// R = B - op(A) X for nrhs >= 1 columns at once (A read once per group of 8
+// columns; fp64, fixed summation order); maxes[3c .. 3c+2] receive the bit
+// patterns of max|r|, max|x|, max|b| of column c.
+lu_status launch_residual_multi(cudaStream_t st, int64_t n, int64_t nrhs, const float* A,
+                                int64_t lda, const double* B, int64_t ldb, const double* X,
+                                int64_t ldx, double* R, int64_t ldr, bool trans,
+                                unsigned long long* maxes);
+
 // x += d
 lu_status launch_axpy(cudaStream_t st, int64_t n, const double* d, double* x);
 

@@ -79,6 +79,18 @@ def test_convert_bit_exact(built, dt, fmt, m, n, lda):
             np.testing.assert_array_equal(got, want)
 
 
+def test_convert_large_bit_exact(built):
+    """8192 x 8192 fp32 -> fp16 (256 MB in, larger than L2), scale 2^-2."""
+    n = 8192
+    rng = np.random.default_rng(8)
+    a = np.asfortranarray((rng.standard_normal((n, n)) * 300).astype(np.float32))
+    da = to_dev(a)
+    out = rb.colmajor_empty(n, n, n, torch.float16)
+    rb.convert(da, out, scale_log2=-2)
+    got = out.float().cpu().numpy()
+    np.testing.assert_array_equal(got, O.round_fmt(a, 1, -2))
+
+
 def test_convert_f16_matches_reference(built, ref):
     rng = np.random.default_rng(3)
     m, n = 128, 40

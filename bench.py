@@ -51,7 +51,8 @@ WORKLOADS = {
                                alpha=1.5, kscale=0, oracle_fmt=4),
 }
 # Workloads with their own step (see the run_* functions below).
-SPECIAL = ("batch_10000_n16_512", "ll_f16_n16384", "precision_n32768", "adjoint_n8192")
+SPECIAL = ("batch_10000_n16_512", "ll_f16_n16384", "precision_n32768", "adjoint_n8192",
+           "c2_grid_n16384")
 DEFAULT_WORKLOAD = "lu_tc32_rl_n16384"
 NVML_REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x10: "sync_boost",
                 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
@@ -742,6 +743,101 @@ def run_adjoint(args, torch, rb):
     print(json.dumps(line), flush=True)
 
 
+def run_c2_grid(args, torch, rb):
+    """The n = 16384 mixed-precision workload over its matrix family: A = R +
+    D (R ~ N(0,1)/sqrt(n)), row dominance alpha in {1.05, 1.5, 4}, entries
+    scaled by 2^k, k in {0, 8} (seeds 1..6).  Per matrix: (i) right-looking,
+    fp32 storage, fp16 tensor-core updates; (ii) left-looking with fp16
+    storage (the matrix scaled by a power of two first if it exceeds the
+    fp16 range, which rescales U exactly).  Reported per run: TFLOP/s, info,
+    finite factors, the backward error of the unrefined solve and the FP64
+    refinement steps to 1e-14.  value = the smallest right-looking TFLOP/s."""
+    import math
+    n = 16384
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    xt = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    runs = []
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = _events(torch)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return sorted(ts)[len(ts) // 2]
+
+    def solve_quality(a32, lu32):
+        b = torch.zeros(n, dtype=torch.float64, device="cuda")
+        for j0 in range(0, n, 2048):
+            b += a32[:, j0:j0 + 2048].double() @ xt[j0:j0 + 2048]
+        _, _, be0 = rb.refine(a32, lu32, b, tol=1e-14, max_iter=0)
+        x, it, be = rb.refine(a32, lu32, b, tol=1e-14, max_iter=30)
+        return be0, it, be
+
+    seed = 1
+    reps = max(args.steps, 1)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for alpha in (1.05, 1.5, 4.0):
+            for k in (0, 8):
+                a = rb.gen_matrix(n, seed=seed, kind=1, alpha=alpha, kscale=k)
+                amax = float(a.abs().max())
+                lu = rb.colmajor_empty(n, n, n, torch.float32)
+                info = torch.zeros(1, dtype=torch.int32, device="cuda")
+                ms = timed(lambda: (lu.copy_(a), rb.lu_nopiv_rl(lu, nb=256, outer=rb.TC32,
+                                                                 info=info)), reps)
+                t_copy = timed(lambda: lu.copy_(a), reps)
+                ms_f = max(ms - t_copy, 1e-6)
+                lu.copy_(a)
+                rb.lu_nopiv_rl(lu, nb=256, outer=rb.TC32, info=info)
+                be0, it, be = solve_quality(a, lu)
+                rl = {"tflops": lu_flops(n) / (ms_f / 1e3) / 1e12, "ms": ms_f,
+                      "info": int(info.item()), "finite": bool(torch.isfinite(lu).all()),
+                      "berr_unrefined": be0, "refine_iters": it, "berr": be}
+                # (ii) fp16 storage, left-looking
+                s_log2 = 0
+                while amax * 2.0 ** (-s_log2) > 30000.0:
+                    s_log2 += 1
+                a16 = rb.colmajor_empty(n, n, n, torch.float16)
+                a16.copy_(a * 2.0 ** (-s_log2))
+                w16 = rb.colmajor_empty(n, n, n, torch.float16)
+                ms16 = timed(lambda: (w16.copy_(a16), rb.lu_nopiv_ll(w16, nb=128, outer=rb.TC32,
+                                                                      info=info)), reps)
+                t16 = timed(lambda: w16.copy_(a16), reps)
+                ms16_f = max(ms16 - t16, 1e-6)
+                w16.copy_(a16)
+                rb.lu_nopiv_ll(w16, nb=128, outer=rb.TC32, info=info)
+                info16 = int(info.item())
+                lu.copy_(w16)
+                if s_log2:
+                    lu.copy_(torch.tril(lu, -1) + torch.triu(lu) * 2.0 ** s_log2)
+                be0h, ith, beh = solve_quality(a, lu)
+                ll = {"tflops": lu_flops(n) / (ms16_f / 1e3) / 1e12, "ms": ms16_f,
+                      "info": info16, "finite": bool(torch.isfinite(w16).all()),
+                      "fp16_scale_log2": -s_log2, "berr_unrefined": be0h,
+                      "refine_iters": ith, "berr": beh}
+                runs.append({"alpha": alpha, "kscale": k, "seed": seed, "max_abs_a": amax,
+                             "rl_tc32_f32": rl, "ll_f16": ll})
+                del a, lu, a16, w16
+                torch.cuda.empty_cache()
+                seed += 1
+    worst = min(r["rl_tc32_f32"]["tflops"] for r in runs)
+    line = _base_line(args, "LU TFLOP/s (2n^3/3), smallest over the C2 matrix grid", worst,
+                      "TFLOP/s", lu_flops(n) / worst / 1e9,
+                      dtype="f32 storage + TC32 (RL); f16 storage + TC32 (LL)",
+                      config={"workload": args.workload, "n": n, "nb_rl": 256, "nb_ll": 128,
+                              "matrix": "2^k (R + D), R ~ N(0,1)/sqrt(n), dominance alpha",
+                              "grid": "alpha in {1.05, 1.5, 4} x k in {0, 8}, seeds 1..6"})
+    line["runs"] = runs
+    line["clocks"] = clk.summary()
+    print(json.dumps(line), flush=True)
+
+
 def run_special(args) -> None:
     if args.impl == "reference":
         print(json.dumps({"impl": "reference", "workload": args.workload,
@@ -753,7 +849,8 @@ def run_special(args) -> None:
     import remifa_b200 as rb
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     fn = {"batch_10000_n16_512": run_batch, "ll_f16_n16384": run_ll16,
-          "precision_n32768": run_precision, "adjoint_n8192": run_adjoint}[args.workload]
+          "precision_n32768": run_precision, "adjoint_n8192": run_adjoint,
+          "c2_grid_n16384": run_c2_grid}[args.workload]
     fn(args, torch, rb)
 
 

@@ -192,7 +192,7 @@ struct DevStreams {
   cudaEvent_t copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
-  cudaEvent_t done_with[2] = {nullptr, nullptr};  // U2 finished reading buffer b
+  cudaEvent_t done_with[3] = {nullptr, nullptr, nullptr};  // U2 finished reading buffer b
 };
 
 static lu_status dev_streams(DevStreams** out) {
@@ -218,7 +218,7 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
-                           &d.done_with[0], &d.done_with[1], &d.copied,
+                           &d.done_with[0], &d.done_with[1], &d.done_with[2], &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
                            &d.u1_done, &d.join_s,
                            &d.spack_done})
@@ -308,15 +308,53 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     return LU_SUCCESS;
   }
   if (is_tc(p->outer) && n > p->nb) {
-    // two operand buffers: with look-ahead, step k+1 packs while the bulk
-    // update of step k still reads step k's copies
+    // three operand buffers: with look-ahead the panel of step k writes its
+    // copies while the bulk updates of steps k-1 and k-2 still read theirs
     const int64_t t = n - p->nb;
     TcWs w = tc_ws_layout(off, t, t, p->nb, tc_kind(p->outer));
     p->off_lcopy = w.off_a;
-    off += 2 * w.bytes;
+    off += 3 * w.bytes;
   }
   p->ws_bytes = off;
   return LU_SUCCESS;
+}
+
+// Where a step's panel launches write the tensor-core operand copies of the
+// rows / columns they finish (fp16 / bf16 kinds: no separate packing pass).
+struct PackTarget {
+  char* ws = nullptr;
+  const TcWs* w = nullptr;
+  int64_t ldk = 0, nb = 0;
+  int bf16 = 0;
+  // the launch of sub-block p0 (width wd) whose L rows / U columns start
+  // offL / offU past the sub-block's edge
+  LuPack at(int64_t p0, int wd, int64_t offL, int64_t offU) const {
+    LuPack k;
+    if (!ws) return k;
+    k.pa = ws + w->off_a;
+    k.pb = ws + w->off_b;
+    k.ldk = ldk;
+    k.row0 = p0 + wd + offL - nb;
+    k.col0 = p0 + wd + offU - nb;
+    k.k0 = (int)p0;
+    k.bf16 = bf16;
+    return k;
+  }
+};
+
+static bool fused_pack(lu_compute outer) {
+  return is_tc(outer) && !tc_scaled(tc_kind(outer));
+}
+
+static PackTarget pack_target(const Plan& p, char* ws, const TcWs& w) {
+  PackTarget t;
+  if (!fused_pack(p.outer)) return t;
+  t.ws = ws;
+  t.w = &w;
+  t.ldk = tc_packed_k(tc_kind(p.outer), p.nb);
+  t.nb = p.nb;
+  t.bf16 = tc_kind(p.outer) == TcOperand::BF16;
+  return t;
 }
 
 // Factor the outer block column/row starting at (ofs, ofs): width `in`,
@@ -324,7 +362,8 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
 // a whole factorization; fewer columns when only a column range is present).
 static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
                               int64_t lda, int64_t ofs, int64_t in,
-                              int64_t updm, int64_t updc, int* first_bad) {
+                              int64_t updm, int64_t updc, int* first_bad,
+                              const PackTarget& pt = PackTarget()) {
   float* blk = a + ofs + ofs * lda;
   for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
     const int w = (int)std::min<int64_t>(in - p0, p.diag_w);
@@ -337,7 +376,8 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
     if (rest > 0 || restc > 0) {
       ProfScope ps("lupanel", st, 8.0 * (rest + restc) * w,
                    (double)(rest + restc) * (double)w * w);
-      LUB_TRY(launch_lupanel(st, dg, lda, w, rest, restc));
+      const LuPack pk = pt.at(p0, w, 0, 0);
+      LUB_TRY(launch_lupanel(st, dg, lda, w, rest, restc, false, 0, 0, &pk));
     }
     if (p0 + w < in) {
       ProfScope ps("sgemm_chunk8", st, 0.0,
@@ -365,10 +405,11 @@ static lu_status factor_block(const Plan& p, cudaStream_t st, float* a,
 // operations in the same order as in factor_block.
 static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* S,
                                     float* a, int64_t lda, int64_t ofs, int64_t in,
-                                    int64_t updm, int64_t updc, int* first_bad) {
+                                    int64_t updm, int64_t updc, int* first_bad,
+                                    const PackTarget& pt = PackTarget()) {
   const int w = p.diag_w;
   if (in != 2 * w || updm <= in)
-    return factor_block(p, st, a, lda, ofs, in, updm, updc, first_bad);
+    return factor_block(p, st, a, lda, ofs, in, updm, updc, first_bad, pt);
   cudaStream_t ss = S->side;
   float* blk = a + ofs + ofs * lda;
   const int64_t big = updm - 2 * w;   // L rows beyond the outer block
@@ -387,7 +428,8 @@ static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* 
   LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->diag_done, 0));
   {
     ProfScope ps("lupanel", ss, 8.0 * (big + bigc) * w, (double)(big + bigc) * (double)w * w);
-    LUB_TRY(launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w));
+    const LuPack pk = pt.at(0, w, w, w);
+    LUB_TRY(launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w, &pk));
   }
   LUB_CUDA_TRY(cudaStreamWaitEvent(ss, S->small_done, 0));
   {
@@ -414,7 +456,8 @@ static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* 
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->big_done, 0));
   {
     ProfScope ps("lupanel", st, 8.0 * (big + bigc) * w, (double)(big + bigc) * (double)w * w);
-    LUB_TRY(launch_lupanel(st, dg1, lda, w, big, bigc));
+    const LuPack pk = pt.at(w, w, 0, 0);
+    LUB_TRY(launch_lupanel(st, dg1, lda, w, big, bigc, false, 0, 0, &pk));
   }
   return LU_SUCCESS;
 }
@@ -474,27 +517,31 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t n = p.n, nb = p.nb;
   if (col_end < 0) col_end = n;
   const bool tc = is_tc(p.outer);
-  TcWs w2[2];
+  TcWs w2[3];
   if (tc && n > nb) {
     w2[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
-    w2[1] = w2[0];
     const size_t shift = w2[0].bytes;
-    w2[1].off_a += shift; w2[1].off_b += shift; w2[1].off_sa += shift;
-    w2[1].off_sb += shift; w2[1].off_tmp += shift;
+    for (int b = 1; b < 3; ++b) {
+      w2[b] = w2[0];
+      w2[b].off_a += b * shift; w2[b].off_b += b * shift; w2[b].off_sa += b * shift;
+      w2[b].off_sb += b * shift; w2[b].off_tmp += b * shift;
+    }
   }
+  const bool fused = fused_pack(p.outer);
   const bool la = p.lookahead && n > 2 * nb &&
                   !(tc && tc_scaled(tc_kind(p.outer)) && nb % 128 != 0);
   if (!la) {
     for (int64_t ofs = col_begin; ofs < col_end; ofs += nb) {
       const int64_t in = std::min(n - ofs, nb);
-      LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, col_end - ofs, first_bad));
+      LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, col_end - ofs, first_bad,
+                           pack_target(p, ws, w2[0])));
       if (sink)
         LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h + ofs * sink->ldh, (size_t)sink->ldh * 4,
                                        a + ofs * lda, (size_t)lda * 4, (size_t)n * 4,
                                        (size_t)in, cudaMemcpyDeviceToHost, st));
       const int64_t tr = n - (ofs + nb), tcn = col_end - (ofs + nb);
       if (tr <= 0 || tcn <= 0) continue;
-      if (tc)
+      if (tc && !fused)
         LUB_TRY(tc_pack(st, tc_kind(p.outer), tr, tcn, nb, a + (ofs + nb) + ofs * lda,
                         lda, a + ofs + (ofs + nb) * lda, lda, ws, w2[0]));
       LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tr, 0, tcn, ws, w2[0], err, 0));
@@ -544,8 +591,14 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     const int64_t updm = n - ofs, updc = col_end - ofs;
     const int64_t tr = n - (ofs + nb);        // trailing rows
     const int64_t tcn = col_end - (ofs + nb); // trailing columns
-    const int buf = (int)(step & 1);
+    const int buf = (int)(step % 3);
     const TcWs& wk = w2[buf];
+    const PackTarget pt = pack_target(p, ws, wk);
+    // this step's panel writes operand buffer `buf`: the bulk update of step
+    // k-3 must have finished reading it
+    if (tc && step >= 3 && (!ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0)) ||
+                            !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))))
+      break;
     // the previous step's update of this block column / row ran partly on
     // the side stream: a deep step only touches the diagonal square on the
     // panel stream and everything else on the side stream after it, any
@@ -577,7 +630,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       if (!ok(cudaStreamWaitEvent(ss, S->diag_done, 0))) break;
       {
         ProfScope ps("lupanel", ss, 8.0 * (big + bigc) * w, (double)(big + bigc) * w * w);
-        if ((status = launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w)) != LU_SUCCESS)
+        const LuPack pk = pt.at(0, w, w, w);
+        if ((status = launch_lupanel(ss, blk, lda, w, big, bigc, false, w, w, &pk)) !=
+            LU_SUCCESS)
           break;
       }
       if (!ok(cudaStreamWaitEvent(ss, S->small_done, 0))) break;
@@ -613,23 +668,24 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       const int64_t mh = std::min(sq, big), nh = std::min(sq, bigc);
       {
         ProfScope ps("lupanel", sp, 8.0 * (mh + nh) * w, (double)(mh + nh) * w * w);
-        if ((status = launch_lupanel(sp, dg1, lda, w, mh, nh, false, 0, 0)) != LU_SUCCESS)
+        const LuPack pk = pt.at(w, w, 0, 0);
+        if ((status = launch_lupanel(sp, dg1, lda, w, mh, nh, false, 0, 0, &pk)) != LU_SUCCESS)
           break;
       }
       if (!ok(cudaStreamWaitEvent(ss, S->diag1_done, 0))) break;
       {
         ProfScope ps("lupanel", ss, 8.0 * (big - mh + bigc - nh) * w,
                      (double)(big - mh + bigc - nh) * w * w);
-        if ((status = launch_lupanel(ss, dg1, lda, w, big - mh, bigc - nh, false, mh, nh)) !=
-            LU_SUCCESS)
+        const LuPack pk = pt.at(w, w, mh, nh);
+        if ((status = launch_lupanel(ss, dg1, lda, w, big - mh, bigc - nh, false, mh, nh,
+                                     &pk)) != LU_SUCCESS)
           break;
       }
       if (sink && !sink_column(ofs, in, true)) break;
       // L21 rows / U12 columns relative to the trailing part (ofs + nb)
       const float* L21 = a + (ofs + nb) + ofs * lda;
       const float* U12 = a + ofs + (ofs + nb) * lda;
-      if (tc) {
-        if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
+      if (tc && !fused) {
         if ((status = tc_pack_range(sp, kind, 0, sq, 0, sq, nb, L21, lda, U12, lda, ws, wk)) !=
             LU_SUCCESS)
           break;
@@ -650,8 +706,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
         if (!ok(cudaEventRecord(S->diag_done, sp))) break;
       }
       // side stream: the rest of the packing and of U1
-      if (tc) {
-        if (step >= 2 && !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))) break;
+      if (tc && !fused) {
         if ((status = tc_pack_range(ss, kind, sq, tr, sq, tcn, nb, L21, lda, U12, lda, ws,
                                     wk)) != LU_SUCCESS)
           break;
@@ -667,16 +722,14 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       if (!ok(cudaEventRecord(S->u1_done, ss))) break;
       prev_deep = true;
     } else {
-      status = factor_block_split(p, sp, S, a, lda, ofs, in, updm, updc, first_bad);
+      status = factor_block_split(p, sp, S, a, lda, ofs, in, updm, updc, first_bad, pt);
       if (status != LU_SUCCESS) break;
       // factor_block_split ends on sp after the side stream's share
       if (sink && !sink_column(ofs, in, false)) break;
       prev_deep = false;
       pre = false;
       if (tr <= 0 || tcn <= 0) continue;
-      if (tc) {
-        // U2 of step k-2 read this buffer
-        if (step >= 2 && !ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0))) break;
+      if (tc && !fused) {
         status = tc_pack(sp, kind, tr, tcn, nb, a + (ofs + nb) + ofs * lda, lda,
                          a + ofs + (ofs + nb) * lda, lda, ws, wk);
         if (status != LU_SUCCESS) break;

@@ -162,9 +162,12 @@ sgemm_update_kernel(int64_t M, int64_t N, int64_t K, float alpha,
 }
 
 // Rank-8-chunked update C -= A * B over up to two independent regions in one
-// launch (the rest of an outer block column and of its block row), 64 x 64
-// tiles, 4 x 4 outputs per thread: the skinny shapes of these updates
-// (K <= 128, one dimension 128 wide) need many small tiles to fill the GPU.
+// launch (the rest of an outer block column and of its block row), TM x TM
+// outputs per thread on CB x CB tiles (CB = 16 TM: 64 for the wide updates,
+// 32 for the small ones, which then get four times as many CTAs): the skinny
+// shapes of these updates (K <= 128, one dimension 128 wide) need many small
+// tiles to fill the GPU.  Every element's sum runs over K in chunks of 8
+// (acc from 0, then subtracted) whatever the tile size.
 struct ChunkRegion {
   int64_t M, N, K;
   const float* A; int64_t lda;
@@ -173,10 +176,11 @@ struct ChunkRegion {
   int tiles_m, tiles;
 };
 
-constexpr int CB = 64;
-
+template <int TM>
 __global__ void __launch_bounds__(NT)
 sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
+  constexpr int CB = 16 * TM;            // tile edge
+  constexpr int LA = CB * BK / NT;       // tile elements loaded per thread
   __shared__ __align__(16) float As[2][BK][CB];
   __shared__ __align__(16) float Bs[2][BK][CB];
   const bool second = (int)blockIdx.x >= r0.tiles;
@@ -186,33 +190,34 @@ sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
   const int64_t n0 = (int64_t)(t / r.tiles_m) * CB;
   const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;
-  const int a_col = tid / 32, a_row = (tid % 32) * 2;  // A tile CB x BK
-  const int b_col = tid / 4, b_k = (tid % 4) * 2;      // B tile BK x CB
+  const int a_col = tid / (CB / LA), a_row = (tid % (CB / LA)) * LA;  // A tile CB x BK
+  const int b_col = tid / (BK / LA), b_k = (tid % (BK / LA)) * LA;    // B tile BK x CB
 
-  float ra[2], rb[2];
+  float ra[LA], rb[LA];
   auto load_tiles = [&](int64_t k0) {
     const int64_t ak = k0 + a_col;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < LA; ++i)
       ra[i] = (ak < r.K && m0 + a_row + i < r.M) ? r.A[m0 + a_row + i + ak * r.lda] : 0.0f;
     const int64_t bc = n0 + b_col;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < LA; ++i)
       rb[i] = (bc < r.N && k0 + b_k + i < r.K) ? r.B[k0 + b_k + i + bc * r.ldb] : 0.0f;
   };
   auto store_tiles = [&](int buf) {
-    As[buf][a_col][a_row] = ra[0];
-    As[buf][a_col][a_row + 1] = ra[1];
-    Bs[buf][b_k][b_col] = rb[0];
-    Bs[buf][b_k + 1][b_col] = rb[1];
+#pragma unroll
+    for (int i = 0; i < LA; ++i) {
+      As[buf][a_col][a_row + i] = ra[i];
+      Bs[buf][b_k + i][b_col] = rb[i];
+    }
   };
 
-  float cr[4][4], acc[4][4];
+  float cr[TM][TM], acc[TM][TM];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int64_t row = m0 + tx * 4 + i, col = n0 + ty * 4 + j;
+    for (int j = 0; j < TM; ++j) {
+      const int64_t row = m0 + tx * TM + i, col = n0 + ty * TM + j;
       cr[i][j] = (row < r.M && col < r.N) ? r.C[row + col * r.ldc] : 0.0f;
       acc[i][j] = 0.0f;
     }
@@ -225,20 +230,28 @@ sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
     if (kt + 1 < nk) load_tiles((kt + 1) * BK);
 #pragma unroll
     for (int k = 0; k < BK; ++k) {
-      const float4 a4 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
-      const float4 b4 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
-      const float a[4] = {a4.x, a4.y, a4.z, a4.w};
-      const float b[4] = {b4.x, b4.y, b4.z, b4.w};
+      float a[TM], b[TM];
+      if constexpr (TM == 4) {
+        const float4 a4 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
+        const float4 b4 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+        a[0] = a4.x; a[1] = a4.y; a[2] = a4.z; a[3] = a4.w;
+        b[0] = b4.x; b[1] = b4.y; b[2] = b4.z; b[3] = b4.w;
+      } else {
+        const float2 a2 = *reinterpret_cast<const float2*>(&As[buf][k][tx * 2]);
+        const float2 b2 = *reinterpret_cast<const float2*>(&Bs[buf][k][ty * 2]);
+        a[0] = a2.x; a[1] = a2.y;
+        b[0] = b2.x; b[1] = b2.y;
+      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < TM; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
     }
     // one rank-8 chunk done: C -= acc (the reference's K = 8 GEMM)
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < TM; ++j) {
         cr[i][j] = __fsub_rn(cr[i][j], acc[i][j]);
         acc[i][j] = 0.0f;
       }
@@ -248,10 +261,10 @@ sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
     }
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int64_t row = m0 + tx * 4 + i, col = n0 + ty * 4 + j;
+    for (int j = 0; j < TM; ++j) {
+      const int64_t row = m0 + tx * TM + i, col = n0 + ty * TM + j;
       if (row < r.M && col < r.N) r.C[row + col * r.ldc] = cr[i][j];
     }
 }
@@ -266,16 +279,26 @@ lu_status launch_sgemm_chunk8_2(cudaStream_t st, int64_t M0, int64_t N0,
                                 int64_t ldb1, float* C1, int64_t ldc1) {
   ChunkRegion r0{M0, N0, K0, A0, lda0, B0, ldb0, C0, ldc0, 0, 0};
   ChunkRegion r1{M1, N1, K1, A1, lda1, B1, ldb1, C1, ldc1, 0, 0};
-  for (ChunkRegion* r : {&r0, &r1}) {
-    if (r->M > 0 && r->N > 0 && r->K > 0) {
-      r->tiles_m = (int)ceil_div(r->M, CB);
-      r->tiles = r->tiles_m * (int)ceil_div(r->N, CB);
+  // 64 x 64 tiles unless that leaves fewer than 64 CTAs (then 32 x 32)
+  auto count = [&](int cb) {
+    int64_t total = 0;
+    for (ChunkRegion* r : {&r0, &r1}) {
+      r->tiles_m = r->tiles = 0;
+      if (r->M > 0 && r->N > 0 && r->K > 0) {
+        r->tiles_m = (int)ceil_div(r->M, cb);
+        r->tiles = r->tiles_m * (int)ceil_div(r->N, cb);
+      }
+      total += r->tiles;
     }
-  }
-  const int64_t grid = (int64_t)r0.tiles + r1.tiles;
+    return total;
+  };
+  int64_t grid = count(64);
+  const bool small = grid > 0 && grid < 64;
+  if (small) grid = count(32);
   if (grid == 0) return LU_SUCCESS;
   if (grid > INT32_MAX) return LU_ERR_INVALID_ARG;
-  sgemm_chunk8_kernel<<<(unsigned)grid, NT, 0, st>>>(r0, r1);
+  if (small) sgemm_chunk8_kernel<2><<<(unsigned)grid, NT, 0, st>>>(r0, r1);
+  else sgemm_chunk8_kernel<4><<<(unsigned)grid, NT, 0, st>>>(r0, r1);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

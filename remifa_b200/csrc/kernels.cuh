@@ -9,13 +9,29 @@ namespace lub {
 size_t diag_smem_bytes(int w);
 lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
                              int64_t col0, int* first_bad);
+// Low-precision K-major copies a panel launch also writes (fp16 or bf16:
+// the tensor-core operands of the trailing update).  L row r of the launch
+// (counted from its first item) goes to pa[(row0 + r) * ldk + k0 + c],
+// c < w; U column q to pb[(col0 + q) * ldk + k0 + i], i < w.  Rows and
+// columns whose packed index is negative lie inside the outer block and are
+// not copied.
+struct LuPack {
+  void* pa = nullptr;
+  void* pb = nullptr;
+  int64_t ldk = 0;
+  int64_t row0 = 0, col0 = 0;
+  int k0 = 0;
+  int bf16 = 0;
+};
+
 // L rows (M of them, below) and U columns (N, right) of the w x w factored
 // diagonal block dg, one launch.  left: left-looking (Crout) update order.
 // offL / offU: the first L row / U column handled is that many rows below /
-// columns right of the block's edge.
+// columns right of the block's edge.  pack: also write the finished rows /
+// columns as low-precision operand copies.
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
                          int64_t M, int64_t N, bool left = false, int64_t offL = 0,
-                         int64_t offU = 0);
+                         int64_t offU = 0, const LuPack* pack = nullptr);
 // Left-looking (Crout) factorization of a w x w (w <= 128) diagonal block.
 lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
                             int64_t col0, int* first_bad);

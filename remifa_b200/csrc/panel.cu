@@ -468,7 +468,7 @@ __device__ __forceinline__ void lupanel_strip(const float* F, int lf, const floa
 
 __global__ void __launch_bounds__(kPanelT)
 lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
-               int64_t N, int nL, bool left, int64_t offL, int64_t offU) {
+               int64_t N, int nL, bool left, int64_t offL, int64_t offU, LuPack pk) {
   extern __shared__ __align__(16) float smem[];
   const int tid = threadIdx.x;
   const int wp = ((w + 7) / 8) * 8;  // padded width (zero filled)
@@ -541,6 +541,50 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
       const int i = idx % w, qq = idx / w;
       const int64_t col = item0 + qq;
       if (col < N) A[i + col * lda] = S[qq * ls + i];
+    }
+  }
+  // the finished items as tensor-core operands: item qq's w values are
+  // contiguous along K in both copies (consecutive threads, consecutive k)
+  void* dst = is_l ? pk.pa : pk.pb;
+  if (dst) {
+    const int64_t lim = is_l ? M : N;
+    const int64_t base = (is_l ? pk.row0 : pk.col0) + item0;
+    if (w % 8 == 0 && pk.ldk % 8 == 0 && pk.k0 % 8 == 0) {
+      // 8 values -> one 16-byte store
+      const int w8 = w / 8;
+      for (int idx = tid; idx < kItems * w8; idx += kPanelT) {
+        const int c8 = idx % w8, qq = idx / w8;
+        const int64_t pr = base + qq;
+        if (item0 + qq < lim && pr >= 0) {
+          float v[8];
+          ld8(&S[qq * ls + 8 * c8], v);
+          uint4 out;
+          uint32_t* o32 = reinterpret_cast<uint32_t*>(&out);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            if (pk.bf16) {
+              const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+              o32[e] = *reinterpret_cast<const uint32_t*>(&h);
+            } else {
+              const __half2 h = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
+              o32[e] = *reinterpret_cast<const uint32_t*>(&h);
+            }
+          }
+          *reinterpret_cast<uint4*>(static_cast<uint16_t*>(dst) + pr * pk.ldk + pk.k0 +
+                                    8 * c8) = out;
+        }
+      }
+    } else {
+      for (int idx = tid; idx < kItems * w; idx += kPanelT) {
+        const int c = idx % w, qq = idx / w;
+        const int64_t pr = base + qq;
+        if (item0 + qq < lim && pr >= 0) {
+          const float v = S[qq * ls + c];
+          const int64_t o = pr * pk.ldk + pk.k0 + c;
+          if (pk.bf16) static_cast<__nv_bfloat16*>(dst)[o] = __float2bfloat16_rn(v);
+          else static_cast<__half*>(dst)[o] = __float2half_rn(v);
+        }
+      }
     }
   }
   (void)nitems;
@@ -646,15 +690,17 @@ static size_t lupanel_smem_bytes(int w, bool left) {
 }
 
 lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
-                         int64_t M, int64_t N, bool left, int64_t offL, int64_t offU) {
+                         int64_t M, int64_t N, bool left, int64_t offL, int64_t offU,
+                         const LuPack* pack) {
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
   const int64_t nL = M > 0 ? ceil_div(M, kItems) : 0;
   const int64_t nU = N > 0 ? ceil_div(N, kItems) : 0;
   if (nL + nU == 0) return LU_SUCCESS;
   const size_t sm = lupanel_smem_bytes(w, left);
   LUB_CUDA_TRY(set_smem_limit((const void*)lupanel_kernel, sm));
+  const LuPack pk = pack ? *pack : LuPack{};
   lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL,
-                                                           left, offL, offU);
+                                                           left, offL, offU, pk);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

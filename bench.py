@@ -352,12 +352,14 @@ def main() -> None:
     # each finished block column goes back while the factorization runs; the
     # host matrix is reset from a pinned source between steps (outside the
     # timed region)
-    host_src = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
-    host_src.copy_(base)
-    host_a = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
-    dA = mats[0]
+    # (--e2e-steps 0 leaves it out: a profiling convenience, no e2e figure)
     e_ms = []
-    for i in range(args.e2e_steps + 1):
+    if args.e2e_steps > 0:
+        host_src = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+        host_src.copy_(base)
+        host_a = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()
+        dA = mats[0]
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         host_a.copy_(host_src)
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -371,12 +373,12 @@ def main() -> None:
         torch.cuda.synchronize(dev)
         if i > 0:  # first iteration warms the pinned paths
             e_ms.append(e0.elapsed_time(e1))
-    e2e_ms = sum(e_ms) / len(e_ms)
-    if world > 1:
+    e2e_ms = sum(e_ms) / len(e_ms) if e_ms else None
+    if world > 1 and e_ms:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = world * lu_flops(n) / (e2e_ms / 1e3) / 1e12
+    e2e_value = world * lu_flops(n) / (e2e_ms / 1e3) / 1e12 if e_ms else None
 
     if rank != 0:
         if world > 1:
@@ -433,7 +435,7 @@ def main() -> None:
                 "h2d_bytes_per_step": 4 * n * n, "d2h_bytes_per_step": 4 * n * n,
                 "path": "lu_nopiv_rl_host_c via remifa_b200.lu_nopiv_rl_host: pinned host "
                         "matrix in by column chunks overlapping the factorization, finished "
-                        "block columns streamed back"},
+                        "block columns streamed back"} if e_ms else None,
         "gpu_launches": launches,
         "roofline": roofline,
         "kernels": {k: {"launches": v["launches"], "ms": v["total_ms"]}

@@ -136,7 +136,7 @@ static lu_status tc_pack_range(cudaStream_t st, TcOperand kind, int64_t r0, int6
 static lu_status tc_apply(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                           int64_t K, int64_t r0, int64_t c0, float* c,
                           int64_t ldc, char* ws, const TcWs& w, int* err,
-                          int tiles_per_cta) {
+                          int tiles_per_cta, int max_ctas = 0) {
   if (M <= 0 || N <= 0) return LU_SUCCESS;
   const int64_t ldk = tc_packed_k(kind, K);
   const int64_t es = tc_operand_bytes(kind);
@@ -154,7 +154,7 @@ static lu_status tc_apply(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                2.0 * M * N * kk);
   return launch_tc_update(st, kind, M, N, kk, -1.0f, ws + w.off_a + r0 * ldk * es,
                           ldk, ws + w.off_b + c0 * ldk * es, ldk, c, ldc, sa, sb,
-                          err, 0, tiles_per_cta);
+                          err, max_ctas, tiles_per_cta);
 }
 
 // C (fp32) -= A * B through the tensor cores (pack, then update).
@@ -467,23 +467,29 @@ static lu_status factor_block_split(const Plan& p, cudaStream_t st, DevStreams* 
 static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
                               int64_t lda, int64_t ofs, int64_t r0, int64_t rows,
                               int64_t c0, int64_t cols, char* ws, const TcWs& w,
-                              int* err, int tiles_per_cta) {
+                              int* err, int tiles_per_cta, int max_ctas = 0) {
   if (rows <= 0 || cols <= 0) return LU_SUCCESS;
   const int64_t nb = p.nb, ofst = ofs + nb;
   float* c = a + (ofst + r0) + (ofst + c0) * lda;
   if (is_tc(p.outer))
     return tc_apply(st, tc_kind(p.outer), rows, cols, nb, r0, c0, c, lda, ws, w,
-                    err, tiles_per_cta);
+                    err, tiles_per_cta, max_ctas);
   ProfScope ps("sgemm_update", st, 8.0 * rows * cols, 2.0 * rows * cols * (double)nb);
   return launch_sgemm_update(st, rows, cols, nb, -1.0f, a + (ofst + r0) + ofs * lda,
                              lda, a + ofs + (ofst + c0) * lda, lda, 1.0f, c, lda,
                              false);
 }
 
-// Tiles per CTA of the bulk trailing update under look-ahead: few, so SMs
-// free up often and the high-priority panel kernels get them quickly
-// (measured on B200 at n = 16384: 2 tiles 133 TF/s, 8 tiles 124, 16 tiles 122).
+// Tiles per CTA of the trailing updates under look-ahead: few, so SMs free
+// up often and the high-priority panel kernels get them quickly (measured on
+// B200 at n = 16384: 2 tiles 133 TF/s, 8 tiles 124, 16 tiles 122).
 constexpr int kU2Tiles = 2;
+// ... except the bulk update U2b when it is large: then it runs as
+// persistent CTAs on half of the SMs (streaming C ahead of the accumulator),
+// leaving the other half to the panel streams.  B200, nb = 256, threshold
+// 2048 tiles of 128 x 256: n = 16384 165 -> 181 TF/s, n = 32768 238 -> 243,
+// n = 8192 unchanged (below the threshold it keeps the 2-tile CTAs).
+constexpr int64_t kU2bPersistTiles = 2048;
 
 // Right-looking factorization of the steps whose outer block starts in
 // [col_begin, col_end), restricted to the columns [0, col_end) (rows always
@@ -756,8 +762,11 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       if (!ok(cudaEventRecord(S->updated, su))) break;
       // U2b: the rest
       if (tr > 2 * nb && tcn > 2 * nb) {
+        const int64_t t2b = ceil_div(tr - 2 * nb, 128) * ceil_div(tcn - 2 * nb, 256);
+        const bool persist = tc && t2b >= kU2bPersistTiles;
         status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
-                              tcn - 2 * nb, ws, wk, err, kU2Tiles);
+                              tcn - 2 * nb, ws, wk, err, persist ? 0 : kU2Tiles,
+                              persist ? std::max(1, sm_count() / 2) : 0);
         if (status != LU_SUCCESS) break;
       }
       if (!ok(cudaEventRecord(S->done_with[buf], su))) break;

@@ -24,6 +24,109 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kStrip = 64;  // rows (lpanel) / columns (upanel) per CTA
+// diag_factor_kernel: threads 0-255 eliminate the L rows / U columns of a
+// tile, threads 32-511 its trailing rank-8 update (16 warps hide the shared
+// memory latency of the 4 x 4 micro-tiles).
+constexpr int kDiagT = 512;
+
+// Block copies between global memory and shared memory, by all NT threads
+// of the CTA: warps take columns, lanes consecutive rows, so no index is
+// divided by a runtime extent.  Both sides column-major unless noted.
+
+// dst[r + c*ldd] = src[r + c*lds] asynchronously (complete with
+// cp_async_wait_all); 16-byte copies when every column start is 16-byte
+// aligned on both sides.
+template <int NT>
+__device__ __forceinline__ void stage_cols_async(float* dst, int ldd, const float* src,
+                                                 int64_t lds, int rows, int cols) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kNW = NT / 32;
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0 &&
+                   (lds & 3) == 0 && (ldd & 3) == 0 && (rows & 3) == 0;
+  if (vec) {
+    for (int c = warp; c < cols; c += kNW) {
+      const float* s = src + (int64_t)c * lds;
+      float* d = dst + c * ldd;
+      for (int r = 4 * lane; r < rows; r += 128) cp_async16(d + r, s + r);
+    }
+  } else {
+    for (int c = warp; c < cols; c += kNW) {
+      const float* s = src + (int64_t)c * lds;
+      float* d = dst + c * ldd;
+      for (int r = lane; r < rows; r += 32) cp_async4(d + r, s + r);
+    }
+  }
+}
+
+// dst[r + c*ldd] = src[r + c*lds] (shared -> global), 16-byte stores when
+// every column start is 16-byte aligned on both sides.
+template <int NT>
+__device__ __forceinline__ void store_cols(float* dst, int64_t ldd, const float* src,
+                                           int lds, int rows, int cols) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kNW = NT / 32;
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0 &&
+                   (ldd & 3) == 0 && (lds & 3) == 0 && (rows & 3) == 0;
+  if (vec) {
+    for (int c = warp; c < cols; c += kNW) {
+      const float* s = src + c * lds;
+      float* d = dst + (int64_t)c * ldd;
+      for (int r = 4 * lane; r < rows; r += 128)
+        *reinterpret_cast<float4*>(d + r) = *reinterpret_cast<const float4*>(s + r);
+    }
+  } else {
+    for (int c = warp; c < cols; c += kNW) {
+      const float* s = src + c * lds;
+      float* d = dst + (int64_t)c * ldd;
+      for (int r = lane; r < rows; r += 32) d[r] = s[r];
+    }
+  }
+}
+
+// Transposing load: dst[r*ldd + c] = src[r + c*lds] for r < rows, c < cols,
+// and 0 for cols <= c < round4(cols).  Each thread reads four columns of
+// one row (coalesced across the lanes) and writes them as one 16-byte
+// shared store; dst 16-byte aligned, ldd % 4 == 0.
+template <int NT>
+__device__ __forceinline__ void stage_rows_t(float* dst, int ldd, const float* src,
+                                             int64_t lds, int rows, int cols) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kNW = NT / 32;
+  const int nq = (cols + 3) >> 2;
+  for (int q = warp; q < nq; q += kNW) {
+    const int c0 = 4 * q;
+    const float* s = src + (int64_t)c0 * lds;
+#pragma unroll 2
+    for (int r = lane; r < rows; r += 32) {
+      float v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[e] = (c0 + e < cols) ? s[r + e * lds] : 0.0f;
+      *reinterpret_cast<float4*>(dst + r * ldd + c0) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+  }
+}
+
+// Transposing store: dst[r + c*ldd] = src[r*lds + c] for r < rows,
+// c < cols (16-byte shared reads; src 16-byte aligned, lds % 4 == 0).
+template <int NT>
+__device__ __forceinline__ void store_rows_t(float* dst, int64_t ldd, const float* src,
+                                             int lds, int rows, int cols) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kNW = NT / 32;
+  const int nq = (cols + 3) >> 2;
+  for (int q = warp; q < nq; q += kNW) {
+    const int c0 = 4 * q;
+    float* d = dst + (int64_t)c0 * ldd;
+#pragma unroll 2
+    for (int r = lane; r < rows; r += 32) {
+      const float4 v4 = *reinterpret_cast<const float4*>(src + r * lds + c0);
+      const float v[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (c0 + e < cols) d[r + e * ldd] = v[e];
+    }
+  }
+}
 
 // Factor the 8x8 tile whose rows live in lanes 0..7 of warp 0 (lane r holds
 // row r in v[0..7]); tw <= 8 columns are factored.  Returns via v; writes
@@ -89,7 +192,7 @@ __device__ __forceinline__ void factor_tile_thread(float* T, int LD, int tw,
 // Shared: D (w x w, column-major, leading dimension LD = round4(w) + 4 so
 // 4-row groups are 16-byte aligned), plus the L and U strips of the current
 // tile (Ls[k][i], Us[k][j]) for vectorised rank-8 updates.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kDiagT)
 diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
                    int* first_bad) {
   extern __shared__ __align__(16) float smem[];
@@ -100,10 +203,7 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
   float* inv = Us + 8 * 128;          // [8]
   const int tid = threadIdx.x;
 
-  for (int idx = tid; idx < w * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    cp_async4(&D[i + j * LD], &a[i + (int64_t)j * lda]);
-  }
+  stage_cols_async<kDiagT>(D, LD, a, lda, w, w);
   cp_async_wait_all();
   __syncthreads();
 
@@ -194,7 +294,7 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     }
     const int nb4 = (s + 3) / 4;
     const bool vec = (s % 4 == 0);
-    for (int b = tid - 32; b < nb4 * nb4; b += kThreads - 32) {
+    for (int b = tid - 32; b < nb4 * nb4; b += kDiagT - 32) {
       if (b < 0) break;
       const int li = 4 * (b % nb4), lj = 4 * (b / nb4);  // local to the block
       if (li < 8 && lj < 8) continue;  // the next tile: thread 0
@@ -241,10 +341,7 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     __syncthreads();
   }
 
-  for (int idx = tid; idx < w * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    a[i + (int64_t)j * lda] = D[i + j * LD];
-  }
+  store_cols<kDiagT>(a, lda, D, LD, w, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -262,10 +359,7 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
   float* D = smem;
   float* inv = D + (size_t)LD * w;  // 8
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < w * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    cp_async4(&D[i + j * LD], &a[i + (int64_t)j * lda]);
-  }
+  stage_cols_async<kThreads>(D, LD, a, lda, w, w);
   cp_async_wait_all();
   __syncthreads();
   const int nt = (w + 7) / 8;
@@ -327,10 +421,7 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < w * w; idx += kThreads) {
-    const int i = idx % w, j = idx / w;
-    a[i + (int64_t)j * lda] = D[i + j * LD];
-  }
+  store_cols<kThreads>(a, lda, D, LD, w, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -342,10 +433,11 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 //   (a) one thread per item eliminates tile T of its item: L rows
 //       x_k *= 1/d_k, x_j -= x_k U[k][j] (src/lu_nopiv.cu:141-168); U
 //       columns x_j -= L[j][k] x_k (src/lu_nopiv.cu:304-316);
-//   (b) all threads apply the rank-8 update of tile T to the item positions
-//       right of it, acc = sum_k fma(x_k, F_k) over the tile's 8 columns
-//       then one subtraction -- the reference's K = 8 GEMMs -- in register
-//       micro-tiles of 4 items x 8 positions (256 FMAs per 24 vector loads).
+//   (b) the rank-8 update of tile T to the item positions right of it,
+//       acc = sum_k fma(x_k, F_k) over the tile's 8 columns then one
+//       subtraction -- the reference's K = 8 GEMMs; the positions of tile
+//       T+1 are updated and eliminated first, by the item threads, while
+//       the other warps update the rest (lupanel_strip).
 // Each element receives the reference's operations in the reference's
 // order.  Left-looking mode (src/lu_nopiv_inner_ll.hxx:225-300) keeps one
 // running sum per element across the earlier tiles (ACC) and subtracts it
@@ -365,66 +457,100 @@ __device__ __forceinline__ void st8(float* p, const float (&v)[8]) {
   *reinterpret_cast<float4*>(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
 }
 
+// Eliminate tile columns [t0, t0 + tw) of one item held in x[0..8):
+// L rows x_c -= x_k U[k][c] (k < c), then x_c *= 1/d_c
+// (src/lu_nopiv.cu:141-168); U columns x_c -= L[c][k] x_k
+// (src/lu_nopiv.cu:304-316).
+template <bool IS_L>
+__device__ __forceinline__ void lupanel_elim(const float* F, int lf, const float* inv,
+                                             int t0, int tw, float (&x)[8]) {
+  if (tw == 8) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      float f[8];
+      ld8(F + (t0 + c) * lf + t0, f);  // f[k] = U[k][c] (L) / L[c][k] (U)
+      if (IS_L) {
+#pragma unroll
+        for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
+        x[c] = __fmul_rn(x[c], inv[t0 + c]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (c < tw) {
+        const float* f = F + (t0 + c) * lf + t0;
+        if (IS_L) {
+#pragma unroll
+          for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
+          x[c] = __fmul_rn(x[c], inv[t0 + c]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
+        }
+      }
+    }
+  }
+}
+
 // F[pos * lf + k]: the factor values that multiply item value k for
 // position pos -- U[k][pos] (L blocks, F column-major) or L[pos][k] (U
 // blocks, F row-major) -- so the 8 values of one tile are two float4.
+// Per tile T, after one barrier:
+//   warps 0-1 (one thread per item) apply tile T's rank-8 update to the
+//     8 positions of tile T+1 and eliminate tile T+1 at once (look-ahead);
+//   warps 2-7 apply tile T's rank-8 update to the positions right of tile
+//     T+1 in register micro-tiles of 4 items x 8 positions (256 FMAs per 24
+//     vector loads).
+// Every element still receives acc = sum_k fma(x_k, F_k) over the tile's 8
+// columns in k order, then one subtraction (left-looking: one running sum,
+// subtracted just before the element's own tile is eliminated).
 template <bool IS_L, bool LEFT>
 __device__ __forceinline__ void lupanel_strip(const float* F, int lf, const float* inv,
                                               float* S, int ls, float* ACC, int w) {
-  constexpr int nitems = kItems;
+  constexpr int kIG = kItems / kMicroI;  // 16 item groups
   const int tid = threadIdx.x;
   const int nt = (w + 7) / 8;
-  for (int T = 0; T < nt; ++T) {
-    const int t0 = 8 * T;
-    const int tw = min(8, w - t0);
-    // (a) tile elimination, one thread per item
-    if (tid < nitems) {
-      float* xr = S + tid * ls + t0;
-      float x[8];
-      ld8(xr, x);
-      if (LEFT && T > 0) {
-        float acc[8];
-        ld8(ACC + tid * ls + t0, acc);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) x[c] = __fsub_rn(x[c], acc[c]);
-      }
-      if (tw == 8) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          float f[8];
-          ld8(F + (t0 + c) * lf + t0, f);  // f[k] = U[k][c] (L) / L[c][k] (U)
-          if (IS_L) {
-#pragma unroll
-            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
-            x[c] = __fmul_rn(x[c], inv[t0 + c]);
-          } else {
-#pragma unroll
-            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
-          }
-        }
+  if (tid < kItems) {  // tile 0
+    float* xr = S + tid * ls;
+    float x[8];
+    ld8(xr, x);
+    lupanel_elim<IS_L>(F, lf, inv, 0, min(8, w), x);
+    st8(xr, x);
+  }
+  __syncthreads();
+  for (int T = 0; T + 1 < nt; ++T) {
+    const int t0 = 8 * T, p0 = t0 + 8;
+    if (tid < kItems) {
+      float* xr = S + tid * ls;
+      float xv[8], x[8], acc[8];
+      ld8(xr + t0, xv);
+      ld8(xr + p0, x);
+      if (LEFT) {
+        ld8(ACC + tid * ls + p0, acc);
       } else {
-        for (int c = 0; c < tw; ++c) {
-          const float* f = F + (t0 + c) * lf + t0;
-          if (IS_L) {
-            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-x[k], f[k], x[c]);
-            x[c] = __fmul_rn(x[c], inv[t0 + c]);
-          } else {
-            for (int k = 0; k < c; ++k) x[c] = __fmaf_rn(-f[k], x[k], x[c]);
-          }
-        }
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[b] = 0.0f;
       }
-      st8(xr, x);
-    }
-    __syncthreads();
-    // (b) rank-8 update of positions [t0 + 8, w); thread m takes items
-    // ig, ig + 16, ig + 32, ig + 48 (ig = m % 16: consecutive lanes hit
-    // distinct banks) and 8 consecutive positions
-    const int p0 = t0 + 8;
-    if (p0 < w) {
-      constexpr int kIG = kItems / kMicroI;  // 16 item groups
-      const int npos = (w - p0 + kMicroP - 1) / kMicroP;
-      for (int m = tid; m < npos * kIG; m += kPanelT) {
-        const int ig = m % kIG, pp = p0 + (m / kIG) * kMicroP;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        float f[8];
+        ld8(F + (p0 + b) * lf + t0, f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[b] = __fmaf_rn(xv[k], f[k], acc[b]);
+      }
+#pragma unroll
+      for (int b = 0; b < 8; ++b) x[b] = __fsub_rn(x[b], acc[b]);
+      lupanel_elim<IS_L>(F, lf, inv, p0, min(8, w - p0), x);
+      st8(xr + p0, x);
+    } else {
+      const int q0 = p0 + 8;
+      const int npos = (w - q0 + kMicroP - 1) / kMicroP;
+      for (int m = tid - kItems; m < npos * kIG; m += kPanelT - kItems) {
+        const int ig = m % kIG, pp = q0 + (m / kIG) * kMicroP;
         float xv[kMicroI][8];
 #pragma unroll
         for (int a = 0; a < kMicroI; ++a) ld8(S + (ig + a * kIG) * ls + t0, xv[a]);
@@ -481,12 +607,15 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   const bool is_l = (int)blockIdx.x < nL;
 
   // Stage the factored diagonal block: column-major (F[c*lf + r]) for L
-  // blocks, row-major (F[r*lf + c]) for U blocks.
-  for (int idx = tid; idx < wp * wp; idx += kPanelT) {
-    const int r = idx % wp, c = idx / wp;
-    float* dst = is_l ? &F[c * lf + r] : &F[r * lf + c];
-    if (r < w && c < w) cp_async4(dst, &dg[r + (int64_t)c * lda]);
-    else *dst = 0.0f;
+  // blocks, row-major (F[r*lf + c]) for U blocks; the padding rows and
+  // columns [w, wp) are zero.
+  if (is_l) stage_cols_async<kPanelT>(F, lf, dg, lda, w, w);
+  else stage_rows_t<kPanelT>(F, lf, dg, lda, w, w);
+  if (wp != w) {
+    for (int idx = tid; idx < wp * wp; idx += kPanelT) {
+      const int r = idx % wp, c = idx / wp;
+      if (r >= w || c >= (is_l ? w : ((w + 3) & ~3))) F[is_l ? c * lf + r : r * lf + c] = 0.0f;
+    }
   }
   int64_t item0;
   float* A;
@@ -495,26 +624,23 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
     item0 = (int64_t)blockIdx.x * kItems;
     A = dg + w + offL;               // first row of this launch's L rows
     nitems = (int)std::min<int64_t>(kItems, M - item0);
-    // S[q*ls + c] = A[row q, column c]; consecutive threads read
-    // consecutive rows of one column
-    for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
-      const int qq = idx % kItems, c = idx / kItems;
-      const int64_t row = item0 + qq;
-      if (row < M && c < w) cp_async4(&S[qq * ls + c], &A[row + (int64_t)c * lda]);
-      else S[qq * ls + c] = 0.0f;
-    }
+    // S[q*ls + c] = A[row item0 + q, column c]
+    stage_rows_t<kPanelT>(S, ls, A + item0, lda, nitems, w);
   } else {
     item0 = (int64_t)(blockIdx.x - nL) * kItems;
     A = dg + (w + offU) * lda;       // first column of this launch's U columns
     nitems = (int)std::min<int64_t>(kItems, N - item0);
-    // S[q*ls + i] = A[row i, column q]; consecutive threads read
-    // consecutive rows of one column
-    for (int idx = tid; idx < kItems * wp; idx += kPanelT) {
-      const int i = idx % wp, qq = idx / wp;
-      const int64_t col = item0 + qq;
-      if (col < N && i < w) cp_async4(&S[qq * ls + i], &A[i + col * lda]);
-      else S[qq * ls + i] = 0.0f;
-    }
+    // S[q*ls + i] = A[row i, column item0 + q]
+    stage_cols_async<kPanelT>(S, ls, A + item0 * lda, lda, w, nitems);
+  }
+  // zero the positions [w, wp) of every item and the items past the end
+  {
+    const int wq = is_l ? ((w + 3) & ~3) : w;  // the L staging zeroed up to round4(w)
+    const int padc = wp - wq;
+    if (padc > 0)
+      for (int idx = tid; idx < kItems * padc; idx += kPanelT)
+        S[(idx / padc) * ls + wq + idx % padc] = 0.0f;
+    for (int idx = nitems * ls + tid; idx < kItems * ls; idx += kPanelT) S[idx] = 0.0f;
   }
   if (left)
     for (int idx = tid; idx < kItems * ls; idx += kPanelT) ACC[idx] = 0.0f;
@@ -530,19 +656,8 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
     if (left) lupanel_strip<false, true>(F, lf, inv, S, ls, ACC, w);
     else lupanel_strip<false, false>(F, lf, inv, S, ls, ACC, w);
   }
-  if (is_l) {
-    for (int idx = tid; idx < kItems * w; idx += kPanelT) {
-      const int qq = idx % kItems, c = idx / kItems;
-      const int64_t row = item0 + qq;
-      if (row < M) A[row + (int64_t)c * lda] = S[qq * ls + c];
-    }
-  } else {
-    for (int idx = tid; idx < kItems * w; idx += kPanelT) {
-      const int i = idx % w, qq = idx / w;
-      const int64_t col = item0 + qq;
-      if (col < N) A[i + col * lda] = S[qq * ls + i];
-    }
-  }
+  if (is_l) store_rows_t<kPanelT>(A + item0, lda, S, ls, nitems, w);
+  else store_cols<kPanelT>(A + item0 * lda, lda, S, ls, w, nitems);
   // the finished items as tensor-core operands: item qq's w values are
   // contiguous along K in both copies (consecutive threads, consecutive k)
   void* dst = is_l ? pk.pa : pk.pb;
@@ -551,11 +666,11 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
     const int64_t base = (is_l ? pk.row0 : pk.col0) + item0;
     if (w % 8 == 0 && pk.ldk % 8 == 0 && pk.k0 % 8 == 0) {
       // 8 values -> one 16-byte store
-      const int w8 = w / 8;
-      for (int idx = tid; idx < kItems * w8; idx += kPanelT) {
-        const int c8 = idx % w8, qq = idx / w8;
+      const int w8 = w / 8;  // <= 16
+      for (int idx = tid; idx < kItems * 16; idx += kPanelT) {
+        const int c8 = idx & 15, qq = idx >> 4;
         const int64_t pr = base + qq;
-        if (item0 + qq < lim && pr >= 0) {
+        if (c8 < w8 && item0 + qq < lim && pr >= 0) {
           float v[8];
           ld8(&S[qq * ls + 8 * c8], v);
           uint4 out;
@@ -668,7 +783,7 @@ lu_status launch_diag_factor(cudaStream_t st, float* a, int64_t lda, int w,
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
   const size_t sm = diag_smem_bytes(w);
   LUB_CUDA_TRY(set_smem_limit((const void*)diag_factor_kernel, sm));
-  diag_factor_kernel<<<1, kThreads, sm, st>>>(a, lda, w, col0, first_bad);
+  diag_factor_kernel<<<1, kDiagT, sm, st>>>(a, lda, w, col0, first_bad);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

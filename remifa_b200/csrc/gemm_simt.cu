@@ -168,6 +168,12 @@ sgemm_update_kernel(int64_t M, int64_t N, int64_t K, float alpha,
 // shapes of these updates (K <= 128, one dimension 128 wide) need many small
 // tiles to fill the GPU.  Every element's sum runs over K in chunks of 8
 // (acc from 0, then subtracted) whatever the tile size.
+//
+// K <= 128 is small enough to keep the CTA's whole A panel (CB x K) and B
+// panel (K x CB) in shared memory: both are requested at once with cp.async
+// (A as 16-byte column segments, B transposed by 4-byte copies into rows of
+// CB + 4 floats, 4-way bank aliasing at most), the C tile is read while they
+// are in flight, and the chunks then run back to back with no barrier.
 struct ChunkRegion {
   int64_t M, N, K;
   const float* A; int64_t lda;
@@ -176,41 +182,58 @@ struct ChunkRegion {
   int tiles_m, tiles;
 };
 
+constexpr int kChunkMaxK = 128;
+
+template <int TM>
+constexpr size_t chunk8_smem_bytes() {
+  return sizeof(float) * (size_t)kChunkMaxK * (16 * TM + 16 * TM + 4);
+}
+
 template <int TM>
 __global__ void __launch_bounds__(NT)
 sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
   constexpr int CB = 16 * TM;            // tile edge
-  constexpr int LA = CB * BK / NT;       // tile elements loaded per thread
-  __shared__ __align__(16) float As[2][BK][CB];
-  __shared__ __align__(16) float Bs[2][BK][CB];
+  constexpr int LB = CB + 4;             // row length of the B panel
+  extern __shared__ __align__(16) float smem[];
+  float* As = smem;                      // [Kp][CB]: As[k*CB + m]
+  float* Bs = smem + kChunkMaxK * CB;    // [Kp][LB]: Bs[k*LB + n]
   const bool second = (int)blockIdx.x >= r0.tiles;
   const ChunkRegion& r = second ? r1 : r0;
   const int t = second ? (int)blockIdx.x - r0.tiles : (int)blockIdx.x;
   const int64_t m0 = (int64_t)(t % r.tiles_m) * CB;
   const int64_t n0 = (int64_t)(t / r.tiles_m) * CB;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tx = tid % 16, ty = tid / 16;
-  const int a_col = tid / (CB / LA), a_row = (tid % (CB / LA)) * LA;  // A tile CB x BK
-  const int b_col = tid / (BK / LA), b_k = (tid % (BK / LA)) * LA;    // B tile BK x CB
+  const int K = (int)r.K;
+  const int Kp = (K + 7) & ~7;           // chunks of 8, zero padded
 
-  float ra[LA], rb[LA];
-  auto load_tiles = [&](int64_t k0) {
-    const int64_t ak = k0 + a_col;
-#pragma unroll
-    for (int i = 0; i < LA; ++i)
-      ra[i] = (ak < r.K && m0 + a_row + i < r.M) ? r.A[m0 + a_row + i + ak * r.lda] : 0.0f;
-    const int64_t bc = n0 + b_col;
-#pragma unroll
-    for (int i = 0; i < LA; ++i)
-      rb[i] = (bc < r.N && k0 + b_k + i < r.K) ? r.B[k0 + b_k + i + bc * r.ldb] : 0.0f;
-  };
-  auto store_tiles = [&](int buf) {
-#pragma unroll
-    for (int i = 0; i < LA; ++i) {
-      As[buf][a_col][a_row + i] = ra[i];
-      Bs[buf][b_k + i][b_col] = rb[i];
+  // A panel: rows m0.., columns 0..K (column-major in global memory)
+  {
+    const float* A = r.A + m0;
+    const bool vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (r.lda & 3) == 0 &&
+                     m0 + CB <= r.M;
+    for (int k = warp; k < Kp; k += NT / 32) {
+      float* d = As + k * CB;
+      if (vec && k < K) {
+        const float* sc = A + (int64_t)k * r.lda;
+        for (int m = 4 * lane; m < CB; m += 128) cp_async16(d + m, sc + m);
+      } else {
+        for (int m = lane; m < CB; m += 32) {
+          if (k < K && m0 + m < r.M) cp_async4(d + m, A + m + (int64_t)k * r.lda);
+          else d[m] = 0.0f;
+        }
+      }
     }
-  };
+  }
+  // B panel: rows 0..K, columns n0.. (k contiguous in global memory)
+  for (int n = warp; n < CB; n += NT / 32) {
+    const bool in = n0 + n < r.N;
+    const float* sc = r.B + (n0 + n) * r.ldb;
+    for (int k = lane; k < Kp; k += 32) {
+      if (in && k < K) cp_async4(Bs + k * LB + n, sc + k);
+      else Bs[k * LB + n] = 0.0f;
+    }
+  }
 
   float cr[TM][TM], acc[TM][TM];
 #pragma unroll
@@ -221,24 +244,21 @@ sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
       cr[i][j] = (row < r.M && col < r.N) ? r.C[row + col * r.ldc] : 0.0f;
       acc[i][j] = 0.0f;
     }
-  const int64_t nk = (r.K + BK - 1) / BK;
-  load_tiles(0);
-  store_tiles(0);
+  cp_async_wait_all();
   __syncthreads();
-  for (int64_t kt = 0; kt < nk; ++kt) {
-    const int buf = (int)(kt & 1);
-    if (kt + 1 < nk) load_tiles((kt + 1) * BK);
+
+  for (int k0 = 0; k0 < Kp; k0 += 8) {
 #pragma unroll
-    for (int k = 0; k < BK; ++k) {
+    for (int k = k0; k < k0 + 8; ++k) {
       float a[TM], b[TM];
       if constexpr (TM == 4) {
-        const float4 a4 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
-        const float4 b4 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+        const float4 a4 = *reinterpret_cast<const float4*>(As + k * CB + tx * 4);
+        const float4 b4 = *reinterpret_cast<const float4*>(Bs + k * LB + ty * 4);
         a[0] = a4.x; a[1] = a4.y; a[2] = a4.z; a[3] = a4.w;
         b[0] = b4.x; b[1] = b4.y; b[2] = b4.z; b[3] = b4.w;
       } else {
-        const float2 a2 = *reinterpret_cast<const float2*>(&As[buf][k][tx * 2]);
-        const float2 b2 = *reinterpret_cast<const float2*>(&Bs[buf][k][ty * 2]);
+        const float2 a2 = *reinterpret_cast<const float2*>(As + k * CB + tx * 2);
+        const float2 b2 = *reinterpret_cast<const float2*>(Bs + k * LB + ty * 2);
         a[0] = a2.x; a[1] = a2.y;
         b[0] = b2.x; b[1] = b2.y;
       }
@@ -255,10 +275,6 @@ sgemm_chunk8_kernel(ChunkRegion r0, ChunkRegion r1) {
         cr[i][j] = __fsub_rn(cr[i][j], acc[i][j]);
         acc[i][j] = 0.0f;
       }
-    if (kt + 1 < nk) {
-      store_tiles(buf ^ 1);
-      __syncthreads();
-    }
   }
 #pragma unroll
   for (int i = 0; i < TM; ++i)
@@ -297,8 +313,17 @@ lu_status launch_sgemm_chunk8_2(cudaStream_t st, int64_t M0, int64_t N0,
   if (small) grid = count(32);
   if (grid == 0) return LU_SUCCESS;
   if (grid > INT32_MAX) return LU_ERR_INVALID_ARG;
-  if (small) sgemm_chunk8_kernel<2><<<(unsigned)grid, NT, 0, st>>>(r0, r1);
-  else sgemm_chunk8_kernel<4><<<(unsigned)grid, NT, 0, st>>>(r0, r1);
+  if ((r0.tiles > 0 && K0 > kChunkMaxK) || (r1.tiles > 0 && K1 > kChunkMaxK))
+    return LU_ERR_INVALID_ARG;
+  if (small) {
+    constexpr size_t sm = chunk8_smem_bytes<2>();
+    LUB_CUDA_TRY(set_smem_limit((const void*)sgemm_chunk8_kernel<2>, sm));
+    sgemm_chunk8_kernel<2><<<(unsigned)grid, NT, sm, st>>>(r0, r1);
+  } else {
+    constexpr size_t sm = chunk8_smem_bytes<4>();
+    LUB_CUDA_TRY(set_smem_limit((const void*)sgemm_chunk8_kernel<4>, sm));
+    sgemm_chunk8_kernel<4><<<(unsigned)grid, NT, sm, st>>>(r0, r1);
+  }
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

@@ -158,7 +158,8 @@ def test_gemmex_fp32_bit_exact(built, m, n, k, lda):
 
 CASES = [(1, 256, 0), (7, 256, 0), (8, 8, 0), (9, 8, 0), (63, 64, 0), (64, 64, 0),
          (65, 64, 0), (200, 256, 0), (257, 256, 0), (520, 256, 0), (520, 64, 8),
-         (1024, 256, 64), (1024, 128, 128), (777, 136, 24)]
+         (1024, 256, 64), (1024, 128, 128), (777, 136, 24), (13, 256, 0),
+         (150, 256, 0), (1000, 256, 40)]
 
 
 @pytest.mark.parametrize("n,nb,dw", CASES)

@@ -488,7 +488,9 @@ constexpr int kU2Tiles = 2;
 // persistent CTAs on half of the SMs (streaming C ahead of the accumulator),
 // leaving the other half to the panel streams.  B200, nb = 256, threshold
 // 2048 tiles of 128 x 256: n = 16384 165 -> 181 TF/s, n = 32768 238 -> 243,
-// n = 8192 unchanged (below the threshold it keeps the 2-tile CTAs).
+// n = 8192 unchanged (below the threshold it keeps the 2-tile CTAs).  Not
+// for the split-fp16 update: two MMAs per tile make it compute-heavy enough
+// to want every SM (n = 32768: 150 ms with all SMs, 194 ms capped).
 constexpr int64_t kU2bPersistTiles = 2048;
 
 // Right-looking factorization of the steps whose outer block starts in
@@ -763,7 +765,8 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       // U2b: the rest
       if (tr > 2 * nb && tcn > 2 * nb) {
         const int64_t t2b = ceil_div(tr - 2 * nb, 128) * ceil_div(tcn - 2 * nb, 256);
-        const bool persist = tc && t2b >= kU2bPersistTiles;
+        const bool persist = tc && tc_kind(p.outer) != TcOperand::SPLIT16 &&
+                             t2b >= kU2bPersistTiles;
         status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
                               tcn - 2 * nb, ws, wk, err, persist ? 0 : kU2Tiles,
                               persist ? std::max(1, sm_count() / 2) : 0);

@@ -180,7 +180,10 @@ struct DevStreams {
   cudaStream_t panel = nullptr, update = nullptr, copy = nullptr, side = nullptr;
   cudaStream_t copy_out = nullptr;  // device-to-host, concurrent with `copy`
   cudaStream_t catchup = nullptr;   // the host entry's catch_up of arrived chunks
+  cudaStream_t catchup_bulk = nullptr;  // its bulk updates (look-ahead)
   cudaEvent_t cu_done = nullptr;
+  cudaEvent_t cu_packed = nullptr, cu_u2[2] = {nullptr, nullptr}, cu_join = nullptr;
+  cudaEvent_t cu_out = nullptr;  // a chunk's catch-up done: its rows above it can go out
   // per outer step of the host entry: the step's block column is final
   // once what was queued on the panel (p) and side (s) streams has run
   std::vector<cudaEvent_t> step_p, step_s;
@@ -215,7 +218,10 @@ static lu_status dev_streams(DevStreams** out) {
     }
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.out_done, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup, cudaStreamNonBlocking, least));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_bulk, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
+    for (cudaEvent_t* e : {&d.cu_packed, &d.cu_u2[0], &d.cu_u2[1], &d.cu_join, &d.cu_out})
+      LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
                            &d.done_with[0], &d.done_with[1], &d.done_with[2], &d.copied,
@@ -510,8 +516,9 @@ constexpr int64_t kU2bPersistTiles = 2048;
 // receives its updates in the same order, so results are identical either
 // way.
 // Where rl_factor sends each finished block column (host-memory entry):
-// after a step's panel, rows [0, n) of its block column are final; they go
-// to h (ldh) on the copy stream `out`.
+// after a step's panel, the rows [col_begin, n) of its block column are
+// final (the rows above col_begin were final after catch_up and have gone
+// out already); they go to h (ldh) on the copy stream `out`.
 struct ColumnSink {
   float* h = nullptr;
   int64_t ldh = 0;
@@ -544,8 +551,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, col_end - ofs, first_bad,
                            pack_target(p, ws, w2[0])));
       if (sink)
-        LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h + ofs * sink->ldh, (size_t)sink->ldh * 4,
-                                       a + ofs * lda, (size_t)lda * 4, (size_t)n * 4,
+        LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h + col_begin + ofs * sink->ldh,
+                                       (size_t)sink->ldh * 4, a + col_begin + ofs * lda,
+                                       (size_t)lda * 4, (size_t)(n - col_begin) * 4,
                                        (size_t)in, cudaMemcpyDeviceToHost, st));
       const int64_t tr = n - (ofs + nb), tcn = col_end - (ofs + nb);
       if (tr <= 0 || tcn <= 0) continue;
@@ -590,8 +598,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     if (!ok(cudaEventRecord(ep, sp)) || !ok(cudaEventRecord(es, side ? ss : sp)) ||
         !ok(cudaStreamWaitEvent(sink->out, ep, 0)) || !ok(cudaStreamWaitEvent(sink->out, es, 0)))
       return false;
-    return ok(cudaMemcpy2DAsync(sink->h + ofs * sink->ldh, (size_t)sink->ldh * 4, a + ofs * lda,
-                                (size_t)lda * 4, (size_t)n * 4, (size_t)in,
+    return ok(cudaMemcpy2DAsync(sink->h + col_begin + ofs * sink->ldh, (size_t)sink->ldh * 4,
+                                a + col_begin + ofs * lda, (size_t)lda * 4,
+                                (size_t)(n - col_begin) * 4, (size_t)in,
                                 cudaMemcpyDeviceToHost, sink->out));
   };
   for (int64_t ofs = col_begin; ofs < col_end && status == LU_SUCCESS; ofs += nb, ++step) {
@@ -798,33 +807,48 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
 // over the whole matrix, so the factors are bit-identical.
 // With S given, step t waits for S->step_p / step_s[t] first (the step's
 // block column final), so the catch-up of an arrived chunk can run beside
-// the factorization of the chunk before it.
+// the factorization of the chunk before it; and the trailing update of
+// step t is split into U1 (the next block row, rows [nb, 2 nb) of the
+// trailing part, on st) and U2 (the rest, on S->catchup_bulk), so that U2
+// of step t runs beside the solves and U1 of step t+1: the solves of step
+// t need U1 of t-1 and U2 of t-2, U1 of step t needs U2 of t-1 (per-parity
+// events), and U2 runs in step order on its own stream.  The operands of
+// step t go to buffer t % 2 of wk: packing step t+2 follows U1 of step
+// t+1, which follows U2 of step t, the last reader of that buffer.
 static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda, char* ws,
-                          const TcWs& wk, int* err, int64_t c0, int64_t c1,
-                          const DevStreams* S = nullptr) {
+                          const TcWs* wk, int* err, int64_t c0, int64_t c1,
+                          DevStreams* S = nullptr) {
   const int64_t n = p.n, nb = p.nb, nc = c1 - c0;
   const bool tc = is_tc(p.outer);
   const TcOperand kind = tc_kind(p.outer);
+  cudaStream_t sb = S ? S->catchup_bulk : nullptr;
+  if (S) {
+    LUB_CUDA_TRY(cudaEventRecord(S->cu_join, st));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_join, 0));
+  }
   for (int64_t ofs = 0; ofs < c0; ofs += nb) {
+    const int64_t t = ofs / nb;
+    const TcWs& w = wk[S ? t % 2 : 0];
     if (S) {
-      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[ofs / nb], 0));
-      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[ofs / nb], 0));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[t], 0));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[t], 0));
+      if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[t % 2], 0));
     }
     const int64_t in = std::min(n - ofs, nb);
     float* blk = a + ofs + ofs * lda;
     for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
-      const int w = (int)std::min<int64_t>(in - p0, p.diag_w);
+      const int dw = (int)std::min<int64_t>(in - p0, p.diag_w);
       float* dg = blk + p0 + p0 * lda;
       {
-        ProfScope ps("lupanel", st, 8.0 * nc * w, (double)nc * w * w);
-        LUB_TRY(launch_lupanel(st, dg, lda, w, 0, nc, false, 0, c0 - (ofs + p0 + w)));
+        ProfScope ps("lupanel", st, 8.0 * nc * dw, (double)nc * dw * dw);
+        LUB_TRY(launch_lupanel(st, dg, lda, dw, 0, nc, false, 0, c0 - (ofs + p0 + dw)));
       }
-      if (p0 + w < in) {
-        ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * w * (double)(in - p0 - w) * nc);
+      if (p0 + dw < in) {
+        ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * dw * (double)(in - p0 - dw) * nc);
         LUB_TRY(launch_sgemm_chunk8_2(st, 0, 0, 0, nullptr, lda, nullptr, lda, nullptr, lda,
-                                      in - (p0 + w), nc, w, dg + w, lda,
+                                      in - (p0 + dw), nc, dw, dg + dw, lda,
                                       blk + p0 + (c0 - ofs) * lda, lda,
-                                      blk + (p0 + w) + (c0 - ofs) * lda, lda));
+                                      blk + (p0 + dw) + (c0 - ofs) * lda, lda));
       }
     }
     const int64_t tr = n - (ofs + nb);
@@ -832,8 +856,24 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
     const int64_t cr = c0 - (ofs + nb);  // column offset in the trailing part
     if (tc)
       LUB_TRY(tc_pack_range(st, kind, 0, tr, cr, cr + nc, nb, a + (ofs + nb) + ofs * lda, lda,
-                            a + ofs + (ofs + nb) * lda, lda, ws, wk));
-    LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tr, cr, nc, ws, wk, err, 0));
+                            a + ofs + (ofs + nb) * lda, lda, ws, w));
+    if (!S) {
+      LUB_TRY(outer_update(p, st, a, lda, ofs, 0, tr, cr, nc, ws, w, err, 0));
+      continue;
+    }
+    const int64_t r1 = std::min(tr, nb);  // U1: rows [0, r1) of the trailing part
+    if (tr > r1) {
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
+      LUB_TRY(outer_update(p, sb, a, lda, ofs, r1, tr - r1, cr, nc, ws, w, err, 0));
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_u2[t % 2], sb));
+    }
+    if (t >= 1) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[(t - 1) % 2], 0));
+    LUB_TRY(outer_update(p, st, a, lda, ofs, 0, r1, cr, nc, ws, w, err, 0));
+  }
+  if (S) {
+    LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sb));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   }
   return LU_SUCCESS;
 }
@@ -1075,15 +1115,18 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
     // Under look-ahead rl_factor marks each step's finished block column
     // with an event, and the catch-up of an arrived chunk runs on its own
     // stream beside the factorization of the chunk before it (with its own
-    // operand buffer); otherwise the catch-up runs in order on the stream.
+    // operand buffers, two: see catch_up); otherwise the catch-up runs in
+    // order on the stream.
     const bool la = p.lookahead && n > 2 * nb && !(tc && tc_scaled(kind) && nb % 128 != 0);
     cudaStream_t cu = la && S ? S->catchup : st;
-    TcWs wcu = wk;
+    TcWs wcu[2] = {wk, wk};
     char* cubuf = wsb;
     void* cu_alloc = nullptr;
     if (s == LU_SUCCESS && la && tc) {
-      wcu = tc_ws_layout(0, n - nb, n - nb, nb, kind);
-      if (cudaMallocAsync(&cu_alloc, wcu.bytes, st) != cudaSuccess) s = LU_ERR_ALLOC;
+      wcu[0] = tc_ws_layout(0, n - nb, n - nb, nb, kind);
+      wcu[1] = tc_ws_layout(wcu[0].bytes, n - nb, n - nb, nb, kind);
+      if (cudaMallocAsync(&cu_alloc, wcu[0].bytes + wcu[1].bytes, st) != cudaSuccess)
+        s = LU_ERR_ALLOC;
       cubuf = static_cast<char*>(cu_alloc);
     }
     if (s == LU_SUCCESS && ok(cudaEventRecord(S->fork, st)) &&
@@ -1099,6 +1142,14 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         if (q > 0) {
           s = catch_up(p, cu, d_a, ldda, cubuf, wcu, err, c0, c1, la ? S : nullptr);
           if (s != LU_SUCCESS) break;
+          // the rows [0, c0) of the chunk are final now: out at once, ahead
+          // of the chunk's own steps (which send the rows [c0, n) of each
+          // block column as it finishes)
+          if (!ok(cudaEventRecord(S->cu_out, cu)) || !ok(cudaStreamWaitEvent(co, S->cu_out, 0)) ||
+              !ok(cudaMemcpy2DAsync(h_a + c0 * lda, (size_t)lda * 4, d_a + c0 * ldda,
+                                    (size_t)ldda * 4, (size_t)c0 * 4, (size_t)(c1 - c0),
+                                    cudaMemcpyDeviceToHost, co)))
+            break;
         }
         if (la && (!ok(cudaEventRecord(S->cu_done, cu)) ||
                    !ok(cudaStreamWaitEvent(st, S->cu_done, 0))))
@@ -1110,6 +1161,8 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
       if (la) {
         cudaEventRecord(S->cu_done, cu);
         cudaStreamWaitEvent(st, S->cu_done, 0);
+        cudaEventRecord(S->cu_join, S->catchup_bulk);
+        cudaStreamWaitEvent(st, S->cu_join, 0);
       }
       cudaEventRecord(S->out_done, co);
       cudaStreamWaitEvent(st, S->out_done, 0);

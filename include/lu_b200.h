@@ -123,13 +123,14 @@ LU_API lu_status lu_nopiv_rl_c(const lu_opts* opts, lu_stream_t stream, int64_t 
  * reference takes device pointers only).  h_a (n x n, lda) is copied into
  * the device buffer d_a (ldda) by column chunks of whole outer blocks on an
  * internal copy stream; each chunk, once in, receives the outer steps of the
- * earlier chunks (beside the factorization of the previous chunk), then its
- * own steps, each of which sends its finished block column back into h_a on
- * a second internal copy stream -- so both transfers overlap the
- * factorization.  The factors are bit-identical to lu_nopiv_rl_c's.  With
- * look-ahead and tensor-core updates one extra operand buffer (the size of
- * one packed L21 / U12 pair) is taken from cudaMallocAsync on `stream`
- * besides the workspace.  h_a should be pinned host memory (cudaHostAlloc /
+ * earlier chunks (beside the factorization of the previous chunk), sends
+ * its rows above the chunk (final by then) back into h_a on a second
+ * internal copy stream, then runs its own steps, each of which sends the
+ * rest of its finished block column back the same way -- so both transfers
+ * overlap the factorization.  The factors are bit-identical to
+ * lu_nopiv_rl_c's.  With look-ahead and tensor-core updates two extra
+ * operand buffers (each the size of one packed L21 / U12 pair) are taken
+ * from cudaMallocAsync on `stream` besides the workspace.  h_a should be pinned host memory (cudaHostAlloc /
  * cudaHostRegister) for the copies to run asynchronously.  d_info as for
  * lu_nopiv_rl_c.  Asynchronous: synchronise `stream` before reading h_a. */
 LU_API lu_status lu_nopiv_rl_host_c(const lu_opts* opts, lu_stream_t stream, int64_t n,

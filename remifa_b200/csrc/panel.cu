@@ -23,7 +23,6 @@ namespace lub {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kStrip = 64;  // rows (lpanel) / columns (upanel) per CTA
 // diag_factor_kernel: threads 0-255 eliminate the L rows / U columns of a
 // tile, threads 32-511 its trailing rank-8 update (16 warps hide the shared
 // memory latency of the 4 x 4 micro-tiles).

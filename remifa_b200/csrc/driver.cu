@@ -550,11 +550,13 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
       const int64_t in = std::min(n - ofs, nb);
       LUB_TRY(factor_block(p, st, a, lda, ofs, in, n - ofs, col_end - ofs, first_bad,
                            pack_target(p, ws, w2[0])));
-      if (sink)
+      if (sink) {
+        ProfScope ps("copy_d2h", st, 4.0 * (double)(n - col_begin) * in);
         LUB_CUDA_TRY(cudaMemcpy2DAsync(sink->h + col_begin + ofs * sink->ldh,
                                        (size_t)sink->ldh * 4, a + col_begin + ofs * lda,
                                        (size_t)lda * 4, (size_t)(n - col_begin) * 4,
                                        (size_t)in, cudaMemcpyDeviceToHost, st));
+      }
       const int64_t tr = n - (ofs + nb), tcn = col_end - (ofs + nb);
       if (tr <= 0 || tcn <= 0) continue;
       if (tc && !fused)
@@ -598,6 +600,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     if (!ok(cudaEventRecord(ep, sp)) || !ok(cudaEventRecord(es, side ? ss : sp)) ||
         !ok(cudaStreamWaitEvent(sink->out, ep, 0)) || !ok(cudaStreamWaitEvent(sink->out, es, 0)))
       return false;
+    ProfScope ps("copy_d2h", sink->out, 4.0 * (double)(n - col_begin) * in);
     return ok(cudaMemcpy2DAsync(sink->h + col_begin + ofs * sink->ldh, (size_t)sink->ldh * 4,
                                 a + col_begin + ofs * lda, (size_t)lda * 4,
                                 (size_t)(n - col_begin) * 4, (size_t)in,
@@ -1133,8 +1136,13 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         ok(cudaStreamWaitEvent(ci, S->fork, 0)) && ok(cudaStreamWaitEvent(co, S->fork, 0)) &&
         (!la || ok(cudaStreamWaitEvent(cu, S->fork, 0)))) {
       int q = 0;
-      for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q)
-        if (ok(h2d(ci, c0, std::min(n, c0 + cw)))) ok(cudaEventRecord(S->chunk_in[q], ci));
+      for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
+        {
+          ProfScope ps("copy_h2d", ci, 4.0 * (double)n * (std::min(n, c0 + cw) - c0));
+          if (!ok(h2d(ci, c0, std::min(n, c0 + cw)))) break;
+        }
+        if (!ok(cudaEventRecord(S->chunk_in[q], ci))) break;
+      }
       q = 0;
       for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
         const int64_t c1 = std::min(n, c0 + cw);
@@ -1145,8 +1153,10 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
           // the rows [0, c0) of the chunk are final now: out at once, ahead
           // of the chunk's own steps (which send the rows [c0, n) of each
           // block column as it finishes)
-          if (!ok(cudaEventRecord(S->cu_out, cu)) || !ok(cudaStreamWaitEvent(co, S->cu_out, 0)) ||
-              !ok(cudaMemcpy2DAsync(h_a + c0 * lda, (size_t)lda * 4, d_a + c0 * ldda,
+          if (!ok(cudaEventRecord(S->cu_out, cu)) || !ok(cudaStreamWaitEvent(co, S->cu_out, 0)))
+            break;
+          ProfScope ps("copy_d2h", co, 4.0 * (double)c0 * (c1 - c0));
+          if (!ok(cudaMemcpy2DAsync(h_a + c0 * lda, (size_t)lda * 4, d_a + c0 * ldda,
                                     (size_t)ldda * 4, (size_t)c0 * 4, (size_t)(c1 - c0),
                                     cudaMemcpyDeviceToHost, co)))
             break;

@@ -64,6 +64,21 @@ def lu_flops(n: int) -> float:
     return 2.0 * n ** 3 / 3.0
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (every multi-GPU time is the slowest
+    rank's); a collective, so every rank calls it at the same point."""
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: float, ms: float) -> float:
+    """Units per second over the whole job: each of `world` replicas
+    processes units_per_rank in the slowest rank's time `ms`."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -340,12 +355,10 @@ def main() -> None:
         torch.cuda.synchronize(dev)
     ms_prof = p_start.elapsed_time(p_end)
     if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
         dist.barrier()
     bad = int((infos != 0).sum().item())
-    value = world * args.steps * lu_flops(n) / (ms / 1e3) / 1e12
+    value = whole_job_rate(world, args.steps * lu_flops(n), ms) / 1e12
 
     # ---- end to end through lu_nopiv_rl_host_c: the pinned host matrix goes
     # in by column chunks while the device factors the chunks already in, and
@@ -375,10 +388,8 @@ def main() -> None:
             e_ms.append(e0.elapsed_time(e1))
     e2e_ms = sum(e_ms) / len(e_ms) if e_ms else None
     if world > 1 and e_ms:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * lu_flops(n) / (e2e_ms / 1e3) / 1e12 if e_ms else None
+        e2e_ms = max_over_ranks(e2e_ms, dist, dev)
+    e2e_value = whole_job_rate(world, lu_flops(n), e2e_ms) / 1e12 if e_ms else None
 
     if rank != 0:
         if world > 1:
@@ -864,6 +875,8 @@ def run_c2_grid(args, torch, rb):
 
 def run_special(args) -> None:
     if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return  # under torchrun rank 0 alone reports
         print(json.dumps({"impl": "reference", "workload": args.workload,
                           "unavailable": "the reference has no batched, fp16-left-looking "
                                          "timing harness, refinement or adjoint for this "

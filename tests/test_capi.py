@@ -76,12 +76,34 @@ def test_factor_argument_validation_without_device(built):
                                                        _lib.ERR_NO_DEVICE)
 
 
+def _rl_host(n=64, h=1, lda=64, d=1, ldda=64, info=1, variant=None):
+    o = rb.make_opts()
+    if variant is not None:
+        o.variant = variant
+    vp = lambda x: ctypes.c_void_p(x) if x else None
+    return _lib.lib().lu_nopiv_rl_host_c(ctypes.byref(o), None, n, vp(h), lda, vp(d), ldda,
+                                         vp(info), None, 0)
+
+
+def test_host_entry_argument_validation_without_device(built):
+    # the host-memory entry also reports argument errors before any device call
+    assert _rl_host(info=0) == _lib.ERR_INVALID_ARG
+    assert _rl_host(lda=10) == _lib.ERR_INVALID_ARG
+    assert _rl_host(ldda=10) == _lib.ERR_INVALID_ARG
+    assert _rl_host(h=0) == _lib.ERR_INVALID_ARG
+    assert _rl_host(d=0) == _lib.ERR_INVALID_ARG
+    assert _rl_host(n=-1) == _lib.ERR_INVALID_ARG
+
+
 def test_no_cpu_fallback(built):
     import torch
     if torch.cuda.is_available():
         pytest.skip("a device is present")
     # valid arguments, no device: the call must fail, not compute on the host
     assert _rl() == _lib.ERR_NO_DEVICE
+    assert _rl_host() == _lib.ERR_NO_DEVICE
+    # the entry is right-looking by name: opts.variant is overridden
+    assert _rl_host(variant=_lib.LEFT_LOOKING) == _lib.ERR_NO_DEVICE
     st = _lib.lib().lu_convert_c(None, 4, 4, ctypes.c_void_p(1), _lib.F32, 4,
                                  ctypes.c_void_p(1), _lib.F16, 4, 0)
     assert st == _lib.ERR_NO_DEVICE

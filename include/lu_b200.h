@@ -82,7 +82,12 @@ typedef struct lu_opts {
   int32_t lookahead;    /* 1: factor panel k+1 while update k runs */
   int32_t diag_width;   /* width of the one-CTA diagonal factorization
                            (multiple of 8, <= 128; 0 = default 128) */
-  int32_t reserved[8];
+  int32_t panel_fp32;   /* fp16 storage, left-looking: 1 keeps each block
+                           column / row update in fp32 until its panel is
+                           factored (the reference's OP = OF = fp32 wrappers,
+                           src/lu_nopiv_ll.hxx:172-201); 0 rounds the update
+                           to fp16 first (OP = fp16).  Ignored for fp32 storage. */
+  int32_t reserved[7];
 } lu_opts;
 
 /* Defaults: nb = 256, ib = 8, FP32/FP32, right-looking, look-ahead on. */
@@ -180,6 +185,24 @@ LU_API lu_status lu_gemm_update_c(lu_stream_t stream, lu_compute compute, int64_
                            double beta, void* c, int64_t ldc, void* workspace,
                            size_t ws_bytes);
 
+/* lu_gemm_update_c with the storage types of A, B (both LU_F32 or both
+ * LU_F16) and C (LU_F32 or LU_F16): the reference's gemmex instantiations
+ * with fp16 operands (src/gemm.cu:17-316).
+ *   LU_COMPUTE_FP32 : fp32 A, B, C only (SIMT).
+ *   LU_COMPUTE_TC32 : fp16 (or fp32, rounded to fp16) A, B; C fp32 or fp16
+ *                     (C = rn16(C + alpha * acc) with acc and the sum in fp32).
+ *   LU_COMPUTE_TC16, LU_COMPUTE_FP16 : as TC32 (the reference accumulates in
+ *                     fp16; the tensor cores here accumulate in fp32 and round
+ *                     the result once).
+ *   the other tensor-core kinds: fp32 A, B, C as lu_gemm_update_c.
+ * Tensor-core kinds need beta = 1. */
+LU_API lu_status lu_gemm_update_ex_c(lu_stream_t stream, lu_compute compute, int64_t m,
+                                     int64_t n, int64_t k, double alpha, const void* a,
+                                     lu_dtype type_a, int64_t lda, const void* b,
+                                     lu_dtype type_b, int64_t ldb, double beta, void* c,
+                                     lu_dtype type_c, int64_t ldc, void* workspace,
+                                     size_t ws_bytes);
+
 /* Seeded, counter-based test-matrix generator (bit-identical to the CPU
  * oracle): kind 0: r_ij = U[-1,1); kind 1: r_ij ~ N(0,1)/sqrt(n);
  * a_ii = alpha * sum_{j!=i} |r_ij|; all entries * 2^kscale; row i scaled by
@@ -222,9 +245,12 @@ LU_API lu_status lu_refine_c(lu_stream_t stream, int64_t n, const float* d_a,
  * scratch is one array compiled into the library (LU_REFINE_STATIC_SCRATCH_BYTES
  * of device memory per device), so n <= LU_REFINE_STATIC_MAX_N, else
  * LU_ERR_INVALID_ARG with nothing enqueued.  For callers that cannot hand
- * over or allocate device memory.  The first call on a device looks the
- * array up (cudaGetSymbolAddress) and should come before any stream capture;
- * calls overlapping in time on one device share the array and race. */
+ * over or allocate device memory.  Arguments are checked as lu_refine_c
+ * checks them, before any device call.  The first call on a device (and the
+ * first after cudaDeviceReset) looks the array up (cudaGetSymbolAddress).
+ * Like lu_refine_c it synchronises the stream once per iteration, so it must
+ * not be called while the stream is being captured.  Calls overlapping in
+ * time on one device share the array and race. */
 #define LU_REFINE_STATIC_MAX_N 4096
 #define LU_REFINE_STATIC_SCRATCH_BYTES 614400
 LU_API lu_status lu_refine_static_c(lu_stream_t stream, int64_t n, const float* d_a,
@@ -366,7 +392,6 @@ LU_API void lu_profile_begin(void);
 /* Stop recording, wait for the recorded events and write up to max_entries
  * aggregated entries; returns the number of kernel classes seen. */
 LU_API int lu_profile_end(lu_profile_entry* out, int max_entries);
-/* Number of kernels this library has launched in this process. */
 /* Per-launch timeline of the last profiled region (after lu_profile_end):
  * kernel class, stream (numbered in order of first use) and start / end in
  * ms from the first recorded launch.  Returns the number of launches. */
@@ -376,6 +401,7 @@ typedef struct lu_trace_entry {
   double start_ms, end_ms;
 } lu_trace_entry;
 LU_API int lu_profile_trace(lu_trace_entry* out, int max_entries);
+/* Number of kernels this library has launched in this process. */
 LU_API long long lu_launch_count(void);
 
 #ifdef __cplusplus

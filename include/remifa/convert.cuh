@@ -1,0 +1,5 @@
+// Same file name as the reference's src/convert.cuh (remifa::convert).
+// With -I include/remifa -I include, code written against the reference
+// compiles unchanged against the header-only drop-in over liblu_b200.so.
+#pragma once
+#include "../remifa_shim.hxx"

@@ -72,6 +72,9 @@ def lib():
                                           ctypes.c_int, _i64, _i64]
         L.orc_lu_ll_f32.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int]
         L.orc_lu_ll_f16.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int]
+        L.orc_lu_ll_f32_sub.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int, _i64]
+        L.orc_lu_ll_f16_ex.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int, _i64,
+                                       ctypes.c_int]
         L.orc_lu_f64.argtypes = [_i64, _f64p, _i64]
         L.orc_lu_solve_f64.argtypes = [_i64, _f64p, _i64, _f64p]
         L.orc_lu_solve_f32.argtypes = [_i64, _f32p, _i64, _f32p]
@@ -176,15 +179,22 @@ def lu_rl(a: np.ndarray, nb: int = 256, outer_fmt: int = 0, threads: int = 0) ->
 
 
 def lu_ll(a: np.ndarray, nb: int = 256, threads: int = 0,
-          fp16_storage: bool = False) -> np.ndarray:
+          fp16_storage: bool = False, panel_fp32: bool = False,
+          sub: int = 128) -> np.ndarray:
     """Factor a copy of `a` with the restated reference left-looking
     algorithm (fp16_storage: the fp16-matrix variant; `a` must then hold
-    fp16-representable values)."""
+    fp16-representable values; panel_fp32: its OP = OF = fp32 form).  Outer
+    blocks wider than `sub` are factored as sub-blocks of that width, as the
+    product library does (for nb <= sub this is the reference's loop)."""
     lda = ld(a) if a.strides[0] == a.itemsize else a.shape[0]
     out = colmajor(a.shape[0], a.shape[1], lda)
     out[:, :] = a
-    fn = lib().orc_lu_ll_f16 if fp16_storage else lib().orc_lu_ll_f32
-    fn(a.shape[0], a.shape[1], nb, _p32(out), ld(out), threads)
+    if fp16_storage:
+        lib().orc_lu_ll_f16_ex(a.shape[0], a.shape[1], nb, _p32(out), ld(out), threads,
+                               sub, int(bool(panel_fp32)))
+    else:
+        lib().orc_lu_ll_f32_sub(a.shape[0], a.shape[1], nb, _p32(out), ld(out), threads,
+                                sub)
     return out
 
 

@@ -449,6 +449,47 @@ static void inner_ll(int64_t m, int64_t n, float* a, int64_t lda) {
   }
 }
 
+// The product library's inside of a left-looking outer block wider than
+// its one-CTA Crout kernel (sub columns): sub-block c first receives the
+// K = c update from the block's own earlier columns (column below, row to
+// the right), then inner_ll.  For n <= sub this is inner_ll itself.
+static void inner_ll_blocked(int64_t m, int64_t n, float* a, int64_t lda, int64_t sub) {
+  for (int64_t c = 0; c < n; c += sub) {
+    const int64_t w = std::min(sub, n - c);
+    if (c > 0) {
+      orc_gemm_sub_f32(m - c, w, c, a + c, lda, a + c * lda, lda, a + c + c * lda, lda);
+      if (m - c > w)
+        orc_gemm_sub_f32(w, m - c - w, c, a + c, lda, a + (c + w) * lda, lda,
+                         a + c + (c + w) * lda, lda);
+    }
+    inner_ll(m - c, w, a + c + c * lda, lda);
+  }
+}
+
+// reference src/lu_nopiv_ll.hxx:208-575 for W = OP = OF = float, I = O = FP32
+// (the lu_nopiv_ll_f32 wrapper, src/lu_nopiv_ll.cxx:14-29); outer blocks
+// wider than `sub` factored as inner_ll_blocked
+void orc_lu_ll_f32_sub(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                       int threads, int64_t sub) {
+  const int saved = omp_get_max_threads();
+  if (threads > 0) omp_set_num_threads(threads);
+  const int64_t nc = (n - 1) / nb + 1;
+  for (int64_t kk = 0; kk < nc; ++kk) {
+    const int64_t ofs = kk * nb;
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = m - ofs;
+    if (ofs > 0) {
+      orc_gemm_sub_f32(updm, in, ofs, a + ofs, lda, a + ofs * lda, lda,
+                       a + ofs + ofs * lda, lda);
+      if (updm > in)
+        orc_gemm_sub_f32(in, updm - in, ofs, a + ofs, lda, a + (ofs + in) * lda,
+                         lda, a + ofs + (ofs + in) * lda, lda);
+    }
+    inner_ll_blocked(updm, in, a + ofs + ofs * lda, lda, sub);
+  }
+  omp_set_num_threads(saved);
+}
+
 // reference src/lu_nopiv_ll.hxx:208-575 for W = OP = OF = float, I = O = FP32
 // (the lu_nopiv_ll_f32 wrapper, src/lu_nopiv_ll.cxx:14-29)
 void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
@@ -480,6 +521,40 @@ void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
 // inner Crout elimination in fp32 with its results rounded to fp16 (the
 // product library's fp16 variant; the reference's fp16 wrappers factor the
 // panel in fp16 arithmetic instead).
+// panel_fp32 = 1 (the reference's OP = OF = fp32 wrappers,
+// src/lu_nopiv_ll.hxx:172-201): the updated block column / row is not
+// rounded to fp16 before its elimination.  Outer blocks wider than `sub` are
+// factored as inner_ll_blocked.
+void orc_lu_ll_f16_ex(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                      int threads, int64_t sub, int panel_fp32) {
+  const int saved = omp_get_max_threads();
+  if (threads > 0) omp_set_num_threads(threads);
+  auto round_block = [&](int64_t rows, int64_t cols, float* p) {
+    for (int64_t j = 0; j < cols; ++j)
+      for (int64_t i = 0; i < rows; ++i) p[i + j * lda] = round_fmt(p[i + j * lda], 1);
+  };
+  const int64_t nc = (n - 1) / nb + 1;
+  for (int64_t kk = 0; kk < nc; ++kk) {
+    const int64_t ofs = kk * nb;
+    const int64_t in = std::min(n - ofs, nb);
+    const int64_t updm = m - ofs;
+    float* blk = a + ofs + ofs * lda;
+    if (ofs > 0) {
+      orc_gemm_sub_f32(updm, in, ofs, a + ofs, lda, a + ofs * lda, lda, blk, lda);
+      if (!panel_fp32) round_block(updm, in, blk);
+      if (updm > in) {
+        orc_gemm_sub_f32(in, updm - in, ofs, a + ofs, lda, a + (ofs + in) * lda, lda,
+                         blk + in * lda, lda);
+        if (!panel_fp32) round_block(in, updm - in, blk + in * lda);
+      }
+    }
+    inner_ll_blocked(updm, in, blk, lda, sub);
+    round_block(updm, in, blk);
+    if (updm > in) round_block(in, updm - in, blk + in * lda);
+  }
+  omp_set_num_threads(saved);
+}
+
 void orc_lu_ll_f16(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int threads) {
   const int saved = omp_get_max_threads();

@@ -94,6 +94,12 @@ void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
  * rounded to fp16, the inner Crout elimination in fp32 rounded to fp16. */
 void orc_lu_ll_f16(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int threads);
+/* Outer blocks wider than `sub` factored as sub-blocks (the product's
+ * nesting for nb > 128); panel_fp32: the fp16 variant with OP = OF = fp32. */
+void orc_lu_ll_f32_sub(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                       int threads, int64_t sub);
+void orc_lu_ll_f16_ex(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
+                      int threads, int64_t sub, int panel_fp32);
 
 /* ---- FP64 oracle ----------------------------------------------------- */
 void orc_lu_f64(int64_t n, double* a, int64_t lda);

@@ -8,7 +8,8 @@
 //   * ref_panel_f32      -> remifa::lu_nopiv_panel<float,8>   (src/lu_nopiv.cu:364-400)
 //   * ref_convert_*      -> remifa::convert<TA,TAO>           (src/convert.cu:324-360)
 //   * ref_lu_nopiv_rl_*  -> remifa::lu_nopiv_rl<float,I,O,8>  (src/lu_nopiv.hxx:44-208)
-//   * ref_lu_nopiv_ll_*  -> remifa::lu_nopiv_ll_* wrappers    (src/lu_nopiv_ll.cxx:14-296)
+//   * ref_lu_nopiv_ll_*  -> remifa::lu_nopiv_ll_* wrappers    (src/lu_nopiv_ll.cxx:14-636)
+//   * ref_panel_f16      -> remifa::lu_nopiv_panel<half,8>
 // Nothing here is copied from the reference; it only calls it.
 #include <cstdint>
 #include <stdexcept>
@@ -109,6 +110,75 @@ int ref_lu_nopiv_ll_f16_tc32(void* stream, int m, int n, int nb, void* d_a,
   }
   cublasDestroy(h);
   return rc;
+}
+
+// Every cuBLAS (non-CUTLASS) W = fp16 wrapper of src/lu_nopiv_ll.cxx, by
+// number:
+//   0 lu_nopiv_ll_f16                                   (:191, I=O=FP16)
+//   1 lu_nopiv_ll_f16_tc16xtc16                         (:246, I=O=TC16)
+//   2 lu_nopiv_ll_f16_tc32xtc32                         (:282, I=O=TC32)
+//   3 lu_nopiv_ll_f16_f16xtc32                          (:338, I=FP16, O=TC32)
+//   4 lu_nopiv_ll_f16_f16xtc32_fp32                     (:393, OP=fp32)
+//   5 lu_nopiv_ll_f16_f16xtc16                          (:507, I=FP16, O=TC16)
+//   6 lu_nopiv_ll_f16_tc32xtc32_fp16xfp32_fp16xfp32     (:563, IP=IF=fp32)
+//   7 lu_nopiv_ll_f16_tc32xtc32_fp32xfp32_fp32xfp32     (:618, OP=OF=IP=IF=fp32)
+// Returns -3 for an unknown number.
+int ref_lu_nopiv_ll_f16_variant(void* stream, int variant, int m, int n, int nb,
+                                void* d_a, int lda, int* d_info) {
+  cublasHandle_t h = make_handle((cudaStream_t)stream);
+  if (!h) return -1;
+  half* a = (half*)d_a;
+  int rc = 0;
+  try {
+    switch (variant) {
+      case 0: remifa::lu_nopiv_ll_f16(h, m, n, nb, a, lda, d_info); break;
+      case 1: remifa::lu_nopiv_ll_f16_tc16xtc16(h, m, n, nb, a, lda, d_info); break;
+      case 2: remifa::lu_nopiv_ll_f16_tc32xtc32(h, m, n, nb, a, lda, d_info); break;
+      case 3: remifa::lu_nopiv_ll_f16_f16xtc32(h, m, n, nb, a, lda, d_info); break;
+      case 4: remifa::lu_nopiv_ll_f16_f16xtc32_fp32(h, m, n, nb, a, lda, d_info); break;
+      case 5: remifa::lu_nopiv_ll_f16_f16xtc16(h, m, n, nb, a, lda, d_info); break;
+      case 6:
+        remifa::lu_nopiv_ll_f16_tc32xtc32_fp16xfp32_fp16xfp32(h, m, n, nb, a, lda, d_info);
+        break;
+      case 7:
+        remifa::lu_nopiv_ll_f16_tc32xtc32_fp32xfp32_fp32xfp32(h, m, n, nb, a, lda, d_info);
+        break;
+      default: rc = -3;
+    }
+  } catch (std::exception& e) {
+    std::fprintf(stderr, "[ref_shim] %s\n", e.what());
+    rc = -2;
+  }
+  cublasDestroy(h);
+  return rc;
+}
+
+// W = fp32 left-looking with tensor-core outer updates, which need the fp16
+// copy buffer (src/lu_nopiv_ll.cxx:74-89 fp32xtc32, :131-146 tc32xtc32).
+int ref_lu_nopiv_ll_f32_tc(void* stream, int inner_tc, int m, int n, int nb,
+                           float* d_a, int lda, int* d_info, void* d_cpy, int ld_cpy) {
+  cublasHandle_t h = make_handle((cudaStream_t)stream);
+  if (!h) return -1;
+  int rc = 0;
+  try {
+    if (inner_tc)
+      remifa::lu_nopiv_ll_f32_tc32xtc32(h, m, n, nb, d_a, lda, d_info, (half*)d_cpy, ld_cpy);
+    else
+      remifa::lu_nopiv_ll_f32_fp32xtc32(h, m, n, nb, d_a, lda, d_info, (half*)d_cpy, ld_cpy);
+  } catch (std::exception& e) {
+    std::fprintf(stderr, "[ref_shim] %s\n", e.what());
+    rc = -2;
+  }
+  cublasDestroy(h);
+  return rc;
+}
+
+// lu_nopiv_panel<half, 8> (src/lu_nopiv.cu:364-400 instantiated for half)
+int ref_panel_f16(void* stream, int m, int n, const void* d, int ldd, void* l,
+                  int ldl, void* u, int ldu, int* stat) {
+  remifa::lu_nopiv_panel<half, 8>((cudaStream_t)stream, m, n, (const half*)d, ldd,
+                                  (half*)l, ldl, (half*)u, ldu, stat);
+  return (int)cudaGetLastError();
 }
 
 }  // extern "C"

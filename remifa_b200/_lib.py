@@ -34,7 +34,8 @@ class LuOpts(ctypes.Structure):
         ("variant", ctypes.c_int32),
         ("lookahead", ctypes.c_int32),
         ("diag_width", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 8),
+        ("panel_fp32", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 
@@ -93,6 +94,9 @@ SIGNATURES = {
     "lu_gemm_update_c": (_int, [_vp, _int, _i64, _i64, _i64, ctypes.c_double,
                                 _vp, _i64, _vp, _i64, ctypes.c_double, _vp,
                                 _i64, _vp, ctypes.c_size_t]),
+    "lu_gemm_update_ex_c": (_int, [_vp, _int, _i64, _i64, _i64, ctypes.c_double,
+                                   _vp, _int, _i64, _vp, _int, _i64, ctypes.c_double, _vp,
+                                   _int, _i64, _vp, ctypes.c_size_t]),
     "lu_gen_matrix_c": (_int, [_vp, _i64, _vp, _i64, ctypes.c_uint64, _int,
                                ctypes.c_double, _int, ctypes.c_double]),
     "lu_solve_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int]),

@@ -89,7 +89,8 @@ def _stream(stream=None):
 
 
 def make_opts(nb: int = 256, inner=FP32, outer=FP32, lookahead: bool = True,
-              diag_width: int = 0, variant: int = _lib.RIGHT_LOOKING) -> _lib.LuOpts:
+              diag_width: int = 0, variant: int = _lib.RIGHT_LOOKING,
+              panel_fp32: bool = False) -> _lib.LuOpts:
     o = _lib.LuOpts()
     _lib.lib().lu_opts_default(ctypes.byref(o))
     o.nb = int(nb)
@@ -98,6 +99,7 @@ def make_opts(nb: int = 256, inner=FP32, outer=FP32, lookahead: bool = True,
     o.lookahead = int(bool(lookahead))
     o.diag_width = int(diag_width)
     o.variant = int(variant)
+    o.panel_fp32 = int(bool(panel_fp32))
     return o
 
 
@@ -112,14 +114,14 @@ def workspace_size(n: int, nb: int = 256, inner=FP32, outer=FP32,
 
 
 def _factor(fn_name: str, variant: int, a: torch.Tensor, nb: int, inner, outer,
-            a_cpy, info, lookahead, diag_width, workspace, stream):
+            a_cpy, info, lookahead, diag_width, workspace, stream, panel_fp32=False):
     if not a.is_cuda:
         raise ValueError(f"{fn_name}: the matrix must be a CUDA tensor")
     m, n = a.shape
     lda = ld(a)
     if info is None:
         info = torch.zeros(1, dtype=torch.int32, device=a.device)
-    o = make_opts(nb, inner, outer, lookahead, diag_width, variant)
+    o = make_opts(nb, inner, outer, lookahead, diag_width, variant, panel_fp32)
     ws_ptr, ws_bytes = None, 0
     if workspace is not None:
         ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
@@ -173,10 +175,13 @@ def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=
 def lu_nopiv_ll(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
                 a_cpy: torch.Tensor | None = None, info: torch.Tensor | None = None,
                 lookahead: bool = True, diag_width: int = 0,
-                workspace: torch.Tensor | None = None, stream=None) -> torch.Tensor:
-    """In-place left-looking (Crout) no-pivot LU (remifa::lu_nopiv_ll)."""
+                workspace: torch.Tensor | None = None, stream=None,
+                panel_fp32: bool = False) -> torch.Tensor:
+    """In-place left-looking (Crout) no-pivot LU (remifa::lu_nopiv_ll).
+    panel_fp32 (fp16 matrices): keep each block column / row update in fp32
+    until its panel is factored (the reference's OP = OF = fp32 wrappers)."""
     return _factor("lu_nopiv_ll_c", _lib.LEFT_LOOKING, a, nb, inner, outer,
-                   a_cpy, info, lookahead, diag_width, workspace, stream)
+                   a_cpy, info, lookahead, diag_width, workspace, stream, panel_fp32)
 
 
 def lu_nopiv_panel(m: int, n: int, d: torch.Tensor, l: torch.Tensor,
@@ -207,18 +212,23 @@ def convert(a: torch.Tensor, out: torch.Tensor, scale_log2: int = 0,
 def gemmex(compute, alpha: float, a: torch.Tensor, b: torch.Tensor, beta: float,
            c: torch.Tensor, workspace: torch.Tensor | None = None,
            stream=None) -> torch.Tensor:
-    """remifa::gemmex: c = alpha * a @ b + beta * c (column-major fp32)."""
+    """remifa::gemmex: c = alpha * a @ b + beta * c (column-major; a and b
+    both float32 or both float16, c float32 or float16)."""
     m, k = a.shape
     k2, n = b.shape
     if k != k2 or tuple(c.shape) != (m, n):
         raise ValueError("gemmex: shape mismatch")
+    for name, t in (("a", a), ("b", b), ("c", c)):
+        if t.dtype not in (torch.float32, torch.float16) or not t.is_cuda:
+            raise ValueError(f"gemmex: {name} must be a float32 / float16 CUDA tensor")
     ws_ptr, ws_bytes = None, 0
     if workspace is not None:
         ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
-    st = _lib.lib().lu_gemm_update_c(_stream(stream), int(compute), m, n, k,
-                                     float(alpha), _ptr(a), ld(a), _ptr(b), ld(b),
-                                     float(beta), _ptr(c), ld(c), ws_ptr, ws_bytes)
-    _lib.check(st, "lu_gemm_update_c")
+    st = _lib.lib().lu_gemm_update_ex_c(_stream(stream), int(compute), m, n, k,
+                                        float(alpha), _ptr(a), _DTYPES[a.dtype], ld(a),
+                                        _ptr(b), _DTYPES[b.dtype], ld(b), float(beta),
+                                        _ptr(c), _DTYPES[c.dtype], ld(c), ws_ptr, ws_bytes)
+    _lib.check(st, "lu_gemm_update_ex_c")
     return c
 
 
@@ -294,13 +304,37 @@ def lu_solve(lu: torch.Tensor, b: torch.Tensor, trans: bool = False,
     return b
 
 
+def _check_refine_args(fn: str, a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
+                       x: torch.Tensor | None) -> int:
+    """The checks the C ABI cannot make on raw pointers: a and lu float32
+    n x n column-major, b and x float64 vectors of n contiguous elements, all
+    CUDA tensors on one device.  Returns n; raises ValueError otherwise."""
+    if a.dim() != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError(f"{fn}: a must be a square matrix")
+    n = a.shape[0]
+    for name, t in (("a", a), ("lu", lu)):
+        if t.dtype != torch.float32 or t.dim() != 2 or tuple(t.shape) != (n, n):
+            raise ValueError(f"{fn}: {name} must be a float32 {n} x {n} matrix")
+        ld(t)  # column-major
+    vecs = [("b", b)] + ([("x", x)] if x is not None else [])
+    for name, t in vecs:
+        if t.dtype != torch.float64 or t.dim() != 1 or t.numel() != n or \
+                not t.is_contiguous():
+            raise ValueError(f"{fn}: {name} must be a contiguous float64 vector of {n} "
+                             "elements")
+    for name, t in [("a", a), ("lu", lu)] + vecs:
+        if not t.is_cuda or t.device != a.device:
+            raise ValueError(f"{fn}: {name} must be a CUDA tensor on a's device")
+    return n
+
+
 def refine(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
            x: torch.Tensor | None = None, tol: float = 1e-14, max_iter: int = 30,
            stream=None, raise_on_stall: bool = False):
     """FP64 iterative refinement of A x = b with (possibly low-precision)
     factors `lu` of the fp32 matrix `a`.  Returns (x, iterations, berr)
     where berr = ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf)."""
-    n = a.shape[0]
+    n = _check_refine_args("refine", a, lu, b, x)
     if x is None:
         x = torch.empty(n, dtype=torch.float64, device=a.device)
     it = ctypes.c_int(0)
@@ -333,7 +367,7 @@ def refine_static(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
     scratch is compiled into the library, so n <= 4096 and calls must not
     overlap in time on one device.  x (fp64, n) receives the solution.
     Returns (iterations, berr)."""
-    n = a.shape[0]
+    n = _check_refine_args("refine_static", a, lu, b, x)
     it = ctypes.c_int(0)
     be = ctypes.c_double(0.0)
     st = _lib.lib().lu_refine_static_c(_stream(stream), n, _ptr(a), ld(a), _ptr(lu),

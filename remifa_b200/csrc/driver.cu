@@ -257,28 +257,38 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   if (o.nb < 8 || o.nb % 8 != 0 || o.nb > 4096) return LU_ERR_INVALID_ARG;
   const int dw = o.diag_width == 0 ? 128 : o.diag_width;
   if (dw < 8 || dw > 128 || dw % 8 != 0) return LU_ERR_INVALID_ARG;
-  // fp16 storage: the left-looking variant with fp16 tensor-core updates
-  if (dtype == LU_F16 &&
-      !(o.variant == LU_LEFT_LOOKING && o.outer_update == LU_COMPUTE_TC32))
-    return LU_ERR_UNSUPPORTED;
   if (dtype != LU_F32 && dtype != LU_F16) return LU_ERR_UNSUPPORTED;
   if (o.variant != LU_RIGHT_LOOKING && o.variant != LU_LEFT_LOOKING)
     return LU_ERR_INVALID_ARG;
-  if (o.inner_update != LU_COMPUTE_FP32) return LU_ERR_UNSUPPORTED;
-  if (o.outer_update != LU_COMPUTE_FP32 && !is_tc((lu_compute)o.outer_update))
+  // fp16 storage: the left-looking variant with fp16 tensor-core updates;
+  // TC16 and FP16 (fp16 accumulation in the reference) run as TC32 with one
+  // rounding of the fp32 sum to fp16
+  lu_compute outer = (lu_compute)o.outer_update;
+  if (dtype == LU_F16) {
+    if (o.variant != LU_LEFT_LOOKING) return LU_ERR_UNSUPPORTED;
+    if (outer == LU_COMPUTE_TC16 || outer == LU_COMPUTE_FP16) outer = LU_COMPUTE_TC32;
+    if (outer != LU_COMPUTE_TC32) return LU_ERR_UNSUPPORTED;
+  }
+  // inner (rank-8 and within-block) updates always run in fp32, at least as
+  // accurate as the reference's TC32 (any storage) or FP16 / TC16 (fp16
+  // storage) inner updates
+  const lu_compute inner = (lu_compute)o.inner_update;
+  if (!(inner == LU_COMPUTE_FP32 || inner == LU_COMPUTE_TC32 ||
+        (dtype == LU_F16 && (inner == LU_COMPUTE_FP16 || inner == LU_COMPUTE_TC16))))
     return LU_ERR_UNSUPPORTED;
+  if (outer != LU_COMPUTE_FP32 && !is_tc(outer)) return LU_ERR_UNSUPPORTED;
   if (o.variant == LU_LEFT_LOOKING) {
-    // one diagonal kernel covers the outer block; e4m3 tile scales would
-    // have to follow the growing K range of the left-looking products
-    if (o.nb > 128) return LU_ERR_UNSUPPORTED;
-    if (o.outer_update == LU_COMPUTE_TC32_E4M3 || o.outer_update == LU_COMPUTE_TC32_SPLIT)
+    // e4m3 tile scales would have to follow the growing K range of the
+    // left-looking products
+    if (outer == LU_COMPUTE_TC32_E4M3 || outer == LU_COMPUTE_TC32_SPLIT)
       return LU_ERR_UNSUPPORTED;
   }
   p->n = n;
   p->nb = o.nb;
   p->diag_w = (int)std::min<int64_t>(dw, o.nb);
-  p->inner = (lu_compute)o.inner_update;
-  p->outer = (lu_compute)o.outer_update;
+  p->inner = LU_COMPUTE_FP32;
+  p->outer = outer;
+  p->panel_fp32 = dtype == LU_F16 && o.variant == LU_LEFT_LOOKING && o.panel_fp32 != 0;
   p->variant = (lu_variant)o.variant;
   p->lookahead = o.lookahead != 0;
   p->dtype = dtype;
@@ -286,7 +296,7 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
   p->off_status = off;  // [0] first bad pivot, [1] device wait error
   off += 256;
   if (p->variant == LU_LEFT_LOOKING && dtype == LU_F16) {
-    p->diag_w = (int)p->nb;
+    p->diag_w = (int)std::min<int64_t>(p->nb, kLlSub);
     const int64_t ldk = (n + 15) / 16 * 16;
     p->ld_shadow = std::max<int64_t>(4, (n + 3) / 4 * 4);
     off = align_up(off, 1024);
@@ -298,7 +308,7 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     return LU_SUCCESS;
   }
   if (p->variant == LU_LEFT_LOOKING) {
-    p->diag_w = (int)p->nb;
+    p->diag_w = (int)std::min<int64_t>(p->nb, kLlSub);
     if (is_tc(p->outer) && n > p->nb) {
       // low-precision copies of all factored L columns (row-major) and U
       // rows (column-major), leading dimension round16(n)
@@ -881,11 +891,47 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
   return LU_SUCCESS;
 }
 
-// Left-looking (Crout) factorization, restating src/lu_nopiv_ll.hxx:208-575
-// with nb <= 128: per outer block, one K = ofs update of the block column and
-// the block row (FP32 SIMT, or tensor cores on the low-precision copies of
-// all earlier factors), then the Crout diagonal kernel and the left-looking
-// L/U panels.  The FP32 path applies every update in the reference's order.
+// The inside of one left-looking outer block (columns [ofs, ofs + in) of an
+// n x n matrix x, ld ldx, already updated by all columns left of ofs): the
+// block is factored as sub-blocks of at most kLlSub columns; sub-block c
+// first receives the FP32 update from the block's own columns [ofs, c)
+// (its column below and its row to the right), then the Crout diagonal
+// kernel and the left-looking L / U panels eliminate it.  For in <= kLlSub
+// this is exactly the reference's inner Crout loop
+// (src/lu_nopiv_inner_ll.hxx:197-370); wider blocks nest one more level.
+static lu_status ll_block(cudaStream_t st, float* x, int64_t ldx, int64_t n, int64_t ofs,
+                          int64_t in, int* first_bad) {
+  for (int64_t c = ofs; c < ofs + in; c += kLlSub) {
+    const int64_t w = std::min(kLlSub, ofs + in - c);
+    const int64_t rest = n - c - w;
+    float* dg = x + c + c * ldx;
+    if (c > ofs) {
+      const int64_t k = c - ofs;
+      ProfScope ps("sgemm_update", st, 0.0, 2.0 * k * ((double)(n - c) * w + (double)w * rest));
+      LUB_TRY(launch_sgemm_update(st, n - c, w, k, -1.0f, x + c + ofs * ldx, ldx,
+                                  x + ofs + c * ldx, ldx, 1.0f, dg, ldx, false));
+      if (rest > 0)
+        LUB_TRY(launch_sgemm_update(st, w, rest, k, -1.0f, x + c + ofs * ldx, ldx,
+                                    x + ofs + (c + w) * ldx, ldx, 1.0f, dg + w * ldx, ldx,
+                                    false));
+    }
+    {
+      ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * (double)w / 3.0);
+      LUB_TRY(launch_diag_crout(st, dg, ldx, (int)w, c, first_bad));
+    }
+    if (rest > 0) {
+      ProfScope ps("lupanel", st, 16.0 * rest * w, 2.0 * rest * (double)w * w);
+      LUB_TRY(launch_lupanel(st, dg, ldx, (int)w, rest, rest, true));
+    }
+  }
+  return LU_SUCCESS;
+}
+
+// Left-looking (Crout) factorization, restating src/lu_nopiv_ll.hxx:208-575:
+// per outer block, one K = ofs update of the block column and the block row
+// (FP32 SIMT, or tensor cores on the low-precision copies of all earlier
+// factors), then ll_block.  The FP32 path applies every update in the
+// reference's order (for nb <= kLlSub).
 static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
                            int64_t lda, char* ws, int* first_bad, int* err) {
   const int64_t n = p.n, nb = p.nb;
@@ -921,40 +967,34 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
                                       lda, false));
       }
     }
-    {
-      ProfScope ps("diag_factor", st, 8.0 * in * in, 2.0 * in * in * (double)in / 3.0);
-      LUB_TRY(launch_diag_crout(st, blk, lda, (int)in, ofs, first_bad));
-    }
+    LUB_TRY(ll_block(st, a, lda, n, ofs, in, first_bad));
     const int64_t rest = updm - in;
-    if (rest > 0) {
-      {
-        ProfScope ps("lupanel", st, 16.0 * rest * in, 2.0 * rest * (double)in * in);
-        LUB_TRY(launch_lupanel(st, blk, lda, (int)in, rest, rest, true));
-      }
-      if (tc) {
-        ProfScope ps("pack_operands", st, 2.0 * rest * in * (4.0 + es));
-        // L21 rows [ofs+in, n) of the block's columns -> row-major copy;
-        // U12 columns [ofs+in, n) of the block's rows -> column-major copy
-        LUB_TRY(launch_pack_a(st, kind, rest, in, blk + in, lda,
-                              Lc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
-        LUB_TRY(launch_pack_b(st, kind, in, rest, blk + in * lda, lda,
-                              Uc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
-      }
+    if (rest > 0 && tc) {
+      ProfScope ps("pack_operands", st, 2.0 * rest * in * (4.0 + es));
+      // L21 rows [ofs+in, n) of the block's columns -> row-major copy;
+      // U12 columns [ofs+in, n) of the block's rows -> column-major copy
+      LUB_TRY(launch_pack_a(st, kind, rest, in, blk + in, lda,
+                            Lc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
+      LUB_TRY(launch_pack_b(st, kind, in, rest, blk + in * lda, lda,
+                            Uc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
     }
   }
   return LU_SUCCESS;
 }
 
 // Left-looking factorization of an fp16 matrix (the reference's W = fp16
-// wrappers, src/lu_nopiv_ll.hxx:646-790, with O = TC32).  Per outer block:
-// one K = ofs tensor-core update of the block column and the block row read
-// straight from the fp16 matrix (U, column-major = K-major) and from a
-// row-major fp16 copy of the factored L columns, the sum formed in fp32 and
-// stored back to fp16 once; then the block column and row are copied to
-// fp32, factored there by the Crout diagonal kernel and the left-looking
-// panels, and rounded back to fp16.  The reference's fp16 wrappers factor
-// the panel in fp16 or with fp16 tensor-core inner updates; here the inner
-// elimination always runs in fp32, so its results are at least as accurate.
+// wrappers, src/lu_nopiv_ll.hxx:646-790).  Per outer block: one K = ofs
+// tensor-core update of the block column and the block row read straight
+// from the fp16 matrix (U, column-major = K-major) and from a row-major fp16
+// copy of the factored L columns, the sum formed in fp32; then the block
+// column and row are factored in an fp32 shadow (ll_block) and rounded back
+// to fp16.  panel_fp32 = false (OP = fp16): the updated block is stored to
+// fp16 once, then copied to the shadow.  panel_fp32 = true (OP = OF = fp32,
+// src/lu_nopiv_ll.hxx:172-201): the block is copied to the shadow first
+// and the update lands there in fp32, unrounded.  The reference's fp16
+// wrappers factor the panel in fp16 arithmetic or with fp16 tensor-core
+// inner updates; here the inner elimination always runs in fp32, so its
+// results are at least as accurate.
 static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_t lda,
                                char* ws, int* first_bad, int* err) {
   const int64_t n = p.n, nb = p.nb;
@@ -968,30 +1008,39 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
     const int64_t rest = updm - in;
     __half* blk = a + ofs + ofs * lda;
     float* sblk = S + ofs + ofs * lds;
+    auto to_shadow = [&]() -> lu_status {
+      LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
+      if (rest > 0)
+        LUB_TRY(launch_convert(st, in, rest, blk + in * lda, LU_F16, lda, sblk + in * lds,
+                               LU_F32, lds, 0));
+      return LU_SUCCESS;
+    };
+    if (p.panel_fp32) LUB_TRY(to_shadow());
     if (ofs > 0) {
       ProfScope ps("tc_update", st,
-                   4.0 * updm * in + 4.0 * in * rest + 2.0 * (double)ofs * (updm + in),
+                   (p.panel_fp32 ? 8.0 : 4.0) * ((double)updm * in + (double)in * rest) +
+                       2.0 * (double)ofs * (updm + in),
                    2.0 * ofs * ((double)updm * in + (double)in * rest));
-      LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                 Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
-                                 err));
-      if (rest > 0)
-        LUB_TRY(launch_tc_update_h(st, TcOperand::F16, in, rest, ofs, -1.0f,
+      if (p.panel_fp32) {
+        LUB_TRY(launch_tc_update(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                 Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk, lds,
+                                 nullptr, nullptr, err));
+        if (rest > 0)
+          LUB_TRY(launch_tc_update(st, TcOperand::F16, in, rest, ofs, -1.0f,
                                    Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
-                                   blk + in * lda, lda, err));
+                                   sblk + in * lds, lds, nullptr, nullptr, err));
+      } else {
+        LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                   Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
+                                   err));
+        if (rest > 0)
+          LUB_TRY(launch_tc_update_h(st, TcOperand::F16, in, rest, ofs, -1.0f,
+                                     Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
+                                     blk + in * lda, lda, err));
+      }
     }
-    LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
-    if (rest > 0)
-      LUB_TRY(launch_convert(st, in, rest, blk + in * lda, LU_F16, lda, sblk + in * lds,
-                             LU_F32, lds, 0));
-    {
-      ProfScope ps("diag_factor", st, 8.0 * in * in, 2.0 * in * in * (double)in / 3.0);
-      LUB_TRY(launch_diag_crout(st, sblk, lds, (int)in, ofs, first_bad));
-    }
-    if (rest > 0) {
-      ProfScope ps("lupanel", st, 16.0 * rest * in, 2.0 * rest * (double)in * in);
-      LUB_TRY(launch_lupanel(st, sblk, lds, (int)in, rest, rest, true));
-    }
+    if (!p.panel_fp32) LUB_TRY(to_shadow());
+    LUB_TRY(ll_block(st, S, lds, n, ofs, in, first_bad));
     LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
     if (rest > 0) {
       LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,
@@ -1211,6 +1260,70 @@ lu_status gemm_update(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
   if (s == LU_SUCCESS)
     s = tc_update_fp32(st, tc_kind(compute), m, n, k, (float)alpha, a, lda, b,
                        ldb, c, ldc, wsb, w, err);
+  if (owned) cudaFreeAsync(ws, st);
+  return s;
+}
+
+// gemmex with operand / result storage types (the reference's gemmex
+// instantiations, src/gemm.cu:17-316): fp32 operands and result on the SIMT
+// fp32 path or any tensor-core kind as gemm_update; fp16 operands and / or an
+// fp16 result on the tensor cores with fp16 operands and fp32 accumulation
+// (LU_COMPUTE_TC32, and TC16 / FP16, whose fp16 accumulation the tensor
+// cores replace by fp32 accumulation with one rounding of the result).
+lu_status gemm_update_ex(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
+                         int64_t k, double alpha, const void* a, lu_dtype ta, int64_t lda,
+                         const void* b, lu_dtype tb, int64_t ldb, double beta, void* c,
+                         lu_dtype tc, int64_t ldc, void* workspace, size_t ws_bytes) {
+  const bool f32ops = ta == LU_F32 && tb == LU_F32;
+  const bool f16ops = ta == LU_F16 && tb == LU_F16;
+  if ((!f32ops && !f16ops) || (tc != LU_F32 && tc != LU_F16)) return LU_ERR_UNSUPPORTED;
+  if (compute == LU_COMPUTE_FP32) {
+    if (!f32ops || tc != LU_F32) return LU_ERR_UNSUPPORTED;
+    return gemm_update(compute, st, m, n, k, alpha, (const float*)a, lda, (const float*)b,
+                       ldb, beta, (float*)c, ldc, workspace, ws_bytes);
+  }
+  const lu_compute kc = (compute == LU_COMPUTE_FP16 || compute == LU_COMPUTE_TC16)
+                            ? LU_COMPUTE_TC32 : compute;
+  if (!is_tc(kc)) return LU_ERR_UNSUPPORTED;
+  if (f32ops && tc == LU_F32)
+    return gemm_update(kc, st, m, n, k, alpha, (const float*)a, lda, (const float*)b, ldb,
+                       beta, (float*)c, ldc, workspace, ws_bytes);
+  if (kc != LU_COMPUTE_TC32) return LU_ERR_UNSUPPORTED;  // fp16 data: fp16 operands
+  if (beta != 1.0) return LU_ERR_UNSUPPORTED;  // the update form C += alpha*A*B
+  if (k <= 0) return LU_SUCCESS;
+  const TcWs w = tc_ws_layout(256, m, n, k, TcOperand::F16);
+  const size_t need = 256 + w.bytes;
+  if (workspace != nullptr && ws_bytes < need) return LU_ERR_WORKSPACE;
+  void* ws = workspace;
+  bool owned = false;
+  if (ws == nullptr) {
+    if (cudaMallocAsync(&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
+    owned = true;
+  }
+  char* wsb = static_cast<char*>(ws);
+  int* err = reinterpret_cast<int*>(wsb);
+  const int64_t ldk = tc_packed_k(TcOperand::F16, k);
+  __half* ap = reinterpret_cast<__half*>(wsb + w.off_a);
+  __half* bp = reinterpret_cast<__half*>(wsb + w.off_b);
+  lu_status s = launch_fill_int(st, err, 0, 1);
+  if (s == LU_SUCCESS) {
+    ProfScope ps("pack_operands", st, (double)(m + n) * (double)k * (f16ops ? 4.0 : 6.0));
+    if (f16ops) {
+      s = launch_pack_a_f16(st, m, k, (const __half*)a, lda, ap, ldk);
+      if (s == LU_SUCCESS) s = launch_pack_b_f16(st, k, n, (const __half*)b, ldb, bp, ldk);
+    } else {
+      s = tc_pack(st, TcOperand::F16, m, n, k, (const float*)a, lda, (const float*)b, ldb,
+                  wsb, w);
+    }
+  }
+  if (s == LU_SUCCESS) {
+    ProfScope ps("tc_update", st, (tc == LU_F32 ? 8.0 : 4.0) * m * n + 2.0 * (m + n) * k,
+                 2.0 * m * n * k);
+    s = tc == LU_F32 ? launch_tc_update(st, TcOperand::F16, m, n, k, (float)alpha, ap, ldk,
+                                        bp, ldk, (float*)c, ldc, nullptr, nullptr, err)
+                     : launch_tc_update_h(st, TcOperand::F16, m, n, k, (float)alpha, ap, ldk,
+                                          bp, ldk, (__half*)c, ldc, err);
+  }
   if (owned) cudaFreeAsync(ws, st);
   return s;
 }

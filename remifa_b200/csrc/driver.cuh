@@ -5,6 +5,10 @@
 
 namespace lub {
 
+// Left-looking outer blocks wider than this are factored as sub-blocks of
+// this width (the one-CTA Crout diagonal kernel's limit).
+constexpr int64_t kLlSub = 128;
+
 // Everything a factorization call needs to know before enqueueing work.
 struct Plan {
   int64_t n = 0;
@@ -15,6 +19,7 @@ struct Plan {
   lu_variant variant = LU_RIGHT_LOOKING;
   bool lookahead = true;
   lu_dtype dtype = LU_F32;
+  bool panel_fp32 = false;  // fp16 storage: block update kept in fp32
   // workspace layout (byte offsets into one device allocation)
   size_t off_status = 0;    // int first_bad
   size_t off_lcopy = 0;     // low-precision L21 copy (row-major)
@@ -40,5 +45,9 @@ lu_status gemm_update(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
                       int64_t k, double alpha, const float* a, int64_t lda,
                       const float* b, int64_t ldb, double beta, float* c,
                       int64_t ldc, void* workspace, size_t ws_bytes);
+lu_status gemm_update_ex(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
+                         int64_t k, double alpha, const void* a, lu_dtype ta, int64_t lda,
+                         const void* b, lu_dtype tb, int64_t ldb, double beta, void* c,
+                         lu_dtype tc, int64_t ldc, void* workspace, size_t ws_bytes);
 
 }  // namespace lub

@@ -130,6 +130,22 @@ lu_status lu_gemm_update_c(lu_stream_t stream, lu_compute compute, int64_t m,
                      (float*)c, ldc, workspace, ws_bytes);
 }
 
+lu_status lu_gemm_update_ex_c(lu_stream_t stream, lu_compute compute, int64_t m,
+                              int64_t n, int64_t k, double alpha, const void* a,
+                              lu_dtype type_a, int64_t lda, const void* b, lu_dtype type_b,
+                              int64_t ldb, double beta, void* c, lu_dtype type_c,
+                              int64_t ldc, void* workspace, size_t ws_bytes) {
+  if (m < 0 || n < 0 || k < 0) return LU_ERR_INVALID_ARG;
+  if (m == 0 || n == 0) return LU_SUCCESS;
+  if (!a || !b || !c) return LU_ERR_INVALID_ARG;
+  if (lda < std::max<int64_t>(1, m) || ldb < std::max<int64_t>(1, k) ||
+      ldc < std::max<int64_t>(1, m))
+    return LU_ERR_INVALID_ARG;
+  LUB_TRY(check_device());
+  return gemm_update_ex(compute, (cudaStream_t)stream, m, n, k, alpha, a, type_a, lda, b,
+                        type_b, ldb, beta, c, type_c, ldc, workspace, ws_bytes);
+}
+
 lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
                           int64_t lda, uint64_t seed, int kind, double alpha,
                           int kscale, double gamma_bits) {

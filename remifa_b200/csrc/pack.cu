@@ -23,11 +23,16 @@ template <> __device__ __forceinline__ uint8_t to_low<uint8_t>(float x) {
   return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
 }
 
+__device__ __forceinline__ float to_f32(float x) { return x; }
+__device__ __forceinline__ float to_f32(__half x) { return __half2float(x); }
+
 constexpr int TA = 64;  // tile edge of the transposing pack
 
-template <typename T>
+// S: source element type (fp32, or fp16 for the fp16-operand gemm entry,
+// whose values pass through unchanged).
+template <typename T, typename S = float>
 __global__ void __launch_bounds__(256)
-pack_a_kernel(int64_t M, int64_t K, const float* __restrict__ src, int64_t lds,
+pack_a_kernel(int64_t M, int64_t K, const S* __restrict__ src, int64_t lds,
               T* __restrict__ dst, int64_t ldd, const int* __restrict__ scale) {
   __shared__ float tile[TA][TA + 1];  // [k][i]
   const int64_t i0 = (int64_t)blockIdx.x * TA;
@@ -37,7 +42,7 @@ pack_a_kernel(int64_t M, int64_t K, const float* __restrict__ src, int64_t lds,
   for (int q = tid; q < TA * TA; q += 256) {
     const int i = q % TA, k = q / TA;
     const int64_t gi = i0 + i, gk = k0 + k;
-    tile[k][i] = (gi < M && gk < K) ? src[gi + gk * lds] : 0.0f;
+    tile[k][i] = (gi < M && gk < K) ? to_f32(src[gi + gk * lds]) : 0.0f;
   }
   __syncthreads();
   // store: consecutive threads write consecutive k of one row
@@ -105,14 +110,14 @@ pack_b_split_kernel(int64_t K, int64_t kp, int64_t N, const float* __restrict__ 
   }
 }
 
-template <typename T>
+template <typename T, typename S = float>
 __global__ void __launch_bounds__(256)
-pack_b_kernel(int64_t K, int64_t N, const float* __restrict__ src, int64_t lds,
+pack_b_kernel(int64_t K, int64_t N, const S* __restrict__ src, int64_t lds,
               T* __restrict__ dst, int64_t ldd, const int* __restrict__ scale) {
   const int64_t k = (int64_t)blockIdx.x * 256 + threadIdx.x;
   if (k >= K) return;
   for (int64_t j = blockIdx.y; j < N; j += gridDim.y) {
-    float x = src[k + j * lds];
+    float x = to_f32(src[k + j * lds]);
     if (scale) x = ldexpf(x, scale[j / 128]);
     dst[k + j * ldd] = to_low<T>(x);
   }
@@ -234,6 +239,24 @@ lu_status launch_pack_b(cudaStream_t st, TcOperand kind, int64_t K, int64_t N,
     }
   }
   return LU_ERR_INVALID_ARG;
+}
+
+lu_status launch_pack_a_f16(cudaStream_t st, int64_t M, int64_t K, const __half* src,
+                            int64_t lds, __half* dst, int64_t ldd) {
+  if (M <= 0 || K <= 0) return LU_SUCCESS;
+  dim3 grid((unsigned)ceil_div(M, TA), (unsigned)ceil_div(K, TA));
+  pack_a_kernel<__half, __half><<<grid, 256, 0, st>>>(M, K, src, lds, dst, ldd, nullptr);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+lu_status launch_pack_b_f16(cudaStream_t st, int64_t K, int64_t N, const __half* src,
+                            int64_t lds, __half* dst, int64_t ldd) {
+  if (N <= 0 || K <= 0) return LU_SUCCESS;
+  dim3 grid((unsigned)ceil_div(K, 256), (unsigned)std::min<int64_t>(N, 65535));
+  pack_b_kernel<__half, __half><<<grid, 256, 0, st>>>(K, N, src, lds, dst, ldd, nullptr);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
 }
 
 lu_status launch_scale_rowtiles(cudaStream_t st, int64_t M, int64_t K,

@@ -8,9 +8,15 @@
 // pivoting the rows of L21 and the columns of U12 are independent of each
 // other once the diagonal block is factored, so this file splits that loop
 // into
-//   diag_factor_kernel : the w x w diagonal block, one CTA, in shared memory;
-//   lpanel_kernel      : rows below the block, 64 rows per CTA;
-//   upanel_kernel      : columns right of the block, 64 columns per CTA;
+//   diag_factor_kernel : the w x w diagonal block, one CTA, in shared memory
+//                        (diag_crout_kernel: the same for the left-looking
+//                        variant's Crout order);
+//   lupanel_kernel     : the L21 rows below the block and the U12 columns
+//                        right of it, 64 rows or 64 columns per CTA (one grid
+//                        for both strips), optionally writing the K-major
+//                        tensor-core operand copies of what it finishes;
+//   ref_panel_kernel   : remifa::lu_nopiv_panel<float,8> as a standalone
+//                        entry point (lu_panel_c);
 // each replaying, per element, the reference's exact operation sequence
 // (the 8-column elimination, then rank-8 updates accumulated
 // acc = fma(l, u, acc) over the 8 columns and subtracted once).

@@ -154,6 +154,25 @@ lu_status refine_multi(lu_stream_t stream, int64_t n, int64_t nrhs, const float*
 
 }  // namespace
 
+namespace lub {
+
+lu_status refine_check_args(int64_t n, int64_t nrhs, const float* d_a, int64_t lda,
+                            const float* d_lu, int64_t ldlu, const double* d_b,
+                            int64_t ldb, const double* d_x, int64_t ldx, int trans,
+                            double tol, int max_iter) {
+  if (n < 0 || nrhs < 0 || lda < std::max<int64_t>(1, n) ||
+      ldlu < std::max<int64_t>(1, n) || ldb < std::max<int64_t>(1, n) ||
+      ldx < std::max<int64_t>(1, n) || max_iter < 0 || !(tol >= 0.0) ||
+      (trans != 0 && trans != 1))
+    return LU_ERR_INVALID_ARG;
+  if (n > 0 && nrhs > 0 && (!d_a || !d_lu || !d_b || !d_x)) return LU_ERR_INVALID_ARG;
+  return LU_SUCCESS;
+}
+
+lu_status refine_check_device() { return check_device_local(); }
+
+}  // namespace lub
+
 extern "C" {
 
 LU_API lu_status lu_refine_ex_workspace_size(int64_t n, int64_t nrhs, size_t* bytes) {
@@ -168,15 +187,11 @@ LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
                                 double* d_x, int64_t ldx, int trans, double tol,
                                 int max_iter, int* iters, double* berr,
                                 void* workspace, size_t ws_bytes) {
-  if (n < 0 || nrhs < 0 || lda < std::max<int64_t>(1, n) ||
-      ldlu < std::max<int64_t>(1, n) || ldb < std::max<int64_t>(1, n) ||
-      ldx < std::max<int64_t>(1, n) || max_iter < 0 || !(tol >= 0.0) ||
-      (trans != 0 && trans != 1))
-    return LU_ERR_INVALID_ARG;
+  LUB_TRY(refine_check_args(n, nrhs, d_a, lda, d_lu, ldlu, d_b, ldb, d_x, ldx, trans,
+                            tol, max_iter));
   if (iters) *iters = 0;
   if (berr) *berr = 0.0;
   if (n == 0 || nrhs == 0) return LU_SUCCESS;
-  if (!d_a || !d_lu || !d_b || !d_x) return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device_local());
   const RefineWs w = refine_layout(n, nrhs);
   if (workspace && ws_bytes < w.bytes) return LU_ERR_WORKSPACE;

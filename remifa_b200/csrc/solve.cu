@@ -855,7 +855,11 @@ lu_status launch_nr(cudaStream_t st, const Args& a, int nr) {
 // ---- residual r = b - A x (fp32 A, fp64 b, x, r) -------------------------
 // Column chunks of kRC columns give partial dot products P[chunk][row]; a
 // second pass adds them in chunk order, so the result does not depend on
-// scheduling.
+// scheduling.  kRC also sizes the partial sums (n x ceil(n / kRC) doubles)
+// and with them the compiled-in scratch of lu_refine_static_c
+// (LU_REFINE_STATIC_SCRATCH_BYTES, checked against refine's layout at
+// n = LU_REFINE_STATIC_MAX_N by a CPU test): a smaller kRC needs a larger
+// array.
 constexpr int kRC = 256;
 
 __global__ void __launch_bounds__(kT)

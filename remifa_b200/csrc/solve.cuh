@@ -55,4 +55,14 @@ lu_status launch_residual_t(cudaStream_t st, int64_t n, const float* A,
 lu_status launch_norm_one(cudaStream_t st, int64_t n, const float* A,
                           int64_t lda, unsigned long long* out);
 
+// refine.cu: the host-side argument checks of lu_refine_ex_c (sizes, leading
+// dimensions, tol, max_iter, trans, and non-null pointers when there is work)
+// and its device check (an sm_100 device current).  Neither touches the
+// device's memory or loads a module.
+lu_status refine_check_args(int64_t n, int64_t nrhs, const float* d_a, int64_t lda,
+                            const float* d_lu, int64_t ldlu, const double* d_b,
+                            int64_t ldb, const double* d_x, int64_t ldx, int trans,
+                            double tol, int max_iter);
+lu_status refine_check_device();
+
 }  // namespace lub

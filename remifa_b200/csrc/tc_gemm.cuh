@@ -58,6 +58,12 @@ lu_status launch_scale_coltiles(cudaStream_t st, int64_t K, int64_t N,
 lu_status launch_pack_a(cudaStream_t st, TcOperand kind, int64_t M, int64_t K,
                         const float* src, int64_t lds, void* dst, int64_t ldd,
                         const int* scale);
+// The same copies of fp16 sources (F16 kind, no scales): A transposed into
+// the row-major copy, B into the compact column-major copy.
+lu_status launch_pack_a_f16(cudaStream_t st, int64_t M, int64_t K, const __half* src,
+                            int64_t lds, __half* dst, int64_t ldd);
+lu_status launch_pack_b_f16(cudaStream_t st, int64_t K, int64_t N, const __half* src,
+                            int64_t lds, __half* dst, int64_t ldd);
 // B operand: dst[k + j*ldd] = round(src[k + j*lds] * 2^scale[j/128]).
 lu_status launch_pack_b(cudaStream_t st, TcOperand kind, int64_t K, int64_t N,
                         const float* src, int64_t lds, void* dst, int64_t ldd,

@@ -1,6 +1,6 @@
 """Generate golden vectors from the REFERENCE's own compiled code (GPU).
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir]   (default: this folder)
 
 Runs oracle/_ref/libremifa_ref.so (the reference's src/lu_nopiv.cu,
 src/convert.cu, src/gemm.cu, src/lu_nopiv_ll.cxx compiled unmodified) on a
@@ -37,6 +37,7 @@ def ref_lib():
     L.ref_lu_nopiv_rl_f32.argtypes = [vp, i64, i64, i64, vp, i64, vp, i, i, vp, i64]
     L.ref_lu_nopiv_ll_f32.argtypes = [vp, i, i, i, vp, i, vp]
     L.ref_lu_nopiv_ll_f16_tc32.argtypes = [vp, i, i, i, vp, i, vp]
+    L.ref_lu_nopiv_ll_f16_variant.argtypes = [vp, i, i, i, i, vp, i, vp]
     return L
 
 
@@ -128,8 +129,28 @@ def main(outdir: str) -> None:
     torch.cuda.synchronize()
     np.savez_compressed(os.path.join(outdir, f"ref_ll_f32_n{nn}_nb{nb}.npz"),
                         a_in=np.array(a), lu=np.array(from_dev(da, nn)))
+
+    # 6. left-looking on an fp16 matrix (W = fp16), n = 256, nb = 64, input
+    #    gen_diagdom rounded to fp16: the wrappers lu_nopiv_ll_f16_tc32xtc32
+    #    (variant 2, src/lu_nopiv_ll.cxx:282), lu_nopiv_ll_f16_tc16xtc16
+    #    (variant 1, :246) and lu_nopiv_ll_f16_tc32xtc32_fp32xfp32_fp32xfp32
+    #    (variant 7, :618).
+    nn, nb = 256, 64
+    a16 = oracle.gen_diagdom(nn, lda=nn).astype(np.float16)
+    for variant, tag in ((2, "tc32"), (1, "tc16"), (7, "tc32_fp32panel")):
+        dh = to_dev(np.asfortranarray(a16))
+        rc = L.ref_lu_nopiv_ll_f16_variant(st, variant, nn, nn, nb,
+                                           ctypes.c_void_p(dh.data_ptr()), nn,
+                                           ctypes.c_void_p(info.data_ptr()))
+        torch.cuda.synchronize()
+        if rc != 0:
+            print(f"variant {variant} ({tag}) returned {rc}; skipped")
+            continue
+        np.savez_compressed(os.path.join(outdir, f"ref_ll_f16_{tag}_n{nn}_nb{nb}.npz"),
+                            a_in=np.asfortranarray(a16), lu=np.array(from_dev(dh, nn)))
     print("golden vectors written to", outdir)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    # default: next to this script (the committed fixtures)
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))

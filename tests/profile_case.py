@@ -1,6 +1,6 @@
 """A small, fixed factorization to put under a profiler.
 
-    python -m remifa_b200.profile_case [n] [compute] [reps]
+    python tests/profile_case.py [n] [compute] [reps]
 
 factors the seeded matrix A = R + D (R ~ N(0,1)/sqrt(n), row dominance 1.5,
 the generator of the benchmarks) `reps` times on cuda:0 with the
@@ -11,11 +11,13 @@ factorizations (the diagonal blocks are always 128 x 128, the sub-panels 128
 wide), while the device holds only a few hundred MB, so a profiler capture
 of one launch ends quickly.
 """
+import os
 import sys
 
 import torch
 
-from . import api
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from remifa_b200 import api  # noqa: E402
 
 
 def main(argv=None) -> None:

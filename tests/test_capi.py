@@ -118,3 +118,54 @@ def test_python_layer_raises_like_reference(built):
         _lib.check(_lib.ERR_CUDA, "x")
     assert rb.align_lda(100) == 112 and rb.align_lda(16) == 16
     assert rb.align_lda(100, 2) == 128
+
+
+def test_refine_python_checks_before_the_call(built):
+    """refine / refine_static check dtypes, lengths and devices before the C
+    call: the C ABI only sees raw pointers, so a float32 or short x would be
+    written out of bounds."""
+    import torch
+    n = 8
+    a = torch.zeros((n, n), dtype=torch.float32).t()
+    lu = torch.zeros((n, n), dtype=torch.float32).t()
+    b = torch.zeros(n, dtype=torch.float64)
+    x = torch.zeros(n, dtype=torch.float64)
+    bad = [
+        dict(b=b.float()),                                  # b float32
+        dict(x=x.float()),                                  # x float32
+        dict(x=torch.zeros(n - 1, dtype=torch.float64)),    # x too short
+        dict(b=torch.zeros((n, 2), dtype=torch.float64)),   # b not a vector
+        dict(lu=torch.zeros((n, n), dtype=torch.float64)),  # lu float64
+        dict(a=torch.zeros((n, n + 1), dtype=torch.float32)),  # a not square
+        dict(x=torch.zeros(2 * n, dtype=torch.float64)[::2]),  # x not contiguous
+        dict(),                                             # host tensors
+    ]
+    for kw in bad:
+        args = dict(a=a, lu=lu, b=b, x=x)
+        args.update(kw)
+        with pytest.raises(ValueError):
+            rb.refine(args["a"], args["lu"], args["b"], args["x"])
+        with pytest.raises(ValueError):
+            rb.api.refine_static(args["a"], args["lu"], args["b"], args["x"])
+
+
+def test_refine_static_checks_arguments_before_any_device_call(built):
+    """lu_refine_static_c rejects bad arguments exactly as lu_refine_c does,
+    before looking up its scratch array (which would touch the device)."""
+    L = _lib.lib()
+    vp = ctypes.c_void_p
+    ok = vp(64)
+    # null matrix, lda < n, negative max_iter, negative tol
+    assert L.lu_refine_static_c(None, 10, None, 10, ok, 10, ok, ok, 1e-14, 30,
+                                None, None) == _lib.ERR_INVALID_ARG
+    assert L.lu_refine_static_c(None, 10, ok, 9, ok, 10, ok, ok, 1e-14, 30,
+                                None, None) == _lib.ERR_INVALID_ARG
+    assert L.lu_refine_static_c(None, 10, ok, 10, ok, 10, ok, ok, 1e-14, -1,
+                                None, None) == _lib.ERR_INVALID_ARG
+    assert L.lu_refine_static_c(None, 10, ok, 10, ok, 10, ok, ok, -1.0, 30,
+                                None, None) == _lib.ERR_INVALID_ARG
+    import torch
+    if not torch.cuda.is_available():
+        # valid arguments without a device: no scratch lookup, no fallback
+        assert L.lu_refine_static_c(None, 10, ok, 10, ok, 10, ok, ok, 1e-14, 30,
+                                    None, None) == _lib.ERR_NO_DEVICE

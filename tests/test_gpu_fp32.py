@@ -243,7 +243,10 @@ def test_workspace_caller_provided(built):
 
 # ------------------------------------------------------------ left-looking
 
-LL_CASES = [(7, 8), (64, 64), (200, 64), (257, 128), (520, 64), (1024, 128), (777, 32)]
+# nb > 128: outer blocks factored as 128-wide sub-blocks (the oracle restates
+# that nesting with sub = 128)
+LL_CASES = [(7, 8), (64, 64), (200, 64), (257, 128), (520, 64), (1024, 128), (777, 32),
+            (1000, 256), (777, 192), (300, 512)]
 
 
 @pytest.mark.parametrize("n,nb", LL_CASES)
@@ -298,9 +301,34 @@ def test_lu_ll_tensor_core(built, compute):
 def test_lu_ll_limits(built):
     a = to_dev(O.gen_matrix(300, seed=1, kind=0, alpha=2.0))
     with pytest.raises(NotImplementedError):
-        rb.lu_nopiv_ll(a, nb=256)
-    with pytest.raises(NotImplementedError):
         rb.lu_nopiv_ll(a, nb=128, outer=rb.compute_type.TC32_E4M3)
+    with pytest.raises(NotImplementedError):  # fp16 inner updates need fp16 storage
+        rb.lu_nopiv_ll(a, nb=128, inner=rb.FP16)
+
+
+def test_lu_ll_nb256_vs_reference_gpu(built):
+    """The reference's default outer block (nb = 256) on the left-looking
+    variant: the reference factors it with one 8-column Crout loop, this
+    library as two 128-wide sub-blocks; same factors up to rounding."""
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference library not built")
+    L = ctypes.CDLL(REF_SO)
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    L.ref_lu_nopiv_ll_f32.argtypes = [vp, i, i, i, vp, i, vp]
+    n, nb = 1024, 256
+    a = O.gen_diagdom(n, lda=n)
+    mine, theirs = to_dev(a), to_dev(a)
+    rb.lu_nopiv_ll(mine, nb=nb)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert L.ref_lu_nopiv_ll_f32(_st(), n, n, nb, ctypes.c_void_p(theirs.data_ptr()), n,
+                                 ctypes.c_void_p(info.data_ptr())) == 0
+    torch.cuda.synchronize()
+    lm, lr = to_host(mine), to_host(theirs)
+    assert np.abs(lm - lr).max() / np.abs(lr).max() <= 4 * n * 2.0 ** -24
+    b = O.gen_rhs(a, np.ones(n, np.float32))
+    e_m = O.nwerr(a, b, O.lu_solve_f32(lm, b))
+    e_r = O.nwerr(a, b, O.lu_solve_f32(lr, b))
+    assert e_m <= 4 * e_r and e_r <= 4 * e_m
 
 
 @pytest.mark.parametrize("n,nb,outer,la,pad", [

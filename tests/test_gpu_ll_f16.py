@@ -61,3 +61,37 @@ def test_ll_f16_argument_checks(built):
         rb.lu_nopiv_ll(b, nb=64, outer=rb.FP32)
     with pytest.raises(NotImplementedError):  # and the left-looking variant
         rb.lu_nopiv_rl(b, nb=64, outer=rb.TC32)
+
+
+@pytest.mark.parametrize("n,nb", [(1000, 128), (777, 256), (2048, 256)])
+def test_ll_f16_panel_fp32_matches_oracle(built, n, nb):
+    """OP = OF = fp32 (the reference's ..._fp32xfp32_fp32xfp32 wrappers): the
+    block update stays in fp32 until the panel is factored."""
+    a = O.round_fmt(O.gen_matrix(n, seed=n + 5, kind=1, alpha=1.5), O.FMT_FP16)
+    lda = (n + 7) // 8 * 8
+    d = fp16_dev(a, lda)
+    info = rb.lu_nopiv_ll(d, nb=nb, outer=rb.TC32, panel_fp32=True)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    got = np.asfortranarray(d.float().cpu().numpy())
+    want = O.lu_ll(a, nb=nb, fp16_storage=True, panel_fp32=True)
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel < 8 * 2.0 ** -11, rel
+    fe_g, fe_o = O.factor_error(a, got), O.factor_error(a, want)
+    assert fe_g <= 1.5 * fe_o + 1e-6 and fe_o <= 1.5 * fe_g + 1e-6, (fe_g, fe_o)
+
+
+def test_ll_f16_update_kinds(built):
+    """fp16 storage: TC16 / FP16 outer and FP16 / TC16 / TC32 inner updates
+    (the reference's W = fp16 wrappers) run the same fp32-accumulated tensor
+    -core update and fp32 elimination, so they give TC32's factors exactly."""
+    n, nb = 640, 128
+    a = O.round_fmt(O.gen_matrix(n, seed=9, kind=1, alpha=1.5), O.FMT_FP16)
+    base = fp16_dev(a, n)
+    rb.lu_nopiv_ll(base, nb=nb, outer=rb.TC32)
+    for inner, outer in [(rb.FP16, rb.TC16), (rb.TC16, rb.TC16), (rb.FP16, rb.TC32),
+                         (rb.TC32, rb.TC32), (rb.FP16, rb.FP16)]:
+        d = fp16_dev(a, n)
+        rb.lu_nopiv_ll(d, nb=nb, inner=inner, outer=outer)
+        torch.cuda.synchronize()
+        assert torch.equal(d, base), (inner, outer)

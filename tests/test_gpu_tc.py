@@ -257,3 +257,40 @@ def test_lookahead_is_bit_identical(built, compute, n, nb):
     rb.lu_nopiv_rl(d2, nb=nb, outer=compute, lookahead=True)
     torch.cuda.synchronize()
     assert torch.equal(d1, d2)
+
+
+@pytest.mark.parametrize("compute", [rb.TC32, rb.TC16, rb.FP16])
+@pytest.mark.parametrize("c_half", [False, True])
+@pytest.mark.parametrize("M,N,K", [(300, 500, 256), (128, 256, 64), (1000, 777, 200)])
+def test_gemmex_fp16_operands(built, compute, c_half, M, N, K):
+    """gemmex with fp16 A and B (the reference's TC32 / TC16 / FP16 gemmex
+    instantiations): fp32 accumulation of the exact fp16 products, C fp32 or
+    rounded to fp16 once."""
+    rng = np.random.default_rng(M + N + K)
+    A = rng.standard_normal((M, K)).astype(np.float16)
+    B = (rng.standard_normal((K, N)) * 3).astype(np.float16)
+    C = rng.standard_normal((M, N)).astype(np.float16 if c_half else np.float32)
+    want = C.astype(np.float64) - A.astype(np.float64) @ B.astype(np.float64)
+    mag = np.abs(A.astype(np.float64)) @ np.abs(B.astype(np.float64))
+    bound = 2 * K * U32 * mag + 2 * U32 * np.abs(want) + 1e-30
+    if c_half:
+        bound = bound + 2.0 ** -11 * np.abs(want) + 2.0 ** -24
+    dt = torch.float16
+    dA = rb.colmajor(torch.from_numpy(A).cuda(), lda=(M + 7) // 8 * 8)
+    dB = rb.colmajor(torch.from_numpy(B).cuda(), lda=(K + 7) // 8 * 8)
+    dC = rb.colmajor(torch.from_numpy(C).cuda())
+    assert dA.dtype == dt
+    rb.gemmex(compute, -1.0, dA, dB, 1.0, dC)
+    torch.cuda.synchronize()
+    got = np.asfortranarray(dC.double().cpu().numpy())
+    err = np.abs(got - want)
+    assert np.all(err <= bound), (err / bound).max()
+
+
+def test_gemmex_fp16_rejections(built):
+    a = rb.colmajor_empty(64, 64, 64, torch.float16)
+    c = rb.colmajor_empty(64, 64, 64, torch.float32)
+    with pytest.raises(NotImplementedError):  # fp16 operands on the SIMT fp32 path
+        rb.gemmex(rb.FP32, -1.0, a, a, 1.0, c)
+    with pytest.raises(NotImplementedError):  # bf16 kind with fp16 data
+        rb.gemmex(rb.compute_type.TC32_BF16, -1.0, a, a, 1.0, c)

@@ -296,3 +296,43 @@ def test_golden_ref_ll_f32():
     e_ref = O.nwerr(a, b, O.lu_solve_f32(np.asfortranarray(ref), b))
     e_orc = O.nwerr(a, b, O.lu_solve_f32(lu, b))
     assert e_orc <= 4 * e_ref + 1e-12 and e_ref <= 4 * e_orc + 1e-12
+
+
+@pytest.mark.parametrize("tag,panel_fp32", [("tc32", False), ("tc16", False),
+                                            ("tc32_fp32panel", True)])
+def test_golden_ref_ll_f16(tag, panel_fp32):
+    """Left-looking factorization of an fp16 matrix: the reference's
+    lu_nopiv_ll_f16_tc32xtc32 / _tc16xtc16 / _tc32xtc32_fp32xfp32_fp32xfp32
+    (src/lu_nopiv_ll.cxx:282, 246, 618) against the oracle's restatement
+    with the fp32 elimination this library uses (the reference eliminates in
+    fp16 arithmetic for the first two, in fp32 for the third).  Bounds: max
+    difference <= 1 u16 of the largest factor entry, backward error and
+    ||A - LU|| within 1.5x; with OP = fp32 on both sides at least 95% of the
+    factor entries identical."""
+    g = _golden(f"ref_ll_f16_{tag}_n256_nb64.npz")
+    a = np.asfortranarray(g["a_in"].astype(np.float32))
+    np.testing.assert_array_equal(
+        a, O.gen_diagdom(256, lda=256).astype(np.float16).astype(np.float32))
+    ref = np.asfortranarray(g["lu"].astype(np.float32))
+    lu = O.lu_ll(a, nb=64, fp16_storage=True, panel_fp32=panel_fp32)
+    assert np.abs(lu - ref).max() <= 2.0 ** -11 * np.abs(ref).max()
+    b = O.gen_rhs(a, np.ones(256, np.float32))
+    e_r = O.nwerr(a, b, O.lu_solve_f32(ref, b))
+    e_o = O.nwerr(a, b, O.lu_solve_f32(lu, b))
+    assert e_o <= 1.5 * e_r and e_r <= 1.5 * e_o, (e_o, e_r)
+    f_r, f_o = O.factor_error(a, ref), O.factor_error(a, lu)
+    assert f_o <= 1.5 * f_r and f_r <= 1.5 * f_o, (f_o, f_r)
+    if panel_fp32:
+        assert np.mean(lu == ref) >= 0.95
+
+
+@pytest.mark.parametrize("n,nb", [(300, 256), (520, 192), (257, 512)])
+def test_lu_ll_wide_blocks_against_fp64(n, nb):
+    """Outer blocks wider than 128 (factored as 128-wide sub-blocks): the
+    same factorization as the reference's single Crout loop up to rounding."""
+    a = O.gen_matrix(n, seed=n + 2, kind=1, alpha=1.5)
+    lu = O.lu_ll(a, nb=nb)
+    assert O.factor_error(a, lu) <= 10 * n * U32
+    flat = O.lu_ll(a, nb=nb, sub=nb)  # the reference's loop over the whole block
+    assert np.abs(lu - flat).max() <= 8 * n * U32 * np.abs(lu).max()
+    assert not np.array_equal(lu, flat) or nb <= 128

@@ -215,18 +215,104 @@ def run_reference(args, wl) -> None:
     print(json.dumps(line), flush=True)
 
 
-def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2):
+def run_reference_gpu(args, wl) -> None:
+    """--impl reference --ref-device gpu: the reference's own GPU code
+    (src/lu_nopiv.cu, gemm.cu, convert.cu, lu_nopiv.hxx compiled unmodified
+    into oracle/_ref by oracle/Makefile; cuBLAS inside) on the same workload:
+    remifa::lu_nopiv_rl<float, FP32, O, 8> with O = FP32 or TC32 (the fp16
+    copy buffer it requires allocated beforehand), timed with CUDA events
+    around each call.  The call allocates and frees its own workspace and
+    synchronises, as the reference does.  Not part of any default line: it
+    reproduces the reference-on-B200 figures next to this library's."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import ctypes
+    import numpy as np
+    import oracle as O
+    import torch
+    if wl["outer"] not in ("FP32", "TC32"):
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "unavailable": "the reference has no " + wl["outer"] +
+                                         " trailing update"}))
+        return
+    so = os.path.join(ROOT, "oracle", "_ref", "libremifa_ref.so")
+    if not os.path.exists(so):
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "unavailable": "oracle/_ref/libremifa_ref.so not built"}))
+        return
+    L = ctypes.CDLL(so)
+    vp, i64, i = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    L.ref_lu_nopiv_rl_f32.argtypes = [vp, i64, i64, i64, vp, i64, vp, i, i, vp, i64]
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, nb = wl["n"], wl["nb"] if args.nb is None else args.nb
+    tc = wl["outer"] == "TC32"
+    a = O.gen_matrix(n, seed=1, kind=wl["kind"], alpha=wl["alpha"], kscale=wl["kscale"])
+    base = torch.from_numpy(np.ascontiguousarray(a).T.copy()).cuda()  # column-major
+    work = torch.empty_like(base)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    cpy = torch.empty((n, n), dtype=torch.float16, device="cuda") if tc else None
+    st = torch.cuda.current_stream()
+    times = []
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    try:
+        for k in range(args.warmup + args.steps):
+            work.copy_(base)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            sys.stdout.flush()
+            os.dup2(devnull, 1)  # the reference prints a banner per call
+            e0.record(st)
+            rc = L.ref_lu_nopiv_rl_f32(ctypes.c_void_p(st.cuda_stream), n, n, nb,
+                                       ctypes.c_void_p(work.data_ptr()), n,
+                                       ctypes.c_void_p(info.data_ptr()), 0, int(tc),
+                                       ctypes.c_void_p(cpy.data_ptr()) if tc else None,
+                                       n if tc else 0)
+            e1.record(st)
+            torch.cuda.synchronize()
+            os.dup2(saved, 1)
+            if rc != 0:
+                raise RuntimeError(f"reference call failed ({rc})")
+            if k >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+    finally:
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+    ms = statistics.median(times)
+    value = lu_flops(n) / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "LU TFLOP/s (2n^3/3)", "value": value, "unit": "TFLOP/s",
+        "impl": "reference", "reference_device": "gpu", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "ms_all": times,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if not tc else "f32 storage, fp16 tensor-core update (cuBLAS)",
+        "data": "synthetic (seeded generator of the tests, host)",
+        "config": config_of(args, wl),
+        "code": "the reference's src/lu_nopiv.cu, gemm.cu, convert.cu and lu_nopiv.hxx "
+                "compiled unmodified for sm_100a (oracle/Makefile), cuBLAS 12.9 inside",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2, solver="classic",
+                     xt=None, b=None):
     """Time to an fp64-level solution of A x = b (b = A x_true, x_true ~
     N(0,1), fp64): copy A, factor with `outer`, refine in fp64 until the
-    normwise backward error is <= tol.  Device time with CUDA events (the
-    refinement reads its backward error once per iteration)."""
+    normwise backward error is <= tol -- classic refinement (`solver` =
+    "classic", lu_refine_c) or GMRES-IR ("gmres", lu_gmres_ir_c).  Device
+    time with CUDA events (the refinement reads its backward error back once
+    per iteration)."""
     dev = base.device
-    g = torch.Generator(device=dev)
-    g.manual_seed(7)
-    xt = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
-    b = torch.zeros(n, dtype=torch.float64, device=dev)
-    for j0 in range(0, n, 2048):  # b = A x_true in fp64, column blocks
-        b += base[:, j0:j0 + 2048].double() @ xt[j0:j0 + 2048]
+    if xt is None:
+        g = torch.Generator(device=dev)
+        g.manual_seed(7)
+        xt = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    if b is None:
+        b = torch.zeros(n, dtype=torch.float64, device=dev)
+        for j0 in range(0, n, 2048):  # b = A x_true in fp64, column blocks
+            b += base[:, j0:j0 + 2048].double() @ xt[j0:j0 + 2048]
     lu = rb.colmajor_empty(n, n, n, torch.float32, dev)
     ws = torch.empty(rb.workspace_size(n, nb=nb, outer=outer), dtype=torch.uint8, device=dev)
     best = None
@@ -237,12 +323,19 @@ def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2):
         s0.record()
         lu.copy_(base)
         info = rb.lu_nopiv_rl(lu, nb=nb, outer=outer, workspace=ws, lookahead=la)
-        x, it, be = rb.refine(base, lu, b, tol=tol, max_iter=50)
+        if solver == "gmres":
+            x, it, inner, be = rb.gmres_ir(base, lu, b, tol=tol, max_outer=20, restart=40)
+        else:
+            x, it, be = rb.refine(base, lu, b, tol=tol, max_iter=50)
+            inner = None
         s1.record()
         torch.cuda.synchronize(dev)
         ms = s0.elapsed_time(s1)
         fe = float(((x - xt).abs().max() / xt.abs().max()).item())
-        rec = {"ms": ms, "iters": it, "berr": be, "fwd_err": fe, "info": int(info.item())}
+        rec = {"ms": ms, "solver": solver, "iters": it, "berr": be, "fwd_err": fe,
+               "info": int(info.item())}
+        if inner is not None:
+            rec["arnoldi_steps"] = inner
         if best is None or ms < best["ms"]:
             best = rec
     del lu, ws
@@ -269,10 +362,15 @@ def main() -> None:
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     choices=sorted(WORKLOADS) + list(SPECIAL))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-device", default="cpu", choices=["cpu", "gpu"],
+                    help="--impl reference: the CPU restatement on the host cores "
+                         "(default) or the reference's own GPU code (oracle/_ref)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tts", action="store_true",
-                    help="skip the time-to-solution measurement")
+                    help="skip the time-to-solution measurements")
+    ap.add_argument("--no-n32768", action="store_true",
+                    help="skip the n = 32768 time-to-solution study of the default line")
     ap.add_argument("--no-lookahead", action="store_true",
                     help="factor each outer block strictly after the previous update")
     ap.add_argument("--nb", type=int, default=None, help="override the outer block size")
@@ -287,7 +385,10 @@ def main() -> None:
         return
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
-        run_reference(args, wl)
+        if args.ref_device == "gpu":
+            run_reference_gpu(args, wl)
+        else:
+            run_reference(args, wl)
         return
 
     import torch
@@ -467,6 +568,12 @@ def main() -> None:
             "tol": 1e-14, "backward_error": "||b-Ax||inf/(||A||inf ||x||inf + ||b||inf)",
             wl["outer"]: t_mixed, "FP32": t_fp32,
             "speedup_vs_fp32_plain": t_fp32["ms"] / t_mixed["ms"]}
+        if args.workload == DEFAULT_WORKLOAD and not args.no_n32768:
+            # the time-to-solution target's own size: n = 32768, every
+            # update precision against FP32 plain at kappa ~ 1e2 / 1e4 / 1e6
+            del base
+            torch.cuda.empty_cache()
+            line["time_to_solution_n32768"] = precision_study(torch, rb, reps=1)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)
     print(json.dumps(line), flush=True)
@@ -667,51 +774,77 @@ def _condest(torch, rb, a, lu, n, iters=4):
     return est
 
 
-def run_precision(args, torch, rb):
-    """n = 32768: time to an fp64-level solution (backward error <= 1e-14)
-    of A x = b, b = A x_true (x_true ~ N(0,1), fp64), for each Schur-update
-    precision (bf16, e4m3 with per-tile 2^k scales, split fp16, fp16, fp32
-    plain) on row-scaled diagonally dominant matrices A = S (R + D) with
-    kappa tuned to ~1e2, 1e4, 1e6.  value = FP32-plain time / best
-    mixed-precision time at kappa ~1e2."""
-    import math
-    n, nb = 32768, 256
-    precs = ["TC32_BF16", "TC32_E4M3", "TC32_SPLIT", "TC32", "FP32"]
-    results = []
-    base0 = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5)
-    lu0 = rb.colmajor(base0)
-    rb.lu_nopiv_rl(lu0, nb=nb, outer=rb.compute_type.TC32_SPLIT)
-    an = float(base0.abs().sum(dim=0).max())
-    k0 = an * _condest(torch, rb, base0, lu0, n)
-    del base0, lu0
-    torch.cuda.empty_cache()
-    for target in (1e2, 1e4, 1e6):
-        gamma = max(0.0, math.log2(target / k0))
-        base = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5, gamma_bits=gamma)
+PRECISIONS = ["TC32_BF16", "TC32_E4M3", "TC32_SPLIT", "TC32", "FP32"]
+
+
+def precision_study(torch, rb, n=32768, nb=256, reps=2, kappas=(1e2, 1e4, 1e6)):
+    """Time to an fp64-level solution (backward error <= 1e-14) of A x = b,
+    b = A x_true (x_true ~ N(0,1) seed 7, fp64), per Schur-update precision
+    (bf16, e4m3 with per-tile 2^k scales, split fp16, fp16, fp32 plain) and
+    per condition number.  A = alpha diag(|R| 1) - |R| with |R| ~ |N(0,1)|/sqrt(n)
+    (generator kind 2): row dominance alpha = 1 + 1.06 / kappa sets
+    kappa_2(A) ~ kappa.  Each precision is refined both ways (classic and
+    GMRES-IR); its time to solution is the faster one that converged."""
+    rows = []
+    for target in kappas:
+        alpha = 1.0 + 1.06 / target
+        base = rb.gen_matrix(n, seed=1, kind=2, alpha=alpha)
+        g = torch.Generator(device=base.device)
+        g.manual_seed(7)
+        xt = torch.randn(n, dtype=torch.float64, device=base.device, generator=g)
+        b = torch.zeros(n, dtype=torch.float64, device=base.device)
+        for j0 in range(0, n, 2048):
+            b += base[:, j0:j0 + 2048].double() @ xt[j0:j0 + 2048]
         lu = rb.colmajor(base)
         rb.lu_nopiv_rl(lu, nb=nb, outer=rb.compute_type.TC32_SPLIT)
-        kappa = float(base.abs().sum(dim=0).max()) * _condest(torch, rb, base, lu, n)
+        kappa1 = float(base.abs().sum(dim=0).max()) * _condest(torch, rb, base, lu, n)
         del lu
         torch.cuda.empty_cache()
-        row = {"kappa_target": target, "gamma_bits": gamma, "kappa1_est": kappa}
-        for pr in precs:
-            r = time_to_solution(rb, torch, base, n, nb, getattr(rb.compute_type, pr), True,
-                                 reps=2)
-            row[pr] = r
+        row = {"kappa_target": target, "alpha": alpha, "kappa1_est": kappa1}
+        for pr in PRECISIONS:
+            outer = getattr(rb.compute_type, pr)
+            c = time_to_solution(rb, torch, base, n, nb, outer, True, reps=reps,
+                                 solver="classic", xt=xt, b=b)
+            g2 = time_to_solution(rb, torch, base, n, nb, outer, True, reps=reps,
+                                  solver="gmres", xt=xt, b=b)
+            ok = [r for r in (c, g2) if r["berr"] <= 1e-14]
+            row[pr] = {"classic": c, "gmres": g2,
+                       "time_to_solution_ms": min(r["ms"] for r in ok) if ok else None}
             torch.cuda.empty_cache()
-        results.append(row)
-        del base
+        fp32 = row["FP32"]["time_to_solution_ms"]
+        mixed = [row[p]["time_to_solution_ms"] for p in PRECISIONS[:-1]
+                 if row[p]["time_to_solution_ms"] is not None]
+        row["speedup_best_mixed_vs_fp32"] = fp32 / min(mixed) if (fp32 and mixed) else None
+        row["speedup_per_precision"] = {
+            p: (fp32 / row[p]["time_to_solution_ms"]
+                if fp32 and row[p]["time_to_solution_ms"] else None) for p in PRECISIONS[:-1]}
+        rows.append(row)
+        del base, b, xt
         torch.cuda.empty_cache()
-    first = results[0]
-    mixed = min(first[p]["ms"] for p in precs[:-1] if first[p]["berr"] <= 1e-14)
-    line = _base_line(args, "time-to-solution speedup vs FP32 plain (berr <= 1e-14)",
-                      first["FP32"]["ms"] / mixed, "x", mixed,
-                      dtype="f32 storage; bf16 / e4m3 / split-fp16 / fp16 updates; fp64 IR",
-                      config={"workload": args.workload, "n": n, "nb": nb,
-                              "matrix": "S (R + D), R ~ N(0,1)/sqrt(n), row dominance 1.5, "
-                                        "S = diag(2^-round(gamma i/(n-1)))",
-                              "x_true": "N(0,1) seed 7, b = A x_true in fp64"})
-    line["results"] = results
+    speed = [r["speedup_best_mixed_vs_fp32"] for r in rows]
+    summary = {"n": n, "nb": nb, "reps": reps,
+               "matrix": "alpha diag(|R| 1) - |R|, |R| ~ |N(0,1)|/sqrt(n) seed 1, "
+                         "alpha = 1 + 1.06/kappa (kappa_2 ~ kappa)",
+               "x_true": "N(0,1) seed 7, b = A x_true in fp64",
+               "min_speedup_over_kappa": min(s for s in speed if s) if any(speed) else None,
+               "results": rows}
+    return summary
+
+
+def run_precision(args, torch, rb):
+    """n = 32768: precision_study at kappa ~ 1e2, 1e4, 1e6.  value = the
+    smallest, over the three condition numbers, of (FP32-plain time to
+    solution) / (best mixed-precision time to solution)."""
+    st = precision_study(torch, rb, reps=max(1, min(args.steps, 2)))
+    line = _base_line(args, "time-to-solution speedup vs FP32 plain (berr <= 1e-14), "
+                      "smallest over kappa", st["min_speedup_over_kappa"], "x",
+                      min(r[p]["time_to_solution_ms"] for r in st["results"]
+                          for p in PRECISIONS[:-1] if r[p]["time_to_solution_ms"]),
+                      dtype="f32 storage; bf16 / e4m3 / split-fp16 / fp16 updates; fp64 IR "
+                            "(classic or GMRES)",
+                      config={"workload": args.workload, "n": st["n"], "nb": st["nb"],
+                              "matrix": st["matrix"], "x_true": st["x_true"]})
+    line["results"] = st["results"]
     print(json.dumps(line), flush=True)
 
 

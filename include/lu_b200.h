@@ -87,7 +87,14 @@ typedef struct lu_opts {
                            factored (the reference's OP = OF = fp32 wrappers,
                            src/lu_nopiv_ll.hxx:172-201); 0 rounds the update
                            to fp16 first (OP = fp16).  Ignored for fp32 storage. */
-  int32_t reserved[7];
+  int32_t bulk_steps;   /* right-looking with look-ahead and fp16 / bf16 trailing
+                           updates: 0 (default) or 2 applies two consecutive
+                           outer steps' updates of the bulk of the trailing
+                           matrix in one pass (C - (L_k U_k + L_k+1 U_k+1),
+                           one fp32 accumulator, C read and written once); 1
+                           applies every step separately, the reference's
+                           rounding order.  Ignored elsewhere. */
+  int32_t reserved[6];
 } lu_opts;
 
 /* Defaults: nb = 256, ib = 8, FP32/FP32, right-looking, look-ahead on. */
@@ -212,6 +219,23 @@ LU_API lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
                           int64_t lda, uint64_t seed, int kind, double alpha,
                           int kscale, double gamma_bits);
 
+/* Equilibration in place by powers of two: LAPACK geequb's row / column
+ * scales and laqge's decision (rows when rowcnd < 0.1 or amax is outside
+ * the safe range, columns when colcnd < 0.1), as the reference applies them
+ * on the host before factoring (tests/testing_lu_gpu.hxx:288-311); force =
+ * 1 applies both scalings whatever laqge decides (a matrix scaled as a whole
+ * by a large power of two keeps rowcnd = colcnd = 1, yet its entries may lie
+ * outside the fp16 range of the tensor-core operands).  d_a
+ * (fp32, n x n) becomes R A C; d_r / d_c (device, n floats) receive the
+ * diagonals of R and C (ones where not applied); *equed (host) 'N', 'R',
+ * 'C' or 'B'; *rowcnd / *colcnd / *amax (host, may be NULL) geequb's ratios
+ * and max |a_ij|.  Every scale is a power of two, so R A C is exact and
+ * A x = b becomes (R A C) y = R b with x = C y.  Synchronises the stream
+ * (the decision is taken on the host). */
+LU_API lu_status lu_equilibrate_c(lu_stream_t stream, int64_t n, float* d_a, int64_t lda,
+                                  float* d_r, float* d_c, int force, char* equed,
+                                  double* rowcnd, double* colcnd, double* amax);
+
 /* ---- solve and iterative refinement (new: the reference solves on the
  * host with LAPACK getrs, tests/testing_lu_gpu.hxx:1309-1313) ------------ */
 
@@ -257,6 +281,26 @@ LU_API lu_status lu_refine_static_c(lu_stream_t stream, int64_t n, const float* 
                                     int64_t lda, const float* d_lu, int64_t ldlu,
                                     const double* d_b, double* d_x, double tol,
                                     int max_iter, int* iters, double* berr);
+
+/* GMRES-based FP64 refinement (GMRES-IR; new): each correction A d = r is
+ * solved by restarted GMRES on (LU)^-1 A d = (LU)^-1 r in fp64 (classical
+ * Gram-Schmidt applied twice; at most `restart` Arnoldi steps per outer
+ * iteration, fewer once the GMRES residual estimate falls below inner_tol
+ * times its start), which converges where classic refinement stalls
+ * (kappa(A) times the factors' relative error >= 1: fp16 / bf16 / e4m3
+ * factors of ill-conditioned matrices).  Stops when the backward error
+ * ||r||inf / (||A||inf ||x||inf + ||b||inf) <= tol or after max_outer
+ * outer iterations (LU_ERR_NOT_CONVERGED then).  *outer_iters / *inner_iters
+ * / *berr (host, may be NULL): outer iterations, Arnoldi steps in total,
+ * the final backward error.  Synchronises the stream once per Arnoldi step.
+ * Workspace: lu_gmres_ir_workspace_size (or NULL: stream-ordered). */
+#define LU_GMRES_MAX_RESTART 60
+LU_API lu_status lu_gmres_ir_workspace_size(int64_t n, int restart, size_t* bytes);
+LU_API lu_status lu_gmres_ir_c(lu_stream_t stream, int64_t n, const float* d_a, int64_t lda,
+                               const float* d_lu, int64_t ldlu, const double* d_b,
+                               double* d_x, double tol, int max_outer, int restart,
+                               double inner_tol, int* outer_iters, int* inner_iters,
+                               double* berr, void* workspace, size_t ws_bytes);
 
 /* Several right-hand sides (B, X fp64, n x nrhs) and the transposed system
  * (trans = 1: A^T X = B, backward error with ||A||_1).  All columns are
@@ -377,6 +421,35 @@ LU_API lu_status lu_gen_batch_c(lu_stream_t stream, int64_t batch, float* const*
  * (used for the 1/d of every pivot) differs from CUDA's __frcp_rn; writes
  * the count to *d_bad (device).  Expected 0. */
 LU_API lu_status lu_selfcheck_rcp_c(lu_stream_t stream, unsigned long long* d_bad);
+
+/* ---- self-tests of the bounded device waits (new) ----------------------
+ * Every cross-role or cross-CTA wait in the library's kernels is bounded;
+ * these entry points make such waits run out on purpose, by construction,
+ * so the give-up path can be tested without a fault or a hang. */
+#define LU_SELFTEST_SCRATCH_BYTES (2 << 20)
+
+/* The tensor-core update (fp16 operands, 512 x 512 x 64) with its TMA
+ * producer withheld: no loads are issued, so every consumer wait runs out
+ * after wait_cycles clock cycles.  streaming = 1 selects the epilogue that
+ * streams C in by TMA (its C loads are then in flight when the waits give
+ * up and must be drained), 0 the reduce-add epilogue.  d_scratch: device,
+ * 1024-byte aligned, LU_SELFTEST_SCRATCH_BYTES.  On completion d_out[0]
+ * (device int) holds the kernel's error code (non-zero: a wait gave up) and
+ * d_out[1] the info a factorization reports for it (-1). */
+LU_API lu_status lu_selftest_wait_update_c(lu_stream_t stream, long long wait_cycles,
+                                           int streaming, void* d_scratch, size_t bytes,
+                                           int* d_out);
+
+/* The forward solve L x = b (unit lower factor d_lu, n >= 128; x fp64 holds b
+ * on entry) with the row block solved first withholding its solution, each
+ * wait bounded by wait_ns nanoseconds: the waits for it run out, x ends with
+ * NaN, *d_expired (device) receives the number of waits that ran out.
+ * d_scratch: device, 256 + 8 n bytes rounded up to a multiple of 256
+ * (lu_refine_workspace_size(n) bytes suffice). */
+LU_API lu_status lu_selftest_wait_solve_c(lu_stream_t stream, unsigned long long wait_ns,
+                                          int64_t n, const float* d_lu, int64_t ldlu,
+                                          double* d_x, void* d_scratch, size_t bytes,
+                                          unsigned* d_expired);
 
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {

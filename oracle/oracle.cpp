@@ -52,7 +52,8 @@ inline int32_t sample_q(uint64_t seed, uint64_t i, uint64_t j, int kind) {
     s += (int64_t)((h >> 42) & 0x1fffff);
     h = mix64(h);
   }
-  return (int32_t)(s - 6ll * (1ll << 21));
+  const int32_t q = (int32_t)(s - 6ll * (1ll << 21));
+  return kind == 2 ? (q < 0 ? q : -q) : q;  // kind 2: -|kind 1|
 }
 
 // Round a finite value to a binary format with p significant bits, minimum

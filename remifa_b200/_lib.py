@@ -35,7 +35,8 @@ class LuOpts(ctypes.Structure):
         ("lookahead", ctypes.c_int32),
         ("diag_width", ctypes.c_int32),
         ("panel_fp32", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("bulk_steps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -99,6 +100,9 @@ SIGNATURES = {
                                    _int, _i64, _vp, ctypes.c_size_t]),
     "lu_gen_matrix_c": (_int, [_vp, _i64, _vp, _i64, ctypes.c_uint64, _int,
                                ctypes.c_double, _int, ctypes.c_double]),
+    "lu_equilibrate_c": (_int, [_vp, _i64, _vp, _i64, _vp, _vp, _int, ctypes.c_char_p,
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_double)]),
     "lu_solve_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _int]),
     "lu_refine_workspace_size": (_int, [_i64, ctypes.POINTER(ctypes.c_size_t)]),
     "lu_refine_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_double,
@@ -106,6 +110,11 @@ SIGNATURES = {
                            _vp, ctypes.c_size_t]),
     "lu_refine_static_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_double,
                                   _int, ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_double)]),
+    "lu_gmres_ir_workspace_size": (_int, [_i64, _int, ctypes.POINTER(ctypes.c_size_t)]),
+    "lu_gmres_ir_c": (_int, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_double,
+                             _int, _int, ctypes.c_double, ctypes.POINTER(_int),
+                             ctypes.POINTER(_int), ctypes.POINTER(ctypes.c_double), _vp,
+                             ctypes.c_size_t]),
     "lu_refine_ex_workspace_size": (_int, [_i64, _i64, ctypes.POINTER(ctypes.c_size_t)]),
     "lu_refine_ex_c": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
                               _i64, _int, ctypes.c_double, _int, ctypes.POINTER(_int),
@@ -131,6 +140,10 @@ SIGNATURES = {
     "lu_gen_batch_c": (_int, [_vp, _i64, _vp, _vp, _vp, ctypes.c_uint64, _int,
                               ctypes.c_double]),
     "lu_selfcheck_rcp_c": (_int, [_vp, _vp]),
+    "lu_selftest_wait_update_c": (_int, [_vp, ctypes.c_longlong, _int, _vp, ctypes.c_size_t,
+                                         _vp]),
+    "lu_selftest_wait_solve_c": (_int, [_vp, ctypes.c_ulonglong, _i64, _vp, _i64, _vp, _vp,
+                                        ctypes.c_size_t, _vp]),
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),

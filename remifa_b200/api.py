@@ -90,7 +90,7 @@ def _stream(stream=None):
 
 def make_opts(nb: int = 256, inner=FP32, outer=FP32, lookahead: bool = True,
               diag_width: int = 0, variant: int = _lib.RIGHT_LOOKING,
-              panel_fp32: bool = False) -> _lib.LuOpts:
+              panel_fp32: bool = False, bulk_steps: int = 0) -> _lib.LuOpts:
     o = _lib.LuOpts()
     _lib.lib().lu_opts_default(ctypes.byref(o))
     o.nb = int(nb)
@@ -100,13 +100,14 @@ def make_opts(nb: int = 256, inner=FP32, outer=FP32, lookahead: bool = True,
     o.diag_width = int(diag_width)
     o.variant = int(variant)
     o.panel_fp32 = int(bool(panel_fp32))
+    o.bulk_steps = int(bulk_steps)
     return o
 
 
 def workspace_size(n: int, nb: int = 256, inner=FP32, outer=FP32,
                    variant: int = _lib.RIGHT_LOOKING, dtype=torch.float32,
-                   lookahead: bool = True) -> int:
-    o = make_opts(nb, inner, outer, lookahead, variant=variant)
+                   lookahead: bool = True, bulk_steps: int = 0) -> int:
+    o = make_opts(nb, inner, outer, lookahead, variant=variant, bulk_steps=bulk_steps)
     sz = ctypes.c_size_t(0)
     _lib.check(_lib.lib().lu_workspace_size(ctypes.byref(o), n, n, _DTYPES[dtype],
                                             ctypes.byref(sz)), "lu_workspace_size")
@@ -114,14 +115,15 @@ def workspace_size(n: int, nb: int = 256, inner=FP32, outer=FP32,
 
 
 def _factor(fn_name: str, variant: int, a: torch.Tensor, nb: int, inner, outer,
-            a_cpy, info, lookahead, diag_width, workspace, stream, panel_fp32=False):
+            a_cpy, info, lookahead, diag_width, workspace, stream, panel_fp32=False,
+            bulk_steps=0):
     if not a.is_cuda:
         raise ValueError(f"{fn_name}: the matrix must be a CUDA tensor")
     m, n = a.shape
     lda = ld(a)
     if info is None:
         info = torch.zeros(1, dtype=torch.int32, device=a.device)
-    o = make_opts(nb, inner, outer, lookahead, diag_width, variant, panel_fp32)
+    o = make_opts(nb, inner, outer, lookahead, diag_width, variant, panel_fp32, bulk_steps)
     ws_ptr, ws_bytes = None, 0
     if workspace is not None:
         ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()
@@ -136,12 +138,17 @@ def _factor(fn_name: str, variant: int, a: torch.Tensor, nb: int, inner, outer,
 def lu_nopiv_rl(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
                 a_cpy: torch.Tensor | None = None, info: torch.Tensor | None = None,
                 lookahead: bool = True, diag_width: int = 0,
-                workspace: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+                workspace: torch.Tensor | None = None, stream=None,
+                bulk_steps: int = 0) -> torch.Tensor:
     """In-place right-looking no-pivot LU of the column-major CUDA matrix `a`
     (remifa::lu_nopiv_rl).  Returns the device info tensor (0 = success,
-    k > 0 = first bad pivot, 1-based).  Asynchronous on `stream`."""
+    k > 0 = first bad pivot, 1-based).  Asynchronous on `stream`.
+    bulk_steps: 0 / 2 lets two consecutive outer steps share one pass over
+    the bulk of the trailing matrix (fp16 / bf16 updates with look-ahead),
+    1 applies every step separately (the reference's rounding order)."""
     return _factor("lu_nopiv_rl_c", _lib.RIGHT_LOOKING, a, nb, inner, outer,
-                   a_cpy, info, lookahead, diag_width, workspace, stream)
+                   a_cpy, info, lookahead, diag_width, workspace, stream,
+                   bulk_steps=bulk_steps)
 
 
 def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=FP32,
@@ -348,15 +355,71 @@ def refine(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
     return x, it.value, be.value
 
 
+def gmres_ir(a: torch.Tensor, lu: torch.Tensor, b: torch.Tensor,
+             x: torch.Tensor | None = None, tol: float = 1e-14, max_outer: int = 20,
+             restart: int = 40, inner_tol: float = 1e-6, stream=None,
+             raise_on_stall: bool = False):
+    """GMRES-based FP64 refinement of A x = b (lu_gmres_ir_c): the
+    corrections are solved by GMRES preconditioned with the (possibly
+    low-precision) factors `lu`, which converges where classic refinement
+    stalls.  Returns (x, outer iterations, Arnoldi steps, berr)."""
+    n = _check_refine_args("gmres_ir", a, lu, b, x)
+    if x is None:
+        x = torch.empty(n, dtype=torch.float64, device=a.device)
+    it = ctypes.c_int(0)
+    inner = ctypes.c_int(0)
+    be = ctypes.c_double(0.0)
+    st = _lib.lib().lu_gmres_ir_c(_stream(stream), n, _ptr(a), ld(a), _ptr(lu), ld(lu),
+                                  _ptr(b), _ptr(x), float(tol), int(max_outer), int(restart),
+                                  float(inner_tol), ctypes.byref(it), ctypes.byref(inner),
+                                  ctypes.byref(be), None, 0)
+    if not (st == _lib.ERR_NOT_CONVERGED and not raise_on_stall):
+        _lib.check(st, "lu_gmres_ir_c")
+    return x, it.value, inner.value, be.value
+
+
+def equilibrate(a: torch.Tensor, force: bool = False, stream=None):
+    """Scale the column-major fp32 CUDA matrix `a` in place by powers of two
+    (LAPACK geequb + laqge, lu_equilibrate_c; force: scale rows and columns
+    whatever laqge decides).  Returns (r, c, equed, rowcnd, colcnd, amax): a
+    became diag(r) a diag(c)."""
+    if a.dtype != torch.float32 or not a.is_cuda or a.dim() != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("equilibrate: a must be a square float32 CUDA matrix")
+    n = a.shape[0]
+    r = torch.empty(n, dtype=torch.float32, device=a.device)
+    c = torch.empty(n, dtype=torch.float32, device=a.device)
+    eq = ctypes.create_string_buffer(1)
+    rc, cc, am = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+    st = _lib.lib().lu_equilibrate_c(_stream(stream), n, _ptr(a), ld(a), _ptr(r), _ptr(c),
+                                     int(bool(force)), eq,
+                                     ctypes.byref(rc), ctypes.byref(cc), ctypes.byref(am))
+    _lib.check(st, "lu_equilibrate_c")
+    return r, c, eq.raw.decode(), rc.value, cc.value, am.value
+
+
 def gesv_mixed(a: torch.Tensor, b: torch.Tensor, outer=TC32, nb: int = 256,
                tol: float = 1e-14, max_iter: int = 30, lookahead: bool = True,
-               stream=None):
+               stream=None, equilibrate_first: bool = False, solver: str = "classic"):
     """Solve A x = b to an fp64-level backward error: factor a copy of the
     fp32 matrix with the `outer` trailing-update precision, then refine in
-    fp64.  Returns (x, info, iterations, berr)."""
+    fp64 (solver "classic": lu_refine_c, "gmres": lu_gmres_ir_c).  With
+    equilibrate_first the copy is scaled to R A C by powers of two first
+    (geequb / laqge), the scaled system R A C y = R b is refined, and x = C y.
+    Returns (x, info, iterations, berr), berr that of the system solved."""
     lu = colmajor(a)
+    if equilibrate_first:
+        r, c, _, _, _, _ = equilibrate(lu, force=True, stream=stream)
+        a_s = colmajor(lu)
+        b_s = b * r.double()
+    else:
+        a_s, b_s = a, b
     info = lu_nopiv_rl(lu, nb=nb, outer=outer, lookahead=lookahead, stream=stream)
-    x, it, be = refine(a, lu, b, tol=tol, max_iter=max_iter, stream=stream)
+    if solver == "gmres":
+        x, it, _, be = gmres_ir(a_s, lu, b_s, tol=tol, max_outer=max_iter, stream=stream)
+    else:
+        x, it, be = refine(a_s, lu, b_s, tol=tol, max_iter=max_iter, stream=stream)
+    if equilibrate_first:
+        x = x * c.double()
     return x, info, it, be
 
 

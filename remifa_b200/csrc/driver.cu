@@ -195,7 +195,7 @@ struct DevStreams {
   cudaEvent_t copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
-  cudaEvent_t done_with[3] = {nullptr, nullptr, nullptr};  // U2 finished reading buffer b
+  cudaEvent_t done_with[4] = {nullptr, nullptr, nullptr, nullptr};  // U2 done reading buffer b
 };
 
 static lu_status dev_streams(DevStreams** out) {
@@ -224,7 +224,8 @@ static lu_status dev_streams(DevStreams** out) {
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
-                           &d.done_with[0], &d.done_with[1], &d.done_with[2], &d.copied,
+                           &d.done_with[0], &d.done_with[1], &d.done_with[2],
+                           &d.done_with[3], &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
                            &d.u1_done, &d.join_s,
                            &d.spack_done})
@@ -323,13 +324,20 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     p->ws_bytes = off;
     return LU_SUCCESS;
   }
+  // two outer steps per bulk pass (look-ahead, unscaled fp16 / bf16
+  // operands): bulk_steps 0 (default) or 2; 1 keeps one pass per step
+  p->bulk_pair = is_tc(p->outer) && !tc_scaled(tc_kind(p->outer)) && p->lookahead &&
+                 o.bulk_steps != 1;
+  if (o.bulk_steps < 0 || o.bulk_steps > 2) return LU_ERR_INVALID_ARG;
   if (is_tc(p->outer) && n > p->nb) {
     // three operand buffers: with look-ahead the panel of step k writes its
-    // copies while the bulk updates of steps k-1 and k-2 still read theirs
+    // copies while the bulk updates of steps k-1 and k-2 still read theirs;
+    // a fourth when two steps share a bulk pass (it reads step k's copies
+    // until the panels of steps k+2 and k+3 are done)
     const int64_t t = n - p->nb;
     TcWs w = tc_ws_layout(off, t, t, p->nb, tc_kind(p->outer));
     p->off_lcopy = w.off_a;
-    off += 3 * w.bytes;
+    off += (p->bulk_pair ? 4 : 3) * w.bytes;
   }
   p->ws_bytes = off;
   return LU_SUCCESS;
@@ -542,11 +550,15 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t n = p.n, nb = p.nb;
   if (col_end < 0) col_end = n;
   const bool tc = is_tc(p.outer);
-  TcWs w2[3];
+  // two steps per bulk pass: the device entry only (the host entry's
+  // catch-up applies the steps one by one)
+  const bool pair = p.bulk_pair && sink == nullptr && col_begin == 0 && col_end == n;
+  const int nbuf = p.bulk_pair ? 4 : 3;
+  TcWs w2[4];
   if (tc && n > nb) {
     w2[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
     const size_t shift = w2[0].bytes;
-    for (int b = 1; b < 3; ++b) {
+    for (int b = 1; b < nbuf; ++b) {
       w2[b] = w2[0];
       w2[b].off_a += b * shift; w2[b].off_b += b * shift; w2[b].off_sa += b * shift;
       w2[b].off_sb += b * shift; w2[b].off_tmp += b * shift;
@@ -602,6 +614,10 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   };
   bool pre = false;       // this step's first diagonal block is already queued
   bool prev_deep = false; // the previous step ran the deep schedule
+  // a step whose bulk (rows and columns beyond its trailing origin + 3 nb)
+  // waits to be applied together with the next step's bulk
+  bool deferred = false;
+  int deferred_buf = 0;
   // block column [ofs, ofs + in) is final once the panel work queued so far
   // on sp (and, with `side`, on ss) has run
   auto sink_column = [&](int64_t ofs, int64_t in, bool side) {
@@ -621,13 +637,13 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     const int64_t updm = n - ofs, updc = col_end - ofs;
     const int64_t tr = n - (ofs + nb);        // trailing rows
     const int64_t tcn = col_end - (ofs + nb); // trailing columns
-    const int buf = (int)(step % 3);
+    const int buf = (int)(step % nbuf);
     const TcWs& wk = w2[buf];
     const PackTarget pt = pack_target(p, ws, wk);
-    // this step's panel writes operand buffer `buf`: the bulk update of step
-    // k-3 must have finished reading it
-    if (tc && step >= 3 && (!ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0)) ||
-                            !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))))
+    // this step's panel writes operand buffer `buf`: the bulk update that
+    // last read it (step k - nbuf's) must have finished
+    if (tc && step >= nbuf && (!ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0)) ||
+                               !ok(cudaStreamWaitEvent(ss, S->done_with[buf], 0))))
       break;
     // the previous step's update of this block column / row ran partly on
     // the side stream: a deep step only touches the diagonal square on the
@@ -784,17 +800,53 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                               err, kU2Tiles);
       if (status != LU_SUCCESS) break;
       if (!ok(cudaEventRecord(S->updated, su))) break;
-      // U2b: the rest
+      // U2b: the rest.  Paired steps: the first of two defers all but the
+      // first block row / column of its U2b, which the second step's U2b
+      // covers exactly; that pass then applies both steps' products.
       if (tr > 2 * nb && tcn > 2 * nb) {
         const int64_t t2b = ceil_div(tr - 2 * nb, 128) * ceil_div(tcn - 2 * nb, 256);
         const bool persist = tc && tc_kind(p.outer) != TcOperand::SPLIT16 &&
                              t2b >= kU2bPersistTiles;
-        status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
-                              tcn - 2 * nb, ws, wk, err, persist ? 0 : kU2Tiles,
-                              persist ? std::max(1, sm_count() / 2) : 0);
-        if (status != LU_SUCCESS) break;
+        const int tiles = persist ? 0 : kU2Tiles;
+        const int ctas = persist ? std::max(1, sm_count() / 2) : 0;
+        // the next step will have a U2b of its own (its trailing part is
+        // one block smaller): defer to it
+        const bool defer = pair && !deferred && tr > 3 * nb && tcn > 3 * nb;
+        if (deferred) {
+          // rows / columns [2 nb, ...) of this step's trailing part = [3 nb,
+          // ...) of the deferred (previous) step's
+          const TcWs& wp = w2[deferred_buf];
+          const int64_t ldk = tc_packed_k(kind, nb);
+          const int64_t es = tc_operand_bytes(kind);
+          float* c = a + (ofs + nb + 2 * nb) + (ofs + nb + 2 * nb) * lda;
+          ProfScope ps("tc_update", su,
+                       8.0 * (tr - 2 * nb) * (tcn - 2 * nb) +
+                           2.0 * es * (tr - 2 * nb + tcn - 2 * nb) * nb,
+                       4.0 * (tr - 2 * nb) * (double)(tcn - 2 * nb) * nb);
+          status = launch_tc_update2(
+              su, kind, tr - 2 * nb, tcn - 2 * nb, nb, ws + wp.off_a + 3 * nb * ldk * es,
+              ws + wp.off_b + 3 * nb * ldk * es, nb, ws + wk.off_a + 2 * nb * ldk * es,
+              ws + wk.off_b + 2 * nb * ldk * es, ldk, c, lda, err, ctas, tiles);
+          if (status != LU_SUCCESS) break;
+          if (!ok(cudaEventRecord(S->done_with[deferred_buf], su))) break;
+          deferred = false;
+        } else if (defer) {
+          status = outer_update(p, su, a, lda, ofs, 2 * nb, nb, 2 * nb, tcn - 2 * nb, ws, wk,
+                                err, kU2Tiles);
+          if (status == LU_SUCCESS)
+            status = outer_update(p, su, a, lda, ofs, 3 * nb, tr - 3 * nb, 2 * nb, nb, ws,
+                                  wk, err, kU2Tiles);
+          if (status != LU_SUCCESS) break;
+          deferred = true;
+          deferred_buf = buf;
+        } else {
+          status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
+                                tcn - 2 * nb, ws, wk, err, tiles, ctas);
+          if (status != LU_SUCCESS) break;
+        }
       }
-      if (!ok(cudaEventRecord(S->done_with[buf], su))) break;
+      if (!(deferred && deferred_buf == buf) && !ok(cudaEventRecord(S->done_with[buf], su)))
+        break;
     } else if (tr > 0 && tcn > 0) {
       cudaStream_t last = prev_deep ? ss : sp;
       if (!ok(cudaEventRecord(S->updated, last))) break;

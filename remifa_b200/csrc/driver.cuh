@@ -20,6 +20,7 @@ struct Plan {
   bool lookahead = true;
   lu_dtype dtype = LU_F32;
   bool panel_fp32 = false;  // fp16 storage: block update kept in fp32
+  bool bulk_pair = false;   // two outer steps per bulk trailing-update pass
   // workspace layout (byte offsets into one device allocation)
   size_t off_status = 0;    // int first_bad
   size_t off_lcopy = 0;     // low-precision L21 copy (row-major)

@@ -84,7 +84,10 @@ struct TcParams {
   float* C;
   int64_t ldc;
   int M, N, K;
-  int kb_count;        // number of BK blocks along K
+  int kb_count;        // number of BK blocks along K (both operand sets)
+  int kb_split;        // blocks [0, kb_split) come from (tmap_a, tmap_b), the
+                       // rest from (tmap_a2, tmap_b2): two outer steps' K = nb
+                       // products summed in one accumulator
   int tiles_m, tiles_n;
   const int* scale_a;  // per 128-row tile of A (log2), or null
   const int* scale_b;  // per 128-column tile of B (log2), or null
@@ -92,6 +95,9 @@ struct TcParams {
   int* err;
   int tiles_per_cta;   // 0: persistent (tile = blockIdx.x, += gridDim.x);
                        // > 0: CTA b owns the consecutive tiles [b*T, b*T+T)
+  long long wait_cycles;  // bound of each barrier wait (kWaitCycles)
+  int withhold;        // self-test of the give-up path only: the producer
+                       // issues no loads, so every consumer wait runs out
 };
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
@@ -102,6 +108,8 @@ template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
                  const __grid_constant__ CUtensorMap tmap_b,
+                 const __grid_constant__ CUtensorMap tmap_a2,
+                 const __grid_constant__ CUtensorMap tmap_b2,
                  const __grid_constant__ CUtensorMap tmap_c, TcParams p,
                  uint32_t idesc) {
   constexpr int kStages = Cfg<EPI>::kStages;
@@ -116,7 +124,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
   uint64_t* tfull = empty + kStages;
   uint64_t* tempty = tfull + 2;
   uint64_t* cfull = tempty + 2;  // EPI 3: four per epilogue warp
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cfull + 4 * kEpiWarps);
+  uint64_t* drain = cfull + 4 * kEpiWarps;  // MMA completion after a give-up
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
 
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
@@ -135,6 +144,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       mbar_init(&tempty[a], kEpiWarps);
     }
     for (int w = 0; w < 4 * kEpiWarps; ++w) mbar_init(&cfull[w], 1);
+    mbar_init(drain, 1);
     fence_barrier_init();
   }
   if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
@@ -148,19 +158,41 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
     if (lane == 0) {
       prefetch_tmap(&tmap_a);
       prefetch_tmap(&tmap_b);
+      if (p.kb_split < p.kb_count) {
+        prefetch_tmap(&tmap_a2);
+        prefetch_tmap(&tmap_b2);
+      }
       int s = 0;
       uint32_t ph = 0;
-      bool ok = true;
+      bool ok = !p.withhold;
+      int armed = 0;
       for (int tile = t_begin; tile < t_end && ok; tile += t_step) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         for (int kb = 0; kb < p.kb_count; ++kb) {
-          if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty)) { ok = false; break; }
+          if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
+            ok = false;
+            break;
+          }
           mbar_arrive_expect_tx(&full[s], kStageA + kStageB);
-          const int kx = kb * kRowBytes;  // element offset along K == bytes for 8-bit
-          const int kelem = KIND == 0 ? kb * (kRowBytes / 2) : kx;
-          tma_load_2d(sA + s * kStageA, &tmap_a, &full[s], kelem, tm * BM);
-          tma_load_2d(sB + s * kStageB, &tmap_b, &full[s], kelem, tn * BN);
+          const bool second = kb >= p.kb_split;
+          const int kk = second ? kb - p.kb_split : kb;
+          const int kx = kk * kRowBytes;  // element offset along K == bytes for 8-bit
+          const int kelem = KIND == 0 ? kk * (kRowBytes / 2) : kx;
+          tma_load_2d(sA + s * kStageA, second ? &tmap_a2 : &tmap_a, &full[s], kelem, tm * BM);
+          tma_load_2d(sB + s * kStageB, second ? &tmap_b2 : &tmap_b, &full[s], kelem, tn * BN);
+          ++armed;
           if (++s == kStages) { s = 0; ph ^= 1; }
+        }
+      }
+      if (!ok) {
+        // a consumer may have given up before these loads landed: wait for
+        // the last kStages armed stages (older ones were consumed) so no
+        // copy into this CTA's shared memory outlives it
+        int ss = s;
+        uint32_t pp = ph;
+        for (int j = 0; j < kStages && j < armed; ++j) {
+          if (ss == 0) { ss = kStages - 1; pp ^= 1; } else { --ss; }
+          mbar_drain(&full[ss], pp);
         }
       }
     }
@@ -171,14 +203,22 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       uint32_t ph = 0;
       int local = 0;
       bool ok = true;
+      bool issued = false;
       for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
-        if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty)) { ok = false; break; }
+        if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty, p.wait_cycles)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + acc * BN;
         for (int kb = 0; kb < p.kb_count; ++kb) {
-          if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull)) { ok = false; break; }
+          if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull, p.wait_cycles)) {
+            ok = false;
+            break;
+          }
+          issued = true;
           tc_fence_after();
           const uint32_t a0 = smem_u32(sA + s * kStageA);
           const uint32_t b0 = smem_u32(sB + s * kStageB);
@@ -194,6 +234,12 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
           if (++s == kStages) { s = 0; ph ^= 1; }
         }
         if (ok) mma_commit(&tfull[acc]);
+      }
+      if (!ok && issued) {
+        // MMAs still running read shared memory and write TMEM: wait for
+        // all of them before the accumulator is freed
+        mma_commit(drain);
+        mbar_drain(drain, 0);
       }
     }
   } else {
@@ -214,7 +260,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       // HBM this way runs faster than reductions performed in L2.
       float* cst = reinterpret_cast<float*>(sEpi + (size_t)ew * 4 * kEpiChunk);
       uint64_t* cb = cfull + ew * 4;
-      uint32_t cph = 0;  // bit c: phase of buffer c
+      uint32_t cph = 0;   // bit c: phase of buffer c
+      uint32_t pend = 0;  // bit c: a load into buffer c not yet waited for
       auto valid = [&](int tile, int c) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         return tm * BM + quarter * 32 < p.M && tn * BN + half * 128 + c * 32 < p.N;
@@ -225,9 +272,12 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         tma_load_2d(cst + c * (kEpiChunk / 4), &tmap_c, &cb[c], tm * BM + quarter * 32,
                     tn * BN + half * 128 + c * 32);
       };
-      if (lane == 0 && t_begin < t_end)
+      if (t_begin < t_end)
         for (int c = 0; c < 4; ++c)
-          if (valid(t_begin, c)) load(t_begin, c);
+          if (valid(t_begin, c)) {
+            if (lane == 0) load(t_begin, c);
+            pend |= 1u << c;
+          }
       for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int acc = local & 1;
@@ -237,7 +287,10 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         const int next = tile + t_step;
         float sa = 1.0f;
         if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
-        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
+        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
@@ -254,8 +307,12 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
             if (lane == 0) mbar_arrive(&tempty[acc]);
           }
           if (v) {
-            if (!mbar_wait(&cb[c], (cph >> c) & 1u, p.err, kErrTimeoutFull)) { ok = false; break; }
+            if (!mbar_wait(&cb[c], (cph >> c) & 1u, p.err, kErrTimeoutFull, p.wait_cycles)) {
+              ok = false;
+              break;
+            }
             cph ^= 1u << c;
+            pend &= ~(1u << c);
             float sc = p.alpha * sa;
             if (p.scale_b) sc = ldexpf(sc, -p.scale_b[cc / 128]);
             float* box = cst + c * (kEpiChunk / 4);
@@ -270,15 +327,22 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
             }
           }
           // buffer c, once read out by the store, takes chunk c of the next tile
-          if (lane == 0 && next < t_end && valid(next, c)) {
-            if (v) bulk_wait_group_read<0>();
-            load(next, c);
+          if (next < t_end && valid(next, c)) {
+            if (lane == 0) {
+              if (v) bulk_wait_group_read<0>();
+              load(next, c);
+            }
+            pend |= 1u << c;
           }
         }
       }
-      // every load was issued for a tile of this loop and waited for in it
-      // (only a bounded wait that gave up can leave one behind)
-      if (lane == 0) bulk_wait_group<0>();
+      // every load was issued for a tile of this loop and waited for in it,
+      // unless a bounded wait gave up: then wait for the loads still in flight
+      if (lane == 0) {
+        for (int c = 0; c < 4; ++c)
+          if (pend & (1u << c)) mbar_drain(&cb[c], (cph >> c) & 1u);
+        bulk_wait_group<0>();
+      }
       __syncwarp();
     } else if constexpr (EPI == 1) {
       float* stage = reinterpret_cast<float*>(sEpi + (size_t)ew * 2 * kEpiChunk);
@@ -290,7 +354,10 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         const int col0 = tn * BN + half * 128;
         float sa = 1.0f;
         if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
-        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
+        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
@@ -345,7 +412,10 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
 #pragma unroll
         for (int j = 0; j < 32; ++j)
           cv[j] = (row_ok && col0 + j < p.N) ? to_f32(cbase[j * ldc]) : 0.0f;
-        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull)) { ok = false; break; }
+        if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
@@ -446,7 +516,10 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                          int64_t K, float alpha, const void* A, int64_t lda_p,
                          const void* B, int64_t ldb_p, void* C, bool c_half,
                          int64_t ldc, const int* scale_a, const int* scale_b,
-                         int* err, int max_ctas, int tiles_per_cta) {
+                         int* err, int max_ctas, int tiles_per_cta,
+                         long long wait_cycles = 0, int withhold = 0,
+                         const void* A2 = nullptr, const void* B2 = nullptr,
+                         int64_t K2 = 0) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
   if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
   const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
@@ -458,9 +531,20 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                          : kind == TcOperand::E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-  CUtensorMap ma, mb;
+  CUtensorMap ma, mb, ma2, mb2;
   if (!make_kmajor_map(&ma, A, dt, esize, K, M, lda_p, BM)) return LU_ERR_CUDA;
   if (!make_kmajor_map(&mb, B, dt, esize, K, N, ldb_p, BN)) return LU_ERR_CUDA;
+  if (K2 > 0) {
+    // the second operand set: same kind and leading dimensions, its own K
+    if (scale_a || scale_b || !A2 || !B2 || (uintptr_t)A2 % 16 != 0 ||
+        (uintptr_t)B2 % 16 != 0 || lda_p < K2 || ldb_p < K2 || K2 > INT32_MAX)
+      return LU_ERR_INVALID_ARG;
+    if (!make_kmajor_map(&ma2, A2, dt, esize, K2, M, lda_p, BM)) return LU_ERR_CUDA;
+    if (!make_kmajor_map(&mb2, B2, dt, esize, K2, N, ldb_p, BN)) return LU_ERR_CUDA;
+  } else {
+    ma2 = ma;
+    mb2 = mb;
+  }
 
   TcParams p;
   p.C = static_cast<float*>(C);
@@ -468,7 +552,8 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   p.M = (int)M;
   p.N = (int)N;
   p.K = (int)K;
-  p.kb_count = (int)ceil_div(K * esize, kRowBytes);
+  p.kb_split = (int)ceil_div(K * esize, kRowBytes);
+  p.kb_count = p.kb_split + (K2 > 0 ? (int)ceil_div(K2 * esize, kRowBytes) : 0);
   p.tiles_m = (int)ceil_div(M, BM);
   p.tiles_n = (int)ceil_div(N, BN);
   p.scale_a = scale_a;
@@ -476,6 +561,8 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   p.alpha = alpha;
   p.err = err;
   p.tiles_per_cta = tiles_per_cta;
+  p.wait_cycles = wait_cycles > 0 ? wait_cycles : sm100::kWaitCycles;
+  p.withhold = withhold ? 1 : 0;
   const int tiles = p.tiles_m * p.tiles_n;
   const int grid = tiles_per_cta > 0
                        ? (int)ceil_div(tiles, tiles_per_cta)
@@ -496,28 +583,28 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   if (c_half) {
     if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
     LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 2>, smem_bytes<2>()));
-    tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(ma, mb, mc, p, idesc);
+    tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
   } else if (kind == TcOperand::E4M3) {
     if (tma_c && !stream_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 1>, smem_bytes<1>()));
-      tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     } else if (tma_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 3>, smem_bytes<3>()));
-      tc_update_kernel<1, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<1, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     } else {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 0>, smem_bytes<0>()));
-      tc_update_kernel<1, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<1, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     }
   } else {
     if (tma_c && !stream_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 1>, smem_bytes<1>()));
-      tc_update_kernel<0, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<0, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     } else if (tma_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 3>, smem_bytes<3>()));
-      tc_update_kernel<0, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<0, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     } else {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 0>, smem_bytes<0>()));
-      tc_update_kernel<0, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, mc, p, idesc);
+      tc_update_kernel<0, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
     }
   }
   LUB_LAUNCH_CHECK();
@@ -534,12 +621,30 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
                         scale_a, scale_b, err, max_ctas, tiles_per_cta);
 }
 
+lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                            int64_t K, const void* A, const void* B, int64_t K2,
+                            const void* A2, const void* B2, int64_t ld_p, float* C,
+                            int64_t ldc, int* err, int max_ctas, int tiles_per_cta) {
+  if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+  return tc_update_impl(st, kind, M, N, K, -1.0f, A, ld_p, B, ld_p, C, false, ldc, nullptr,
+                        nullptr, err, max_ctas, tiles_per_cta, 0, 0, A2, B2, K2);
+}
+
 lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                              int64_t K, float alpha, const void* A, int64_t lda_p,
                              const void* B, int64_t ldb_p, __half* C, int64_t ldc,
                              int* err) {
   return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, true, ldc,
                         nullptr, nullptr, err, 0, 0);
+}
+
+lu_status launch_tc_update_withheld(cudaStream_t st, int64_t M, int64_t N, int64_t K,
+                                    const void* A, int64_t lda_p, const void* B,
+                                    int64_t ldb_p, float* C, int64_t ldc, int* err,
+                                    long long wait_cycles, int tiles_per_cta) {
+  if (wait_cycles <= 0) return LU_ERR_INVALID_ARG;
+  return tc_update_impl(st, TcOperand::F16, M, N, K, -1.0f, A, lda_p, B, ldb_p, C, false,
+                        ldc, nullptr, nullptr, err, 0, tiles_per_cta, wait_cycles, 1);
 }
 
 }  // namespace lub

@@ -10,6 +10,9 @@
 // kind 0: r_ij = q * 2^-23, q uniform in [-2^23, 2^23)      (U[-1,1))
 // kind 1: r_ij = q * 2^-21 / sqrt(n), q = sum of twelve 21-bit uniforms,
 //         centred (Irwin-Hall, ~N(0,1)/sqrt(n))
+// kind 2: r_ij = -|kind 1| (every off-diagonal entry negative: with the
+//         dominant diagonal an M-matrix, A 1 = (alpha - 1) diag(A) 1 / alpha,
+//         so kappa_2(A) ~ 1 / (alpha - 1): the dominance sets the condition)
 // a_ij = r_ij for i != j;  a_ii = alpha * sum_{j != i} |r_ij| (exact integer
 // row sum, then two fp64 multiplies rounded once to fp32); all entries
 // times 2^kscale; row i times 2^-round(gamma_bits * i / (n - 1)).
@@ -39,7 +42,8 @@ __device__ __forceinline__ int32_t sample_q(uint64_t seedmix, uint64_t i,
     s += (int64_t)((h >> 42) & 0x1fffff);
     h = mix64(h);
   }
-  return (int32_t)(s - 6ll * (1ll << 21));
+  const int32_t q = (int32_t)(s - 6ll * (1ll << 21));
+  return kind == 2 ? (q < 0 ? q : -q) : q;
 }
 
 __device__ __forceinline__ int row_shift(double gamma_bits, int64_t i, int64_t n) {
@@ -116,7 +120,7 @@ uint64_t host_mix64(uint64_t z) {
 lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
                             uint64_t seed, int kind, double alpha, int kscale,
                             double gamma_bits) {
-  if (n < 0 || lda < std::max<int64_t>(1, n) || (kind != 0 && kind != 1))
+  if (n < 0 || lda < std::max<int64_t>(1, n) || (kind < 0 || kind > 2))
     return LU_ERR_INVALID_ARG;
   if (n == 0) return LU_SUCCESS;
   if (a == nullptr) return LU_ERR_INVALID_ARG;
@@ -149,7 +153,7 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
 lu_status launch_gen_batch(cudaStream_t st, int64_t batch, float* const* ptrs,
                            const int32_t* ns, const int32_t* ldas, uint64_t seed,
                            int kind, double alpha) {
-  if (batch < 0 || (kind != 0 && kind != 1) || batch > INT32_MAX) return LU_ERR_INVALID_ARG;
+  if (batch < 0 || (kind < 0 || kind > 2) || batch > INT32_MAX) return LU_ERR_INVALID_ARG;
   if (batch == 0) return LU_SUCCESS;
   if (!ptrs || !ns) return LU_ERR_INVALID_ARG;
   gen_batch_kernel<<<(unsigned)batch, 256, 0, st>>>(ptrs, ns, ldas, seed, kind, alpha);

@@ -50,19 +50,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity.  On timeout sets *err
-// (first error wins) and returns false.
+// (first error wins) and returns false; also returns false at once when
+// another role has set *err.  `limit` (cycles) is kWaitCycles except in the
+// library's self-test of the give-up path.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
-                                          int* err, int code) {
+                                          int* err, int code,
+                                          long long limit = kWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       if (err) atomicCAS(err, 0, code);
       return false;
     }
     if (err && *((volatile int*)err) != 0) return false;  // another role gave up
   }
+}
+
+// Bounded wait used while unwinding after a give-up: for copies or MMAs
+// this thread issued itself, which complete on their own; returns whether
+// the phase completed within kWaitCycles (no error recorded).
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
 }
 
 // 2-D TMA tile load global -> shared, completion counted on `bar` (bytes).

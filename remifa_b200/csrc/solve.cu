@@ -54,6 +54,9 @@ struct Args {
   int unit;         // unit diagonal: L or L^T
   int xvec;         // X 16-byte aligned with even ldx (group kernel: cp.async)
   unsigned* sync;
+  unsigned long long wait_ns;  // bound of one wait (kWaitNs)
+  int withhold;     // self-test of the give-up path only: the row block solved
+                    // first (ticket 0) does not publish its solution, -1: none
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -355,7 +358,7 @@ __device__ __forceinline__ void settle_x(double (&x)[NX][NR], const Args& a, int
           ok &= !pending(x[h][c]);
         }
     if (__all_sync(0xffffffffu, ok)) return;
-    const bool expired = global_ns() - t0 > kWaitNs;
+    const bool expired = global_ns() - t0 > a.wait_ns;
     if (__any_sync(0xffffffffu, expired || *(volatile unsigned*)(a.sync + 1) != 0u)) {
 #pragma unroll
       for (int h = 0; h < NX; ++h)
@@ -582,7 +585,7 @@ trsv_kernel(Args a) {
     }
   }
   const int ri = 8 * warp + (lane >> 2);
-  if ((lane & 3) == 0 && ri < rw) {
+  if ((lane & 3) == 0 && ri < rw && ticket != a.withhold) {
 #pragma unroll
     for (int c = 0; c < NR; ++c)
       if (c < nc) st_publish(a.X + (r0 + ri) + (c0 + c) * a.ldx, cv[c]);
@@ -741,7 +744,7 @@ trsv_group_kernel(Args a) {
             v = ld_acquire(done);
             if ((int)v > q) break;
             if (*(volatile unsigned*)abort_word) { ctrl[3] = 1; break; }
-            if (global_ns() - t0 > kWaitNs) {
+            if (global_ns() - t0 > a.wait_ns) {
               atomicExch(abort_word, 1u);
               atomicAdd(a.sync + 2, 1u);
               ctrl[3] = 1;
@@ -1086,7 +1089,8 @@ size_t trsm_ws_bytes(int64_t n, int64_t nrhs) {
 
 lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                       double* X, int64_t ldx, int64_t nrhs, bool upper,
-                      bool trans, unsigned* sync, double* B) {
+                      bool trans, unsigned* sync, double* B,
+                      unsigned long long wait_ns, int withhold) {
   if (n <= 0 || nrhs <= 0) return LU_SUCCESS;
   if (!sync || !B) return LU_ERR_INVALID_ARG;
   const int nr = trsv::group_width(nrhs);
@@ -1106,6 +1110,8 @@ lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
   a.unit = !upper;
   a.xvec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && (ldx % 2 == 0);
   a.sync = sync;
+  a.wait_ns = wait_ns > 0 ? wait_ns : trsv::kWaitNs;
+  a.withhold = withhold;
   if (nr <= 2) {
     const int64_t elems = n * nrhs;
     trsv::trsv_prepare_kernel<<<(unsigned)ceil_div(elems, 256), 256, 0, st>>>(n, nrhs, X, ldx,

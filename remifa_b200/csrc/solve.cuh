@@ -13,9 +13,13 @@ namespace lub {
 // shared with a solve in flight on another stream.  trsm_ws_bytes = both.
 size_t trsm_sync_bytes(int64_t nrhs);
 size_t trsm_ws_bytes(int64_t n, int64_t nrhs);
+// wait_ns / withhold: the self-test of the give-up path only (a bound of
+// wait_ns per wait instead of 4 s; the block solved first does not publish,
+// so the waits for it run out and the solve ends with NaN).
 lu_status launch_trsm(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                       double* X, int64_t ldx, int64_t nrhs, bool upper,
-                      bool trans, unsigned* sync, double* B);
+                      bool trans, unsigned* sync, double* B,
+                      unsigned long long wait_ns = 0, int withhold = -1);
 // X <- (L U)^-1 X (trans: (L U)^-T X): two launch_trsm.
 lu_status launch_lu_solve(cudaStream_t st, int64_t n, const float* lu, int64_t ld,
                           double* X, int64_t ldx, int64_t nrhs, bool trans, unsigned* sync,

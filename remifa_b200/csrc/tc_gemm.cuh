@@ -36,12 +36,31 @@ lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
                            int64_t ldc, const int* scale_a, const int* scale_b,
                            int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
+// C -= A B + A2 B2 in one pass over C: two K-major operand sets (unscaled
+// fp16 or bf16, the same leading dimension ld_p, K and K2 columns) summed
+// in one fp32 accumulator, so C is read and written once for two outer
+// steps' updates (c - (acc1 + acc2), one rounding).
+lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                            int64_t K, const void* A, const void* B, int64_t K2,
+                            const void* A2, const void* B2, int64_t ld_p, float* C,
+                            int64_t ldc, int* err, int max_ctas = 0, int tiles_per_cta = 0);
+
 // The same update with C stored in fp16 (C = rn16(C + alpha * acc), the sum
 // in fp32): the left-looking factorization of an fp16 matrix.
 lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                              int64_t K, float alpha, const void* A, int64_t lda_p,
                              const void* B, int64_t ldb_p, __half* C, int64_t ldc,
                              int* err);
+
+// Self-test of the give-up path: the same fp16 update with the TMA producer
+// issuing no loads and every barrier wait bounded by wait_cycles, so each
+// consumer wait runs out; the kernel records its code in *err, unwinds,
+// frees its TMEM and returns (tiles_per_cta > 2 selects the streaming-C
+// epilogue, otherwise the reduce-add one).
+lu_status launch_tc_update_withheld(cudaStream_t st, int64_t M, int64_t N, int64_t K,
+                                    const void* A, int64_t lda_p, const void* B,
+                                    int64_t ldb_p, float* C, int64_t ldc, int* err,
+                                    long long wait_cycles, int tiles_per_cta);
 
 // Largest power-of-two scale per 128-row tile of the fp32 column-major
 // src (M x K) / per 128-column tile of src (K x N) such that amax * 2^s <=

@@ -348,7 +348,8 @@ def test_host_entry_matches_device_entry(built, n, nb, outer, la, pad):
     compute) gives exactly the device entry point's factors."""
     a = O.gen_matrix(n, seed=n + 3, kind=1, alpha=1.5)
     d = rb.colmajor(torch.from_numpy(a).cuda(), lda=n + pad)
-    rb.lu_nopiv_rl(d, nb=nb, outer=outer, lookahead=la)
+    # the host entry applies the outer steps one by one (no two-step bulk pass)
+    rb.lu_nopiv_rl(d, nb=nb, outer=outer, lookahead=la, bulk_steps=1)
     h = torch.empty((n, n + pad), dtype=torch.float32, pin_memory=True).t()[:n, :]
     h.copy_(torch.from_numpy(a))
     work = rb.colmajor_empty(n, n, n + 2 * pad, torch.float32)

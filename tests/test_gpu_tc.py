@@ -254,9 +254,34 @@ def test_lookahead_is_bit_identical(built, compute, n, nb):
     a = O.gen_matrix(n, seed=3, kind=1, alpha=1.5)
     d1, d2 = to_dev(a), to_dev(a)
     rb.lu_nopiv_rl(d1, nb=nb, outer=compute, lookahead=False)
-    rb.lu_nopiv_rl(d2, nb=nb, outer=compute, lookahead=True)
+    rb.lu_nopiv_rl(d2, nb=nb, outer=compute, lookahead=True, bulk_steps=1)
     torch.cuda.synchronize()
     assert torch.equal(d1, d2)
+
+
+@pytest.mark.parametrize("compute,fmt", [(rb.TC32, O.FMT_FP16),
+                                         (rb.compute_type.TC32_BF16, O.FMT_BF16)])
+@pytest.mark.parametrize("n,nb", [(2048, 256), (1800, 128), (3000, 256)])
+def test_two_step_bulk_pass(built, compute, fmt, n, nb):
+    """bulk_steps 2 (the default under look-ahead): two outer steps' updates
+    of the bulk of the trailing matrix in one pass, C - (L_k U_k + L_k+1
+    U_k+1) with one fp32 accumulator.  Only that rounding differs from the
+    step-by-step order: within 64 n u32 of it and of the oracle, same
+    ||A - LU|| up to 2x."""
+    a = O.gen_matrix(n, seed=n + 11, kind=1, alpha=1.5)
+    d1, d2 = to_dev(a), to_dev(a)
+    rb.lu_nopiv_rl(d1, nb=nb, outer=compute, bulk_steps=1)
+    info = rb.lu_nopiv_rl(d2, nb=nb, outer=compute, bulk_steps=2)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    one, two = to_host(d1), to_host(d2)
+    assert not np.array_equal(one, two)  # the paired passes ran
+    want = O.lu_rl(a, nb=nb, outer_fmt=fmt)
+    scale = np.abs(want).max()
+    assert np.abs(two - one).max() / scale < 64 * n * U32
+    assert np.abs(two - want).max() / scale < 64 * n * U32
+    fe2, feo = O.factor_error(a, two), O.factor_error(a, want)
+    assert fe2 <= 2 * feo + 1e-7 and feo <= 2 * fe2 + 1e-7
 
 
 @pytest.mark.parametrize("compute", [rb.TC32, rb.TC16, rb.FP16])

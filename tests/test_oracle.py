@@ -336,3 +336,16 @@ def test_lu_ll_wide_blocks_against_fp64(n, nb):
     flat = O.lu_ll(a, nb=nb, sub=nb)  # the reference's loop over the whole block
     assert np.abs(lu - flat).max() <= 8 * n * U32 * np.abs(lu).max()
     assert not np.array_equal(lu, flat) or nb <= 128
+
+
+def test_generator_kind2_condition_family():
+    """kind 2 (every off-diagonal entry -|r_ij|, diagonal alpha * row sum):
+    an M-matrix whose 2-norm condition is ~1.06 / (alpha - 1) at any n."""
+    for n in (256, 512):
+        for am1 in (1e-2, 1e-4):
+            a = O.gen_matrix(n, seed=7, kind=2, alpha=1.0 + am1)
+            A = np.array(a, dtype=np.float64)
+            off = A[~np.eye(n, dtype=bool)]
+            assert (off <= 0).all()
+            k2 = np.linalg.cond(A, 2)
+            assert 0.8 / am1 < k2 < 1.3 / am1, (n, am1, k2)

@@ -342,6 +342,51 @@ def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2, solve
     return best
 
 
+def isolated_update_roofline(rb, torch, outer, n, nb, la, peaks, reps=3) -> dict:
+    """The dominant kernel alone: the factorization's largest trailing-update
+    launch shape (the first bulk pass: M = N = n - 4 nb with K = 2 nb when two
+    outer steps share a pass, else n - 3 nb with K = nb), run through the
+    library's update entry on one stream with nothing concurrent; the
+    tensor-core launch is timed with CUDA events on its stream (the operand
+    packing, a separate launch, is not counted)."""
+    paired = la and outer in (rb.TC32, rb.compute_type.TC32_BF16)
+    m = n - (4 if paired else 3) * nb
+    k = (2 if paired else 1) * nb
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    a = rb.colmajor(torch.randn(m, k, device="cuda", generator=g))
+    b = rb.colmajor(torch.randn(k, m, device="cuda", generator=g))
+    c = rb.colmajor(torch.randn(m, m, device="cuda", generator=g))
+    rb.gemmex(outer, -1.0, a, b, 1.0, c)  # warm-up
+    torch.cuda.synchronize()
+    with rb.profile() as pr:
+        for _ in range(reps):
+            rb.gemmex(outer, -1.0, a, b, 1.0, c)
+        torch.cuda.synchronize()
+    e = pr.entries["tc_update"]
+    sec = e["total_ms"] / 1e3
+    gbs = e["bytes"] / sec / 1e9
+    tfs = e["flops"] / sec / 1e12
+    alg = e["bytes"] / e["launches"]
+    tr = profiled_traffic("tc_update_update_m8192_k512")
+    del a, b, c
+    torch.cuda.empty_cache()
+    return {"kernel": "tc_update_kernel (persistent CTAs, C streamed by TMA, all SMs)",
+            "shape": {"M": m, "N": m, "K": k}, "bound": "hbm", "achieved": gbs,
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+            "peak_source": peaks["source"] + " hbm_gbs (copy, burst)",
+            "tensor_tflops": tfs, "tensor_peak": peaks["bf16_tflops"],
+            "tensor_frac": tfs / peaks["bf16_tflops"],
+            "algorithmic_bytes_per_launch": alg,
+            "avg_launch_ms": e["total_ms"] / e["launches"], "launches": e["launches"],
+            "traffic": tr["traffic_over_algorithmic"] * alg if tr else None,
+            "traffic_source": ("ncu dram bytes / algorithmic bytes of the same kernel at "
+                               "M = 8192, K = 512 (profiles/tc_update_update_m8192_k512.json),"
+                               " times this launch's algorithmic bytes") if tr else None,
+            "timing": "CUDA events on the launching stream, the launch alone, "
+                      f"mean of {reps}"}
+
+
 def config_of(args, wl) -> dict:
     return {"workload": args.workload, "n": wl["n"], "nb": getattr(args, "nb", None) or wl["nb"],
             "lookahead": not getattr(args, "no_lookahead", False),
@@ -505,25 +550,22 @@ def main() -> None:
     if ent.get("launches"):
         avg_ms = ent["total_ms"] / ent["launches"]
         if dom == "tc_update":
-            achieved = ent["bytes"] / (ent["total_ms"] / 1e3) / 1e9
-            peak = peaks["hbm_gbs"]
-            tr = profiled_traffic(f"tc_update_{args.workload}")
-            alg = ent["bytes"] / ent["launches"]
-            # DRAM traffic of one captured launch over its algorithmic bytes,
-            # applied to the average launch (traffic grows with the C term)
-            traffic = tr["traffic_over_algorithmic"] * alg if tr else None
-            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved,
-                        "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peaks["source"] + " hbm_gbs",
-                        "traffic": traffic,
-                        "traffic_source": ("ncu dram bytes of one launch "
-                                           f"(profiles/tc_update_{args.workload}.json) "
-                                           "scaled to the average launch") if tr else None,
-                        "algorithmic_bytes_per_launch": alg,
-                        "avg_launch_ms": avg_ms, "launches": ent["launches"],
-                        "event_time_over_wall": ent["total_ms"] / ms_prof,
-                        "timing": "per-launch CUDA events from a second, profiled pass "
-                                  "of the same steps"}
+            roofline = isolated_update_roofline(rb, torch, outer, n, nb, la, peaks)
+            # inside the factorization (three concurrent streams, so per-launch
+            # event times overlap): the update's algorithmic bytes per step
+            # over the whole step's time -- a floor of its achieved rate
+            per_step = ent["bytes"] / args.steps
+            roofline["in_factorization"] = {
+                "bytes_per_step": per_step, "flops_per_step": ent["flops"] / args.steps,
+                "launches_per_step": ent["launches"] / args.steps,
+                "rate_over_step_time_gbs": per_step / (ms / args.steps / 1e3) / 1e9,
+                "frac_of_peak": per_step / (ms / args.steps / 1e3) / 1e9 / peaks["hbm_gbs"],
+                "tensor_tflops_over_step_time":
+                    ent["flops"] / args.steps / (ms / args.steps / 1e3) / 1e12,
+                "avg_launch_event_ms": avg_ms,
+                "event_time_over_wall": ent["total_ms"] / ms_prof,
+                "note": "per-launch CUDA events from a second, profiled pass; launches on "
+                        "the three streams overlap, so only the per-step ratio is a rate"}
         else:
             achieved = ent["flops"] / (ent["total_ms"] / 1e3) / 1e12
             roofline = {"kernel": dom, "bound": "fp32-simt", "achieved": achieved,

@@ -64,6 +64,7 @@ def lib():
         L.orc_convert.argtypes = [_i64, _i64, _f32p, _i64, _f32p, _i64,
                                   ctypes.c_int, ctypes.c_int]
         L.orc_panel_f32.argtypes = [_i64, _i64, _f32p, _i64, _f32p, _i64, _f32p, _i64]
+        L.orc_panel_f16.argtypes = [_i64, _i64, _f32p, _i64, _f32p, _i64, _f32p, _i64]
         L.orc_gemm_sub_f32.argtypes = [_i64, _i64, _i64, _f32p, _i64, _f32p,
                                        _i64, _f32p, _i64]
         L.orc_lu_rl_f32.argtypes = [_i64, _i64, _i64, _f32p, _i64, ctypes.c_int,
@@ -161,6 +162,12 @@ def round_fmt(a: np.ndarray, fmt: int, scale_log2: int = 0) -> np.ndarray:
 def panel(m: int, n: int, d: np.ndarray, a: np.ndarray) -> None:
     """In place on the block column a (m x >=m for the U part)."""
     lib().orc_panel_f32(m, n, _p32(d), ld(d), _p32(a), ld(a), _p32(a), ld(a))
+
+
+def panel_f16(m: int, n: int, d: np.ndarray, a: np.ndarray) -> None:
+    """lu_nopiv_panel<half,8> restated: in place on the block column a
+    (float32 holding fp16 values)."""
+    lib().orc_panel_f16(m, n, _p32(d), ld(d), _p32(a), ld(a), _p32(a), ld(a))
 
 
 def gemm_sub(a: np.ndarray, b: np.ndarray, c: np.ndarray) -> None:

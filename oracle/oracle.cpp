@@ -228,6 +228,48 @@ void orc_panel_f32(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
   }
 }
 
+// reference src/lu_nopiv.cu:105-326 instantiated for half (lu_nopiv_panel
+// <half,8>): the same loops, every operation an IEEE fp16 operation -- the
+// reciprocal 1/d, the scaling, and a - l * u as the product rounded to fp16
+// and then the difference rounded to fp16.  Values are held in floats (each
+// an fp16 number); evaluating each operation in fp32 and rounding once to
+// fp16 gives the correctly rounded fp16 result (exact fp32 products; 24 >=
+// 2 * 11 + 2 bits for the quotient and the difference).
+static float rn16(float x) { return round_fmt(x, 1); }
+
+void orc_panel_f16(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
+                   int64_t ldl, float* u, int64_t ldu) {
+  float T[8][8];
+  float inv[8];
+  for (int r = 0; r < 8; ++r)
+    for (int c = 0; c < 8; ++c) T[r][c] = (r < n && c < n) ? d[r + c * ldd] : 0.0f;
+  auto sub_mul = [](float a, float x, float y) { return rn16(a - rn16(x * y)); };
+  for (int k = 0; k < n; ++k) {
+    inv[k] = rn16(1.0f / T[k][k]);
+    for (int r = k + 1; r < n; ++r) T[r][k] = rn16(T[r][k] * inv[k]);
+    for (int c = k + 1; c < n; ++c)
+      for (int r = k + 1; r < n; ++r) T[r][c] = sub_mul(T[r][c], T[r][k], T[k][c]);
+  }
+  for (int c = 0; c < n; ++c)
+    for (int r = 0; r < n; ++r) l[r + c * ldl] = T[r][c];
+  for (int64_t r = n; r < m; ++r) {
+    float row[8];
+    for (int c = 0; c < n; ++c) row[c] = l[r + c * ldl];
+    for (int k = 0; k < n; ++k) {
+      row[k] = rn16(row[k] * inv[k]);
+      for (int c = k + 1; c < n; ++c) row[c] = sub_mul(row[c], row[k], T[k][c]);
+    }
+    for (int c = 0; c < n; ++c) l[r + c * ldl] = row[c];
+  }
+  for (int64_t c = n; c < m; ++c) {
+    float col[8];
+    for (int r = 0; r < n; ++r) col[r] = u[r + c * ldu];
+    for (int k = 0; k < n; ++k)
+      for (int r = k + 1; r < n; ++r) col[r] = sub_mul(col[r], T[r][k], col[k]);
+    for (int r = 0; r < n; ++r) u[r + c * ldu] = col[r];
+  }
+}
+
 // reference src/gemm.cu:17-35 (gemmex -> cublasSgemm, alpha=-1, beta=1)
 void orc_gemm_sub_f32(int64_t m, int64_t n, int64_t k, const float* a,
                       int64_t lda, const float* b, int64_t ldb, float* c,

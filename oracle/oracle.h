@@ -87,6 +87,9 @@ void orc_lu_rl_f32_range(int64_t m, int64_t n, int64_t nb, float* a,
  * I = O = FP32 (the lu_nopiv_ll_f32 wrapper): left-looking outer blocks
  * (one K = ofs update of the block column and block row), left-looking
  * inner tiles (one K = 8t update), then the panel kernel. */
+/* lu_nopiv_panel<half,8> with fp16 arithmetic (values held in floats). */
+void orc_panel_f16(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
+                   int64_t ldl, float* u, int64_t ldu);
 void orc_lu_ll_f32(int64_t m, int64_t n, int64_t nb, float* a, int64_t lda,
                    int threads);
 /* Left-looking factorization of an fp16 matrix held in fp32 (fp16-valued

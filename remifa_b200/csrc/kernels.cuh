@@ -38,6 +38,10 @@ lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
 lu_status launch_ref_panel(cudaStream_t st, int64_t m, int n, const float* d,
                            int64_t ldd, float* l, int64_t ldl, float* u,
                            int64_t ldu, int* stat);
+// The same with fp16 storage and IEEE fp16 arithmetic (lu_nopiv_panel<half,8>).
+lu_status launch_ref_panel_f16(cudaStream_t st, int64_t m, int n, const __half* d,
+                               int64_t ldd, __half* l, int64_t ldl, __half* u,
+                               int64_t ldu, int* stat);
 
 // gemm_simt.cu
 lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,

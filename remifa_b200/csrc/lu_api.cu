@@ -97,10 +97,13 @@ lu_status lu_nopiv_ll_c(const lu_opts* opts, lu_stream_t stream, int64_t m,
 lu_status lu_panel_c(lu_stream_t stream, lu_dtype dtype, int64_t m, int64_t n,
                      const void* d, int64_t ldd, void* l, int64_t ldl, void* u,
                      int64_t ldu, int* stat) {
-  if (dtype != LU_F32) return LU_ERR_UNSUPPORTED;
+  if (dtype != LU_F32 && dtype != LU_F16) return LU_ERR_UNSUPPORTED;
   if (n <= 0 || n > 8 || m < n || !d || !l || !u) return LU_ERR_INVALID_ARG;
   if (ldd < n || ldl < m || ldu < n) return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device());
+  if (dtype == LU_F16)
+    return launch_ref_panel_f16((cudaStream_t)stream, m, (int)n, (const __half*)d, ldd,
+                                (__half*)l, ldl, (__half*)u, ldu, stat);
   return launch_ref_panel((cudaStream_t)stream, m, (int)n, (const float*)d, ldd,
                           (float*)l, ldl, (float*)u, ldu, stat);
 }

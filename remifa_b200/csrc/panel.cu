@@ -773,6 +773,83 @@ ref_panel_kernel(int64_t m, int n, const float* __restrict__ d, int64_t ldd,
   }
 }
 
+// ---------------------------------------------------------------------------
+// remifa::lu_nopiv_panel<half,8>: the same panel with fp16 storage and the
+// reference's fp16 arithmetic (src/lu_nopiv.cu:105-326 instantiated for
+// half): every operation is an IEEE fp16 operation, rounded to nearest even
+// -- the pivot's reciprocal 1/d, the scaling l * (1/d), and the update
+// a - l * u as a product rounded to fp16 and then a difference rounded to
+// fp16.  Each is evaluated here in fp32 and rounded once to fp16, which is
+// the correctly rounded fp16 result: products of two fp16 numbers are exact
+// in fp32, and for the quotient and the difference fp32's 24 bits are enough
+// that rounding to fp32 first and to fp16 second equals one rounding to fp16
+// (p' >= 2p + 2 for division, 2p + 1 for addition, p = 11).
+__device__ __forceinline__ float rn16(float x) { return __half2float(__float2half_rn(x)); }
+__device__ __forceinline__ float h16_sub_mul(float a, float l, float u) {
+  return rn16(__fsub_rn(a, rn16(__fmul_rn(l, u))));
+}
+
+__global__ void __launch_bounds__(kThreads)
+ref_panel_f16_kernel(int64_t m, int n, const __half* __restrict__ d, int64_t ldd,
+                     __half* __restrict__ l, int64_t ldl, __half* __restrict__ u,
+                     int64_t ldu, int* stat) {
+  __shared__ float T[8][9];
+  __shared__ float inv[8];
+  const int tid = threadIdx.x;
+  if (tid < 64) {
+    const int r = tid % 8, c = tid / 8;
+    T[r][c] = (r < n && c < n) ? __half2float(d[r + c * ldd]) : 0.0f;
+  }
+  __syncthreads();
+  if (tid == 0) {  // the 8 x 8 tile, right-looking, one thread (64 operations)
+    for (int k = 0; k < n; ++k) {
+      inv[k] = rn16(__fdiv_rn(1.0f, T[k][k]));
+      for (int r = k + 1; r < n; ++r) T[r][k] = rn16(__fmul_rn(T[r][k], inv[k]));
+      for (int c = k + 1; c < n; ++c)
+        for (int r = k + 1; r < n; ++r) T[r][c] = h16_sub_mul(T[r][c], T[r][k], T[k][c]);
+    }
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && blockIdx.y == 0) {
+    if (tid < 64) {
+      const int r = tid % 8, c = tid / 8;
+      if (r < n && c < n) l[r + c * ldl] = __float2half_rn(T[r][c]);
+    }
+    if (tid == 0 && stat) *stat = n;
+  }
+  const int64_t q = (int64_t)blockIdx.x * kThreads + tid + n;
+  if (q >= m) return;
+  if (blockIdx.y == 0) {
+    float row[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) row[c] = (c < n) ? __half2float(l[q + c * ldl]) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k < n) {
+        row[k] = rn16(__fmul_rn(row[k], inv[k]));
+#pragma unroll
+        for (int c = k + 1; c < 8; ++c)
+          if (c < n) row[c] = h16_sub_mul(row[c], row[k], T[k][c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (c < n) l[q + c * ldl] = __float2half_rn(row[c]);
+  } else {
+    float col[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) col[r] = (r < n) ? __half2float(u[r + q * ldu]) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int r = k + 1; r < 8; ++r)
+        if (k < n && r < n) col[r] = h16_sub_mul(col[r], T[r][k], col[k]);
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (r < n) u[r + q * ldu] = __float2half_rn(col[r]);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -821,6 +898,17 @@ lu_status launch_lupanel(cudaStream_t st, float* dg, int64_t lda, int w,
   const LuPack pk = pack ? *pack : LuPack{};
   lupanel_kernel<<<(unsigned)(nL + nU), kPanelT, sm, st>>>(dg, lda, w, M, N, (int)nL,
                                                            left, offL, offU, pk);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+lu_status launch_ref_panel_f16(cudaStream_t st, int64_t m, int n, const __half* d,
+                               int64_t ldd, __half* l, int64_t ldl, __half* u,
+                               int64_t ldu, int* stat) {
+  if (n <= 0 || n > 8 || m < n) return LU_ERR_INVALID_ARG;
+  const int64_t rest = m - n;
+  dim3 grid((unsigned)std::max<int64_t>(1, ceil_div(rest, kThreads)), 2);
+  ref_panel_f16_kernel<<<grid, kThreads, 0, st>>>(m, n, d, ldd, l, ldl, u, ldu, stat);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

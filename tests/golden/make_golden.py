@@ -38,6 +38,7 @@ def ref_lib():
     L.ref_lu_nopiv_ll_f32.argtypes = [vp, i, i, i, vp, i, vp]
     L.ref_lu_nopiv_ll_f16_tc32.argtypes = [vp, i, i, i, vp, i, vp]
     L.ref_lu_nopiv_ll_f16_variant.argtypes = [vp, i, i, i, i, vp, i, vp]
+    L.ref_panel_f16.argtypes = [vp, i, i, vp, i, vp, i, vp, i, vp]
     return L
 
 
@@ -148,6 +149,17 @@ def main(outdir: str) -> None:
             continue
         np.savez_compressed(os.path.join(outdir, f"ref_ll_f16_{tag}_n{nn}_nb{nb}.npz"),
                             a_in=np.asfortranarray(a16), lu=np.array(from_dev(dh, nn)))
+    # 7. lu_nopiv_panel<half,8> (fp16 arithmetic) on the fp16 rounding of a
+    #    64-row gen_diagdom panel
+    a16 = np.asfortranarray(oracle.gen_diagdom(64, lda=64).astype(np.float16))
+    d16 = np.asfortranarray(a16[:8, :8].copy())
+    da, dd = to_dev(a16), to_dev(d16)
+    L.ref_panel_f16(st, 64, 8, ctypes.c_void_p(dd.data_ptr()), 8,
+                    ctypes.c_void_p(da.data_ptr()), 64, ctypes.c_void_p(da.data_ptr()), 64,
+                    ctypes.c_void_p(info.data_ptr()))
+    torch.cuda.synchronize()
+    np.savez_compressed(os.path.join(outdir, "ref_panel_f16_64x8.npz"),
+                        a_in=np.array(a16), out=np.array(from_dev(da, 64)))
     print("golden vectors written to", outdir)
 
 

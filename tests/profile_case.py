@@ -1,15 +1,23 @@
-"""A small, fixed factorization to put under a profiler.
+"""Small, fixed cases to put under a profiler.
 
     python tests/profile_case.py [n] [compute] [reps]
+    python tests/profile_case.py update M K [compute] [reps]
 
-factors the seeded matrix A = R + D (R ~ N(0,1)/sqrt(n), row dominance 1.5,
-the generator of the benchmarks) `reps` times on cuda:0 with the
-right-looking driver (nb = 256), each time from a fresh copy, and prints the
-largest factor entry as a check.  Defaults: n = 4096, compute TC32, reps 2.
-Every kernel of the factorization runs with the shapes it has inside larger
-factorizations (the diagonal blocks are always 128 x 128, the sub-panels 128
-wide), while the device holds only a few hundred MB, so a profiler capture
-of one launch ends quickly.
+The first form factors the seeded matrix A = R + D (R ~ N(0,1)/sqrt(n), row
+dominance 1.5, the generator of the benchmarks) `reps` times on cuda:0 with
+the right-looking driver (nb = 256), each time from a fresh copy, and prints
+the largest factor entry as a check.  Defaults: n = 4096, compute TC32,
+reps 2.  Every kernel of the factorization runs with the shapes it has
+inside larger factorizations (the diagonal blocks are always 128 x 128, the
+sub-panels 128 wide), while the device holds only a few hundred MB, so a
+profiler capture of one launch ends quickly.
+
+The second form runs the trailing (Schur) update alone: C (M x M, fp32) -=
+A (M x K) B (K x M) through the library's update entry (operands packed, then
+one persistent tensor-core launch over all SMs streaming C) `reps` times --
+the largest launch of the factorization (M = n - 3 nb, K = 2 nb when two
+outer steps share a pass) at a size whose C (M = 8192: 256 MB) is larger
+than L2 and small enough for a full capture.
 """
 import os
 import sys
@@ -20,8 +28,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 from remifa_b200 import api  # noqa: E402
 
 
-def main(argv=None) -> None:
-    argv = list(sys.argv[1:] if argv is None else argv)
+def factor(argv) -> None:
     n = int(argv[0]) if len(argv) > 0 else 4096
     outer = getattr(api, argv[1]) if len(argv) > 1 else api.TC32
     reps = int(argv[2]) if len(argv) > 2 else 2
@@ -32,6 +39,30 @@ def main(argv=None) -> None:
         api.lu_nopiv_rl(lu, nb=256, outer=outer)
     torch.cuda.synchronize()
     print("ok", float(lu.abs().max()))
+
+
+def update(argv) -> None:
+    m = int(argv[0]) if len(argv) > 0 else 8192
+    k = int(argv[1]) if len(argv) > 1 else 512
+    compute = getattr(api.compute_type, argv[2]) if len(argv) > 2 else api.TC32
+    reps = int(argv[3]) if len(argv) > 3 else 2
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    a = api.colmajor(torch.randn(m, k, device="cuda", generator=g))
+    b = api.colmajor(torch.randn(k, m, device="cuda", generator=g))
+    c = api.colmajor(torch.randn(m, m, device="cuda", generator=g))
+    for _ in range(reps):
+        api.gemmex(compute, -1.0, a, b, 1.0, c)
+    torch.cuda.synchronize()
+    print("ok", float(c.abs().max()))
+
+
+def main(argv=None) -> None:
+    argv = list(sys.argv[1:] if argv is None else argv)
+    if argv and argv[0] == "update":
+        update(argv[1:])
+    else:
+        factor(argv)
 
 
 if __name__ == "__main__":

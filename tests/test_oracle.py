@@ -349,3 +349,14 @@ def test_generator_kind2_condition_family():
             assert (off <= 0).all()
             k2 = np.linalg.cond(A, 2)
             assert 0.8 / am1 < k2 < 1.3 / am1, (n, am1, k2)
+
+
+def test_golden_ref_panel_f16_bit_exact():
+    """lu_nopiv_panel<half,8> (fp16 arithmetic) restated by the oracle, bit
+    for bit against the reference kernel's output."""
+    g = _golden("ref_panel_f16_64x8.npz")
+    a = np.asfortranarray(g["a_in"].astype(np.float32))
+    d = np.asfortranarray(a[:8, :8].copy())
+    got = np.array(a, copy=True, order="F")
+    O.panel_f16(64, 8, d, got)
+    np.testing.assert_array_equal(got, g["out"].astype(np.float32))

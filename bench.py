@@ -416,6 +416,9 @@ def main() -> None:
                     help="skip the time-to-solution measurements")
     ap.add_argument("--no-n32768", action="store_true",
                     help="skip the n = 32768 time-to-solution study of the default line")
+    ap.add_argument("--no-isolated", action="store_true",
+                    help="skip the dominant kernel's isolated timing (roofline): a launch "
+                         "list of the factorization alone")
     ap.add_argument("--no-lookahead", action="store_true",
                     help="factor each outer block strictly after the previous update")
     ap.add_argument("--nb", type=int, default=None, help="override the outer block size")
@@ -550,7 +553,8 @@ def main() -> None:
     if ent.get("launches"):
         avg_ms = ent["total_ms"] / ent["launches"]
         if dom == "tc_update":
-            roofline = isolated_update_roofline(rb, torch, outer, n, nb, la, peaks)
+            roofline = ({} if args.no_isolated else
+                        isolated_update_roofline(rb, torch, outer, n, nb, la, peaks))
             # inside the factorization (three concurrent streams, so per-launch
             # event times overlap): the update's algorithmic bytes per step
             # over the whole step's time -- a floor of its achieved rate

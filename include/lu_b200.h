@@ -9,8 +9,9 @@
  * pivoting is performed.
  *
  * Each entry point names the reference interface (file:line, paths inside
- * the reference project) that it replaces.  remifa_b200/include_cpp/
- * remifa_shim.hxx maps the reference's C++ template names onto these.
+ * the reference project) that it replaces.  include/remifa_shim.hxx (and the
+ * headers with the reference's file names in include/remifa/) maps the
+ * reference's C++ templates and wrappers onto these.
  */
 #ifndef LU_B200_H
 #define LU_B200_H

@@ -229,13 +229,34 @@ void orc_panel_f32(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
 }
 
 // reference src/lu_nopiv.cu:105-326 instantiated for half (lu_nopiv_panel
-// <half,8>): the same loops, every operation an IEEE fp16 operation -- the
-// reciprocal 1/d, the scaling, and a - l * u as the product rounded to fp16
-// and then the difference rounded to fp16.  Values are held in floats (each
-// an fp16 number); evaluating each operation in fp32 and rounding once to
-// fp16 gives the correctly rounded fp16 result (exact fp32 products; 24 >=
-// 2 * 11 + 2 bits for the quotient and the difference).
+// <half,8>): the same loops in fp16 arithmetic -- the reciprocal 1/d and the
+// scaling each rounded to fp16, and a -= l * u, which nvcc contracts into an
+// fp16 fused multiply-add (the reference's outputs agree only with the fused
+// form), rounded once.  Values are held in floats (each an fp16 number).
+// 1/d and l * (1/d): computed in fp32 and rounded once to fp16, which is the
+// correctly rounded fp16 result (exact products; 24 >= 2 * 11 + 2 bits for
+// the quotient).  a - l * u: the product is exact in fp64, the difference is
+// formed exactly as a double-double (two-sum), and the sum rounded to fp16
+// with the low part breaking a tie of the high part.
 static float rn16(float x) { return round_fmt(x, 1); }
+
+static double rn16d(double v) { return round_format(v, 11, -14, 65504.0, false); }
+
+static float fma16(float a, float l, float u) {
+  const double p = (double)l * (double)u;  // exact (22 bits)
+  const double s = (double)a - p;
+  const double bb = s - (double)a;         // two-sum: a - p = s + e exactly
+  const double e = ((double)a - (s - bb)) + (-p - bb);
+  double r = rn16d(s);
+  if (e != 0.0 && std::isfinite(r)) {
+    // s differs from the exact value by less than half a double ulp, so only
+    // a tie (s exactly halfway between two fp16 numbers r and r2) can round
+    // differently: then the exact value lies on e's side of s
+    const double r2 = 2.0 * s - r;
+    if (r2 != r && rn16d(r2) == r2) r = e > 0.0 ? std::max(r, r2) : std::min(r, r2);
+  }
+  return (float)r;
+}
 
 void orc_panel_f16(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
                    int64_t ldl, float* u, int64_t ldu) {
@@ -243,7 +264,7 @@ void orc_panel_f16(int64_t m, int64_t n, const float* d, int64_t ldd, float* l,
   float inv[8];
   for (int r = 0; r < 8; ++r)
     for (int c = 0; c < 8; ++c) T[r][c] = (r < n && c < n) ? d[r + c * ldd] : 0.0f;
-  auto sub_mul = [](float a, float x, float y) { return rn16(a - rn16(x * y)); };
+  auto sub_mul = [](float a, float x, float y) { return fma16(a, x, y); };
   for (int k = 0; k < n; ++k) {
     inv[k] = rn16(1.0f / T[k][k]);
     for (int r = k + 1; r < n; ++r) T[r][k] = rn16(T[r][k] * inv[k]);

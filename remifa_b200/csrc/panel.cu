@@ -776,17 +776,19 @@ ref_panel_kernel(int64_t m, int n, const float* __restrict__ d, int64_t ldd,
 // ---------------------------------------------------------------------------
 // remifa::lu_nopiv_panel<half,8>: the same panel with fp16 storage and the
 // reference's fp16 arithmetic (src/lu_nopiv.cu:105-326 instantiated for
-// half): every operation is an IEEE fp16 operation, rounded to nearest even
-// -- the pivot's reciprocal 1/d, the scaling l * (1/d), and the update
-// a - l * u as a product rounded to fp16 and then a difference rounded to
-// fp16.  Each is evaluated here in fp32 and rounded once to fp16, which is
-// the correctly rounded fp16 result: products of two fp16 numbers are exact
-// in fp32, and for the quotient and the difference fp32's 24 bits are enough
-// that rounding to fp32 first and to fp16 second equals one rounding to fp16
-// (p' >= 2p + 2 for division, 2p + 1 for addition, p = 11).
-__device__ __forceinline__ float rn16(float x) { return __half2float(__float2half_rn(x)); }
+// half, where nvcc contracts each a -= l * u into one fp16 fused multiply-add,
+// which the reference's own outputs show): the pivot's reciprocal 1/d and
+// the scaling l * (1/d) each rounded to fp16, and the update a - l * u
+// rounded once.  The fp16 intrinsics below are the operations those
+// expressions compile to.
+__device__ __forceinline__ float h16_div1(float d) {
+  return __half2float(__hdiv(__float2half(1.0f), __float2half(d)));
+}
+__device__ __forceinline__ float h16_mul(float a, float b) {
+  return __half2float(__hmul(__float2half(a), __float2half(b)));
+}
 __device__ __forceinline__ float h16_sub_mul(float a, float l, float u) {
-  return rn16(__fsub_rn(a, rn16(__fmul_rn(l, u))));
+  return __half2float(__hfma(__hneg(__float2half(l)), __float2half(u), __float2half(a)));
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -803,8 +805,8 @@ ref_panel_f16_kernel(int64_t m, int n, const __half* __restrict__ d, int64_t ldd
   __syncthreads();
   if (tid == 0) {  // the 8 x 8 tile, right-looking, one thread (64 operations)
     for (int k = 0; k < n; ++k) {
-      inv[k] = rn16(__fdiv_rn(1.0f, T[k][k]));
-      for (int r = k + 1; r < n; ++r) T[r][k] = rn16(__fmul_rn(T[r][k], inv[k]));
+      inv[k] = h16_div1(T[k][k]);
+      for (int r = k + 1; r < n; ++r) T[r][k] = h16_mul(T[r][k], inv[k]);
       for (int c = k + 1; c < n; ++c)
         for (int r = k + 1; r < n; ++r) T[r][c] = h16_sub_mul(T[r][c], T[r][k], T[k][c]);
     }
@@ -826,7 +828,7 @@ ref_panel_f16_kernel(int64_t m, int n, const __half* __restrict__ d, int64_t ldd
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       if (k < n) {
-        row[k] = rn16(__fmul_rn(row[k], inv[k]));
+        row[k] = h16_mul(row[k], inv[k]);
 #pragma unroll
         for (int c = k + 1; c < 8; ++c)
           if (c < n) row[c] = h16_sub_mul(row[c], row[k], T[k][c]);

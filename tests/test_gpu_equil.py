@@ -59,12 +59,14 @@ def test_equilibrate_matches_geequb_laqge(built, n, gamma, kscale, force):
 
 
 def test_equilibration_keeps_fp16_operands_in_range(built):
-    """Entries times 2^12 (up to ~6e5, beyond fp16's 65504): the fp16 trailing
-    update overflows without equilibration; with it the factorization is
-    finite and refinement reaches 1e-14."""
+    """Entries times 2^20 (off-diagonal entries up to ~1e5, beyond fp16's
+    65504, in the U12 blocks the tensor cores read): the fp16 trailing update
+    overflows without equilibration; with it the factorization is finite and
+    refinement reaches 1e-14."""
     n = 1024
-    a = rb.gen_matrix(n, seed=4, kind=1, alpha=1.5, kscale=12)
-    assert float(a.abs().max()) > 65504
+    a = rb.gen_matrix(n, seed=4, kind=1, alpha=1.5, kscale=20)
+    off = a - torch.diag(torch.diagonal(a))
+    assert float(off.abs().max()) > 65504
     g = torch.Generator(device="cuda")
     g.manual_seed(1)
     xt = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)

@@ -154,13 +154,14 @@ def lu_nopiv_rl(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
 def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=FP32,
                      outer=FP32, info: torch.Tensor | None = None, lookahead: bool = True,
                      diag_width: int = 0, workspace: torch.Tensor | None = None,
-                     stream=None) -> torch.Tensor:
+                     stream=None, bulk_steps: int = 0) -> torch.Tensor:
     """Factor the column-major fp32 matrix in (pinned) host memory `h_a` in
     place, using the device matrix `d_a` (same shape) as the working copy.
     The matrix goes in by column chunks while the device works on the chunks
     already in, and each chunk's factors go back as soon as they are final
-    (lu_nopiv_rl_host_c); the factors equal lu_nopiv_rl's bit for bit.
-    Returns the device info tensor."""
+    (lu_nopiv_rl_host_c); with bulk_steps = 1 the factors equal
+    lu_nopiv_rl's (bulk_steps = 1) bit for bit.  Returns the device info
+    tensor."""
     if h_a.is_cuda or not d_a.is_cuda:
         raise ValueError("lu_nopiv_rl_host: h_a must be a host tensor, d_a a CUDA tensor")
     if h_a.dtype != torch.float32 or d_a.dtype != torch.float32 or h_a.shape != d_a.shape:
@@ -168,7 +169,8 @@ def lu_nopiv_rl_host(h_a: torch.Tensor, d_a: torch.Tensor, nb: int = 256, inner=
     n = h_a.shape[0]
     if info is None:
         info = torch.zeros(1, dtype=torch.int32, device=d_a.device)
-    o = make_opts(nb, inner, outer, lookahead, diag_width, _lib.RIGHT_LOOKING)
+    o = make_opts(nb, inner, outer, lookahead, diag_width, _lib.RIGHT_LOOKING,
+                  bulk_steps=bulk_steps)
     ws_ptr, ws_bytes = None, 0
     if workspace is not None:
         ws_ptr, ws_bytes = _ptr(workspace), workspace.numel() * workspace.element_size()

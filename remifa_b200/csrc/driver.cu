@@ -550,9 +550,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t n = p.n, nb = p.nb;
   if (col_end < 0) col_end = n;
   const bool tc = is_tc(p.outer);
-  // two steps per bulk pass: the device entry only (the host entry's
-  // catch-up applies the steps one by one)
-  const bool pair = p.bulk_pair && sink == nullptr && col_begin == 0 && col_end == n;
+  // two steps per bulk pass (the host entry's chunks too, restricted to
+  // their columns)
+  const bool pair = p.bulk_pair;
   const int nbuf = p.bulk_pair ? 4 : 3;
   TcWs w2[4];
   if (tc && n > nb) {
@@ -891,6 +891,15 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
     LUB_CUDA_TRY(cudaEventRecord(S->cu_join, st));
     LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_join, 0));
   }
+  // Two steps per bulk pass (look-ahead, unscaled operands): an even step
+  // updates only the block row below its U1 (U2a) and leaves the rest to the
+  // next step, whose U2 region is exactly that rest; the odd step's pass
+  // then applies both steps' products (C - (L_t U_t + L_t+1 U_t+1)).  Both
+  // operand buffers stay in use until that pass, whose completion releases
+  // them (cu_u2 of both parities).
+  const int64_t nsteps = ceil_div(c0, nb);
+  const bool pairing = S && tc && p.bulk_pair && !tc_scaled(kind);
+  bool deferred = false;
   for (int64_t ofs = 0; ofs < c0; ofs += nb) {
     const int64_t t = ofs / nb;
     const TcWs& w = wk[S ? t % 2 : 0];
@@ -927,13 +936,41 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
       continue;
     }
     const int64_t r1 = std::min(tr, nb);  // U1: rows [0, r1) of the trailing part
-    if (tr > r1) {
+    bool u1_ordered = false;
+    if (deferred) {
+      // U1 of this step follows the previous step's U2a (its block row); the
+      // event is about to be re-recorded for the pass below
+      LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[(t - 1) % 2], 0));
+      u1_ordered = true;
+      // rows [nb, tr) of this step = rows [2 nb, ...) of the previous step
       LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
       LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
-      LUB_TRY(outer_update(p, sb, a, lda, ofs, r1, tr - r1, cr, nc, ws, w, err, 0));
+      const TcWs& wp = wk[(t - 1) % 2];
+      const int64_t ldk = tc_packed_k(kind, nb);
+      const int64_t es = tc_operand_bytes(kind);
+      const int64_t crp = cr + nb;  // the chunk's columns in the previous step's copy
+      float* c = a + (ofs + nb + r1) + c0 * lda;
+      ProfScope ps("tc_update", sb, 8.0 * (tr - r1) * nc + 2.0 * es * (tr - r1 + nc) * nb,
+                   4.0 * (tr - r1) * (double)nc * nb);
+      LUB_TRY(launch_tc_update2(sb, kind, tr - r1, nc, nb, ws + wp.off_a + 2 * nb * ldk * es,
+                                ws + wp.off_b + crp * ldk * es, nb,
+                                ws + w.off_a + r1 * ldk * es, ws + w.off_b + cr * ldk * es,
+                                ldk, c, lda, err, 0, 0));
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_u2[(t - 1) % 2], sb));
       LUB_CUDA_TRY(cudaEventRecord(S->cu_u2[t % 2], sb));
+      deferred = false;
+    } else if (tr > r1) {
+      // an even step whose next step still has a U2 region: update only the
+      // block row below U1 now
+      const bool defer = pairing && t % 2 == 0 && t + 1 < nsteps && tr > 2 * nb;
+      const int64_t rows = defer ? nb : tr - r1;
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
+      LUB_TRY(outer_update(p, sb, a, lda, ofs, r1, rows, cr, nc, ws, w, err, 0));
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_u2[t % 2], sb));
+      deferred = defer;
     }
-    if (t >= 1) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[(t - 1) % 2], 0));
+    if (t >= 1 && !u1_ordered) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[(t - 1) % 2], 0));
     LUB_TRY(outer_update(p, st, a, lda, ofs, 0, r1, cr, nc, ws, w, err, 0));
   }
   if (S) {

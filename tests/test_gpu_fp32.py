@@ -353,7 +353,31 @@ def test_host_entry_matches_device_entry(built, n, nb, outer, la, pad):
     h = torch.empty((n, n + pad), dtype=torch.float32, pin_memory=True).t()[:n, :]
     h.copy_(torch.from_numpy(a))
     work = rb.colmajor_empty(n, n, n + 2 * pad, torch.float32)
-    info = rb.lu_nopiv_rl_host(h, work, nb=nb, outer=outer, lookahead=la)
+    info = rb.lu_nopiv_rl_host(h, work, nb=nb, outer=outer, lookahead=la, bulk_steps=1)
     torch.cuda.synchronize()
     assert int(info.item()) == 0
     assert np.array_equal(h.numpy(), d.cpu().numpy())
+
+
+@pytest.mark.parametrize("n,nb,outer", [(4096, 256, rb.TC32), (3000, 128, rb.compute_type.TC32_BF16),
+                                        (8192, 256, rb.TC32)])
+def test_host_entry_two_step_bulk(built, n, nb, outer):
+    """The host entry with two steps per bulk pass (the default, in its chunk
+    factorizations and in the catch-up of arriving chunks): same factors as
+    the step-by-step order up to the one rounding per pass it saves, and as
+    the oracle's restatement."""
+    fmt = O.FMT_FP16 if outer == rb.TC32 else O.FMT_BF16
+    a = O.gen_matrix(n, seed=n + 7, kind=1, alpha=1.5)
+    h = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()[:n, :]
+    h.copy_(torch.from_numpy(a))
+    work = rb.colmajor_empty(n, n, n, torch.float32)
+    info = rb.lu_nopiv_rl_host(h, work, nb=nb, outer=outer)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0
+    got = h.numpy()
+    want = O.lu_rl(a, nb=nb, outer_fmt=fmt)
+    assert np.abs(got - want).max() / np.abs(want).max() < 64 * n * 2.0 ** -24
+    b = O.gen_rhs(a, np.ones(n, np.float32))
+    e_g = O.nwerr(a, b, O.lu_solve_f32(np.asfortranarray(got), b))
+    e_o = O.nwerr(a, b, O.lu_solve_f32(want, b))
+    assert e_g <= 2 * e_o and e_o <= 2 * e_g, (e_g, e_o)

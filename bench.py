@@ -738,9 +738,10 @@ def run_batch(args, torch, rb):
 
 def run_ll16(args, torch, rb):
     """Left-looking factorization of an n = 16384 fp16 matrix (fp16
-    storage, fp16 tensor-core updates, nb = 128), A = R + D with R ~
+    storage, fp16 tensor-core updates, nb = 256 -- the reference's outer
+    block for its fp16 wrappers -- or --nb), A = R + D with R ~
     N(0,1)/sqrt(n), row dominance 1.5."""
-    n, nb = 16384, 128
+    n, nb = 16384, args.nb or 256
     base32 = rb.gen_matrix(n, seed=1, kind=1, alpha=1.5)
     base = rb.colmajor_empty(n, n, n, torch.float16)
     base.copy_(base32)

@@ -250,6 +250,19 @@ static lu_status step_events(DevStreams* S, int64_t steps) {
   return LU_SUCCESS;
 }
 
+// Work queued on the side stream after this point follows what st has
+// queued so far; join_side makes st wait for it.
+static lu_status fork_side(cudaStream_t st, DevStreams* S) {
+  LUB_CUDA_TRY(cudaEventRecord(S->fork, st));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(S->side, S->fork, 0));
+  return LU_SUCCESS;
+}
+static lu_status join_side(cudaStream_t st, DevStreams* S) {
+  LUB_CUDA_TRY(cudaEventRecord(S->join_s, S->side));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->join_s, 0));
+  return LU_SUCCESS;
+}
+
 lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
                     Plan* p) {
   if (m != n) return LU_ERR_UNSUPPORTED;
@@ -1030,21 +1043,33 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t es = tc_operand_bytes(kind);
   char* Lc = ws + p.off_lcopy;
   char* Uc = ws + p.off_ucopy;
+  DevStreams* S = nullptr;
+  if (tc) LUB_TRY(dev_streams(&S));
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
     const int64_t in = std::min(n - ofs, nb);
     const int64_t updm = n - ofs;
     float* blk = a + ofs + ofs * lda;
     if (ofs > 0) {
       if (tc) {
-        ProfScope ps("tc_update", st,
-                     8.0 * updm * in + 8.0 * in * (updm - in) + es * (double)ofs * (updm + in),
-                     2.0 * ofs * ((double)updm * in + (double)in * (updm - in)));
-        LUB_TRY(launch_tc_update(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es, ldk,
-                                 Uc + ofs * ldk * es, ldk, blk, lda, nullptr, nullptr, err));
-        if (updm > in)
-          LUB_TRY(launch_tc_update(st, kind, in, updm - in, ofs, -1.0f,
+        // the block column (on st) and the block row (on the side stream)
+        // are disjoint: both updates run at once, so the two narrow grids
+        // fill the SMs together
+        const bool row = updm > in;
+        if (row) LUB_TRY(fork_side(st, S));
+        {
+          ProfScope ps("tc_update", st, 8.0 * updm * in + es * (double)ofs * (updm + in),
+                       2.0 * ofs * (double)updm * in);
+          LUB_TRY(launch_tc_update(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es, ldk,
+                                   Uc + ofs * ldk * es, ldk, blk, lda, nullptr, nullptr, err));
+        }
+        if (row) {
+          ProfScope ps("tc_update", S->side, 8.0 * in * (updm - in) + es * (double)ofs * updm,
+                       2.0 * ofs * (double)in * (updm - in));
+          LUB_TRY(launch_tc_update(S->side, kind, in, updm - in, ofs, -1.0f,
                                    Lc + ofs * ldk * es, ldk, Uc + (ofs + in) * ldk * es,
                                    ldk, blk + in * lda, lda, nullptr, nullptr, err));
+          LUB_TRY(join_side(st, S));
+        }
       } else {
         ProfScope ps("sgemm_update", st, 0.0,
                      2.0 * ofs * ((double)updm * in + (double)in * (updm - in)));
@@ -1089,14 +1114,16 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
   const int64_t n = p.n, nb = p.nb;
   const int64_t ldk = (n + 15) / 16 * 16;
   char* Lc = ws + p.off_lcopy;
-  float* S = reinterpret_cast<float*>(ws + p.off_shadow);
+  float* Sh = reinterpret_cast<float*>(ws + p.off_shadow);
   const int64_t lds = p.ld_shadow;
+  DevStreams* S = nullptr;
+  LUB_TRY(dev_streams(&S));
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
     const int64_t in = std::min(n - ofs, nb);
     const int64_t updm = n - ofs;
     const int64_t rest = updm - in;
     __half* blk = a + ofs + ofs * lda;
-    float* sblk = S + ofs + ofs * lds;
+    float* sblk = Sh + ofs + ofs * lds;
     auto to_shadow = [&]() -> lu_status {
       LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
       if (rest > 0)
@@ -1106,30 +1133,37 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
     };
     if (p.panel_fp32) LUB_TRY(to_shadow());
     if (ofs > 0) {
-      ProfScope ps("tc_update", st,
-                   (p.panel_fp32 ? 8.0 : 4.0) * ((double)updm * in + (double)in * rest) +
-                       2.0 * (double)ofs * (updm + in),
-                   2.0 * ofs * ((double)updm * in + (double)in * rest));
-      if (p.panel_fp32) {
-        LUB_TRY(launch_tc_update(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                 Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk, lds,
-                                 nullptr, nullptr, err));
-        if (rest > 0)
-          LUB_TRY(launch_tc_update(st, TcOperand::F16, in, rest, ofs, -1.0f,
+      // block column on st, block row on the side stream (disjoint, at once)
+      const double cb = p.panel_fp32 ? 8.0 : 4.0;
+      if (rest > 0) LUB_TRY(fork_side(st, S));
+      {
+        ProfScope ps("tc_update", st, cb * updm * in + 2.0 * (double)ofs * (updm + in),
+                     2.0 * ofs * (double)updm * in);
+        if (p.panel_fp32)
+          LUB_TRY(launch_tc_update(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                   Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk, lds,
+                                   nullptr, nullptr, err));
+        else
+          LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                     Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
+                                     err));
+      }
+      if (rest > 0) {
+        ProfScope ps("tc_update", S->side, cb * in * rest + 2.0 * (double)ofs * (in + rest),
+                     2.0 * ofs * (double)in * rest);
+        if (p.panel_fp32)
+          LUB_TRY(launch_tc_update(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
                                    Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
                                    sblk + in * lds, lds, nullptr, nullptr, err));
-      } else {
-        LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                   Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
-                                   err));
-        if (rest > 0)
-          LUB_TRY(launch_tc_update_h(st, TcOperand::F16, in, rest, ofs, -1.0f,
+        else
+          LUB_TRY(launch_tc_update_h(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
                                      Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
                                      blk + in * lda, lda, err));
+        LUB_TRY(join_side(st, S));
       }
     }
     if (!p.panel_fp32) LUB_TRY(to_shadow());
-    LUB_TRY(ll_block(st, S, lds, n, ofs, in, first_bad));
+    LUB_TRY(ll_block(st, Sh, lds, n, ofs, in, first_bad));
     LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
     if (rest > 0) {
       LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,

@@ -522,8 +522,7 @@ static lu_status outer_update(const Plan& p, cudaStream_t st, float* a,
 // B200 at n = 16384: 2 tiles 133 TF/s, 8 tiles 124, 16 tiles 122).
 constexpr int kU2Tiles = 2;
 // ... except the bulk update U2b when it is large: then it runs as
-// persistent CTAs on half of the SMs (streaming C ahead of the accumulator),
-// leaving the other half to the panel streams.  B200, nb = 256, threshold
+// persistent CTAs on part of the SMs, leaving the rest to the panel streams.  B200, nb = 256, threshold
 // 2048 tiles of 128 x 256: n = 16384 165 -> 181 TF/s, n = 32768 238 -> 243,
 // n = 8192 unchanged (below the threshold it keeps the 2-tile CTAs).  Not
 // for the split-fp16 update: two MMAs per tile make it compute-heavy enough
@@ -821,7 +820,12 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
         const bool persist = tc && tc_kind(p.outer) != TcOperand::SPLIT16 &&
                              t2b >= kU2bPersistTiles;
         const int tiles = persist ? 0 : kU2Tiles;
-        const int ctas = persist ? std::max(1, sm_count() / 2) : 0;
+        // the bulk's share of the SMs (the rest for the panel streams): 2/3,
+        // 3/4 for the largest passes (B200, two steps per pass: n = 16384
+        // 232 TF/s at 1/2, 242 at 2/3, 241 at 3/4; n = 32768 308 / 341 / 353)
+        const int ctas = persist ? std::max(1, sm_count() * (t2b >= 2 * kU2bPersistTiles ? 3 : 2) /
+                                                   (t2b >= 2 * kU2bPersistTiles ? 4 : 3))
+                                 : 0;
         // the next step will have a U2b of its own (its trailing part is
         // one block smaller): defer to it
         const bool defer = pair && !deferred && tr > 3 * nb && tcn > 3 * nb;

@@ -574,10 +574,14 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                      make_c_map(&mc, static_cast<float*>(C), M, N, ldc);
   // C epilogue: CTAs that stay for many tiles stream C by TMA load / store,
   // its loads running ahead of the accumulator (B200, 16128^2 x 256:
-  // 5.5 TB/s against 4.6 for the L2 reduce-add); CTAs of one or two tiles --
+  // 5.6 TB/s against 4.7 for the L2 reduce-add); CTAs of one or two tiles --
   // the trailing updates under look-ahead, which hand SMs back to the panel
   // kernels quickly -- have no pipeline to fill and keep the reduce-add.
-  const bool stream_c = tiles_per_cta <= 0 || tiles_per_cta > 2;
+  // With more than four 128-byte operand blocks along K (K = 512 at fp16:
+  // two outer steps per pass) the operand feed bounds the tile, and the reduce-add
+  // epilogue's smaller shared-memory footprint leaves room for a third
+  // operand stage: 15360^2 x 512, 0.408 ms against 0.457 streaming C.
+  const bool stream_c = (tiles_per_cta <= 0 || tiles_per_cta > 2) && p.kb_count <= 4;
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
   if (c_half) {

@@ -2,6 +2,7 @@
 
     python tests/profile_case.py [n] [compute] [reps]
     python tests/profile_case.py update M K [compute] [reps]
+    python tests/profile_case.py ll16 [n] [nb] [reps]
 
 The first form factors the seeded matrix A = R + D (R ~ N(0,1)/sqrt(n), row
 dominance 1.5, the generator of the benchmarks) `reps` times on cuda:0 with
@@ -18,6 +19,10 @@ one persistent tensor-core launch over all SMs streaming C) `reps` times --
 the largest launch of the factorization (M = n - 3 nb, K = 2 nb when two
 outer steps share a pass) at a size whose C (M = 8192: 256 MB) is larger
 than L2 and small enough for a full capture.
+
+The third form factors an fp16 matrix with the left-looking driver and fp16
+tensor-core updates (fp16 storage, nb = 256 by default): its block-column
+updates have K up to n and N = nb, the shapes of the fp16-storage workload.
 """
 import os
 import sys
@@ -57,10 +62,27 @@ def update(argv) -> None:
     print("ok", float(c.abs().max()))
 
 
+def factor_f16(argv) -> None:
+    n = int(argv[0]) if len(argv) > 0 else 4096
+    nb = int(argv[1]) if len(argv) > 1 else 256
+    reps = int(argv[2]) if len(argv) > 2 else 2
+    a32 = api.gen_matrix(n, seed=1, kind=1, alpha=1.5)
+    a = api.colmajor_empty(n, n, n, torch.float16)
+    api.convert(a32, a)
+    lu = api.colmajor_empty(n, n, n, torch.float16)
+    for _ in range(reps):
+        lu.copy_(a)
+        api.lu_nopiv_ll(lu, nb=nb, outer=api.TC32)
+    torch.cuda.synchronize()
+    print("ok", float(lu.float().abs().max()))
+
+
 def main(argv=None) -> None:
     argv = list(sys.argv[1:] if argv is None else argv)
     if argv and argv[0] == "update":
         update(argv[1:])
+    elif argv and argv[0] == "ll16":
+        factor_f16(argv[1:])
     else:
         factor(argv)
 

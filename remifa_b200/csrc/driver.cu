@@ -263,6 +263,20 @@ static lu_status join_side(cudaStream_t st, DevStreams* S) {
   return LU_SUCCESS;
 }
 
+// Left-looking tensor-core updates have N = nb (block column) or M = nb
+// (block row) and K = ofs: at most 2 n / 128 tiles, long in K, so they are
+// split along K (up to kLlSplitMax ways) to fill the SMs.  Two regions of
+// kLlSplitMax slabs, one per update of a step (they run at once).
+constexpr int kLlSplitMax = 4;
+static size_t ll_part_layout(Plan* p, size_t off) {
+  const int64_t n = p->n, nb = p->nb;
+  const int64_t slab = std::max(((n + 3) / 4 * 4) * nb, ((nb + 3) / 4 * 4) * n);
+  off = align_up(off, 1024);
+  p->off_part = off;
+  p->part_bytes = align_up((size_t)kLlSplitMax * slab * 4, 1024);
+  return off + 2 * p->part_bytes;
+}
+
 lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
                     Plan* p) {
   if (m != n) return LU_ERR_UNSUPPORTED;
@@ -318,6 +332,7 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     off = align_up(off + (size_t)p->ld_shadow * n * 4, 1024);
     p->off_lcopy = off;
     off = align_up(off + (size_t)n * ldk * 2, 1024);
+    off = ll_part_layout(p, off);
     p->ws_bytes = off;
     return LU_SUCCESS;
   }
@@ -333,6 +348,7 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
       off = align_up(off + (size_t)n * ldk * es, 1024);
       p->off_ucopy = off;
       off = align_up(off + (size_t)n * ldk * es, 1024);
+      off = ll_part_layout(p, off);
     }
     p->ws_bytes = off;
     return LU_SUCCESS;
@@ -997,6 +1013,15 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
   return LU_SUCCESS;
 }
 
+// K splits of a step's two concurrent left-looking updates (block column
+// updm x in, block row in x (updm - in), K = ofs), chosen over their tiles
+// together.
+static int ll_split(int64_t updm, int64_t in, int64_t ofs, int64_t es) {
+  const int64_t tiles = ceil_div(updm, 128) * ceil_div(in, 256) +
+                        (updm > in ? ceil_div(in, 128) * ceil_div(updm - in, 256) : 0);
+  return tc_split_choice(tiles, ofs, (int)es, sm_count(), kLlSplitMax);
+}
+
 // The inside of one left-looking outer block (columns [ofs, ofs + in) of an
 // n x n matrix x, ld ldx, already updated by all columns left of ofs): the
 // block is factored as sub-blocks of at most kLlSub columns; sub-block c
@@ -1006,20 +1031,30 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
 // this is exactly the reference's inner Crout loop
 // (src/lu_nopiv_inner_ll.hxx:197-370); wider blocks nest one more level.
 static lu_status ll_block(cudaStream_t st, float* x, int64_t ldx, int64_t n, int64_t ofs,
-                          int64_t in, int* first_bad) {
+                          int64_t in, int* first_bad, DevStreams* S) {
   for (int64_t c = ofs; c < ofs + in; c += kLlSub) {
     const int64_t w = std::min(kLlSub, ofs + in - c);
     const int64_t rest = n - c - w;
     float* dg = x + c + c * ldx;
     if (c > ofs) {
+      // the sub-block's column (st) and row (side stream, when given) are
+      // disjoint: their two narrow grids run at once
       const int64_t k = c - ofs;
-      ProfScope ps("sgemm_update", st, 0.0, 2.0 * k * ((double)(n - c) * w + (double)w * rest));
-      LUB_TRY(launch_sgemm_update(st, n - c, w, k, -1.0f, x + c + ofs * ldx, ldx,
-                                  x + ofs + c * ldx, ldx, 1.0f, dg, ldx, false));
-      if (rest > 0)
-        LUB_TRY(launch_sgemm_update(st, w, rest, k, -1.0f, x + c + ofs * ldx, ldx,
+      const bool side = S != nullptr && rest > 0;
+      if (side) LUB_TRY(fork_side(st, S));
+      {
+        ProfScope ps("sgemm_update", st, 0.0, 2.0 * k * (double)(n - c) * w);
+        LUB_TRY(launch_sgemm_update(st, n - c, w, k, -1.0f, x + c + ofs * ldx, ldx,
+                                    x + ofs + c * ldx, ldx, 1.0f, dg, ldx, false));
+      }
+      if (rest > 0) {
+        cudaStream_t sr = side ? S->side : st;
+        ProfScope ps("sgemm_update", sr, 0.0, 2.0 * k * (double)w * rest);
+        LUB_TRY(launch_sgemm_update(sr, w, rest, k, -1.0f, x + c + ofs * ldx, ldx,
                                     x + ofs + (c + w) * ldx, ldx, 1.0f, dg + w * ldx, ldx,
                                     false));
+      }
+      if (side) LUB_TRY(join_side(st, S));
     }
     {
       ProfScope ps("diag_factor", st, 8.0 * w * w, 2.0 * w * w * (double)w / 3.0);
@@ -1047,8 +1082,10 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t es = tc_operand_bytes(kind);
   char* Lc = ws + p.off_lcopy;
   char* Uc = ws + p.off_ucopy;
+  float* Pc = reinterpret_cast<float*>(ws + p.off_part);
+  float* Pr = reinterpret_cast<float*>(ws + p.off_part + p.part_bytes);
   DevStreams* S = nullptr;
-  if (tc) LUB_TRY(dev_streams(&S));
+  LUB_TRY(dev_streams(&S));
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
     const int64_t in = std::min(n - ofs, nb);
     const int64_t updm = n - ofs;
@@ -1056,36 +1093,46 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
     if (ofs > 0) {
       if (tc) {
         // the block column (on st) and the block row (on the side stream)
-        // are disjoint: both updates run at once, so the two narrow grids
-        // fill the SMs together
+        // are disjoint: both updates run at once, split along K so that
+        // their units fill the SMs together
         const bool row = updm > in;
+        const int ks = ll_split(updm, in, ofs, es);
         if (row) LUB_TRY(fork_side(st, S));
         {
           ProfScope ps("tc_update", st, 8.0 * updm * in + es * (double)ofs * (updm + in),
                        2.0 * ofs * (double)updm * in);
-          LUB_TRY(launch_tc_update(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es, ldk,
-                                   Uc + ofs * ldk * es, ldk, blk, lda, nullptr, nullptr, err));
+          LUB_TRY(launch_tc_update_split(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es,
+                                         ldk, Uc + ofs * ldk * es, ldk, blk, false, lda,
+                                         nullptr, 0, ks, Pc, err));
         }
         if (row) {
           ProfScope ps("tc_update", S->side, 8.0 * in * (updm - in) + es * (double)ofs * updm,
                        2.0 * ofs * (double)in * (updm - in));
-          LUB_TRY(launch_tc_update(S->side, kind, in, updm - in, ofs, -1.0f,
-                                   Lc + ofs * ldk * es, ldk, Uc + (ofs + in) * ldk * es,
-                                   ldk, blk + in * lda, lda, nullptr, nullptr, err));
+          LUB_TRY(launch_tc_update_split(S->side, kind, in, updm - in, ofs, -1.0f,
+                                         Lc + ofs * ldk * es, ldk, Uc + (ofs + in) * ldk * es,
+                                         ldk, blk + in * lda, false, lda, nullptr, 0, ks, Pr,
+                                         err));
           LUB_TRY(join_side(st, S));
         }
       } else {
-        ProfScope ps("sgemm_update", st, 0.0,
-                     2.0 * ofs * ((double)updm * in + (double)in * (updm - in)));
-        LUB_TRY(launch_sgemm_update(st, updm, in, ofs, -1.0f, a + ofs, lda,
-                                    a + ofs * lda, lda, 1.0f, blk, lda, false));
-        if (updm > in)
-          LUB_TRY(launch_sgemm_update(st, in, updm - in, ofs, -1.0f, a + ofs, lda,
+        // block column and block row at once, as above
+        const bool row = updm > in;
+        if (row) LUB_TRY(fork_side(st, S));
+        {
+          ProfScope ps("sgemm_update", st, 0.0, 2.0 * ofs * (double)updm * in);
+          LUB_TRY(launch_sgemm_update(st, updm, in, ofs, -1.0f, a + ofs, lda,
+                                      a + ofs * lda, lda, 1.0f, blk, lda, false));
+        }
+        if (row) {
+          ProfScope ps("sgemm_update", S->side, 0.0, 2.0 * ofs * (double)in * (updm - in));
+          LUB_TRY(launch_sgemm_update(S->side, in, updm - in, ofs, -1.0f, a + ofs, lda,
                                       a + (ofs + in) * lda, lda, 1.0f, blk + in * lda,
                                       lda, false));
+          LUB_TRY(join_side(st, S));
+        }
       }
     }
-    LUB_TRY(ll_block(st, a, lda, n, ofs, in, first_bad));
+    LUB_TRY(ll_block(st, a, lda, n, ofs, in, first_bad, S));
     const int64_t rest = updm - in;
     if (rest > 0 && tc) {
       ProfScope ps("pack_operands", st, 2.0 * rest * in * (4.0 + es));
@@ -1120,6 +1167,8 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
   char* Lc = ws + p.off_lcopy;
   float* Sh = reinterpret_cast<float*>(ws + p.off_shadow);
   const int64_t lds = p.ld_shadow;
+  float* Pc = reinterpret_cast<float*>(ws + p.off_part);
+  float* Pr = reinterpret_cast<float*>(ws + p.off_part + p.part_bytes);
   DevStreams* S = nullptr;
   LUB_TRY(dev_streams(&S));
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
@@ -1129,50 +1178,61 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
     __half* blk = a + ofs + ofs * lda;
     float* sblk = Sh + ofs + ofs * lds;
     auto to_shadow = [&]() -> lu_status {
+      ProfScope ps("convert", st, 6.0 * (double)in * (updm + rest));
       LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
       if (rest > 0)
         LUB_TRY(launch_convert(st, in, rest, blk + in * lda, LU_F16, lda, sblk + in * lds,
                                LU_F32, lds, 0));
       return LU_SUCCESS;
     };
-    if (p.panel_fp32) LUB_TRY(to_shadow());
+    if (p.panel_fp32 || ofs == 0) LUB_TRY(to_shadow());
     if (ofs > 0) {
-      // block column on st, block row on the side stream (disjoint, at once)
-      const double cb = p.panel_fp32 ? 8.0 : 4.0;
+      // block column on st, block row on the side stream (disjoint, at once,
+      // split along K to fill the SMs together).  panel_fp32: the update
+      // lands in the shadow; otherwise in the fp16 matrix (one rounding),
+      // and the finishing kernel also writes the stored values to the shadow
+      const double cb = p.panel_fp32 ? 8.0 : 10.0;
+      const int ks = ll_split(updm, in, ofs, 2);
       if (rest > 0) LUB_TRY(fork_side(st, S));
       {
         ProfScope ps("tc_update", st, cb * updm * in + 2.0 * (double)ofs * (updm + in),
                      2.0 * ofs * (double)updm * in);
         if (p.panel_fp32)
-          LUB_TRY(launch_tc_update(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                   Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk, lds,
-                                   nullptr, nullptr, err));
+          LUB_TRY(launch_tc_update_split(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                         Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk,
+                                         false, lds, nullptr, 0, ks, Pc, err));
         else
-          LUB_TRY(launch_tc_update_h(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                     Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk, lda,
-                                     err));
+          LUB_TRY(launch_tc_update_split(st, TcOperand::F16, updm, in, ofs, -1.0f,
+                                         Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk,
+                                         true, lda, sblk, lds, ks, Pc, err));
       }
       if (rest > 0) {
         ProfScope ps("tc_update", S->side, cb * in * rest + 2.0 * (double)ofs * (in + rest),
                      2.0 * ofs * (double)in * rest);
         if (p.panel_fp32)
-          LUB_TRY(launch_tc_update(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
-                                   Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
-                                   sblk + in * lds, lds, nullptr, nullptr, err));
+          LUB_TRY(launch_tc_update_split(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
+                                         Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
+                                         sblk + in * lds, false, lds, nullptr, 0, ks, Pr,
+                                         err));
         else
-          LUB_TRY(launch_tc_update_h(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
-                                     Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
-                                     blk + in * lda, lda, err));
+          LUB_TRY(launch_tc_update_split(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
+                                         Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
+                                         blk + in * lda, true, lda, sblk + in * lds, lds, ks,
+                                         Pr, err));
         LUB_TRY(join_side(st, S));
       }
     }
-    if (!p.panel_fp32) LUB_TRY(to_shadow());
-    LUB_TRY(ll_block(st, Sh, lds, n, ofs, in, first_bad));
-    LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
+    LUB_TRY(ll_block(st, Sh, lds, n, ofs, in, first_bad, S));
+    {
+      ProfScope ps("convert", st, 6.0 * (double)in * (updm + rest));
+      LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
+      if (rest > 0)
+        LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,
+                               LU_F16, lda, 0));
+    }
     if (rest > 0) {
-      LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,
-                             LU_F16, lda, 0));
       // L rows [ofs+in, n) of the block's columns, rounded exactly as stored
+      ProfScope ps("pack_operands", st, 6.0 * (double)rest * in);
       LUB_TRY(launch_pack_a(st, TcOperand::F16, rest, in, sblk + in, lds,
                             Lc + ((ofs + in) * ldk + ofs) * 2, ldk, nullptr));
     }

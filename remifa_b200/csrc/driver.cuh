@@ -28,6 +28,8 @@ struct Plan {
   size_t off_scales = 0;    // int per-tile scales (fp8)
   size_t off_shadow = 0;    // fp16 storage: fp32 copy of the current block
   int64_t ld_shadow = 0;    //   column and row, where the panel is factored
+  size_t off_part = 0;      // left-looking tensor-core updates: split-K
+  size_t part_bytes = 0;    //   partial slabs, block column then block row
   size_t lcopy_bytes = 0, ucopy_bytes = 0, scale_bytes = 0;
   size_t ws_bytes = 0;
 };

@@ -68,6 +68,10 @@ template <> struct Cfg<3> {  // TMA load + store epilogue: each warp's 32 x 128 
   static constexpr int kStages = 2;
   static constexpr size_t kEpiBytes = (size_t)kEpiWarps * 4 * kEpiChunk;
 };
+template <> struct Cfg<4> {  // split K: the raw partial stored to its slab
+  static constexpr int kStages = 4;
+  static constexpr size_t kEpiBytes = 0;
+};
 template <int EPI>
 constexpr size_t smem_bytes() {
   return 1024 /*align slack*/ + (size_t)Cfg<EPI>::kStages * (kStageA + kStageB) +
@@ -98,12 +102,20 @@ struct TcParams {
   long long wait_cycles;  // bound of each barrier wait (kWaitCycles)
   int withhold;        // self-test of the give-up path only: the producer
                        // issues no loads, so every consumer wait runs out
+  // split K (EPI 4): work unit u = tile u % tiles over the K blocks
+  // [s kb_per, (s + 1) kb_per) of split s = u / tiles, whose raw fp32
+  // product goes to slab s (part + s part_stride, column-major, part_ld);
+  // ksplit = 1, kb_per = kb_count otherwise
+  int ksplit, kb_per;
+  float* part;
+  int64_t part_ld, part_stride;
 };
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
 // EPI  0: C loaded/stored by the epilogue threads; 1: TMA reduce-add;
 //      2: as 0 with C stored in fp16 (C + alpha * acc in fp32, rounded once
-//         to fp16; p.C then points at __half).
+//         to fp16; p.C then points at __half); 3: C streamed by TMA;
+//      4: split K, the raw accumulator stored to the unit's slab.
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
@@ -129,9 +141,11 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
 
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
+  // work units: tiles, times the K splits (unit == tile when ksplit == 1)
   const int num_tiles = p.tiles_m * p.tiles_n;
+  const int num_units = num_tiles * p.ksplit;
   const int t_begin = p.tiles_per_cta > 0 ? (int)blockIdx.x * p.tiles_per_cta : (int)blockIdx.x;
-  const int t_end = p.tiles_per_cta > 0 ? min(num_tiles, t_begin + p.tiles_per_cta) : num_tiles;
+  const int t_end = p.tiles_per_cta > 0 ? min(num_units, t_begin + p.tiles_per_cta) : num_units;
   const int t_step = p.tiles_per_cta > 0 ? 1 : (int)gridDim.x;
 
   if (threadIdx.x == 0) {
@@ -166,9 +180,12 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       uint32_t ph = 0;
       bool ok = !p.withhold;
       int armed = 0;
-      for (int tile = t_begin; tile < t_end && ok; tile += t_step) {
+      for (int unit = t_begin; unit < t_end && ok; unit += t_step) {
+        const int tile = unit % num_tiles;
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
-        for (int kb = 0; kb < p.kb_count; ++kb) {
+        const int kb0 = (unit / num_tiles) * p.kb_per;
+        const int kb1 = min(p.kb_count, kb0 + p.kb_per);
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
             ok = false;
             break;
@@ -204,16 +221,18 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       int local = 0;
       bool ok = true;
       bool issued = false;
-      for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
+      for (int unit = t_begin; unit < t_end && ok; unit += t_step, ++local) {
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
+        const int kb0 = (unit / num_tiles) * p.kb_per;
+        const int kb1 = min(p.kb_count, kb0 + p.kb_per);
         if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty, p.wait_cycles)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + acc * BN;
-        for (int kb = 0; kb < p.kb_count; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull, p.wait_cycles)) {
             ok = false;
             break;
@@ -226,7 +245,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
           for (int k = 0; k < 4; ++k) {  // 4 MMAs of 32 bytes of K each
             const uint64_t ad = sw128_kmajor_desc(a0 + k * 32);
             const uint64_t bd = sw128_kmajor_desc(b0 + k * 32);
-            const uint32_t accum = (kb > 0 || k > 0) ? 1u : 0u;
+            const uint32_t accum = (kb > kb0 || k > 0) ? 1u : 0u;
             if (KIND == 0) mma_f16(d_tmem, ad, bd, idesc, accum);
             else mma_f8(d_tmem, ad, bd, idesc, accum);
           }
@@ -396,7 +415,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
       __syncwarp();
     } else {
       using CT = typename std::conditional<EPI == 2, __half, float>::type;
-      for (int tile = t_begin; tile < t_end && ok; tile += t_step, ++local) {
+      for (int unit = t_begin; unit < t_end && ok; unit += t_step, ++local) {
+        const int tile = unit % num_tiles;
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
@@ -405,13 +425,16 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         const int col0 = tn * BN + half * 128;
         float sa = 1.0f;
         if (p.scale_a) sa = ldexpf(1.0f, -p.scale_a[tm]);
-        const int64_t ldc = p.ldc;
-        CT* cbase = reinterpret_cast<CT*>(p.C) + row + (int64_t)col0 * ldc;
+        // EPI 4: the unit's slab instead of C, nothing loaded
+        const int64_t ldc = EPI == 4 ? p.part_ld : p.ldc;
+        CT* cbase = (EPI == 4 ? reinterpret_cast<CT*>(p.part + (unit / num_tiles) * p.part_stride)
+                              : reinterpret_cast<CT*>(p.C)) +
+                    row + (int64_t)col0 * ldc;
         float cv[32];
         // load the first chunk of C before waiting for the accumulator
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-          cv[j] = (row_ok && col0 + j < p.N) ? to_f32(cbase[j * ldc]) : 0.0f;
+          cv[j] = (EPI != 4 && row_ok && col0 + j < p.N) ? to_f32(cbase[j * ldc]) : 0.0f;
         if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) {
           ok = false;
           break;
@@ -421,7 +444,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         for (int c = 0; c < 4; ++c) {
           CT* cp = cbase + (int64_t)(c * 32) * ldc;
           const int cc = col0 + c * 32;
-          if (c > 0) {
+          if (EPI != 4 && c > 0) {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
               cv[j] = (row_ok && cc + j < p.N) ? to_f32(cp[j * ldc]) : 0.0f;
@@ -434,8 +457,12 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
           float s = p.alpha * sa;
           if (p.scale_b) s = ldexpf(s, -p.scale_b[cc / 128]);
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (row_ok && cc + j < p.N) cp[j * ldc] = from_f32<CT>(__fmaf_rn(s, av[j], cv[j]));
+          for (int j = 0; j < 32; ++j) {
+            if (row_ok && cc + j < p.N) {
+              if (EPI == 4) cp[j * ldc] = from_f32<CT>(av[j]);
+              else cp[j * ldc] = from_f32<CT>(__fmaf_rn(s, av[j], cv[j]));
+            }
+          }
         }
         tc_fence_before();
         __syncwarp();
@@ -519,7 +546,7 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                          int* err, int max_ctas, int tiles_per_cta,
                          long long wait_cycles = 0, int withhold = 0,
                          const void* A2 = nullptr, const void* B2 = nullptr,
-                         int64_t K2 = 0) {
+                         int64_t K2 = 0, int ksplit = 1, float* part = nullptr) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
   if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
   const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
@@ -563,14 +590,29 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   p.tiles_per_cta = tiles_per_cta;
   p.wait_cycles = wait_cycles > 0 ? wait_cycles : sm100::kWaitCycles;
   p.withhold = withhold ? 1 : 0;
-  const int tiles = p.tiles_m * p.tiles_n;
+  // split K: every split non-empty, one unit per CTA (the block scheduler
+  // then interleaves concurrent launches' units)
+  p.kb_per = p.kb_count;
+  p.ksplit = 1;
+  p.part = nullptr;
+  p.part_ld = p.part_stride = 0;
+  if (part) {
+    if (ksplit < 1 || A2 || scale_a || scale_b || c_half) return LU_ERR_INVALID_ARG;
+    p.kb_per = (int)ceil_div(p.kb_count, ksplit);
+    p.ksplit = (int)ceil_div(p.kb_count, p.kb_per);
+    p.part = part;
+    p.part_ld = (M + 3) / 4 * 4;
+    p.part_stride = p.part_ld * N;
+    tiles_per_cta = 1;
+  }
+  const int tiles = p.tiles_m * p.tiles_n * p.ksplit;
   const int grid = tiles_per_cta > 0
                        ? (int)ceil_div(tiles, tiles_per_cta)
                        : std::min(tiles, max_ctas > 0 ? max_ctas : sm_count());
   // TMA reduce-add needs a 16-byte aligned C with a 16-byte multiple stride
   CUtensorMap mc;
   std::memset(&mc, 0, sizeof(mc));
-  const bool tma_c = !c_half && ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) &&
+  const bool tma_c = !part && !c_half && ((uintptr_t)C % 16 == 0) && (ldc % 4 == 0) &&
                      make_c_map(&mc, static_cast<float*>(C), M, N, ldc);
   // C epilogue: CTAs that stay for many tiles stream C by TMA load / store,
   // its loads running ahead of the accumulator (B200, 16128^2 x 256:
@@ -584,7 +626,11 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   const bool stream_c = (tiles_per_cta <= 0 || tiles_per_cta > 2) && p.kb_count <= 4;
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
-  if (c_half) {
+  if (part) {
+    if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+    LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 4>, smem_bytes<4>()));
+    tc_update_kernel<0, 4><<<grid, kThreads, smem_bytes<4>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+  } else if (c_half) {
     if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
     LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 2>, smem_bytes<2>()));
     tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
@@ -640,6 +686,73 @@ lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t
                              int* err) {
   return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, true, ldc,
                         nullptr, nullptr, err, 0, 0);
+}
+
+// C = rn(C + alpha * (part_0 + part_1 + ... + part_{S-1})), the partial
+// sums added in split order (deterministic), the product scaled and added
+// with one fma as in the unsplit epilogue; shadow (if given) receives the
+// stored value widened to fp32.
+template <typename CT>
+__global__ void __launch_bounds__(256)
+splitk_finish_kernel(int64_t M, int S, const float* __restrict__ part, int64_t part_ld,
+                     int64_t part_stride, float alpha, CT* __restrict__ C, int64_t ldc,
+                     float* __restrict__ shadow, int64_t lds) {
+  const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  const int64_t j = blockIdx.y;
+  if (i >= M) return;
+  const float* q = part + i + j * part_ld;
+  float t = q[0];
+  for (int s = 1; s < S; ++s) t = __fadd_rn(t, q[s * part_stride]);
+  CT& c = C[i + j * ldc];
+  const CT v = from_f32<CT>(__fmaf_rn(alpha, t, to_f32(c)));
+  c = v;
+  if (shadow) shadow[i + j * lds] = to_f32(v);
+}
+
+lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                 int64_t K, float alpha, const void* A, int64_t lda_p,
+                                 const void* B, int64_t ldb_p, void* C, bool c_half,
+                                 int64_t ldc, float* shadow, int64_t lds, int ksplit,
+                                 float* part, int* err) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
+  if (!part || ksplit < 1 || N > 65535 || (shadow && lds < M)) return LU_ERR_INVALID_ARG;
+  LUB_TRY(tc_update_impl(st, kind, M, N, K, 1.0f, A, lda_p, B, ldb_p, nullptr, false, M,
+                         nullptr, nullptr, err, 0, 0, 0, 0, nullptr, nullptr, 0, ksplit,
+                         part));
+  const int esize = tc_operand_bytes(kind);
+  const int kb = (int)ceil_div(K * esize, kRowBytes);
+  const int per = (int)ceil_div(kb, ksplit);
+  const int S = (int)ceil_div(kb, per);
+  const int64_t pld = (M + 3) / 4 * 4;
+  dim3 grid((unsigned)ceil_div(M, 256), (unsigned)N);
+  if (c_half)
+    splitk_finish_kernel<__half><<<grid, 256, 0, st>>>(M, S, part, pld, pld * N, alpha,
+                                                        static_cast<__half*>(C), ldc, shadow,
+                                                        lds);
+  else
+    splitk_finish_kernel<float><<<grid, 256, 0, st>>>(M, S, part, pld, pld * N, alpha,
+                                                       static_cast<float*>(C), ldc, shadow,
+                                                       lds);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+int tc_split_choice(int64_t tiles, int64_t K, int esize, int sms, int smax) {
+  const int64_t kb = ceil_div(K * esize, kRowBytes);
+  int best = 1;
+  double best_t = 0.0;
+  for (int s = 1; s <= smax; ++s) {
+    const int64_t per = ceil_div(kb, (int64_t)s);
+    if (s > 1 && per < 4) break;  // at least K = 256 (fp16) per split
+    const int64_t waves = ceil_div(tiles * s, (int64_t)sms);
+    // a split costs a little extra (the partial written and summed)
+    const double t = (double)waves * (double)per * (1.0 + 0.02 * (s - 1));
+    if (s == 1 || t < best_t) {
+      best = s;
+      best_t = t;
+    }
+  }
+  return best;
 }
 
 lu_status launch_tc_update_withheld(cudaStream_t st, int64_t M, int64_t N, int64_t K,

@@ -373,21 +373,67 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
     const int tw = min(8, w - t0);
     if (t0 > 0) {
       // (a) tile column: rows [t0, w) x cols [t0, t0+tw); tile row: rows
-      // [t0, t0+tw) x cols [t0+tw, w)
-      const int ncol = (w - t0) * tw;
-      const int nrow = tw * (w - t0 - tw);
-      for (int e = tid; e < ncol + nrow; e += kThreads) {
-        int i, c;
-        if (e < ncol) { i = t0 + e % (w - t0); c = t0 + e / (w - t0); }
-        else { const int f = e - ncol; i = t0 + f % tw; c = t0 + tw + f / tw; }
-        float acc = 0.0f;
-        for (int k = 0; k < t0; ++k) acc = __fmaf_rn(D[i + k * LD], D[k + c * LD], acc);
-        D[i + c * LD] = __fsub_rn(D[i + c * LD], acc);
+      // [t0, t0+tw) x cols [t0+tw, w).  Items of 4 rows x 2 columns (tile
+      // column) or 4 rows x 1 column (tile row), K walked 4 at a time with
+      // 16-byte reads of L (4 rows of column k) and U (4 k of column c);
+      // every element's sum still runs k = 0, 1, ..., t0 - 1 in order.
+      const int RG = (w + 3) >> 2;  // 4-row groups (rows >= w never stored)
+      const int g0 = t0 >> 2;
+      const int ncg = RG - g0;
+      const int nci = ncg * ((tw + 1) >> 1);
+      const int nri = 2 * (w - t0 - tw);  // tw == 8 whenever this is > 0
+      for (int e = tid; e < nci + nri; e += kThreads) {
+        int i0, c, nc;
+        if (e < nci) {
+          i0 = 4 * (g0 + e % ncg);
+          c = t0 + 2 * (e / ncg);
+          nc = min(2, t0 + tw - c);
+        } else {
+          const int f = e - nci;
+          i0 = t0 + 4 * (f & 1);
+          c = t0 + tw + (f >> 1);
+          nc = 1;
+        }
+        float acc0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, acc1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const float* U0 = D + (size_t)c * LD;
+        const float* U1 = D + (size_t)(nc > 1 ? c + 1 : c) * LD;
+        for (int k = 0; k < t0; k += 4) {
+          float l[4][4];
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const float4 v = *reinterpret_cast<const float4*>(D + i0 + (size_t)(k + kk) * LD);
+            l[kk][0] = v.x; l[kk][1] = v.y; l[kk][2] = v.z; l[kk][3] = v.w;
+          }
+          const float4 a4 = *reinterpret_cast<const float4*>(U0 + k);
+          const float4 b4 = *reinterpret_cast<const float4*>(U1 + k);
+          const float u0[4] = {a4.x, a4.y, a4.z, a4.w};
+          const float u1[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              acc0[r] = __fmaf_rn(l[kk][r], u0[kk], acc0[r]);
+              acc1[r] = __fmaf_rn(l[kk][r], u1[kk], acc1[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (i0 + r < w) {
+            float* p0 = D + (i0 + r) + (size_t)c * LD;
+            *p0 = __fsub_rn(*p0, acc0[r]);
+            if (nc > 1) {
+              float* p1 = p0 + LD;
+              *p1 = __fsub_rn(*p1, acc1[r]);
+            }
+          }
+        }
       }
       __syncthreads();
     }
-    // (b) factor the tile
-    if (tid == 0) factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
+    // (b) factor the tile (in registers when its pivots are in the fast
+    // reciprocal's range, else the exact path that also reports them)
+    if (tid == 0 && !(tw == 8 && factor_tile8_fast(D + t0 + t0 * LD, LD, inv)))
+      factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
     __syncthreads();
     const int s = w - t0 - tw;
     if (s <= 0) break;

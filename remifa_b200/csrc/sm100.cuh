@@ -50,21 +50,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity.  On timeout sets *err
-// (first error wins) and returns false; also returns false at once when
-// another role has set *err.  `limit` (cycles) is kWaitCycles except in the
-// library's self-test of the give-up path.
+// (first error wins) and returns false; also returns false when another
+// role has set *err.  `limit` (cycles) is kWaitCycles except in the
+// library's self-test of the give-up path.  The clock and the error word (a
+// global load, hundreds of cycles) are looked at every 64th poll only, so a
+// poll in progress when the phase completes is a try_wait, which returns at
+// once (B200: K = 512 update 0.404 ms against 0.413 checking every poll).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           int* err, int code,
                                           long long limit = kWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (true) {
+  for (int spins = 1;; ++spins) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > limit) {
-      if (err) atomicCAS(err, 0, code);
-      return false;
+    if ((spins & 63) == 0) {
+      if (clock64() - t0 > limit) {
+        if (err) atomicCAS(err, 0, code);
+        return false;
+      }
+      if (err && *((volatile int*)err) != 0) return false;  // another role gave up
     }
-    if (err && *((volatile int*)err) != 0) return false;  // another role gave up
   }
 }
 

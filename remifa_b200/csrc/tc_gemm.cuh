@@ -52,6 +52,25 @@ lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t
                              const void* B, int64_t ldb_p, __half* C, int64_t ldc,
                              int* err);
 
+// Split-K form of the update (unscaled fp16 / bf16 operands): the K blocks
+// are cut into ksplit near-equal ranges, each tile x range a work unit (one
+// CTA each, so concurrent launches share the SMs unit by unit) whose raw
+// fp32 product goes to its own slab of `part` (ksplit x round4(M) x N
+// floats); a second kernel adds the slabs in split order and stores
+// C = rn(C + alpha * sum) (fp16 when c_half), and the stored value widened
+// to fp32 into `shadow` (ld lds) when given.  The same result for every
+// run, whatever the scheduling.
+lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                 int64_t K, float alpha, const void* A, int64_t lda_p,
+                                 const void* B, int64_t ldb_p, void* C, bool c_half,
+                                 int64_t ldc, float* shadow, int64_t lds, int ksplit,
+                                 float* part, int* err);
+
+// Number of K splits (1..smax, at least K = 256 fp16 per split) that
+// minimises waves x K blocks per split for `tiles` 128 x 256 tiles on `sms`
+// SMs (tiles: all the tiles launched at the same time).
+int tc_split_choice(int64_t tiles, int64_t K, int esize, int sms, int smax);
+
 // Self-test of the give-up path: the same fp16 update with the TMA producer
 // issuing no loads and every barrier wait bounded by wait_cycles, so each
 // consumer wait runs out; the kernel records its code in *err, unwinds,

@@ -282,6 +282,24 @@ def test_lu_ll_fp32_vs_reference_gpu(built):
     assert e_m <= 4 * e_r and e_r <= 4 * e_m
 
 
+def test_lu_ll_tensor_core_split_k_repeatable(built):
+    """n = 4096, nb = 256 on fp32 storage: the later steps' K = ofs updates
+    run split along K; the partial sums are added in a fixed order, so the
+    factors are identical run to run."""
+    n, nb = 4096, 256
+    a = rb.gen_matrix(n, seed=32, kind=1, alpha=1.5)
+    runs = []
+    for _ in range(2):
+        d = rb.colmajor(a.clone())
+        info = rb.lu_nopiv_ll(d, nb=nb, outer=rb.TC32)
+        torch.cuda.synchronize()
+        assert int(info.item()) == 0
+        runs.append(d)
+    assert torch.equal(runs[0], runs[1])
+    fe = O.factor_error(to_host(a), to_host(runs[0]))
+    assert fe < 2e-4, fe
+
+
 @pytest.mark.parametrize("compute", [rb.TC32, rb.compute_type.TC32_BF16])
 def test_lu_ll_tensor_core(built, compute):
     n, nb = 1500, 128

@@ -95,3 +95,28 @@ def test_ll_f16_update_kinds(built):
         rb.lu_nopiv_ll(d, nb=nb, inner=inner, outer=outer)
         torch.cuda.synchronize()
         assert torch.equal(d, base), (inner, outer)
+
+
+@pytest.mark.parametrize("panel_fp32", [False, True])
+def test_ll_f16_split_k_repeatable(built, panel_fp32):
+    """n = 4096, nb = 256: the block-column and block-row updates of the later
+    steps are split along K (partial sums in per-split slabs, added in split
+    order), so two factorizations of the same matrix give identical factors,
+    and they stay within the fp16 tolerance of the oracle's restatement."""
+    n, nb = 4096, 256
+    a32 = rb.gen_matrix(n, seed=31, kind=1, alpha=1.5)
+    src = rb.colmajor_empty(n, n, n, torch.float16)
+    rb.convert(a32, src)
+    runs = []
+    for _ in range(2):
+        d = src.clone()
+        info = rb.lu_nopiv_ll(d, nb=nb, outer=rb.TC32, panel_fp32=panel_fp32)
+        torch.cuda.synchronize()
+        assert int(info.item()) == 0
+        runs.append(d)
+    assert torch.equal(runs[0], runs[1])
+    a = np.asfortranarray(src.float().cpu().numpy())
+    got = np.asfortranarray(runs[0].float().cpu().numpy())
+    want = O.lu_ll(a, nb=nb, fp16_storage=True, panel_fp32=panel_fp32)
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel < 8 * 2.0 ** -11, rel

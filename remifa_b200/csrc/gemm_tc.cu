@@ -32,6 +32,7 @@
 #include "sm100.cuh"
 #include "tc_gemm.cuh"
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -480,6 +481,216 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair form for the large passes (fp16 / bf16 operands, fp32 C updated
+// by TMA reduce-add): a cluster of two CTAs owns 256 x 256 tiles, and the
+// even CTA issues tcgen05.mma.cta_group::2 (M = 256, N = 256) over both.
+// Each CTA stages its own 128 rows of A and 128 columns of B per K block
+// (32 KB, where a 128 x 256 tile alone needs 48 KB), so B crosses from L2
+// once per 256 rows and five stages fit beside the epilogue buffers.  Both
+// CTAs' copies count their bytes on the even CTA's `full` barrier; its
+// commits arrive on the `empty` / `tfull` barriers of both CTAs; each CTA's
+// epilogue reads its own accumulator rows and arrives on the even CTA's
+// `tempty`.  Every element's products are accumulated in the same K order
+// as by the single-CTA kernel.  No multicast loads: each CTA loads only
+// what it stages itself.
+constexpr int kPairRows = 128;                   // rows of A / columns of B per CTA
+constexpr int kPairStage = kPairRows * kRowBytes;  // 16 KB each for A and B
+constexpr int kPairStages = 5;
+constexpr size_t kPairEpiBytes = (size_t)kEpiWarps * 2 * kEpiChunk;
+constexpr size_t pair_smem_bytes() {
+  return 1024 + (size_t)kPairStages * 2 * kPairStage + kPairEpiBytes + 512;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+tc_update_pair_kernel(const __grid_constant__ CUtensorMap tmap_a,
+                      const __grid_constant__ CUtensorMap tmap_b,
+                      const __grid_constant__ CUtensorMap tmap_a2,
+                      const __grid_constant__ CUtensorMap tmap_b2,
+                      const __grid_constant__ CUtensorMap tmap_c, TcParams p,
+                      uint32_t idesc) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + kPairStages * kPairStage;
+  uint8_t* sEpi = sB + kPairStages * kPairStage;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sEpi + kPairEpiBytes);
+  uint64_t* empty = full + kPairStages;
+  uint64_t* tfull = empty + kPairStages;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int num_tiles = p.tiles_m * p.tiles_n;  // 256 x 256 tiles
+  const int pair = (int)blockIdx.x >> 1;
+  const int npairs = (int)gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kPairStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 2 * kEpiWarps);  // both CTAs' epilogue warps
+    }
+    mbar_init(drain, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc_pair(tmem_slot, kTmemCols);
+  tc_fence_before();
+  cluster_sync();  // both CTAs' barriers initialised and tensor memory allocated
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      prefetch_tmap(&tmap_a);
+      prefetch_tmap(&tmap_b);
+      if (p.kb_split < p.kb_count) {
+        prefetch_tmap(&tmap_a2);
+        prefetch_tmap(&tmap_b2);
+      }
+      const uint32_t full0 = cluster_addr(&full[0], 0);  // the even CTA's barriers
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      int armed = 0;
+      for (int tile = pair; tile < num_tiles && ok; tile += npairs) {
+        const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        for (int kb = 0; kb < p.kb_count; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
+            ok = false;
+            break;
+          }
+          if (leader) mbar_arrive_expect_tx(&full[s], 4 * kPairStage);
+          const bool second = kb >= p.kb_split;
+          const int kelem = (second ? kb - p.kb_split : kb) * (kRowBytes / 2);
+          const uint32_t bar = full0 + (uint32_t)(s * sizeof(uint64_t));
+          tma_load_2d_pair(sA + s * kPairStage, second ? &tmap_a2 : &tmap_a, bar, kelem,
+                           tm * 2 * kPairRows + (int)rank * kPairRows);
+          tma_load_2d_pair(sB + s * kPairStage, second ? &tmap_b2 : &tmap_b, bar, kelem,
+                           tn * 2 * kPairRows + (int)rank * kPairRows);
+          ++armed;
+          if (++s == kPairStages) { s = 0; ph ^= 1; }
+        }
+      }
+      if (!ok && leader) {
+        // the last stages' copies (both CTAs', counted here) must land
+        // before this CTA's shared memory goes away
+        int ss = s;
+        uint32_t pp = ph;
+        for (int j = 0; j < kPairStages && j < armed; ++j) {
+          if (ss == 0) { ss = kPairStages - 1; pp ^= 1; } else { --ss; }
+          mbar_drain(&full[ss], pp);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (even CTA) ----------------
+    if (lane == 0 && leader) {
+      int s = 0;
+      uint32_t ph = 0;
+      int local = 0;
+      bool ok = true;
+      bool issued = false;
+      for (int tile = pair; tile < num_tiles && ok; tile += npairs, ++local) {
+        const int acc = local & 1;
+        const uint32_t aph = (local >> 1) & 1;
+        if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty, p.wait_cycles)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + acc * BN;
+        for (int kb = 0; kb < p.kb_count; ++kb) {
+          if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull, p.wait_cycles)) {
+            ok = false;
+            break;
+          }
+          issued = true;
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * kPairStage);
+          const uint32_t b0 = smem_u32(sB + s * kPairStage);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            mma_f16_pair(d_tmem, sw128_kmajor_desc(a0 + k * 32), sw128_kmajor_desc(b0 + k * 32),
+                         idesc, (kb > 0 || k > 0) ? 1u : 0u);
+          mma_commit_pair(&empty[s]);  // frees stage s in both CTAs
+          if (++s == kPairStages) { s = 0; ph ^= 1; }
+        }
+        if (ok) mma_commit_pair(&tfull[acc]);
+      }
+      if (!ok && issued) {
+        mma_commit_pair(drain);
+        mbar_drain(drain, 0);
+      }
+    }
+  } else {
+    // ---------------- epilogue (both CTAs): TMA reduce-add ----------------
+    const int ew = warp - 2;
+    const int quarter = warp & 3;
+    const int half = ew / 4;
+    const uint32_t tempty0 = cluster_addr(&tempty[0], 0);
+    float* stage = reinterpret_cast<float*>(sEpi + (size_t)ew * 2 * kEpiChunk);
+    int issued = 0;
+    int local = 0;
+    for (int tile = pair; tile < num_tiles; tile += npairs, ++local) {
+      const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+      const int acc = local & 1;
+      const uint32_t aph = (local >> 1) & 1;
+      const int row0 = tm * 2 * kPairRows + (int)rank * kPairRows + quarter * 32;
+      const int col0 = tn * BN + half * 128;
+      if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int c = 0; c < 4; ++c) {
+        const int cc = col0 + c * 32;
+        float av[32];
+        tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                      (uint32_t)(acc * BN + half * 128 + c * 32),
+                  av);
+        tmem_ld_wait();
+        if (c == 3) {  // accumulator read out: hand it back to the even CTA
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0)
+            mbar_arrive_cluster(tempty0 + (uint32_t)(acc * sizeof(uint64_t)));
+        }
+        if (cc >= p.N || row0 >= p.M) continue;
+        float* buf = stage + (issued & 1) * (kEpiChunk / 4);
+        if (lane == 0) bulk_wait_group_read<1>();
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) buf[j * 32 + lane] = p.alpha * av[j];
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          tma_reduce_add_2d(&tmap_c, buf, row0, cc);
+          bulk_commit_group();
+        }
+        ++issued;
+      }
+    }
+    if (lane == 0) bulk_wait_group<0>();
+    __syncwarp();
+  }
+
+  __syncwarp();
+  tc_fence_before();
+  cluster_sync();  // the peer has finished: no arrivals or copies into this CTA remain
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, kTmemCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side: tensor maps through the driver entry point (no -lcuda)
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
@@ -539,6 +750,9 @@ bool make_kmajor_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
 }  // namespace
 
 namespace {
+// persistent passes of at least this many 128 x 256 tiles run as CTA pairs
+constexpr int kPairMinTiles = 2 * 148;
+
 lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                          int64_t K, float alpha, const void* A, int64_t lda_p,
                          const void* B, int64_t ldb_p, void* C, bool c_half,
@@ -624,6 +838,15 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   // epilogue's smaller shared-memory footprint leaves room for a third
   // operand stage: 15360^2 x 512, 0.408 ms against 0.457 streaming C.
   const bool stream_c = (tiles_per_cta <= 0 || tiles_per_cta > 2) && p.kb_count <= 4;
+  // large persistent passes with unscaled 16-bit operands and K >= 512:
+  // CTA pairs (B200, 15360^2: K = 1024 0.473 ms against 0.563, K = 512 in
+  // the factorization's bulk passes 2-3% faster; at K = 256 the streaming
+  // epilogue of the single-CTA kernel wins, 0.375 against 0.474 ms)
+  if (tma_c && !part && tiles_per_cta <= 0 && !withhold && !scale_a && !scale_b &&
+      (kind == TcOperand::F16 || kind == TcOperand::BF16) && tiles >= kPairMinTiles &&
+      p.kb_count >= 8)
+    return launch_tc_update_pair(st, kind, M, N, K, A, lda_p, B, ldb_p, K2, A2, B2,
+                                 static_cast<float*>(C), ldc, alpha, err, max_ctas);
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
   if (part) {
@@ -678,6 +901,91 @@ lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t 
   if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
   return tc_update_impl(st, kind, M, N, K, -1.0f, A, ld_p, B, ld_p, C, false, ldc, nullptr,
                         nullptr, err, max_ctas, tiles_per_cta, 0, 0, A2, B2, K2);
+}
+
+// Clusters of two tc_update_pair_kernel CTAs resident at once on this
+// device (cached per device; 0 if the query fails).
+static int pair_capacity() {
+  static int cache[64];
+  static std::once_flag once[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  std::call_once(once[dev], [dev] {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(2 * 148, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = pair_smem_bytes();
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (const void*)tc_update_pair_kernel, &cfg) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    cache[dev] = n;
+  });
+  return cache[dev];
+}
+
+lu_status launch_tc_update_pair(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                int64_t K, const void* A, int64_t lda_p, const void* B,
+                                int64_t ldb_p, int64_t K2, const void* A2, const void* B2,
+                                float* C, int64_t ldc, float alpha, int* err, int max_ctas) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
+  if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+  if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX || K2 < 0 || K2 > INT32_MAX)
+    return LU_ERR_INVALID_ARG;
+  if ((lda_p * 2) % 16 != 0 || (ldb_p * 2) % 16 != 0 || (uintptr_t)A % 16 != 0 ||
+      (uintptr_t)B % 16 != 0 || lda_p < K || ldb_p < K || lda_p < K2 || ldb_p < K2 ||
+      (K2 > 0 && (!A2 || !B2 || (uintptr_t)A2 % 16 != 0 || (uintptr_t)B2 % 16 != 0)))
+    return LU_ERR_INVALID_ARG;
+  if ((uintptr_t)C % 16 != 0 || ldc % 4 != 0) return LU_ERR_INVALID_ARG;  // TMA reduce-add
+  const CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  CUtensorMap ma, mb, ma2, mb2, mc;
+  if (!make_kmajor_map(&ma, A, dt, 2, K, M, lda_p, kPairRows) ||
+      !make_kmajor_map(&mb, B, dt, 2, K, N, ldb_p, kPairRows))
+    return LU_ERR_CUDA;
+  if (K2 > 0) {
+    if (!make_kmajor_map(&ma2, A2, dt, 2, K2, M, lda_p, kPairRows) ||
+        !make_kmajor_map(&mb2, B2, dt, 2, K2, N, ldb_p, kPairRows))
+      return LU_ERR_CUDA;
+  } else {
+    ma2 = ma;
+    mb2 = mb;
+  }
+  if (!make_c_map(&mc, C, M, N, ldc)) return LU_ERR_CUDA;
+  TcParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.C = C;
+  p.ldc = ldc;
+  p.M = (int)M;
+  p.N = (int)N;
+  p.K = (int)K;
+  p.kb_split = (int)ceil_div(K * 2, kRowBytes);
+  p.kb_count = p.kb_split + (K2 > 0 ? (int)ceil_div(K2 * 2, kRowBytes) : 0);
+  p.tiles_m = (int)ceil_div(M, 2 * kPairRows);
+  p.tiles_n = (int)ceil_div(N, BN);
+  p.alpha = alpha;
+  p.err = err;
+  p.wait_cycles = sm100::kWaitCycles;
+  p.ksplit = 1;
+  p.kb_per = p.kb_count;
+  const int tiles = p.tiles_m * p.tiles_n;
+  LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_pair_kernel, pair_smem_bytes()));
+  // never more pairs than can be resident at once (SM pairs sit inside one
+  // GPC, so an odd SM per GPC stays out): a pair scheduled late would run
+  // its whole share of the tiles after the others
+  const int resident = pair_capacity();
+  if (resident < 1) return LU_ERR_UNSUPPORTED;
+  const int pairs =
+      std::max(1, std::min({tiles, (max_ctas > 0 ? max_ctas : sm_count()) / 2, resident}));
+  const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
+  const uint32_t idesc = sm100::make_idesc(f, f, 2 * kPairRows, BN);
+  tc_update_pair_kernel<<<2 * pairs, kThreads, pair_smem_bytes(), st>>>(ma, mb, ma2, mb2, mc, p,
+                                                                         idesc);
+  LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
 }
 
 lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,

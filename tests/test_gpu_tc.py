@@ -154,6 +154,34 @@ def test_tc_update_repeated_calls_consistent(built):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
+@pytest.mark.parametrize("m,n,k,compute", [(4096, 4096, 512, rb.TC32),
+                                           (3000, 3100, 1000, rb.TC32),
+                                           (4352, 4100, 768, rb.compute_type.TC32_BF16)])
+def test_pair_update_matches_single_cta(built, m, n, k, compute):
+    """A pass of at least 296 tiles of 128 x 256 with K >= 512 runs as CTA
+    pairs (tcgen05 cta_group::2, 256 x 256 tiles); the same product cut into 256-column
+    slices (too few tiles for pairs) runs on the single-CTA kernel.  Every
+    element's sum runs over K in the same order in both, so the results are
+    the same bits; they also meet the rounded-operand bound."""
+    rng = np.random.default_rng(m + k)
+    A = np.asfortranarray(rng.standard_normal((m, k)).astype(np.float32))
+    B = np.asfortranarray(rng.standard_normal((k, n)).astype(np.float32))
+    C = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    dA, dB = to_dev(A), to_dev(B)
+    whole, sliced = to_dev(C), to_dev(C)
+    rb.gemmex(compute, -1.0, dA, dB, 1.0, whole)
+    for j in range(0, n, 256):
+        rb.gemmex(compute, -1.0, dA, dB[:, j:j + 256], 1.0, sliced[:, j:j + 256])
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(to_host(whole), to_host(sliced))
+    fmt = O.FMT_FP16 if compute == rb.TC32 else O.FMT_BF16
+    Ar = O.round_fmt(A, fmt).astype(np.float64)
+    Br = O.round_fmt(B, fmt).astype(np.float64)
+    exact = C.astype(np.float64) - Ar @ Br
+    err = np.abs(to_host(whole) - exact)
+    assert np.all(err <= 2.0 ** -22 * k * (np.abs(Ar) @ np.abs(Br)) + 2 * U32 * np.abs(exact))
+
+
 @pytest.mark.parametrize("n,nb,compute,fmt", [(512, 128, rb.TC32, O.FMT_FP16),
                                               (1000, 256, rb.TC32, O.FMT_FP16),
                                               (768, 128, rb.compute_type.TC32_BF16, O.FMT_BF16),

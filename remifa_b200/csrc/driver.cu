@@ -195,7 +195,7 @@ struct DevStreams {
   cudaEvent_t copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
-  cudaEvent_t done_with[4] = {nullptr, nullptr, nullptr, nullptr};  // U2 done reading buffer b
+  cudaEvent_t done_with[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // U2 done reading buffer b
 };
 
 static lu_status dev_streams(DevStreams** out) {
@@ -225,7 +225,7 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
                            &d.done_with[0], &d.done_with[1], &d.done_with[2],
-                           &d.done_with[3], &d.copied,
+                           &d.done_with[3], &d.done_with[4], &d.done_with[5], &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
                            &d.u1_done, &d.join_s,
                            &d.spack_done})
@@ -276,6 +276,11 @@ static size_t ll_part_layout(Plan* p, size_t off) {
   p->part_bytes = align_up((size_t)kLlSplitMax * slab * 4, 1024);
   return off + 2 * p->part_bytes;
 }
+
+// Outer steps whose bulk trailing updates share one pass by default: the
+// pass then has K = 4 nb = 1024 (AI 256 flop/B of C traffic, where the
+// CTA-pair update reaches ~1 PFLOP/s on B200).
+constexpr int kBulkSteps = 4;
 
 lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
                     Plan* p) {
@@ -353,20 +358,22 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     p->ws_bytes = off;
     return LU_SUCCESS;
   }
-  // two outer steps per bulk pass (look-ahead, unscaled fp16 / bf16
-  // operands): bulk_steps 0 (default) or 2; 1 keeps one pass per step
-  p->bulk_pair = is_tc(p->outer) && !tc_scaled(tc_kind(p->outer)) && p->lookahead &&
-                 o.bulk_steps != 1;
-  if (o.bulk_steps < 0 || o.bulk_steps > 2) return LU_ERR_INVALID_ARG;
+  // several outer steps per bulk pass (look-ahead, unscaled fp16 / bf16
+  // operands): bulk_steps 0 (default: kBulkSteps) or 2..4; 1 keeps one pass
+  // per step
+  if (o.bulk_steps < 0 || o.bulk_steps > 4) return LU_ERR_INVALID_ARG;
+  const bool grouping = is_tc(p->outer) && !tc_scaled(tc_kind(p->outer)) && p->lookahead;
+  p->bulk_group = grouping ? (o.bulk_steps == 0 ? kBulkSteps : o.bulk_steps) : 1;
+  p->bulk_pair = p->bulk_group >= 2;
   if (is_tc(p->outer) && n > p->nb) {
     // three operand buffers: with look-ahead the panel of step k writes its
     // copies while the bulk updates of steps k-1 and k-2 still read theirs;
-    // a fourth when two steps share a bulk pass (it reads step k's copies
-    // until the panels of steps k+2 and k+3 are done)
+    // q + 2 when q steps share a bulk pass (it reads the group's copies
+    // until the panels of the next group's first two steps are done)
     const int64_t t = n - p->nb;
     TcWs w = tc_ws_layout(off, t, t, p->nb, tc_kind(p->outer));
     p->off_lcopy = w.off_a;
-    off += (p->bulk_pair ? 4 : 3) * w.bytes;
+    off += (p->bulk_group >= 2 ? p->bulk_group + 2 : 3) * w.bytes;
   }
   p->ws_bytes = off;
   return LU_SUCCESS;
@@ -578,11 +585,11 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t n = p.n, nb = p.nb;
   if (col_end < 0) col_end = n;
   const bool tc = is_tc(p.outer);
-  // two steps per bulk pass (the host entry's chunks too, restricted to
-  // their columns)
-  const bool pair = p.bulk_pair;
-  const int nbuf = p.bulk_pair ? 4 : 3;
-  TcWs w2[4];
+  // q steps per bulk pass (the host entry's chunks too, restricted to their
+  // columns)
+  const int q = p.bulk_group;
+  const int nbuf = q >= 2 ? q + 2 : 3;
+  TcWs w2[6];
   if (tc && n > nb) {
     w2[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
     const size_t shift = w2[0].bytes;
@@ -642,10 +649,13 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   };
   bool pre = false;       // this step's first diagonal block is already queued
   bool prev_deep = false; // the previous step ran the deep schedule
-  // a step whose bulk (rows and columns beyond its trailing origin + 3 nb)
-  // waits to be applied together with the next step's bulk
-  bool deferred = false;
-  int deferred_buf = 0;
+  // steps of the current group whose bulk (rows and columns beyond their
+  // trailing origin + 3 nb) waits to be applied together with later steps'
+  int ngrp = 0;
+  int grp_buf[4] = {0, 0, 0, 0};
+  int64_t grp_step[4] = {0, 0, 0, 0};
+  const int64_t ldk = tc && n > nb ? tc_packed_k(kind, nb) : 0;
+  const int64_t es = tc ? tc_operand_bytes(kind) : 0;
   // block column [ofs, ofs + in) is final once the panel work queued so far
   // on sp (and, with `side`, on ss) has run
   auto sink_column = [&](int64_t ofs, int64_t in, bool side) {
@@ -842,44 +852,62 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
         const int ctas = persist ? std::max(1, sm_count() * (t2b >= 2 * kU2bPersistTiles ? 3 : 2) /
                                                    (t2b >= 2 * kU2bPersistTiles ? 4 : 3))
                                  : 0;
-        // the next step will have a U2b of its own (its trailing part is
-        // one block smaller): defer to it
-        const bool defer = pair && !deferred && tr > 3 * nb && tcn > 3 * nb;
-        if (deferred) {
-          // rows / columns [2 nb, ...) of this step's trailing part = [3 nb,
-          // ...) of the deferred (previous) step's
-          const TcWs& wp = w2[deferred_buf];
-          const int64_t ldk = tc_packed_k(kind, nb);
-          const int64_t es = tc_operand_bytes(kind);
-          float* c = a + (ofs + nb + 2 * nb) + (ofs + nb + 2 * nb) * lda;
-          ProfScope ps("tc_update", su,
-                       8.0 * (tr - 2 * nb) * (tcn - 2 * nb) +
-                           2.0 * es * (tr - 2 * nb + tcn - 2 * nb) * nb,
-                       4.0 * (tr - 2 * nb) * (double)(tcn - 2 * nb) * nb);
-          status = launch_tc_update2(
-              su, kind, tr - 2 * nb, tcn - 2 * nb, nb, ws + wp.off_a + 3 * nb * ldk * es,
-              ws + wp.off_b + 3 * nb * ldk * es, nb, ws + wk.off_a + 2 * nb * ldk * es,
-              ws + wk.off_b + 2 * nb * ldk * es, ldk, c, lda, err, ctas, tiles);
-          if (status != LU_SUCCESS) break;
-          if (!ok(cudaEventRecord(S->done_with[deferred_buf], su))) break;
-          deferred = false;
-        } else if (defer) {
-          status = outer_update(p, su, a, lda, ofs, 2 * nb, nb, 2 * nb, tcn - 2 * nb, ws, wk,
-                                err, kU2Tiles);
+        // defer this step's bulk too while the group has room and the next
+        // step has a bulk region of its own (one block smaller)
+        const bool defer = q >= 2 && ngrp + 1 < q && tr > 3 * nb && tcn > 3 * nb;
+        // rows [r0, r0 + rows) x columns [c0, c0 + cols) of this step's
+        // trailing part -= the pending steps' products and this step's, in
+        // one pass: step j's copy of this step's trailing row / column x
+        // sits at x + (step - j) nb
+        auto group_update = [&](int64_t r0, int64_t rows, int64_t c0, int64_t cols,
+                                int tiles_, int ctas_) -> lu_status {
+          if (rows <= 0 || cols <= 0) return LU_SUCCESS;
+          int64_t ks[4];
+          const void* as[4];
+          const void* bs[4];
+          int ns = 0;
+          for (int g = 0; g <= ngrp; ++g) {
+            const bool own = g == ngrp;
+            const TcWs& wg = w2[own ? buf : grp_buf[g]];
+            const int64_t sh = own ? 0 : (step - grp_step[g]) * nb;
+            ks[ns] = nb;
+            as[ns] = ws + wg.off_a + (r0 + sh) * ldk * es;
+            bs[ns] = ws + wg.off_b + (c0 + sh) * ldk * es;
+            ++ns;
+          }
+          float* c = a + (ofs + nb + r0) + (ofs + nb + c0) * lda;
+          ProfScope ps("tc_update", su, 8.0 * rows * cols + (double)es * (rows + cols) * nb * ns,
+                       2.0 * rows * (double)cols * nb * ns);
+          return launch_tc_update_sets(su, kind, rows, cols, ns, ks, as, bs, ldk, c, lda, err,
+                                       ctas_, tiles_);
+        };
+        if (defer) {
+          // the block row and column at 2 nb get every pending product now;
+          // everything beyond waits for the group's pass
+          status = group_update(2 * nb, nb, 2 * nb, tcn - 2 * nb, kU2Tiles, 0);
           if (status == LU_SUCCESS)
-            status = outer_update(p, su, a, lda, ofs, 3 * nb, tr - 3 * nb, 2 * nb, nb, ws,
-                                  wk, err, kU2Tiles);
+            status = group_update(3 * nb, tr - 3 * nb, 2 * nb, nb, kU2Tiles, 0);
           if (status != LU_SUCCESS) break;
-          deferred = true;
-          deferred_buf = buf;
+          grp_buf[ngrp] = buf;
+          grp_step[ngrp] = step;
+          ++ngrp;
+        } else if (ngrp > 0) {
+          // the group's pass: rows / columns [2 nb, ...) of this step's
+          // trailing part with all of the group's products
+          status = group_update(2 * nb, tr - 2 * nb, 2 * nb, tcn - 2 * nb, tiles, ctas);
+          if (status != LU_SUCCESS) break;
+          for (int g = 0; g < ngrp; ++g)
+            if (!ok(cudaEventRecord(S->done_with[grp_buf[g]], su))) break;
+          if (status != LU_SUCCESS) break;
+          ngrp = 0;
         } else {
           status = outer_update(p, su, a, lda, ofs, 2 * nb, tr - 2 * nb, 2 * nb,
                                 tcn - 2 * nb, ws, wk, err, tiles, ctas);
           if (status != LU_SUCCESS) break;
         }
       }
-      if (!(deferred && deferred_buf == buf) && !ok(cudaEventRecord(S->done_with[buf], su)))
-        break;
+      const bool pending = ngrp > 0 && grp_buf[ngrp - 1] == buf && grp_step[ngrp - 1] == step;
+      if (!pending && !ok(cudaEventRecord(S->done_with[buf], su))) break;
     } else if (tr > 0 && tcn > 0) {
       cudaStream_t last = prev_deep ? ss : sp;
       if (!ok(cudaEventRecord(S->updated, last))) break;

@@ -20,7 +20,8 @@ struct Plan {
   bool lookahead = true;
   lu_dtype dtype = LU_F32;
   bool panel_fp32 = false;  // fp16 storage: block update kept in fp32
-  bool bulk_pair = false;   // two outer steps per bulk trailing-update pass
+  int bulk_group = 1;       // outer steps per bulk trailing-update pass (1..4)
+  bool bulk_pair = false;   // bulk_group >= 2 (the host entry's catch-up pairs steps)
   // workspace layout (byte offsets into one device allocation)
   size_t off_status = 0;    // int first_bad
   size_t off_lcopy = 0;     // low-precision L21 copy (row-major)

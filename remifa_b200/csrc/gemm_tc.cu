@@ -44,6 +44,7 @@ using namespace sm100;
 
 constexpr int BM = 128;
 constexpr int BN = 256;
+constexpr int kMaxSets = 4;  // operand sets summed in one pass
 constexpr int kRowBytes = 128;                  // bytes of K per tile row
 constexpr int kStageA = BM * kRowBytes;         // 16 KB
 constexpr int kStageB = BN * kRowBytes;         // 32 KB
@@ -85,14 +86,21 @@ template <typename T> __device__ __forceinline__ T from_f32(float x);
 template <> __device__ __forceinline__ float from_f32<float>(float x) { return x; }
 template <> __device__ __forceinline__ __half from_f32<__half>(float x) { return __float2half_rn(x); }
 
+// Tensor maps of up to kMaxSets operand sets (A row-major, B column-major,
+// both K-major), passed by value as one grid constant.
+struct TcMaps {
+  CUtensorMap a[kMaxSets];
+  CUtensorMap b[kMaxSets];
+};
+
 struct TcParams {
   float* C;
   int64_t ldc;
   int M, N, K;
-  int kb_count;        // number of BK blocks along K (both operand sets)
-  int kb_split;        // blocks [0, kb_split) come from (tmap_a, tmap_b), the
-                       // rest from (tmap_a2, tmap_b2): two outer steps' K = nb
-                       // products summed in one accumulator
+  int kb_count;        // number of BK blocks along K (all operand sets)
+  int nsets;           // operand sets (1..kMaxSets): set s supplies the K
+  int kb_end[kMaxSets];  // blocks [kb_end[s-1], kb_end[s]) from maps.a/b[s],
+                       // several outer steps' products summed in one accumulator
   int tiles_m, tiles_n;
   const int* scale_a;  // per 128-row tile of A (log2), or null
   const int* scale_b;  // per 128-column tile of B (log2), or null
@@ -119,10 +127,7 @@ struct TcParams {
 //      4: split K, the raw accumulator stored to the unit's slab.
 template <int KIND, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
-                 const __grid_constant__ CUtensorMap tmap_b,
-                 const __grid_constant__ CUtensorMap tmap_a2,
-                 const __grid_constant__ CUtensorMap tmap_b2,
+tc_update_kernel(const __grid_constant__ TcMaps maps,
                  const __grid_constant__ CUtensorMap tmap_c, TcParams p,
                  uint32_t idesc) {
   constexpr int kStages = Cfg<EPI>::kStages;
@@ -171,11 +176,9 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      prefetch_tmap(&tmap_a);
-      prefetch_tmap(&tmap_b);
-      if (p.kb_split < p.kb_count) {
-        prefetch_tmap(&tmap_a2);
-        prefetch_tmap(&tmap_b2);
+      for (int q = 0; q < p.nsets; ++q) {
+        prefetch_tmap(&maps.a[q]);
+        prefetch_tmap(&maps.b[q]);
       }
       int s = 0;
       uint32_t ph = 0;
@@ -186,18 +189,19 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmap_a,
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
         const int kb0 = (unit / num_tiles) * p.kb_per;
         const int kb1 = min(p.kb_count, kb0 + p.kb_per);
+        int set = 0;
         for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
             ok = false;
             break;
           }
           mbar_arrive_expect_tx(&full[s], kStageA + kStageB);
-          const bool second = kb >= p.kb_split;
-          const int kk = second ? kb - p.kb_split : kb;
+          while (kb >= p.kb_end[set]) ++set;
+          const int kk = kb - (set > 0 ? p.kb_end[set - 1] : 0);
           const int kx = kk * kRowBytes;  // element offset along K == bytes for 8-bit
           const int kelem = KIND == 0 ? kk * (kRowBytes / 2) : kx;
-          tma_load_2d(sA + s * kStageA, second ? &tmap_a2 : &tmap_a, &full[s], kelem, tm * BM);
-          tma_load_2d(sB + s * kStageB, second ? &tmap_b2 : &tmap_b, &full[s], kelem, tn * BN);
+          tma_load_2d(sA + s * kStageA, &maps.a[set], &full[s], kelem, tm * BM);
+          tma_load_2d(sB + s * kStageB, &maps.b[set], &full[s], kelem, tn * BN);
           ++armed;
           if (++s == kStages) { s = 0; ph ^= 1; }
         }
@@ -502,10 +506,7 @@ constexpr size_t pair_smem_bytes() {
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-tc_update_pair_kernel(const __grid_constant__ CUtensorMap tmap_a,
-                      const __grid_constant__ CUtensorMap tmap_b,
-                      const __grid_constant__ CUtensorMap tmap_a2,
-                      const __grid_constant__ CUtensorMap tmap_b2,
+tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
                       const __grid_constant__ CUtensorMap tmap_c, TcParams p,
                       uint32_t idesc) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -550,11 +551,9 @@ tc_update_pair_kernel(const __grid_constant__ CUtensorMap tmap_a,
   if (warp == 0) {
     // ---------------- TMA producer (both CTAs) ----------------
     if (lane == 0) {
-      prefetch_tmap(&tmap_a);
-      prefetch_tmap(&tmap_b);
-      if (p.kb_split < p.kb_count) {
-        prefetch_tmap(&tmap_a2);
-        prefetch_tmap(&tmap_b2);
+      for (int q = 0; q < p.nsets; ++q) {
+        prefetch_tmap(&maps.a[q]);
+        prefetch_tmap(&maps.b[q]);
       }
       const uint32_t full0 = cluster_addr(&full[0], 0);  // the even CTA's barriers
       int s = 0;
@@ -563,18 +562,19 @@ tc_update_pair_kernel(const __grid_constant__ CUtensorMap tmap_a,
       int armed = 0;
       for (int tile = pair; tile < num_tiles && ok; tile += npairs) {
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        int set = 0;
         for (int kb = 0; kb < p.kb_count; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
             ok = false;
             break;
           }
           if (leader) mbar_arrive_expect_tx(&full[s], 4 * kPairStage);
-          const bool second = kb >= p.kb_split;
-          const int kelem = (second ? kb - p.kb_split : kb) * (kRowBytes / 2);
+          while (kb >= p.kb_end[set]) ++set;
+          const int kelem = (kb - (set > 0 ? p.kb_end[set - 1] : 0)) * (kRowBytes / 2);
           const uint32_t bar = full0 + (uint32_t)(s * sizeof(uint64_t));
-          tma_load_2d_pair(sA + s * kPairStage, second ? &tmap_a2 : &tmap_a, bar, kelem,
+          tma_load_2d_pair(sA + s * kPairStage, &maps.a[set], bar, kelem,
                            tm * 2 * kPairRows + (int)rank * kPairRows);
-          tma_load_2d_pair(sB + s * kPairStage, second ? &tmap_b2 : &tmap_b, bar, kelem,
+          tma_load_2d_pair(sB + s * kPairStage, &maps.b[set], bar, kelem,
                            tn * 2 * kPairRows + (int)rank * kPairRows);
           ++armed;
           if (++s == kPairStages) { s = 0; ph ^= 1; }
@@ -753,48 +753,79 @@ namespace {
 // persistent passes of at least this many 128 x 256 tiles run as CTA pairs
 constexpr int kPairMinTiles = 2 * 148;
 
-lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
-                         int64_t K, float alpha, const void* A, int64_t lda_p,
-                         const void* B, int64_t ldb_p, void* C, bool c_half,
-                         int64_t ldc, const int* scale_a, const int* scale_b,
-                         int* err, int max_ctas, int tiles_per_cta,
-                         long long wait_cycles = 0, int withhold = 0,
-                         const void* A2 = nullptr, const void* B2 = nullptr,
-                         int64_t K2 = 0, int ksplit = 1, float* part = nullptr) {
-  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
-  if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return LU_ERR_INVALID_ARG;
-  const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
-  if ((lda_p * esize) % 16 != 0 || (ldb_p * esize) % 16 != 0 ||
-      (uintptr_t)A % 16 != 0 || (uintptr_t)B % 16 != 0)
-    return LU_ERR_INVALID_ARG;
-  if (lda_p < K || ldb_p < K) return LU_ERR_INVALID_ARG;
-  // split copies are plain fp16 operands with a tripled K
-  CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                         : kind == TcOperand::E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-  CUtensorMap ma, mb, ma2, mb2;
-  if (!make_kmajor_map(&ma, A, dt, esize, K, M, lda_p, BM)) return LU_ERR_CUDA;
-  if (!make_kmajor_map(&mb, B, dt, esize, K, N, ldb_p, BN)) return LU_ERR_CUDA;
-  if (K2 > 0) {
-    // the second operand set: same kind and leading dimensions, its own K
-    if (scale_a || scale_b || !A2 || !B2 || (uintptr_t)A2 % 16 != 0 ||
-        (uintptr_t)B2 % 16 != 0 || lda_p < K2 || ldb_p < K2 || K2 > INT32_MAX)
-      return LU_ERR_INVALID_ARG;
-    if (!make_kmajor_map(&ma2, A2, dt, esize, K2, M, lda_p, BM)) return LU_ERR_CUDA;
-    if (!make_kmajor_map(&mb2, B2, dt, esize, K2, N, ldb_p, BN)) return LU_ERR_CUDA;
-  } else {
-    ma2 = ma;
-    mb2 = mb;
-  }
+// Operand sets of one pass: set q is A[q] (M x K[q], row-major, lda_p) and
+// B[q] (K[q] x N, column-major, ldb_p), summed in one accumulator.
+struct OpSets {
+  int n = 1;
+  int64_t K[kMaxSets] = {0, 0, 0, 0};
+  const void* A[kMaxSets] = {nullptr, nullptr, nullptr, nullptr};
+  const void* B[kMaxSets] = {nullptr, nullptr, nullptr, nullptr};
+};
 
+OpSets one_set(int64_t K, const void* A, const void* B) {
+  OpSets o;
+  o.K[0] = K;
+  o.A[0] = A;
+  o.B[0] = B;
+  return o;
+}
+
+// Checks the sets and encodes their tensor maps (box_rows_a / box_rows_b
+// rows per box); fills kb_count / nsets / kb_end.
+lu_status encode_sets(const OpSets& ops, TcOperand kind, int64_t M, int64_t N, int64_t lda_p,
+                      int64_t ldb_p, int box_rows_a, int box_rows_b, TcMaps* maps,
+                      TcParams* p) {
+  if (ops.n < 1 || ops.n > kMaxSets) return LU_ERR_INVALID_ARG;
+  const int esize = (kind == TcOperand::E4M3) ? 1 : 2;
+  if ((lda_p * esize) % 16 != 0 || (ldb_p * esize) % 16 != 0) return LU_ERR_INVALID_ARG;
+  // split copies are plain fp16 operands with a tripled K
+  const CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                               : kind == TcOperand::E4M3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  std::memset(maps, 0, sizeof(*maps));
+  int kb = 0;
+  int64_t ksum = 0;
+  for (int q = 0; q < ops.n; ++q) {
+    const int64_t K = ops.K[q];
+    if (K <= 0 || K > INT32_MAX || lda_p < K || ldb_p < K || !ops.A[q] || !ops.B[q] ||
+        (uintptr_t)ops.A[q] % 16 != 0 || (uintptr_t)ops.B[q] % 16 != 0)
+      return LU_ERR_INVALID_ARG;
+    if (!make_kmajor_map(&maps->a[q], ops.A[q], dt, esize, K, M, lda_p, box_rows_a) ||
+        !make_kmajor_map(&maps->b[q], ops.B[q], dt, esize, K, N, ldb_p, box_rows_b))
+      return LU_ERR_CUDA;
+    kb += (int)ceil_div(K * esize, kRowBytes);
+    ksum += K;
+    p->kb_end[q] = kb;
+  }
+  for (int q = ops.n; q < kMaxSets; ++q) p->kb_end[q] = kb;
+  if (ksum > INT32_MAX) return LU_ERR_INVALID_ARG;
+  p->nsets = ops.n;
+  p->kb_count = kb;
+  p->K = (int)ksum;
+  return LU_SUCCESS;
+}
+
+lu_status tc_update_pair_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                              const OpSets& ops, int64_t lda_p, int64_t ldb_p, float* C,
+                              int64_t ldc, float alpha, int* err, int max_ctas);
+
+lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                         const OpSets& ops, float alpha, int64_t lda_p, int64_t ldb_p,
+                         void* C, bool c_half, int64_t ldc, const int* scale_a,
+                         const int* scale_b, int* err, int max_ctas, int tiles_per_cta,
+                         long long wait_cycles = 0, int withhold = 0, int ksplit = 1,
+                         float* part = nullptr) {
+  if (M <= 0 || N <= 0 || ops.K[0] <= 0) return LU_SUCCESS;
+  if (M > INT32_MAX || N > INT32_MAX) return LU_ERR_INVALID_ARG;
+  if (ops.n > 1 && (scale_a || scale_b)) return LU_ERR_INVALID_ARG;
   TcParams p;
+  std::memset(&p, 0, sizeof(p));
+  TcMaps maps;
+  LUB_TRY(encode_sets(ops, kind, M, N, lda_p, ldb_p, BM, BN, &maps, &p));
   p.C = static_cast<float*>(C);
   p.ldc = ldc;
   p.M = (int)M;
   p.N = (int)N;
-  p.K = (int)K;
-  p.kb_split = (int)ceil_div(K * esize, kRowBytes);
-  p.kb_count = p.kb_split + (K2 > 0 ? (int)ceil_div(K2 * esize, kRowBytes) : 0);
   p.tiles_m = (int)ceil_div(M, BM);
   p.tiles_n = (int)ceil_div(N, BN);
   p.scale_a = scale_a;
@@ -811,7 +842,7 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   p.part = nullptr;
   p.part_ld = p.part_stride = 0;
   if (part) {
-    if (ksplit < 1 || A2 || scale_a || scale_b || c_half) return LU_ERR_INVALID_ARG;
+    if (ksplit < 1 || ops.n > 1 || scale_a || scale_b || c_half) return LU_ERR_INVALID_ARG;
     p.kb_per = (int)ceil_div(p.kb_count, ksplit);
     p.ksplit = (int)ceil_div(p.kb_count, p.kb_per);
     p.part = part;
@@ -845,67 +876,48 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   if (tma_c && !part && tiles_per_cta <= 0 && !withhold && !scale_a && !scale_b &&
       (kind == TcOperand::F16 || kind == TcOperand::BF16) && tiles >= kPairMinTiles &&
       p.kb_count >= 8)
-    return launch_tc_update_pair(st, kind, M, N, K, A, lda_p, B, ldb_p, K2, A2, B2,
-                                 static_cast<float*>(C), ldc, alpha, err, max_ctas);
+    return tc_update_pair_impl(st, kind, M, N, ops, lda_p, ldb_p, static_cast<float*>(C), ldc,
+                               alpha, err, max_ctas);
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, BM, BN);
   if (part) {
     if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
     LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 4>, smem_bytes<4>()));
-    tc_update_kernel<0, 4><<<grid, kThreads, smem_bytes<4>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+    tc_update_kernel<0, 4><<<grid, kThreads, smem_bytes<4>(), st>>>(maps, mc, p, idesc);
   } else if (c_half) {
     if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
     LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 2>, smem_bytes<2>()));
-    tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+    tc_update_kernel<0, 2><<<grid, kThreads, smem_bytes<2>(), st>>>(maps, mc, p, idesc);
   } else if (kind == TcOperand::E4M3) {
     if (tma_c && !stream_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 1>, smem_bytes<1>()));
-      tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<1, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(maps, mc, p, idesc);
     } else if (tma_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 3>, smem_bytes<3>()));
-      tc_update_kernel<1, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<1, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(maps, mc, p, idesc);
     } else {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<1, 0>, smem_bytes<0>()));
-      tc_update_kernel<1, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<1, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(maps, mc, p, idesc);
     }
   } else {
     if (tma_c && !stream_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 1>, smem_bytes<1>()));
-      tc_update_kernel<0, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<0, 1><<<grid, kThreads, smem_bytes<1>(), st>>>(maps, mc, p, idesc);
     } else if (tma_c) {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 3>, smem_bytes<3>()));
-      tc_update_kernel<0, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<0, 3><<<grid, kThreads, smem_bytes<3>(), st>>>(maps, mc, p, idesc);
     } else {
       LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_kernel<0, 0>, smem_bytes<0>()));
-      tc_update_kernel<0, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(ma, mb, ma2, mb2, mc, p, idesc);
+      tc_update_kernel<0, 0><<<grid, kThreads, smem_bytes<0>(), st>>>(maps, mc, p, idesc);
     }
   }
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }
-}  // namespace
-
-lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
-                           int64_t N, int64_t K, float alpha, const void* A,
-                           int64_t lda_p, const void* B, int64_t ldb_p, float* C,
-                           int64_t ldc, const int* scale_a, const int* scale_b,
-                           int* err, int max_ctas, int tiles_per_cta) {
-  return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, false, ldc,
-                        scale_a, scale_b, err, max_ctas, tiles_per_cta);
-}
-
-lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
-                            int64_t K, const void* A, const void* B, int64_t K2,
-                            const void* A2, const void* B2, int64_t ld_p, float* C,
-                            int64_t ldc, int* err, int max_ctas, int tiles_per_cta) {
-  if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
-  return tc_update_impl(st, kind, M, N, K, -1.0f, A, ld_p, B, ld_p, C, false, ldc, nullptr,
-                        nullptr, err, max_ctas, tiles_per_cta, 0, 0, A2, B2, K2);
-}
 
 // Clusters of two tc_update_pair_kernel CTAs resident at once on this
 // device (cached per device; 0 if the query fails).
-static int pair_capacity() {
+int pair_capacity() {
   static int cache[64];
   static std::once_flag once[64];
   int dev = 0;
@@ -927,43 +939,21 @@ static int pair_capacity() {
   return cache[dev];
 }
 
-lu_status launch_tc_update_pair(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
-                                int64_t K, const void* A, int64_t lda_p, const void* B,
-                                int64_t ldb_p, int64_t K2, const void* A2, const void* B2,
-                                float* C, int64_t ldc, float alpha, int* err, int max_ctas) {
-  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
+lu_status tc_update_pair_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                              const OpSets& ops, int64_t lda_p, int64_t ldb_p, float* C,
+                              int64_t ldc, float alpha, int* err, int max_ctas) {
   if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
-  if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX || K2 < 0 || K2 > INT32_MAX)
-    return LU_ERR_INVALID_ARG;
-  if ((lda_p * 2) % 16 != 0 || (ldb_p * 2) % 16 != 0 || (uintptr_t)A % 16 != 0 ||
-      (uintptr_t)B % 16 != 0 || lda_p < K || ldb_p < K || lda_p < K2 || ldb_p < K2 ||
-      (K2 > 0 && (!A2 || !B2 || (uintptr_t)A2 % 16 != 0 || (uintptr_t)B2 % 16 != 0)))
-    return LU_ERR_INVALID_ARG;
   if ((uintptr_t)C % 16 != 0 || ldc % 4 != 0) return LU_ERR_INVALID_ARG;  // TMA reduce-add
-  const CUtensorMapDataType dt = kind == TcOperand::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-  CUtensorMap ma, mb, ma2, mb2, mc;
-  if (!make_kmajor_map(&ma, A, dt, 2, K, M, lda_p, kPairRows) ||
-      !make_kmajor_map(&mb, B, dt, 2, K, N, ldb_p, kPairRows))
-    return LU_ERR_CUDA;
-  if (K2 > 0) {
-    if (!make_kmajor_map(&ma2, A2, dt, 2, K2, M, lda_p, kPairRows) ||
-        !make_kmajor_map(&mb2, B2, dt, 2, K2, N, ldb_p, kPairRows))
-      return LU_ERR_CUDA;
-  } else {
-    ma2 = ma;
-    mb2 = mb;
-  }
-  if (!make_c_map(&mc, C, M, N, ldc)) return LU_ERR_CUDA;
   TcParams p;
   std::memset(&p, 0, sizeof(p));
+  TcMaps maps;
+  LUB_TRY(encode_sets(ops, kind, M, N, lda_p, ldb_p, kPairRows, kPairRows, &maps, &p));
+  CUtensorMap mc;
+  if (!make_c_map(&mc, C, M, N, ldc)) return LU_ERR_CUDA;
   p.C = C;
   p.ldc = ldc;
   p.M = (int)M;
   p.N = (int)N;
-  p.K = (int)K;
-  p.kb_split = (int)ceil_div(K * 2, kRowBytes);
-  p.kb_count = p.kb_split + (K2 > 0 ? (int)ceil_div(K2 * 2, kRowBytes) : 0);
   p.tiles_m = (int)ceil_div(M, 2 * kPairRows);
   p.tiles_n = (int)ceil_div(N, BN);
   p.alpha = alpha;
@@ -982,17 +972,55 @@ lu_status launch_tc_update_pair(cudaStream_t st, TcOperand kind, int64_t M, int6
       std::max(1, std::min({tiles, (max_ctas > 0 ? max_ctas : sm_count()) / 2, resident}));
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
   const uint32_t idesc = sm100::make_idesc(f, f, 2 * kPairRows, BN);
-  tc_update_pair_kernel<<<2 * pairs, kThreads, pair_smem_bytes(), st>>>(ma, mb, ma2, mb2, mc, p,
-                                                                         idesc);
+  tc_update_pair_kernel<<<2 * pairs, kThreads, pair_smem_bytes(), st>>>(maps, mc, p, idesc);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
+}
+
+}  // namespace
+
+lu_status launch_tc_update(cudaStream_t st, TcOperand kind, int64_t M,
+                           int64_t N, int64_t K, float alpha, const void* A,
+                           int64_t lda_p, const void* B, int64_t ldb_p, float* C,
+                           int64_t ldc, const int* scale_a, const int* scale_b,
+                           int* err, int max_ctas, int tiles_per_cta) {
+  return tc_update_impl(st, kind, M, N, one_set(K, A, B), alpha, lda_p, ldb_p, C, false, ldc,
+                        scale_a, scale_b, err, max_ctas, tiles_per_cta);
+}
+
+lu_status launch_tc_update_sets(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                int nsets, const int64_t* K, const void* const* A,
+                                const void* const* B, int64_t ld_p, float* C, int64_t ldc,
+                                int* err, int max_ctas, int tiles_per_cta) {
+  if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+  if (nsets < 1 || nsets > kMaxSets || !K || !A || !B) return LU_ERR_INVALID_ARG;
+  OpSets o;
+  o.n = nsets;
+  for (int q = 0; q < nsets; ++q) {
+    o.K[q] = K[q];
+    o.A[q] = A[q];
+    o.B[q] = B[q];
+  }
+  return tc_update_impl(st, kind, M, N, o, -1.0f, ld_p, ld_p, C, false, ldc, nullptr, nullptr,
+                        err, max_ctas, tiles_per_cta);
+}
+
+lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                            int64_t K, const void* A, const void* B, int64_t K2,
+                            const void* A2, const void* B2, int64_t ld_p, float* C,
+                            int64_t ldc, int* err, int max_ctas, int tiles_per_cta) {
+  const int64_t ks[2] = {K, K2};
+  const void* as[2] = {A, A2};
+  const void* bs[2] = {B, B2};
+  return launch_tc_update_sets(st, kind, M, N, K2 > 0 ? 2 : 1, ks, as, bs, ld_p, C, ldc, err,
+                               max_ctas, tiles_per_cta);
 }
 
 lu_status launch_tc_update_h(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                              int64_t K, float alpha, const void* A, int64_t lda_p,
                              const void* B, int64_t ldb_p, __half* C, int64_t ldc,
                              int* err) {
-  return tc_update_impl(st, kind, M, N, K, alpha, A, lda_p, B, ldb_p, C, true, ldc,
+  return tc_update_impl(st, kind, M, N, one_set(K, A, B), alpha, lda_p, ldb_p, C, true, ldc,
                         nullptr, nullptr, err, 0, 0);
 }
 
@@ -1024,9 +1052,8 @@ lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int
                                  float* part, int* err) {
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
   if (!part || ksplit < 1 || N > 65535 || (shadow && lds < M)) return LU_ERR_INVALID_ARG;
-  LUB_TRY(tc_update_impl(st, kind, M, N, K, 1.0f, A, lda_p, B, ldb_p, nullptr, false, M,
-                         nullptr, nullptr, err, 0, 0, 0, 0, nullptr, nullptr, 0, ksplit,
-                         part));
+  LUB_TRY(tc_update_impl(st, kind, M, N, one_set(K, A, B), 1.0f, lda_p, ldb_p, nullptr, false,
+                         M, nullptr, nullptr, err, 0, 0, 0, 0, ksplit, part));
   const int esize = tc_operand_bytes(kind);
   const int kb = (int)ceil_div(K * esize, kRowBytes);
   const int per = (int)ceil_div(kb, ksplit);
@@ -1068,8 +1095,8 @@ lu_status launch_tc_update_withheld(cudaStream_t st, int64_t M, int64_t N, int64
                                     int64_t ldb_p, float* C, int64_t ldc, int* err,
                                     long long wait_cycles, int tiles_per_cta) {
   if (wait_cycles <= 0) return LU_ERR_INVALID_ARG;
-  return tc_update_impl(st, TcOperand::F16, M, N, K, -1.0f, A, lda_p, B, ldb_p, C, false,
-                        ldc, nullptr, nullptr, err, 0, tiles_per_cta, wait_cycles, 1);
+  return tc_update_impl(st, TcOperand::F16, M, N, one_set(K, A, B), -1.0f, lda_p, ldb_p, C,
+                        false, ldc, nullptr, nullptr, err, 0, tiles_per_cta, wait_cycles, 1);
 }
 
 }  // namespace lub

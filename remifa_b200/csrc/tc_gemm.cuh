@@ -45,19 +45,17 @@ lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t 
                             const void* A2, const void* B2, int64_t ld_p, float* C,
                             int64_t ldc, int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
-// C += alpha (A B + A2 B2) by CTA pairs (tcgen05 cta_group::2, 256 x 256
-// tiles, TMA reduce-add into C): unscaled fp16 / bf16 operands, C 16-byte
-// aligned with ldc % 4 == 0 (LU_ERR_INVALID_ARG otherwise); K2 = 0 for one
-// operand set (A2 with lda_p, B2 with ldb_p).  Persistent over at most
-// max_ctas CTAs (all SMs when 0).  launch_tc_update / launch_tc_update2
-// take this path by themselves for persistent launches of at least 296
-// tiles of 128 x 256 whose C allows it.  Each element's sum runs over K in
-// the same order as the single-CTA kernel's.
-lu_status launch_tc_update_pair(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
-                                int64_t K, const void* A, int64_t lda_p, const void* B,
-                                int64_t ldb_p, int64_t K2, const void* A2, const void* B2,
-                                float* C, int64_t ldc, float alpha, int* err,
-                                int max_ctas = 0);
+// C -= sum_q A[q] B[q] in one pass over C: up to four K-major operand sets
+// (unscaled fp16 or bf16, the same leading dimension ld_p, K[q] columns
+// each) summed in one fp32 accumulator, so C is read and written once for
+// several outer steps' updates.  Persistent launches (tiles_per_cta = 0) of
+// at least 296 tiles of 128 x 256 with K >= 512 in all and a C that TMA can
+// address run as CTA pairs (tcgen05 cta_group::2, 256 x 256 tiles); every
+// element's sum runs over K in the same order either way.
+lu_status launch_tc_update_sets(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                int nsets, const int64_t* K, const void* const* A,
+                                const void* const* B, int64_t ld_p, float* C, int64_t ldc,
+                                int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
 // The same update with C stored in fp16 (C = rn16(C + alpha * acc), the sum
 // in fp32): the left-looking factorization of an fp16 matrix.

@@ -289,17 +289,21 @@ def test_lookahead_is_bit_identical(built, compute, n, nb):
 
 @pytest.mark.parametrize("compute,fmt", [(rb.TC32, O.FMT_FP16),
                                          (rb.compute_type.TC32_BF16, O.FMT_BF16)])
-@pytest.mark.parametrize("n,nb", [(2048, 256), (1800, 128), (3000, 256)])
-def test_two_step_bulk_pass(built, compute, fmt, n, nb):
-    """bulk_steps 2 (the default under look-ahead): two outer steps' updates
-    of the bulk of the trailing matrix in one pass, C - (L_k U_k + L_k+1
-    U_k+1) with one fp32 accumulator.  Only that rounding differs from the
+@pytest.mark.parametrize("n,nb,q", [(2048, 256, 2), (1800, 128, 2), (3000, 256, 2),
+                                    (3000, 128, 3), (2500, 128, 4), (4096, 256, 4),
+                                    (3000, 256, 0)])
+def test_grouped_bulk_pass(built, compute, fmt, n, nb, q):
+    """bulk_steps q (0: the default, 4, under look-ahead): q outer steps'
+    updates of the bulk of the trailing matrix in one pass,
+    C - (L_k U_k + ... + L_k+q-1 U_k+q-1) with one fp32 accumulator, the
+    block row and column each step's successors need applied at once with
+    every pending product.  Only that rounding differs from the
     step-by-step order: within 64 n u32 of it and of the oracle, same
     ||A - LU|| up to 2x."""
-    a = O.gen_matrix(n, seed=n + 11, kind=1, alpha=1.5)
+    a = O.gen_matrix(n, seed=n + 11 + q, kind=1, alpha=1.5)
     d1, d2 = to_dev(a), to_dev(a)
     rb.lu_nopiv_rl(d1, nb=nb, outer=compute, bulk_steps=1)
-    info = rb.lu_nopiv_rl(d2, nb=nb, outer=compute, bulk_steps=2)
+    info = rb.lu_nopiv_rl(d2, nb=nb, outer=compute, bulk_steps=q)
     torch.cuda.synchronize()
     assert int(info.item()) == 0
     one, two = to_host(d1), to_host(d2)

@@ -344,14 +344,19 @@ def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2, solve
 
 def isolated_update_roofline(rb, torch, outer, n, nb, la, peaks, reps=3) -> dict:
     """The dominant kernel alone: the factorization's largest trailing-update
-    launch shape (the first bulk pass: M = N = n - 4 nb with K = 2 nb when two
-    outer steps share a pass, else n - 3 nb with K = nb), run through the
-    library's update entry on one stream with nothing concurrent; the
-    tensor-core launch is timed with CUDA events on its stream (the operand
-    packing, a separate launch, is not counted)."""
-    paired = la and outer in (rb.TC32, rb.compute_type.TC32_BF16)
-    m = n - (4 if paired else 3) * nb
-    k = (2 if paired else 1) * nb
+    launch shape -- under look-ahead with fp16 / bf16 updates the first bulk
+    pass of four outer steps (M = N = n - 6 nb, K = 4 nb, the CTA-pair
+    kernel), else the first step's bulk (M = N = n - 3 nb, K = nb) -- run
+    through the library's update entry on one stream with nothing
+    concurrent; the tensor-core launch is timed with CUDA events on its
+    stream (the operand packing, a separate launch, is not counted).  At
+    K = 4 nb = 1024 each C element's 8 bytes carry 2K = 2048 flops (AI 256
+    flop/B, at the ridge of the measured peaks), so the bound reported is
+    the tensor pipe; the HBM fraction is given beside it."""
+    grouped = la and outer in (rb.TC32, rb.compute_type.TC32_BF16)
+    q = 4 if grouped else 1
+    m = n - (q + 2 if grouped else 3) * nb
+    k = q * nb
     g = torch.Generator(device="cuda")
     g.manual_seed(5)
     a = rb.colmajor(torch.randn(m, k, device="cuda", generator=g))
@@ -368,23 +373,36 @@ def isolated_update_roofline(rb, torch, outer, n, nb, la, peaks, reps=3) -> dict
     gbs = e["bytes"] / sec / 1e9
     tfs = e["flops"] / sec / 1e12
     alg = e["bytes"] / e["launches"]
-    tr = profiled_traffic("tc_update_update_m8192_k512")
+    prof_name = "tc_update_pair_update_m8192_k1024" if grouped else "tc_update_update_m8192_k512"
+    tr = profiled_traffic(prof_name)
     del a, b, c
     torch.cuda.empty_cache()
-    return {"kernel": "tc_update_kernel (persistent CTAs, C streamed by TMA, all SMs)",
-            "shape": {"M": m, "N": m, "K": k}, "bound": "hbm", "achieved": gbs,
-            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
-            "peak_source": peaks["source"] + " hbm_gbs (copy, burst)",
-            "tensor_tflops": tfs, "tensor_peak": peaks["bf16_tflops"],
-            "tensor_frac": tfs / peaks["bf16_tflops"],
-            "algorithmic_bytes_per_launch": alg,
-            "avg_launch_ms": e["total_ms"] / e["launches"], "launches": e["launches"],
-            "traffic": tr["traffic_over_algorithmic"] * alg if tr else None,
-            "traffic_source": ("ncu dram bytes / algorithmic bytes of the same kernel at "
-                               "M = 8192, K = 512 (profiles/tc_update_update_m8192_k512.json),"
-                               " times this launch's algorithmic bytes") if tr else None,
-            "timing": "CUDA events on the launching stream, the launch alone, "
-                      f"mean of {reps}"}
+    out = {"kernel": ("tc_update_pair_kernel (CTA pairs, tcgen05 cta_group::2, 256 x 256 "
+                      "tiles, TMA reduce-add)") if grouped else
+                     "tc_update_kernel (persistent CTAs, C streamed by TMA, all SMs)",
+           "shape": {"M": m, "N": m, "K": k},
+           "algorithmic_bytes_per_launch": alg,
+           "avg_launch_ms": e["total_ms"] / e["launches"], "launches": e["launches"],
+           "traffic": tr["traffic_over_algorithmic"] * alg if tr else None,
+           "traffic_source": (f"ncu dram bytes / algorithmic bytes of the same kernel at "
+                              f"M = 8192 (profiles/{prof_name}.json), times this launch's "
+                              "algorithmic bytes") if tr else None,
+           "timing": "CUDA events on the launching stream, the launch alone, "
+                     f"mean of {reps}"}
+    if grouped:
+        out.update({"bound": "tensor", "achieved": tfs, "peak": peaks["bf16_tflops"],
+                    "unit": "TFLOP/s", "frac": tfs / peaks["bf16_tflops"],
+                    "peak_source": peaks["source"] + " bf16_tflops (cuBLAS, burst)",
+                    "frac_of_sustained": tfs / peaks["bf16_tflops_sustained"]
+                    if peaks.get("bf16_tflops_sustained") else None,
+                    "hbm_gbs": gbs, "hbm_frac": gbs / peaks["hbm_gbs"]})
+    else:
+        out.update({"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": gbs / peaks["hbm_gbs"],
+                    "peak_source": peaks["source"] + " hbm_gbs (copy, burst)",
+                    "tensor_tflops": tfs, "tensor_peak": peaks["bf16_tflops"],
+                    "tensor_frac": tfs / peaks["bf16_tflops"]})
+    return out
 
 
 def config_of(args, wl) -> dict:

@@ -847,11 +847,12 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
                              t2b >= kU2bPersistTiles;
         const int tiles = persist ? 0 : kU2Tiles;
         // the bulk's share of the SMs (the rest for the panel streams): 2/3,
-        // 3/4 for the largest passes (B200, two steps per pass: n = 16384
-        // 232 TF/s at 1/2, 242 at 2/3, 241 at 3/4; n = 32768 308 / 341 / 353)
-        const int ctas = persist ? std::max(1, sm_count() * (t2b >= 2 * kU2bPersistTiles ? 3 : 2) /
-                                                   (t2b >= 2 * kU2bPersistTiles ? 4 : 3))
-                                 : 0;
+        // 3/4 from 4096 tiles, 7/8 from 8192 (B200, four steps per pass:
+        // n = 16384 268 / 270 / 263 TF/s at 2/3, 3/4, 7/8 for its first
+        // passes; n = 32768 478 / 484 / 492; all SMs: 220 and 430)
+        const int share_num = t2b >= 4 * kU2bPersistTiles ? 7 : t2b >= 2 * kU2bPersistTiles ? 3 : 2;
+        const int share_den = t2b >= 4 * kU2bPersistTiles ? 8 : t2b >= 2 * kU2bPersistTiles ? 4 : 3;
+        const int ctas = persist ? std::max(1, sm_count() * share_num / share_den) : 0;
         // defer this step's bulk too while the group has room and the next
         // step has a bulk region of its own (one block smaller)
         const bool defer = q >= 2 && ngrp + 1 < q && tr > 3 * nb && tcn > 3 * nb;

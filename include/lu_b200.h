@@ -89,12 +89,13 @@ typedef struct lu_opts {
                            src/lu_nopiv_ll.hxx:172-201); 0 rounds the update
                            to fp16 first (OP = fp16).  Ignored for fp32 storage. */
   int32_t bulk_steps;   /* right-looking with look-ahead and fp16 / bf16 trailing
-                           updates: 0 (default) or 2 applies two consecutive
-                           outer steps' updates of the bulk of the trailing
-                           matrix in one pass (C - (L_k U_k + L_k+1 U_k+1),
-                           one fp32 accumulator, C read and written once); 1
-                           applies every step separately, the reference's
-                           rounding order.  Ignored elsewhere. */
+                           updates: q = 2, 3 or 4 consecutive outer steps'
+                           updates of the bulk of the trailing matrix in one
+                           pass (C - (L_k U_k + ... + L_k+q-1 U_k+q-1), one
+                           fp32 accumulator, C read and written once per q
+                           steps); 0 = the default, 4; 1 applies every step
+                           separately, the reference's rounding order.
+                           Ignored elsewhere. */
   int32_t reserved[6];
 } lu_opts;
 

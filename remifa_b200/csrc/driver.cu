@@ -196,6 +196,9 @@ struct DevStreams {
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
   cudaEvent_t done_with[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // U2 done reading buffer b
+  // left-looking look-ahead: the previous block is queued (ll_ready); the
+  // early partial products of the block of each parity are done (ll_early)
+  cudaEvent_t ll_ready = nullptr, ll_early[2] = {nullptr, nullptr};
 };
 
 static lu_status dev_streams(DevStreams** out) {
@@ -228,7 +231,7 @@ static lu_status dev_streams(DevStreams** out) {
                            &d.done_with[3], &d.done_with[4], &d.done_with[5], &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
                            &d.u1_done, &d.join_s,
-                           &d.spack_done})
+                           &d.spack_done, &d.ll_ready, &d.ll_early[0], &d.ll_early[1]})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
@@ -265,16 +268,20 @@ static lu_status join_side(cudaStream_t st, DevStreams* S) {
 
 // Left-looking tensor-core updates have N = nb (block column) or M = nb
 // (block row) and K = ofs: at most 2 n / 128 tiles, long in K, so they are
-// split along K (up to kLlSplitMax ways) to fill the SMs.  Two regions of
-// kLlSplitMax slabs, one per update of a step (they run at once).
+// split along K (up to kLlSplitMax ways) to fill the SMs.  With look-ahead
+// the K range [0, ofs - nb) of a block's two updates is computed while the
+// previous block is factored, and the previous block's own K = nb product
+// after it: kLlSplitMax + 1 slabs per update, for blocks of either parity.
 constexpr int kLlSplitMax = 4;
 static size_t ll_part_layout(Plan* p, size_t off) {
   const int64_t n = p->n, nb = p->nb;
   const int64_t slab = std::max(((n + 3) / 4 * 4) * nb, ((nb + 3) / 4 * 4) * n);
   off = align_up(off, 1024);
   p->off_part = off;
-  p->part_bytes = align_up((size_t)kLlSplitMax * slab * 4, 1024);
-  return off + 2 * p->part_bytes;
+  // per region: the early splits and the late (previous block's) product
+  p->part_bytes = align_up((size_t)(kLlSplitMax + 1) * slab * 4, 1024);
+  // regions: block parity x (block column, block row)
+  return off + 4 * p->part_bytes;
 }
 
 // Outer steps whose bulk trailing updates share one pass by default: the
@@ -1111,36 +1118,77 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
   const int64_t es = tc_operand_bytes(kind);
   char* Lc = ws + p.off_lcopy;
   char* Uc = ws + p.off_ucopy;
-  float* Pc = reinterpret_cast<float*>(ws + p.off_part);
-  float* Pr = reinterpret_cast<float*>(ws + p.off_part + p.part_bytes);
   DevStreams* S = nullptr;
   LUB_TRY(dev_streams(&S));
+  // tensor-core path: as ll_factor_f16, the K range [0, ofs - nb) of block
+  // ofs's two updates is computed on the low-priority stream while the
+  // previous block is factored (from the L and U copies of the blocks
+  // before it), the previous block's own K = nb product after it, and one
+  // finishing pass adds the slabs in K order into the fp32 matrix
+  auto slabs = [&](int q, int r) {
+    return reinterpret_cast<float*>(ws + p.off_part + (size_t)(2 * q + r) * p.part_bytes);
+  };
+  int early[2][2] = {{0, 0}, {0, 0}};
+  auto launch_early = [&](int64_t o) -> lu_status {
+    const int q = (int)((o / nb) & 1);
+    early[q][0] = early[q][1] = 0;
+    const int64_t ke = o - nb;
+    if (!tc || o >= n || ke <= 0) return LU_SUCCESS;
+    const int64_t in_ = std::min(n - o, nb), updm_ = n - o, rest_ = updm_ - in_;
+    const int ks = ll_split(updm_, in_, ke, es);
+    ProfScope ps("tc_update", S->update,
+                 8.0 * ks * ((double)updm_ * in_ + (double)in_ * rest_) +
+                     (double)es * ke * (updm_ + in_ + (rest_ > 0 ? in_ + rest_ : 0)),
+                 2.0 * ke * ((double)updm_ * in_ + (double)in_ * rest_));
+    LUB_CUDA_TRY(cudaEventRecord(S->ll_ready, st));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(S->update, S->ll_ready, 0));
+    LUB_TRY(launch_tc_partials(S->update, kind, updm_, in_, ke, Lc + o * ldk * es, ldk,
+                               Uc + o * ldk * es, ldk, ks, slabs(q, 0), 0, &early[q][0], err));
+    if (rest_ > 0)
+      LUB_TRY(launch_tc_partials(S->update, kind, in_, rest_, ke, Lc + o * ldk * es, ldk,
+                                 Uc + (o + in_) * ldk * es, ldk, ks, slabs(q, 1), 0,
+                                 &early[q][1], err));
+    LUB_CUDA_TRY(cudaEventRecord(S->ll_early[q], S->update));
+    return LU_SUCCESS;
+  };
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
     const int64_t in = std::min(n - ofs, nb);
     const int64_t updm = n - ofs;
     float* blk = a + ofs + ofs * lda;
+    const int q = (int)((ofs / nb) & 1);
+    LUB_TRY(launch_early(ofs + nb));
     if (ofs > 0) {
       if (tc) {
-        // the block column (on st) and the block row (on the side stream)
-        // are disjoint: both updates run at once, split along K so that
-        // their units fill the SMs together
+        // the previous block's own product, then the finishing pass: block
+        // column on st, block row on the side stream (disjoint, at once)
         const bool row = updm > in;
-        const int ks = ll_split(updm, in, ofs, es);
+        const int64_t k0 = ofs - nb;
+        const bool wait_early = early[q][0] > 0 || early[q][1] > 0;
         if (row) LUB_TRY(fork_side(st, S));
         {
-          ProfScope ps("tc_update", st, 8.0 * updm * in + es * (double)ofs * (updm + in),
-                       2.0 * ofs * (double)updm * in);
-          LUB_TRY(launch_tc_update_split(st, kind, updm, in, ofs, -1.0f, Lc + ofs * ldk * es,
-                                         ldk, Uc + ofs * ldk * es, ldk, blk, false, lda,
-                                         nullptr, 0, ks, Pc, err));
+          ProfScope ps("tc_update", st,
+                       4.0 * (3 + early[q][0]) * updm * in + es * (double)nb * (updm + in),
+                       2.0 * nb * (double)updm * in);
+          int sl = 0;
+          LUB_TRY(launch_tc_partials(st, kind, updm, in, nb, Lc + (ofs * ldk + k0) * es, ldk,
+                                     Uc + (ofs * ldk + k0) * es, ldk, 1, slabs(q, 0),
+                                     early[q][0], &sl, err));
+          if (wait_early) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->ll_early[q], 0));
+          LUB_TRY(launch_splitk_finish(st, updm, in, early[q][0] + sl, slabs(q, 0), -1.0f, blk,
+                                       false, lda, nullptr, 0));
         }
         if (row) {
-          ProfScope ps("tc_update", S->side, 8.0 * in * (updm - in) + es * (double)ofs * updm,
-                       2.0 * ofs * (double)in * (updm - in));
-          LUB_TRY(launch_tc_update_split(S->side, kind, in, updm - in, ofs, -1.0f,
-                                         Lc + ofs * ldk * es, ldk, Uc + (ofs + in) * ldk * es,
-                                         ldk, blk + in * lda, false, lda, nullptr, 0, ks, Pr,
-                                         err));
+          ProfScope ps("tc_update", S->side,
+                       4.0 * (3 + early[q][1]) * in * (updm - in) + es * (double)nb * updm,
+                       2.0 * nb * (double)in * (updm - in));
+          int sl = 0;
+          LUB_TRY(launch_tc_partials(S->side, kind, in, updm - in, nb,
+                                     Lc + (ofs * ldk + k0) * es, ldk,
+                                     Uc + ((ofs + in) * ldk + k0) * es, ldk, 1, slabs(q, 1),
+                                     early[q][1], &sl, err));
+          if (wait_early) LUB_CUDA_TRY(cudaStreamWaitEvent(S->side, S->ll_early[q], 0));
+          LUB_TRY(launch_splitk_finish(S->side, in, updm - in, early[q][1] + sl, slabs(q, 1),
+                                       -1.0f, blk + in * lda, false, lda, nullptr, 0));
           LUB_TRY(join_side(st, S));
         }
       } else {
@@ -1173,6 +1221,8 @@ static lu_status ll_factor(const Plan& p, cudaStream_t st, float* a,
                             Uc + ((ofs + in) * ldk + ofs) * es, ldk, nullptr));
     }
   }
+  LUB_CUDA_TRY(cudaEventRecord(S->ll_ready, S->update));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->ll_ready, 0));
   return LU_SUCCESS;
 }
 
@@ -1196,16 +1246,50 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
   char* Lc = ws + p.off_lcopy;
   float* Sh = reinterpret_cast<float*>(ws + p.off_shadow);
   const int64_t lds = p.ld_shadow;
-  float* Pc = reinterpret_cast<float*>(ws + p.off_part);
-  float* Pr = reinterpret_cast<float*>(ws + p.off_part + p.part_bytes);
   DevStreams* S = nullptr;
   LUB_TRY(dev_streams(&S));
+  // partial-product slabs of the block column (r = 0) and block row (r = 1)
+  // updates of the blocks of parity q
+  auto slabs = [&](int q, int r) {
+    return reinterpret_cast<float*>(ws + p.off_part + (size_t)(2 * q + r) * p.part_bytes);
+  };
+  int early[2][2] = {{0, 0}, {0, 0}};  // slabs computed ahead, per parity / update
+  // Block column o's updates over K = [0, o - nb) (all factored columns but
+  // the previous block's), on the low-priority stream while the previous
+  // block is factored on st.  Everything they read is final once the block
+  // before the previous one is done: the L copy's columns [0, o - nb) and
+  // the U rows [0, o - nb) of the fp16 matrix.
+  auto launch_early = [&](int64_t o) -> lu_status {
+    const int q = (int)((o / nb) & 1);
+    early[q][0] = early[q][1] = 0;
+    const int64_t ke = o - nb;
+    if (o >= n || ke <= 0) return LU_SUCCESS;
+    const int64_t in_ = std::min(n - o, nb), updm_ = n - o, rest_ = updm_ - in_;
+    const int ks = ll_split(updm_, in_, ke, 2);
+    ProfScope ps("tc_update", S->update,
+                 8.0 * (ks * (double)updm_ * in_ + (rest_ > 0 ? ks * (double)in_ * rest_ : 0.0)) +
+                     2.0 * (double)ke * (updm_ + in_ + (rest_ > 0 ? in_ + rest_ : 0)),
+                 2.0 * ke * ((double)updm_ * in_ + (double)in_ * rest_));
+    LUB_CUDA_TRY(cudaEventRecord(S->ll_ready, st));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(S->update, S->ll_ready, 0));
+    LUB_TRY(launch_tc_partials(S->update, TcOperand::F16, updm_, in_, ke, Lc + o * ldk * 2, ldk,
+                               a + o * lda, lda, ks, slabs(q, 0), 0, &early[q][0], err));
+    if (rest_ > 0)
+      LUB_TRY(launch_tc_partials(S->update, TcOperand::F16, in_, rest_, ke, Lc + o * ldk * 2, ldk,
+                                 a + (o + in_) * lda, lda, ks, slabs(q, 1), 0, &early[q][1],
+                                 err));
+    LUB_CUDA_TRY(cudaEventRecord(S->ll_early[q], S->update));
+    return LU_SUCCESS;
+  };
   for (int64_t ofs = 0; ofs < n; ofs += nb) {
     const int64_t in = std::min(n - ofs, nb);
     const int64_t updm = n - ofs;
     const int64_t rest = updm - in;
+    const int q = (int)((ofs / nb) & 1);
     __half* blk = a + ofs + ofs * lda;
     float* sblk = Sh + ofs + ofs * lds;
+    // the next block's early products, beside this block's work
+    LUB_TRY(launch_early(ofs + nb));
     auto to_shadow = [&]() -> lu_status {
       ProfScope ps("convert", st, 6.0 * (double)in * (updm + rest));
       LUB_TRY(launch_convert(st, updm, in, blk, LU_F16, lda, sblk, LU_F32, lds, 0));
@@ -1216,38 +1300,41 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
     };
     if (p.panel_fp32 || ofs == 0) LUB_TRY(to_shadow());
     if (ofs > 0) {
-      // block column on st, block row on the side stream (disjoint, at once,
-      // split along K to fill the SMs together).  panel_fp32: the update
-      // lands in the shadow; otherwise in the fp16 matrix (one rounding),
-      // and the finishing kernel also writes the stored values to the shadow
-      const double cb = p.panel_fp32 ? 8.0 : 10.0;
-      const int ks = ll_split(updm, in, ofs, 2);
+      // the previous block's own product (K range [ofs - nb, ofs)), then the
+      // sum of all slabs in K order: block column on st, block row on the
+      // side stream (disjoint, at once).  panel_fp32: the update lands in
+      // the shadow; otherwise in the fp16 matrix (one rounding), and the
+      // finishing kernel also writes the stored values to the shadow
+      const int64_t k0 = ofs - nb;
+      const bool wait_early = early[q][0] > 0 || early[q][1] > 0;
       if (rest > 0) LUB_TRY(fork_side(st, S));
       {
-        ProfScope ps("tc_update", st, cb * updm * in + 2.0 * (double)ofs * (updm + in),
-                     2.0 * ofs * (double)updm * in);
-        if (p.panel_fp32)
-          LUB_TRY(launch_tc_update_split(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                         Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, sblk,
-                                         false, lds, nullptr, 0, ks, Pc, err));
-        else
-          LUB_TRY(launch_tc_update_split(st, TcOperand::F16, updm, in, ofs, -1.0f,
-                                         Lc + ofs * ldk * 2, ldk, a + ofs * lda, lda, blk,
-                                         true, lda, sblk, lds, ks, Pc, err));
+        ProfScope ps("tc_update", st, 4.0 * (2 + early[q][0]) * updm * in + 2.0 * (double)nb * (updm + in),
+                     2.0 * nb * (double)updm * in);
+        int sl = 0;
+        LUB_TRY(launch_tc_partials(st, TcOperand::F16, updm, in, nb, Lc + (ofs * ldk + k0) * 2,
+                                   ldk, a + k0 + ofs * lda, lda, 1, slabs(q, 0), early[q][0], &sl,
+                                   err));
+        if (wait_early) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->ll_early[q], 0));
+        LUB_TRY(launch_splitk_finish(st, updm, in, early[q][0] + sl, slabs(q, 0), -1.0f,
+                                     p.panel_fp32 ? (void*)sblk : (void*)blk, !p.panel_fp32,
+                                     p.panel_fp32 ? lds : lda,
+                                     p.panel_fp32 ? nullptr : sblk, lds));
       }
       if (rest > 0) {
-        ProfScope ps("tc_update", S->side, cb * in * rest + 2.0 * (double)ofs * (in + rest),
-                     2.0 * ofs * (double)in * rest);
-        if (p.panel_fp32)
-          LUB_TRY(launch_tc_update_split(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
-                                         Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
-                                         sblk + in * lds, false, lds, nullptr, 0, ks, Pr,
-                                         err));
-        else
-          LUB_TRY(launch_tc_update_split(S->side, TcOperand::F16, in, rest, ofs, -1.0f,
-                                         Lc + ofs * ldk * 2, ldk, a + (ofs + in) * lda, lda,
-                                         blk + in * lda, true, lda, sblk + in * lds, lds, ks,
-                                         Pr, err));
+        ProfScope ps("tc_update", S->side,
+                     4.0 * (2 + early[q][1]) * in * rest + 2.0 * (double)nb * (in + rest),
+                     2.0 * nb * (double)in * rest);
+        int sl = 0;
+        LUB_TRY(launch_tc_partials(S->side, TcOperand::F16, in, rest, nb,
+                                   Lc + (ofs * ldk + k0) * 2, ldk, a + k0 + (ofs + in) * lda, lda,
+                                   1, slabs(q, 1), early[q][1], &sl, err));
+        if (wait_early) LUB_CUDA_TRY(cudaStreamWaitEvent(S->side, S->ll_early[q], 0));
+        LUB_TRY(launch_splitk_finish(S->side, in, rest, early[q][1] + sl, slabs(q, 1), -1.0f,
+                                     p.panel_fp32 ? (void*)(sblk + in * lds)
+                                                  : (void*)(blk + in * lda),
+                                     !p.panel_fp32, p.panel_fp32 ? lds : lda,
+                                     p.panel_fp32 ? nullptr : sblk + in * lds, lds));
         LUB_TRY(join_side(st, S));
       }
     }
@@ -1266,6 +1353,9 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
                             Lc + ((ofs + in) * ldk + ofs) * 2, ldk, nullptr));
     }
   }
+  // the low-priority stream joins the caller's stream
+  LUB_CUDA_TRY(cudaEventRecord(S->ll_ready, S->update));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->ll_ready, 0));
   return LU_SUCCESS;
 }
 

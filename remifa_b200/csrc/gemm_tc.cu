@@ -118,6 +118,9 @@ struct TcParams {
   int ksplit, kb_per;
   float* part;
   int64_t part_ld, part_stride;
+  int store;           // CTA pairs only: TMA store of alpha * acc (slab s at
+                       // columns [s N, (s + 1) N) of tmap_c) instead of the
+                       // reduce-add into C
 };
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
@@ -527,6 +530,7 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   const int num_tiles = p.tiles_m * p.tiles_n;  // 256 x 256 tiles
+  const int num_units = num_tiles * p.ksplit;    // x K ranges (split K)
   const int pair = (int)blockIdx.x >> 1;
   const int npairs = (int)gridDim.x >> 1;
 
@@ -560,10 +564,13 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
       uint32_t ph = 0;
       bool ok = true;
       int armed = 0;
-      for (int tile = pair; tile < num_tiles && ok; tile += npairs) {
+      for (int unit = pair; unit < num_units && ok; unit += npairs) {
+        const int tile = unit % num_tiles;
         const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+        const int kb0 = (unit / num_tiles) * p.kb_per;
+        const int kb1 = min(p.kb_count, kb0 + p.kb_per);
         int set = 0;
-        for (int kb = 0; kb < p.kb_count; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, p.err, kErrTimeoutEmpty, p.wait_cycles)) {
             ok = false;
             break;
@@ -599,16 +606,18 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
       int local = 0;
       bool ok = true;
       bool issued = false;
-      for (int tile = pair; tile < num_tiles && ok; tile += npairs, ++local) {
+      for (int unit = pair; unit < num_units && ok; unit += npairs, ++local) {
         const int acc = local & 1;
         const uint32_t aph = (local >> 1) & 1;
+        const int kb0 = (unit / num_tiles) * p.kb_per;
+        const int kb1 = min(p.kb_count, kb0 + p.kb_per);
         if (!mbar_wait(&tempty[acc], aph ^ 1, p.err, kErrTimeoutTmemEmpty, p.wait_cycles)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + acc * BN;
-        for (int kb = 0; kb < p.kb_count; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&full[s], ph, p.err, kErrTimeoutFull, p.wait_cycles)) {
             ok = false;
             break;
@@ -620,7 +629,7 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
 #pragma unroll
           for (int k = 0; k < 4; ++k)
             mma_f16_pair(d_tmem, sw128_kmajor_desc(a0 + k * 32), sw128_kmajor_desc(b0 + k * 32),
-                         idesc, (kb > 0 || k > 0) ? 1u : 0u);
+                         idesc, (kb > kb0 || k > 0) ? 1u : 0u);
           mma_commit_pair(&empty[s]);  // frees stage s in both CTAs
           if (++s == kPairStages) { s = 0; ph ^= 1; }
         }
@@ -640,12 +649,14 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
     float* stage = reinterpret_cast<float*>(sEpi + (size_t)ew * 2 * kEpiChunk);
     int issued = 0;
     int local = 0;
-    for (int tile = pair; tile < num_tiles; tile += npairs, ++local) {
+    for (int unit = pair; unit < num_units; unit += npairs, ++local) {
+      const int tile = unit % num_tiles;
       const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
       const int acc = local & 1;
       const uint32_t aph = (local >> 1) & 1;
       const int row0 = tm * 2 * kPairRows + (int)rank * kPairRows + quarter * 32;
       const int col0 = tn * BN + half * 128;
+      const int slab_col = (unit / num_tiles) * p.N;  // store mode: the unit's slab
       if (!mbar_wait(&tfull[acc], aph, p.err, kErrTimeoutTmemFull, p.wait_cycles)) break;
       tc_fence_after();
 #pragma unroll 1
@@ -671,7 +682,8 @@ tc_update_pair_kernel(const __grid_constant__ TcMaps maps,
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
-          tma_reduce_add_2d(&tmap_c, buf, row0, cc);
+          if (p.store) tma_store_2d(&tmap_c, buf, row0, slab_col + cc);
+          else tma_reduce_add_2d(&tmap_c, buf, row0, cc);
           bulk_commit_group();
         }
         ++issued;
@@ -807,7 +819,9 @@ lu_status encode_sets(const OpSets& ops, TcOperand kind, int64_t M, int64_t N, i
 
 lu_status tc_update_pair_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                               const OpSets& ops, int64_t lda_p, int64_t ldb_p, float* C,
-                              int64_t ldc, float alpha, int* err, int max_ctas);
+                              int64_t ldc, float alpha, int* err, int max_ctas,
+                              float* part = nullptr, int ksplit = 1, int* nslabs = nullptr);
+int pair_capacity();
 
 lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                          const OpSets& ops, float alpha, int64_t lda_p, int64_t ldb_p,
@@ -875,7 +889,7 @@ lu_status tc_update_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
   // epilogue of the single-CTA kernel wins, 0.375 against 0.474 ms)
   if (tma_c && !part && tiles_per_cta <= 0 && !withhold && !scale_a && !scale_b &&
       (kind == TcOperand::F16 || kind == TcOperand::BF16) && tiles >= kPairMinTiles &&
-      p.kb_count >= 8)
+      p.kb_count >= 8 && pair_capacity() > 0)
     return tc_update_pair_impl(st, kind, M, N, ops, lda_p, ldb_p, static_cast<float*>(C), ldc,
                                alpha, err, max_ctas);
   const uint32_t f = kind == TcOperand::BF16 ? 1u : 0u;
@@ -923,6 +937,12 @@ int pair_capacity() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
   std::call_once(once[dev], [dev] {
+    cache[dev] = 0;
+    // the query needs the kernel's shared-memory limit raised first
+    if (set_smem_limit((const void*)tc_update_pair_kernel, pair_smem_bytes()) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3(2 * 148, 1, 1);
@@ -939,17 +959,35 @@ int pair_capacity() {
   return cache[dev];
 }
 
+// With part != nullptr: split-K partials instead of the update -- the K
+// blocks cut into `ksplit` near-equal ranges, unit (tile, range s) stores
+// its raw product by TMA into slab s of `part` (ld round4(M), slabs
+// round4(M) x N apart); *nslabs receives the number of ranges.
 lu_status tc_update_pair_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
                               const OpSets& ops, int64_t lda_p, int64_t ldb_p, float* C,
-                              int64_t ldc, float alpha, int* err, int max_ctas) {
+                              int64_t ldc, float alpha, int* err, int max_ctas,
+                              float* part, int ksplit, int* nslabs) {
   if (kind != TcOperand::F16 && kind != TcOperand::BF16) return LU_ERR_UNSUPPORTED;
+  if (part) {
+    C = part;
+    ldc = (M + 3) / 4 * 4;
+  }
   if ((uintptr_t)C % 16 != 0 || ldc % 4 != 0) return LU_ERR_INVALID_ARG;  // TMA reduce-add
   TcParams p;
   std::memset(&p, 0, sizeof(p));
   TcMaps maps;
   LUB_TRY(encode_sets(ops, kind, M, N, lda_p, ldb_p, kPairRows, kPairRows, &maps, &p));
+  p.ksplit = 1;
+  p.kb_per = p.kb_count;
+  if (part) {
+    if (ksplit < 1 || ops.n != 1) return LU_ERR_INVALID_ARG;
+    p.kb_per = (int)ceil_div(p.kb_count, ksplit);
+    p.ksplit = (int)ceil_div(p.kb_count, p.kb_per);
+    p.store = 1;
+    if (nslabs) *nslabs = p.ksplit;
+  }
   CUtensorMap mc;
-  if (!make_c_map(&mc, C, M, N, ldc)) return LU_ERR_CUDA;
+  if (!make_c_map(&mc, C, M, part ? N * p.ksplit : N, ldc)) return LU_ERR_CUDA;
   p.C = C;
   p.ldc = ldc;
   p.M = (int)M;
@@ -959,9 +997,7 @@ lu_status tc_update_pair_impl(cudaStream_t st, TcOperand kind, int64_t M, int64_
   p.alpha = alpha;
   p.err = err;
   p.wait_cycles = sm100::kWaitCycles;
-  p.ksplit = 1;
-  p.kb_per = p.kb_count;
-  const int tiles = p.tiles_m * p.tiles_n;
+  const int tiles = p.tiles_m * p.tiles_n * p.ksplit;
   LUB_CUDA_TRY(set_smem_limit((const void*)tc_update_pair_kernel, pair_smem_bytes()));
   // never more pairs than can be resident at once (SM pairs sit inside one
   // GPC, so an odd SM per GPC stays out): a pair scheduled late would run
@@ -1045,19 +1081,43 @@ splitk_finish_kernel(int64_t M, int S, const float* __restrict__ part, int64_t p
   if (shadow) shadow[i + j * lds] = to_f32(v);
 }
 
-lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
-                                 int64_t K, float alpha, const void* A, int64_t lda_p,
-                                 const void* B, int64_t ldb_p, void* C, bool c_half,
-                                 int64_t ldc, float* shadow, int64_t lds, int ksplit,
-                                 float* part, int* err) {
+int64_t splitk_slab_floats(int64_t M, int64_t N) { return (M + 3) / 4 * 4 * N; }
+
+lu_status launch_tc_partials(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                             int64_t K, const void* A, int64_t lda_p, const void* B,
+                             int64_t ldb_p, int ksplit, float* part, int slab0, int* nslabs,
+                             int* err) {
+  if (nslabs) *nslabs = 0;
   if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
-  if (!part || ksplit < 1 || N > 65535 || (shadow && lds < M)) return LU_ERR_INVALID_ARG;
+  if (!part || ksplit < 1 || slab0 < 0) return LU_ERR_INVALID_ARG;
+  float* base = part + (int64_t)slab0 * splitk_slab_floats(M, N);
+  // 16-bit operands with at least 8 K blocks: CTA pairs storing their
+  // partials by TMA (256 x 256 tiles: the split re-chosen for pairs).  The
+  // slabs sit side by side as one tensor of N x S columns, so N must be a
+  // multiple of the 32-column box (no box may reach into the next slab).
+  const int64_t kbs = ceil_div(K * tc_operand_bytes(kind), kRowBytes);
+  if ((kind == TcOperand::F16 || kind == TcOperand::BF16) && kbs >= 8 && N % 32 == 0 &&
+      pair_capacity() > 0 &&
+      (M + 3) / 4 * 4 * N * (int64_t)ksplit < INT32_MAX) {
+    const int64_t tiles2 = ceil_div(M, 2 * kPairRows) * ceil_div(N, BN);
+    const int ks2 = std::min(ksplit, tc_split_choice(tiles2, K, 2, pair_capacity(), ksplit));
+    return tc_update_pair_impl(st, kind, M, N, one_set(K, A, B), lda_p, ldb_p, nullptr, 0, 1.0f,
+                               err, 0, base, ks2, nslabs);
+  }
   LUB_TRY(tc_update_impl(st, kind, M, N, one_set(K, A, B), 1.0f, lda_p, ldb_p, nullptr, false,
-                         M, nullptr, nullptr, err, 0, 0, 0, 0, ksplit, part));
-  const int esize = tc_operand_bytes(kind);
-  const int kb = (int)ceil_div(K * esize, kRowBytes);
+                         M, nullptr, nullptr, err, 0, 0, 0, 0, ksplit,
+                         part + (int64_t)slab0 * splitk_slab_floats(M, N)));
+  const int kb = (int)ceil_div(K * tc_operand_bytes(kind), kRowBytes);
   const int per = (int)ceil_div(kb, ksplit);
-  const int S = (int)ceil_div(kb, per);
+  if (nslabs) *nslabs = (int)ceil_div(kb, per);
+  return LU_SUCCESS;
+}
+
+lu_status launch_splitk_finish(cudaStream_t st, int64_t M, int64_t N, int S, const float* part,
+                               float alpha, void* C, bool c_half, int64_t ldc, float* shadow,
+                               int64_t lds) {
+  if (M <= 0 || N <= 0) return LU_SUCCESS;
+  if (S < 1 || !part || N > 65535 || (shadow && lds < M)) return LU_ERR_INVALID_ARG;
   const int64_t pld = (M + 3) / 4 * 4;
   dim3 grid((unsigned)ceil_div(M, 256), (unsigned)N);
   if (c_half)
@@ -1070,6 +1130,17 @@ lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int
                                                        lds);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
+}
+
+lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                                 int64_t K, float alpha, const void* A, int64_t lda_p,
+                                 const void* B, int64_t ldb_p, void* C, bool c_half,
+                                 int64_t ldc, float* shadow, int64_t lds, int ksplit,
+                                 float* part, int* err) {
+  if (M <= 0 || N <= 0 || K <= 0) return LU_SUCCESS;
+  int S = 0;
+  LUB_TRY(launch_tc_partials(st, kind, M, N, K, A, lda_p, B, ldb_p, ksplit, part, 0, &S, err));
+  return launch_splitk_finish(st, M, N, S, part, alpha, C, c_half, ldc, shadow, lds);
 }
 
 int tc_split_choice(int64_t tiles, int64_t K, int esize, int sms, int smax) {

@@ -78,6 +78,21 @@ lu_status launch_tc_update_split(cudaStream_t st, TcOperand kind, int64_t M, int
                                  int64_t ldc, float* shadow, int64_t lds, int ksplit,
                                  float* part, int* err);
 
+// The two halves of the split-K update, for callers that compute some K
+// ranges ahead of others: launch_tc_partials writes the raw products of the
+// K ranges of (A, B) cut into ksplit near-equal parts to slabs slab0,
+// slab0 + 1, ... of `part` (each splitk_slab_floats(M, N) floats) and
+// returns their number; launch_splitk_finish adds slabs 0 .. S-1 in order
+// and stores C = rn(C + alpha * sum) (and the fp32 shadow when given).
+int64_t splitk_slab_floats(int64_t M, int64_t N);
+lu_status launch_tc_partials(cudaStream_t st, TcOperand kind, int64_t M, int64_t N,
+                             int64_t K, const void* A, int64_t lda_p, const void* B,
+                             int64_t ldb_p, int ksplit, float* part, int slab0, int* nslabs,
+                             int* err);
+lu_status launch_splitk_finish(cudaStream_t st, int64_t M, int64_t N, int S, const float* part,
+                               float alpha, void* C, bool c_half, int64_t ldc, float* shadow,
+                               int64_t lds);
+
 // Number of K splits (1..smax, at least K = 256 fp16 per split) that
 // minimises waves x K blocks per split for `tiles` 128 x 256 tiles on `sms`
 // SMs (tiles: all the tiles launched at the same time).

@@ -479,6 +479,13 @@ LU_API int lu_profile_trace(lu_trace_entry* out, int max_entries);
 /* Number of kernels this library has launched in this process. */
 LU_API long long lu_launch_count(void);
 
+/* Device memory the library allocates for itself (a workspace not supplied
+ * by the caller, the host entry's operand buffers, solve scratch) comes from
+ * a stream-ordered memory pool per device that keeps freed blocks for the
+ * next call.  lu_trim_memory_c synchronises the current device and returns
+ * the pool's unused memory to the driver (no reference counterpart). */
+LU_API lu_status lu_trim_memory_c(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,13 +9,14 @@ from . import batch
 from .api import (FP16, FP32, TC16, TC32, align_lda, colmajor, colmajor_empty,
                   compute_type, convert, equilibrate, gemmex, gen_matrix, gesv_mixed, gmres_ir,
                   launch_count, ld, lu_nopiv_ll, lu_nopiv_panel, lu_nopiv_rl, lu_nopiv_rl_host,
-                  lu_solve, make_opts, profile, refine, workspace_size)
+                  lu_solve, make_opts, profile, refine, trim_memory, workspace_size)
 
 __all__ = [
     "FP16", "FP32", "TC16", "TC32", "align_lda", "colmajor", "colmajor_empty",
     "compute_type", "convert", "gemmex", "gen_matrix", "ld", "lu_nopiv_ll",
     "lu_nopiv_panel", "lu_nopiv_rl", "lu_nopiv_rl_host", "make_opts", "workspace_size", "profile",
     "launch_count", "lu_solve", "refine", "gesv_mixed", "gmres_ir", "equilibrate",
+    "trim_memory",
 ]
 
 

@@ -147,6 +147,7 @@ SIGNATURES = {
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),
+    "lu_trim_memory_c": (_int, []),
     "lu_profile_trace": (_int, [ctypes.POINTER(LuTraceEntry), _int]),
 }
 

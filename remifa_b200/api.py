@@ -298,6 +298,13 @@ def launch_count() -> int:
     return int(_lib.lib().lu_launch_count())
 
 
+def trim_memory() -> None:
+    """Return the unused memory of the library's stream-ordered pool on the
+    current device to the driver (lu_trim_memory_c); calls that leave their
+    workspace to the library keep it pooled in between."""
+    _lib.check(_lib.lib().lu_trim_memory_c(), "lu_trim_memory_c")
+
+
 def lu_solve(lu: torch.Tensor, b: torch.Tensor, trans: bool = False,
              stream=None) -> torch.Tensor:
     """Solve op(A) X = B with the in-place factors `lu` (fp32, column-major)

@@ -176,7 +176,7 @@ LU_API lu_status lu_adjoint_c(lu_stream_t stream, int64_t n, int64_t nrhs,
     void* ws = workspace;
     bool owned = false;
     if (!ws) {
-      if (cudaMallocAsync(&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
+      if (pool_malloc_async((void**)&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
       owned = true;
     }
     double* g0 = static_cast<double*>(ws);

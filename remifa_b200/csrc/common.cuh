@@ -53,6 +53,13 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Stream-ordered allocation from the library's own memory pool on the
+// current device (misc.cu).  Freed blocks (cudaFreeAsync) stay reserved in
+// the pool for the next call instead of going back to the driver, so calls
+// that leave the workspace to the library do not map and unmap up to
+// gigabytes each time; lu_trim_memory_c hands them back.
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t st);
+
 // ---- device helpers -------------------------------------------------------
 
 // Asynchronous 4-byte global -> shared copy (no register round trip, so a

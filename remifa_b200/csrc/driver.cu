@@ -1381,7 +1381,7 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {
-    if (cudaMallocAsync(&ws, p.ws_bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, p.ws_bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   char* wsb = static_cast<char*>(ws);
@@ -1425,7 +1425,7 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {
-    if (cudaMallocAsync(&ws, p.ws_bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, p.ws_bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   char* wsb = static_cast<char*>(ws);
@@ -1483,7 +1483,7 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
     if (s == LU_SUCCESS && la && tc) {
       wcu[0] = tc_ws_layout(0, n - nb, n - nb, nb, kind);
       wcu[1] = tc_ws_layout(wcu[0].bytes, n - nb, n - nb, nb, kind);
-      if (cudaMallocAsync(&cu_alloc, wcu[0].bytes + wcu[1].bytes, st) != cudaSuccess)
+      if (pool_malloc_async((void**)&cu_alloc, wcu[0].bytes + wcu[1].bytes, st) != cudaSuccess)
         s = LU_ERR_ALLOC;
       cubuf = static_cast<char*>(cu_alloc);
     }
@@ -1557,7 +1557,7 @@ lu_status gemm_update(lu_compute compute, cudaStream_t st, int64_t m, int64_t n,
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {
-    if (cudaMallocAsync(&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   char* wsb = static_cast<char*>(ws);
@@ -1603,7 +1603,7 @@ lu_status gemm_update_ex(lu_compute compute, cudaStream_t st, int64_t m, int64_t
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {
-    if (cudaMallocAsync(&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, need, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   char* wsb = static_cast<char*>(ws);

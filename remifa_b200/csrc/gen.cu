@@ -128,7 +128,7 @@ lu_status launch_gen_matrix(cudaStream_t st, int64_t n, float* a, int64_t lda,
       kind == 0 ? ldexpf(1.0f, -23)
                 : (float)(ldexp(1.0, -21) / std::sqrt((double)n));
   unsigned long long* rowsum = nullptr;
-  LUB_CUDA_TRY(cudaMallocAsync((void**)&rowsum, n * sizeof(unsigned long long), st));
+  LUB_CUDA_TRY(pool_malloc_async((void**)&rowsum, n * sizeof(unsigned long long), st));
   LUB_CUDA_TRY(cudaMemsetAsync(rowsum, 0, n * sizeof(unsigned long long), st));
   const uint64_t seedmix = host_mix64(seed);
   dim3 grid((unsigned)ceil_div(n, 256), (unsigned)ceil_div(n, kColsPerBlock));

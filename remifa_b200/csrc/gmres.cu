@@ -166,7 +166,7 @@ LU_API lu_status lu_gmres_ir_c(lu_stream_t stream, int64_t n, const float* d_a, 
   void* ws = workspace;
   bool owned = false;
   if (!ws) {
-    if (cudaMallocAsync(&ws, L.bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, L.bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   char* wb = static_cast<char*>(ws);

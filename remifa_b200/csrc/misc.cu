@@ -3,6 +3,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+#include <cstring>
 #include <mutex>
 #include <unordered_map>
 
@@ -117,5 +118,53 @@ extern "C" LU_API lu_status lu_selfcheck_rcp_c(lu_stream_t stream, unsigned long
   LUB_CUDA_TRY(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), st));
   lub::rcp_check_kernel<<<148 * 16, 256, 0, st>>>(0ull, 1ull << 32, d_bad);
   LUB_LAUNCH_CHECK();
+  return LU_SUCCESS;
+}
+
+namespace lub {
+namespace {
+cudaMemPool_t g_pools[64] = {};
+std::mutex g_pool_mu;
+}  // namespace
+
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, st);
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+      cudaMemPoolProps props;
+      std::memset(&props, 0, sizeof(props));
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t np = nullptr;
+      e = cudaMemPoolCreate(&np, &props);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = UINT64_MAX;  // freed memory stays in the pool
+      e = cudaMemPoolSetAttribute(np, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) {
+        cudaMemPoolDestroy(np);
+        return e;
+      }
+      g_pools[dev] = np;
+    }
+    pool = g_pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+}  // namespace lub
+
+extern "C" LU_API lu_status lu_trim_memory_c(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LU_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lk(lub::g_pool_mu);
+  if (dev >= 0 && dev < 64 && lub::g_pools[dev]) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return LU_ERR_CUDA;
+    if (cudaMemPoolTrimTo(lub::g_pools[dev], 0) != cudaSuccess) return LU_ERR_CUDA;
+  }
   return LU_SUCCESS;
 }

@@ -74,7 +74,7 @@ LU_API lu_status lu_solve_c(lu_stream_t stream, int64_t n, const float* d_lu,
   // the solve's counter words and right-hand-side copy come from the
   // stream-ordered allocator
   void* ws = nullptr;
-  if (cudaMallocAsync(&ws, trsm_ws_bytes(n, nrhs), st) != cudaSuccess) return LU_ERR_ALLOC;
+  if (pool_malloc_async((void**)&ws, trsm_ws_bytes(n, nrhs), st) != cudaSuccess) return LU_ERR_ALLOC;
   const lu_status s = launch_lu_solve(
       st, n, d_lu, ldlu, d_x, ldx, nrhs, trans != 0, static_cast<unsigned*>(ws),
       reinterpret_cast<double*>(static_cast<char*>(ws) + trsm_sync_bytes(nrhs)));
@@ -199,7 +199,7 @@ LU_API lu_status lu_refine_ex_c(lu_stream_t stream, int64_t n, int64_t nrhs,
   void* ws = workspace;
   bool owned = false;
   if (!ws) {
-    if (cudaMallocAsync(&ws, w.bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
+    if (pool_malloc_async((void**)&ws, w.bytes, st) != cudaSuccess) return LU_ERR_ALLOC;
     owned = true;
   }
   double e = 0.0;

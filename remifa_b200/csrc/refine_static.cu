@@ -4,7 +4,7 @@
 //
 // lu_refine_c needs a few hundred KB of device scratch per call (residual
 // and correction vectors, column-chunk partial sums, three max accumulators)
-// and takes it from the caller or from cudaMallocAsync.  Some callers can do
+// and takes it from the caller or from a stream-ordered memory pool.  Some callers can do
 // neither: a service whose caching allocator has already reserved the GPU's
 // memory for itself, code that runs where a device allocation would stall
 // or fail (a fixed-footprint real-time loop, a library callback that must

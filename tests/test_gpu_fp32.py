@@ -399,3 +399,21 @@ def test_host_entry_two_step_bulk(built, n, nb, outer):
     e_g = O.nwerr(a, b, O.lu_solve_f32(np.asfortranarray(got), b))
     e_o = O.nwerr(a, b, O.lu_solve_f32(want, b))
     assert e_g <= 2 * e_o and e_o <= 2 * e_g, (e_g, e_o)
+
+
+def test_library_pool_reuse_and_trim(built):
+    """Without a caller workspace the factorization allocates from the
+    library's stream-ordered pool, which keeps the memory between calls;
+    lu_trim_memory_c hands it back.  Results are the same either way."""
+    n = 2048
+    a = rb.gen_matrix(n, seed=41, kind=1, alpha=1.5)
+    outs = []
+    for trim in (False, False, True):
+        d = rb.colmajor(a.clone())
+        info = rb.lu_nopiv_rl(d, nb=256, outer=rb.TC32)
+        torch.cuda.synchronize()
+        assert int(info.item()) == 0
+        outs.append(d)
+        if trim:
+            rb.trim_memory()
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])

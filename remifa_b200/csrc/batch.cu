@@ -70,7 +70,8 @@ constexpr uint32_t kIdesc = make_idesc(0, 0, kTileM, 64);  // fp16, M128 N64
 enum : int { kErrBatchMma = 11 };
 
 struct Misc {
-  uint64_t bar[2];
+  uint64_t bar[2];     // MMA of stage b done
+  uint64_t ld[2];      // stage b's operand image landed
   uint32_t tmem;
   int item;
   int bad;
@@ -90,7 +91,22 @@ struct BatchArgs {
   int* err;
   int ldc;                // leading dimension of the block column in shared memory
   int use_tc;             // any tensor-core item: allocate TMEM
+  uint8_t* img;           // per CTA: fp16 operand images of the factored L
+                          // columns (img_bytes each), tensor-core items
+  int64_t img_bytes;
 };
+
+// Bytes of the L operand images of one matrix (all its block columns but
+// the last): per block column, one 16 KB image per 128-row tile of the rows
+// below it.
+__host__ __device__ inline int64_t img_tiles_before(int n, int NB, int j) {
+  int64_t t = 0;
+  for (int i = 0; i < j; ++i) {
+    const int rows = n - (i + 1) * NB;
+    if (rows > 0) t += (rows + kTileM - 1) / kTileM;
+  }
+  return t;
+}
 
 size_t smem_bytes_for(int nmax) {
   const int ldc = ((nmax + 3) / 4) * 4 + 4;
@@ -317,17 +333,12 @@ __device__ __forceinline__ void outer_fp32(float* C, int ldc, const float* A,
 // two TMEM accumulators, and the epilogue of the previous tile (all eight
 // warps: lane quarter warp%4, 32 columns each) subtracts its product from
 // the block column while the next MMAs run.
-struct TcState {
-  uint32_t phase[2];
-};
-
-__device__ __forceinline__ void tc_epilogue(float* C, int ldc, int n, int wj,
-                                            int m0, int b, uint32_t tmem,
-                                            Misc* ms, TcState& st, int* err) {
+// Epilogue of one tile, its MMAs known complete: all eight warps (lane
+// quarter warp % 4, 32 columns each) subtract the accumulator from the
+// block column.
+__device__ __forceinline__ void tc_epilogue_read(float* C, int ldc, int n, int wj, int m0,
+                                                 int b, uint32_t tmem) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool ok = mbar_wait(&ms->bar[b], st.phase[b], err, kErrBatchMma);
-  st.phase[b] ^= 1u;
-  if (!ok) ms->abort = 1;
   __syncwarp();
   tc_fence_after();
   const int quarter = warp & 3, half = warp >> 2;
@@ -348,65 +359,108 @@ __device__ __forceinline__ void tc_epilogue(float* C, int ldc, int n, int wj,
   tc_fence_before();
 }
 
-__device__ __forceinline__ void outer_tc(float* C, int ldc, const float* A,
-                                         int64_t lda, int n, int r0, int NB,
-                                         int wj, uint8_t* sA, const uint8_t* sB,
-                                         uint32_t tmem, Misc* ms, TcState& st,
-                                         int* err) {
+// Tensor-core outer update from the operand images of block column k
+// (written once, when k was factored): per 128-row tile one 16 KB bulk copy
+// into a stage (two stages, the next tile's copy issued as soon as its
+// stage is free), NB/16 MMAs into one of two TMEM accumulators, and the
+// epilogue of the previous tile (all eight warps) under the MMAs.
+struct TcState {
+  uint32_t phase[2];
+  uint32_t ldph[2];
+};
+
+// The first two tiles' copies, issued (thread 0) before the U_kj solve so
+// that they land while it runs (the stages are free during the solve).
+__device__ __forceinline__ void outer_tc_prefetch(const uint8_t* img, int n, int r0, int NB,
+                                                  uint8_t* sA, Misc* ms) {
+  const int ntiles = (n - r0 - NB + kTileM - 1) / kTileM;
+  if (threadIdx.x == 0) {
+    fence_proxy_async_smem();  // earlier generic accesses to the stages first
+    for (int t = 0; t < 2 && t < ntiles; ++t) {
+      mbar_arrive_expect_tx(&ms->ld[t], kAStage);
+      bulk_load(sA + t * kAStage, img + (size_t)t * kAStage, kAStage, &ms->ld[t]);
+    }
+  }
+}
+
+__device__ __forceinline__ void outer_tc(float* C, int ldc, const uint8_t* img, int n,
+                                         int r0, int NB, int wj, uint8_t* sA,
+                                         const uint8_t* sB, uint32_t tmem, Misc* ms,
+                                         TcState& st, int* err) {
   const int tid = threadIdx.x;
   const int r1 = r0 + NB;
   const int ntiles = (n - r1 + kTileM - 1) / kTileM;
-  const int nch = NB >> 3;
 #pragma unroll 1
   for (int t = 0; t < ntiles; ++t) {
     const int b = t & 1;
     const int m0 = r1 + t * kTileM;
     uint8_t* sa = sA + b * kAStage;
-    // every thread's (up to 4) items: all 32 loads in flight together
-    const int m = tid & (kTileM - 1);
-    const int gr = m0 + m;
-    float x[4][8];
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      const int ch = (tid >> 7) + 2 * it;
-      const bool ok = gr < n && ch < nch;
-      const float* src = A + gr + (int64_t)(r0 + 8 * ch) * lda;
-#pragma unroll
-      for (int e = 0; e < 8; ++e) x[it][e] = ok ? src[(int64_t)e * lda] : 0.0f;
-    }
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      const int ch = (tid >> 7) + 2 * it;
-      if (ch < nch) {
-        __half2 h0 = __floats2half2_rn(x[it][0], x[it][1]);
-        __half2 h1 = __floats2half2_rn(x[it][2], x[it][3]);
-        __half2 h2 = __floats2half2_rn(x[it][4], x[it][5]);
-        __half2 h3 = __floats2half2_rn(x[it][6], x[it][7]);
-        uint4 pk;
-        pk.x = *reinterpret_cast<uint32_t*>(&h0);
-        pk.y = *reinterpret_cast<uint32_t*>(&h1);
-        pk.z = *reinterpret_cast<uint32_t*>(&h2);
-        pk.w = *reinterpret_cast<uint32_t*>(&h3);
-        *reinterpret_cast<uint4*>(sa + m * 128 + ((ch ^ (m & 7)) << 4)) = pk;
-      }
-    }
-    fence_proxy_async_smem();
     tc_fence_before();
-    __syncthreads();
+    __syncthreads();  // accumulator b read out by the epilogue of tile t - 2
     if (tid == 0) {
       tc_fence_after();
+      if (!mbar_wait(&ms->ld[b], st.ldph[b], err, kErrBatchMma)) ms->abort = 1;
       const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sB);
       for (int kq = 0; kq < NB / 16; ++kq)
         mma_f16(tmem + b * 64, sw128_kmajor_desc(a0 + kq * 32),
                 sw128_kmajor_desc(b0 + kq * 32), kIdesc, kq > 0 ? 1u : 0u);
       mma_commit(&ms->bar[b]);
     }
-    if (t > 0) tc_epilogue(C, ldc, n, wj, m0 - kTileM, b ^ 1, tmem, ms, st, err);
+    st.ldph[b] ^= 1u;
+    if (t > 0) {
+      const int bp = b ^ 1;
+      const bool ok = mbar_wait(&ms->bar[bp], st.phase[bp], err, kErrBatchMma);
+      st.phase[bp] ^= 1u;
+      if (!ok) ms->abort = 1;
+      // stage bp is free: the copy of tile t + 1 goes in now
+      if (tid == 0 && t + 1 < ntiles) {
+        mbar_arrive_expect_tx(&ms->ld[bp], kAStage);
+        bulk_load(sA + bp * kAStage, img + (size_t)(t + 1) * kAStage, kAStage, &ms->ld[bp]);
+      }
+      tc_epilogue_read(C, ldc, n, wj, m0 - kTileM, bp, tmem);
+    }
   }
-  if (ntiles > 0)
-    tc_epilogue(C, ldc, n, wj, r1 + (ntiles - 1) * kTileM, (ntiles - 1) & 1, tmem, ms,
-                st, err);
+  if (ntiles > 0) {
+    const int bl = (ntiles - 1) & 1;
+    const bool ok = mbar_wait(&ms->bar[bl], st.phase[bl], err, kErrBatchMma);
+    st.phase[bl] ^= 1u;
+    if (!ok) ms->abort = 1;
+    tc_epilogue_read(C, ldc, n, wj, r1 + (ntiles - 1) * kTileM, bl, tmem);
+  }
+  tc_fence_before();
   __syncthreads();
+}
+
+// The operand images of block column c0 / NB, from the factored block
+// column in shared memory (global row r, local column c at C[r + c ldc]):
+// rows [c0 + NB, n) of its NB columns, fp16, one
+// 128-row K-major tile with the 128-byte swizzle per 16 KB (rows past n
+// zero), exactly what a stage of the outer update holds.
+__device__ __forceinline__ void write_images(const float* C, int ldc, int n, int c0, int NB,
+                                             uint8_t* img) {
+  const int r1 = c0 + NB;
+  const int ntiles = (n - r1 + kTileM - 1) / kTileM;
+  const int nch = NB >> 3;
+  for (int idx = threadIdx.x; idx < ntiles * kTileM * nch; idx += kT) {
+    const int ch = idx % nch, rem = idx / nch;
+    const int m = rem % kTileM, t = rem / kTileM;
+    const int gr = r1 + t * kTileM + m;
+    uint4 pk = make_uint4(0, 0, 0, 0);
+    if (gr < n) {
+      float x[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) x[e] = C[gr + (8 * ch + e) * ldc];  // local columns
+      __half2 h0 = __floats2half2_rn(x[0], x[1]);
+      __half2 h1 = __floats2half2_rn(x[2], x[3]);
+      __half2 h2 = __floats2half2_rn(x[4], x[5]);
+      __half2 h3 = __floats2half2_rn(x[6], x[7]);
+      pk.x = *reinterpret_cast<uint32_t*>(&h0);
+      pk.y = *reinterpret_cast<uint32_t*>(&h1);
+      pk.z = *reinterpret_cast<uint32_t*>(&h2);
+      pk.w = *reinterpret_cast<uint32_t*>(&h3);
+    }
+    *reinterpret_cast<uint4*>(img + (size_t)t * kAStage + m * 128 + ((ch ^ (m & 7)) << 4)) = pk;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -426,6 +480,8 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
   if (tid == 0) {
     mbar_init(&ms->bar[0], 1);
     mbar_init(&ms->bar[1], 1);
+    mbar_init(&ms->ld[0], 1);
+    mbar_init(&ms->ld[1], 1);
     fence_barrier_init();
     ms->abort = 0;
   }
@@ -436,6 +492,8 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
   const uint32_t tmem = a.use_tc ? ms->tmem : 0u;
   TcState st;
   st.phase[0] = st.phase[1] = 0u;
+  st.ldph[0] = st.ldph[1] = 0u;
+  uint8_t* img = a.img ? a.img + (size_t)blockIdx.x * (size_t)a.img_bytes : nullptr;
 
 #pragma unroll 1
   for (;;) {
@@ -465,6 +523,9 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
 #pragma unroll 1
       for (int k = 0; k < j; ++k) {
         const int r0 = k * NB;
+        if (tc && r0 + NB < n)
+          outer_tc_prefetch(img + (size_t)img_tiles_before(n, NB, k) * kAStage, n, r0, NB, sA,
+                            ms);
         async_block(A + r0 + (int64_t)r0 * lda, lda, NB, NB, false,
                     [&](int r, int c) { return &Lkk[r * kLDT + c]; });
         __syncthreads();
@@ -472,7 +533,9 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
         if (tc) fence_proxy_async_smem();
         __syncthreads();
         if (r0 + NB < n) {
-          if (tc) outer_tc(C, ldc, A, lda, n, r0, NB, wj, sA, sB, tmem, ms, st, a.err);
+          if (tc)
+            outer_tc(C, ldc, img + (size_t)img_tiles_before(n, NB, k) * kAStage, n, r0, NB, wj,
+                     sA, sB, tmem, ms, st, a.err);
           else outer_fp32(C, ldc, A, lda, n, r0, NB, wj, sA, sB);
         }
         if (ms->abort) break;
@@ -480,6 +543,12 @@ __global__ void __launch_bounds__(kT, 1) batch_lu_kernel(BatchArgs a) {
       if (ms->abort) break;
       rows::panel_block<kT>(C, ldc, n, c0, wj, &ms->inv[0][0], &ms->bad, c0);
       store_block(A + (int64_t)c0 * lda, lda, n, wj, vec, C, ldc);
+      // the later block columns' outer updates read this one's L rows as
+      // fp16 operand images, by bulk copy
+      if (tc && j + 1 < nblk) {
+        write_images(C, ldc, n, c0, NB, img + (size_t)img_tiles_before(n, NB, j) * kAStage);
+        fence_proxy_async_global();
+      }
       __syncthreads();
     }
     if (tid == 0)
@@ -532,6 +601,9 @@ struct lu_batch_plan_t {
   int ctas = 0;
   size_t smem = 0;
   bool use_tc = false;
+  uint8_t* d_img = nullptr;  // per CTA: operand images (tensor-core items)
+  int64_t img_bytes = 0;
+  size_t img_alloc = 0;
   lu_opts opts{};
 };
 
@@ -566,6 +638,22 @@ lu_status upload_cfg(lu_batch_plan_t* p) {
       &per_sm, batch_lu_kernel, kT, p->smem));
   if (per_sm < 1) return LU_ERR_UNSUPPORTED;
   p->ctas = (int)std::min<int64_t>((int64_t)sms * per_sm, p->batch);
+  // operand images: the largest matrix's, at the block width needing most
+  p->img_bytes = 0;
+  if (p->use_tc) {
+    const int nm = p->nmax;
+    for (int NB : {32, 64})
+      p->img_bytes = std::max<int64_t>(p->img_bytes,
+                                       img_tiles_before(nm, NB, (nm + NB - 1) / NB) * kAStage);
+    const size_t need = (size_t)p->ctas * (size_t)p->img_bytes;
+    if (need > p->img_alloc) {
+      cudaFree(p->d_img);
+      p->d_img = nullptr;
+      p->img_alloc = 0;
+      if (cudaMalloc(&p->d_img, need) != cudaSuccess) return LU_ERR_ALLOC;
+      p->img_alloc = need;
+    }
+  }
   return LU_SUCCESS;
 }
 
@@ -602,6 +690,8 @@ lu_status launch_plan(const lu_batch_plan_t* p, cudaStream_t st, float* const* d
   a.err = p->d_counter + 1;
   a.ldc = ((p->nmax + 3) / 4) * 4 + 4;
   a.use_tc = p->use_tc ? 1 : 0;
+  a.img = p->use_tc ? p->d_img : nullptr;
+  a.img_bytes = p->img_bytes;
   const int ctas = (int)std::min<int64_t>(p->ctas, count);
   batch_lu_kernel<<<ctas, kT, p->smem, st>>>(a);
   LUB_LAUNCH_CHECK();
@@ -672,6 +762,7 @@ LU_API void lu_batch_plan_destroy(lu_batch_plan plan) {
   cudaFree(plan->d_order);
   cudaFree(plan->d_cfg);
   cudaFree(plan->d_counter);
+  cudaFree(plan->d_img);
   delete plan;
 }
 

@@ -1359,6 +1359,18 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
   return LU_SUCCESS;
 }
 
+// The internal streams and events of a device (dev_streams) are shared by
+// every call on it, so one host thread at a time enqueues a factorization
+// on a device: each call's work is queued whole, with its events recorded
+// and waited for under this lock, and calls from several threads run one
+// after another on the internal streams.
+static std::mutex& device_mutex() {
+  static std::mutex mu[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  return mu[dev & 63];
+}
+
 lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
                     void* d_a, lu_dtype dtype_a, int64_t lda, int* d_info,
                     void* d_a_lowp, int64_t ld_lowp, void* workspace,
@@ -1377,6 +1389,7 @@ lu_status factorize(const lu_opts& o, cudaStream_t st, int64_t m, int64_t n,
     return LU_ERR_INVALID_ARG;
   LUB_TRY(check_device());
   if (workspace != nullptr && ws_bytes < p.ws_bytes) return LU_ERR_WORKSPACE;
+  std::lock_guard<std::mutex> lock(device_mutex());
 
   void* ws = workspace;
   bool owned = false;
@@ -1422,6 +1435,7 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
   LUB_TRY(make_plan(o, n, n, LU_F32, &p));
   LUB_TRY(check_device());
   if (workspace != nullptr && ws_bytes < p.ws_bytes) return LU_ERR_WORKSPACE;
+  std::lock_guard<std::mutex> lock(device_mutex());
   void* ws = workspace;
   bool owned = false;
   if (ws == nullptr) {

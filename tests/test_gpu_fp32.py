@@ -417,3 +417,55 @@ def test_library_pool_reuse_and_trim(built):
         if trim:
             rb.trim_memory()
     assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
+
+
+def test_concurrent_calls_from_two_threads(built):
+    """Two host threads factor different matrices at once, each on its own
+    stream (the library's internal streams are shared per device; a call is
+    enqueued whole under a per-device lock): each result equals the same
+    factorization run alone."""
+    import threading
+    n = 2048
+    mats = [rb.gen_matrix(n, seed=50 + i, kind=1, alpha=1.5) for i in range(2)]
+    alone = []
+    for m in mats:
+        d = rb.colmajor(m.clone())
+        rb.lu_nopiv_rl(d, nb=256, outer=rb.TC32)
+        alone.append(d)
+    torch.cuda.synchronize()
+    for variant in ("rl", "ll"):
+        outs = [rb.colmajor(m.clone()) for m in mats]
+        refs = []
+        for m in mats:
+            d = rb.colmajor(m.clone())
+            if variant == "rl":
+                rb.lu_nopiv_rl(d, nb=256, outer=rb.TC32)
+            else:
+                rb.lu_nopiv_ll(d, nb=256, outer=rb.TC32)
+            refs.append(d)
+        torch.cuda.synchronize()
+        streams = [torch.cuda.Stream() for _ in mats]
+        errs = []
+
+        def work(i):
+            try:
+                for _ in range(3):
+                    with torch.cuda.stream(streams[i]):
+                        outs[i].copy_(mats[i])
+                        if variant == "rl":
+                            rb.lu_nopiv_rl(outs[i], nb=256, outer=rb.TC32, stream=streams[i])
+                        else:
+                            rb.lu_nopiv_ll(outs[i], nb=256, outer=rb.TC32, stream=streams[i])
+                    streams[i].synchronize()
+            except Exception as e:  # pragma: no cover - reported below
+                errs.append(e)
+
+        ts = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        torch.cuda.synchronize()
+        assert not errs, errs
+        for i in range(2):
+            assert torch.equal(outs[i], refs[i]), (variant, i)

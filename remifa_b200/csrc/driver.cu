@@ -181,9 +181,13 @@ struct DevStreams {
   cudaStream_t copy_out = nullptr;  // device-to-host, concurrent with `copy`
   cudaStream_t catchup = nullptr;   // the host entry's catch_up of arrived chunks
   cudaStream_t catchup_bulk = nullptr;  // its bulk updates (look-ahead)
+  cudaStream_t catchup_early = nullptr;  // left-looking catch-up: early partial products
   cudaEvent_t cu_done = nullptr;
   cudaEvent_t cu_packed = nullptr, cu_u2[2] = {nullptr, nullptr}, cu_join = nullptr;
   cudaEvent_t cu_out = nullptr;  // a chunk's catch-up done: its rows above it can go out
+  // left-looking catch-up: a block row's solved rows are packed (cu_xp);
+  // the early partial products of the block row of each parity are done
+  cudaEvent_t cu_xp = nullptr, cu_early[2] = {nullptr, nullptr};
   // per outer step of the host entry: the step's block column is final
   // once what was queued on the panel (p) and side (s) streams has run
   std::vector<cudaEvent_t> step_p, step_s;
@@ -222,8 +226,10 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.out_done, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_bulk, cudaStreamNonBlocking, least));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_early, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
-    for (cudaEvent_t* e : {&d.cu_packed, &d.cu_u2[0], &d.cu_u2[1], &d.cu_join, &d.cu_out})
+    for (cudaEvent_t* e : {&d.cu_packed, &d.cu_u2[0], &d.cu_u2[1], &d.cu_join, &d.cu_out,
+                           &d.cu_xp, &d.cu_early[0], &d.cu_early[1]})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
@@ -932,6 +938,40 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   return status;
 }
 
+// The U part of outer step ofs (block width in) for the columns [c0, c0 +
+// nc) right of its block: the unit-lower solves with the block's diagonal
+// sub-blocks and the rank-w update between them, exactly as factor_block
+// applies them to a column right of the block.  With xp given, the solved
+// rows also go to the fp16 / bf16 B operand xp (column j of the range at
+// xp[j * ldx + ofs + i]).
+static lu_status u_solve_cols(const Plan& p, cudaStream_t st, float* a, int64_t lda,
+                              int64_t ofs, int64_t in, int64_t c0, int64_t nc,
+                              void* xp = nullptr, int64_t ldx = 0, bool bf16 = false) {
+  float* blk = a + ofs + ofs * lda;
+  for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
+    const int dw = (int)std::min<int64_t>(in - p0, p.diag_w);
+    float* dg = blk + p0 + p0 * lda;
+    {
+      ProfScope ps("lupanel", st, 8.0 * nc * dw, (double)nc * dw * dw);
+      LuPack pk;
+      pk.pb = xp;
+      pk.ldk = ldx;
+      pk.k0 = (int)(ofs + p0);
+      pk.bf16 = bf16;
+      LUB_TRY(launch_lupanel(st, dg, lda, dw, 0, nc, false, 0, c0 - (ofs + p0 + dw),
+                             xp ? &pk : nullptr));
+    }
+    if (p0 + dw < in) {
+      ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * dw * (double)(in - p0 - dw) * nc);
+      LUB_TRY(launch_sgemm_chunk8_2(st, 0, 0, 0, nullptr, lda, nullptr, lda, nullptr, lda,
+                                    in - (p0 + dw), nc, dw, dg + dw, lda,
+                                    blk + p0 + (c0 - ofs) * lda, lda,
+                                    blk + (p0 + dw) + (c0 - ofs) * lda, lda));
+    }
+  }
+  return LU_SUCCESS;
+}
+
 // Give the columns [c0, c1) (all rows) the outer steps whose blocks start
 // before c0, in step order: per step the U part of its panel -- the
 // unit-lower solves with the outer block's diagonal sub-blocks and the
@@ -978,22 +1018,7 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
       if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_u2[t % 2], 0));
     }
     const int64_t in = std::min(n - ofs, nb);
-    float* blk = a + ofs + ofs * lda;
-    for (int64_t p0 = 0; p0 < in; p0 += p.diag_w) {
-      const int dw = (int)std::min<int64_t>(in - p0, p.diag_w);
-      float* dg = blk + p0 + p0 * lda;
-      {
-        ProfScope ps("lupanel", st, 8.0 * nc * dw, (double)nc * dw * dw);
-        LUB_TRY(launch_lupanel(st, dg, lda, dw, 0, nc, false, 0, c0 - (ofs + p0 + dw)));
-      }
-      if (p0 + dw < in) {
-        ProfScope ps("sgemm_chunk8", st, 0.0, 2.0 * dw * (double)(in - p0 - dw) * nc);
-        LUB_TRY(launch_sgemm_chunk8_2(st, 0, 0, 0, nullptr, lda, nullptr, lda, nullptr, lda,
-                                      in - (p0 + dw), nc, dw, dg + dw, lda,
-                                      blk + p0 + (c0 - ofs) * lda, lda,
-                                      blk + (p0 + dw) + (c0 - ofs) * lda, lda));
-      }
-    }
+    LUB_TRY(u_solve_cols(p, st, a, lda, ofs, in, c0, nc));
     const int64_t tr = n - (ofs + nb);
     if (tr <= 0) continue;
     const int64_t cr = c0 - (ofs + nb);  // column offset in the trailing part
@@ -1046,6 +1071,131 @@ static lu_status catch_up(const Plan& p, cudaStream_t st, float* a, int64_t lda,
     LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sb));
     LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   }
+  return LU_SUCCESS;
+}
+
+// Operands of the left-looking catch-up (catch_up_ll), kept across the
+// chunks of one host-entry call: the L columns of every outer step left of
+// the last chunk as tensor-core A rows (lp, row stride ldl elements, column
+// k of L at element k), the solved U rows of the current chunk as B
+// columns (xp, stride ldx), and the split-K slabs of its block-row updates.
+struct LlCatchup {
+  char* lp = nullptr;
+  int64_t ldl = 0;
+  char* xp = nullptr;
+  int64_t ldx = 0;
+  float* part = nullptr;  // kLlCatchupSplitMax slabs of `slab` floats
+  int64_t slab = 0;
+  int ksplit_max = 1;
+  int64_t npacked = 0;  // outer steps whose L columns are in lp
+};
+constexpr int kLlCatchupSplitMax = 8;
+// outer steps per pass over the chunk's rows below c0, and per copy out
+constexpr int kLlCatchupGroup = 8;
+
+// The catch-up of the columns [c0, c1) in left-looking order (unscaled fp16 /
+// bf16 operands, several outer steps per bulk pass): block row t of the
+// chunk (rows [t nb, (t+1) nb)) first receives the products of all earlier
+// steps (K = t nb), then the U part of step t (u_solve_cols), whose solves
+// also write the solved rows as the B operand of the later block rows.  The
+// products with the solved rows of steps up to t-2 (the early part, K =
+// (t-1) nb: split-K partial products in fixed slabs, summed in split order,
+// so every run gives the same result) are computed and subtracted on
+// S->catchup_early while block row t-1 is solved; only the last step's
+// product (K = nb) stays on the chain of solves.  The rows [c0, n) receive
+// L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
+// rows come in, and each group's solved rows go to the host at once on
+// sink.out.  Against the step-by-step catch-up this saves the per-step
+// passes over all rows below each block row (the chain of solves runs
+// beside fewer, larger updates); the sums are rounded once per update
+// instead of once per step, as in the grouped bulk passes of the
+// factorization itself.
+static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t lda,
+                             LlCatchup* cu, int* err, int64_t c0, int64_t c1, DevStreams* S,
+                             const ColumnSink& sink) {
+  const int64_t n = p.n, nb = p.nb, nc = c1 - c0;
+  const TcOperand kind = tc_kind(p.outer);
+  const int64_t es = tc_operand_bytes(kind);
+  cudaStream_t sb = S->catchup_bulk, se = S->catchup_early;
+  LUB_CUDA_TRY(cudaEventRecord(S->cu_join, st));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_join, 0));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_join, 0));
+  const int ctas = std::max(1, sm_count() * 3 / 4);
+  const int64_t nsteps = ceil_div(c0, nb);
+  int64_t k0 = 0;  // first row of the group whose bulk pass is pending
+  for (int64_t t = 0; t < nsteps; ++t) {
+    const int64_t ofs = t * nb, in = std::min(nb, c0 - ofs);
+    LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[t], 0));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[t], 0));
+    if (t >= cu->npacked) {
+      // step t's L columns (rows ofs.., final now) as A rows
+      ProfScope ps("pack_operands", st, (4.0 + es) * (double)(n - ofs) * in);
+      LUB_TRY(launch_pack_a(st, kind, n - ofs, in, a + ofs + ofs * lda, lda,
+                            cu->lp + (ofs * cu->ldl + ofs) * es, cu->ldl, nullptr));
+      cu->npacked = t + 1;
+    }
+    float* rows = a + ofs + c0 * lda;
+    if (t > 0) {
+      // the product with the solved rows of step t-1 (the earlier ones were
+      // subtracted on se)
+      const int64_t k_late = ofs - nb;
+      if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_early[t % 2], 0));
+      ProfScope ps("tc_update", st, 8.0 * in * nc + (double)es * (in + nc) * nb,
+                   2.0 * in * (double)nc * nb);
+      LUB_TRY(launch_tc_update(st, kind, in, nc, nb, -1.0f,
+                               cu->lp + (ofs * cu->ldl + k_late) * es, cu->ldl,
+                               cu->xp + k_late * es, cu->ldx, rows, lda, nullptr, nullptr, err));
+    }
+    LUB_TRY(u_solve_cols(p, st, a, lda, ofs, in, c0, nc, cu->xp, cu->ldx,
+                         kind == TcOperand::BF16));
+    // block row t+2's early part (K = (t+1) nb: the solved rows up to this
+    // one) beside the solve of block row t+1
+    if (t + 2 < nsteps) {
+      const int64_t o2 = ofs + 2 * nb, ke = ofs + nb;
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_xp, st));
+      LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_xp, 0));
+      const int64_t in2 = std::min(nb, c0 - o2);
+      const int64_t tiles = ceil_div(in2, 128) * ceil_div(nc, 256);
+      const int ks = tc_split_choice(tiles, ke, (int)es, sm_count(), cu->ksplit_max);
+      int ns = 0;
+      {
+        ProfScope ps("tc_update", se, 4.0 * ks * in2 * nc + (double)es * (in2 + nc) * ke,
+                     2.0 * in2 * (double)nc * ke);
+        LUB_TRY(launch_tc_partials(se, kind, in2, nc, ke, cu->lp + o2 * cu->ldl * es, cu->ldl,
+                                   cu->xp, cu->ldx, ks, cu->part, 0, &ns, err));
+      }
+      {
+        ProfScope ps("splitk_finish", se, 4.0 * (ns + 2) * (double)in2 * nc);
+        LUB_TRY(launch_splitk_finish(se, in2, nc, ns, cu->part, -1.0f, a + o2 + c0 * lda, false,
+                                     lda, nullptr, 0));
+      }
+      LUB_CUDA_TRY(cudaEventRecord(S->cu_early[t % 2], se));
+    }
+    const int64_t k1 = ofs + in;
+    if ((t + 1) % kLlCatchupGroup != 0 && t + 1 < nsteps) continue;
+    LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
+    if (n > c0) {
+      ProfScope ps("tc_update", sb, 8.0 * (n - c0) * nc + (double)es * (n - c0 + nc) * (k1 - k0),
+                   2.0 * (n - c0) * (double)nc * (k1 - k0));
+      LUB_TRY(launch_tc_update(sb, kind, n - c0, nc, k1 - k0, -1.0f,
+                               cu->lp + (c0 * cu->ldl + k0) * es, cu->ldl, cu->xp + k0 * es,
+                               cu->ldx, a + c0 + c0 * lda, lda, nullptr, nullptr, err, ctas, 0));
+    }
+    // rows [k0, k1) of the chunk are final: out at once
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sink.out, S->cu_packed, 0));
+    {
+      ProfScope ps("copy_d2h", sink.out, 4.0 * (double)(k1 - k0) * nc);
+      LUB_CUDA_TRY(cudaMemcpy2DAsync(sink.h + k0 + c0 * sink.ldh, (size_t)sink.ldh * 4,
+                                     a + k0 + c0 * lda, (size_t)lda * 4, (size_t)(k1 - k0) * 4,
+                                     (size_t)nc, cudaMemcpyDeviceToHost, sink.out));
+    }
+    k0 = k1;
+  }
+  LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sb));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
+  LUB_CUDA_TRY(cudaEventRecord(S->cu_join, se));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   return LU_SUCCESS;
 }
 
@@ -1494,7 +1644,27 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
     TcWs wcu[2] = {wk, wk};
     char* cubuf = wsb;
     void* cu_alloc = nullptr;
-    if (s == LU_SUCCESS && la && tc) {
+    // several steps per bulk pass: the left-looking catch-up (catch_up_ll);
+    // one pass per step keeps the step-by-step order of the device entry
+    const bool llc = la && tc && !tc_scaled(kind) && p.bulk_group >= 2;
+    LlCatchup llb;
+    if (s == LU_SUCCESS && llc) {
+      const int64_t c_last = (ceil_div(n, cw) - 1) * cw;  // first column of the last chunk
+      const int64_t es = tc_operand_bytes(kind);
+      llb.ldl = align_up(c_last, 64);
+      llb.ldx = llb.ldl;
+      llb.ksplit_max = kLlCatchupSplitMax;
+      const size_t lp_bytes = align_up((size_t)n * llb.ldl * es, 1024);
+      const size_t xp_bytes = align_up((size_t)llb.ldx * cw * es, 1024);
+      llb.slab = splitk_slab_floats(nb, cw);
+      const size_t part_bytes = (size_t)kLlCatchupSplitMax * llb.slab * 4;
+      if (pool_malloc_async((void**)&cu_alloc, lp_bytes + xp_bytes + part_bytes, st) !=
+          cudaSuccess)
+        s = LU_ERR_ALLOC;
+      llb.lp = static_cast<char*>(cu_alloc);
+      llb.xp = llb.lp + lp_bytes;
+      llb.part = reinterpret_cast<float*>(llb.xp + xp_bytes);
+    } else if (s == LU_SUCCESS && la && tc) {
       wcu[0] = tc_ws_layout(0, n - nb, n - nb, nb, kind);
       wcu[1] = tc_ws_layout(wcu[0].bytes, n - nb, n - nb, nb, kind);
       if (pool_malloc_async((void**)&cu_alloc, wcu[0].bytes + wcu[1].bytes, st) != cudaSuccess)
@@ -1516,7 +1686,11 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
       for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
         const int64_t c1 = std::min(n, c0 + cw);
         if (!ok(cudaStreamWaitEvent(cu, S->chunk_in[q], 0))) break;
-        if (q > 0) {
+        if (q > 0 && llc) {
+          // (its rows above c0 go out group by group inside)
+          if ((s = catch_up_ll(p, cu, d_a, ldda, &llb, err, c0, c1, S, sink)) != LU_SUCCESS)
+            break;
+        } else if (q > 0) {
           s = catch_up(p, cu, d_a, ldda, cubuf, wcu, err, c0, c1, la ? S : nullptr);
           if (s != LU_SUCCESS) break;
           // the rows [0, c0) of the chunk are final now: out at once, ahead

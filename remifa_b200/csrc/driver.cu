@@ -192,6 +192,7 @@ struct DevStreams {
   // once what was queued on the panel (p) and side (s) streams has run
   std::vector<cudaEvent_t> step_p, step_s;
   cudaEvent_t chunk_in[kMaxChunks] = {};
+  cudaEvent_t chunk_top[kMaxChunks] = {};  // the rows above a chunk's first column are in
   cudaEvent_t out_done = nullptr;
   cudaEvent_t diag_done = nullptr, small_done = nullptr, big_done = nullptr;
   cudaEvent_t diag1_done = nullptr;
@@ -222,6 +223,7 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithFlags(&d.copy_out, cudaStreamNonBlocking));
     for (int q = 0; q < kMaxChunks; ++q) {
       LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.chunk_in[q], cudaEventDisableTiming));
+      LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.chunk_top[q], cudaEventDisableTiming));
     }
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.out_done, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup, cudaStreamNonBlocking, least));
@@ -1104,21 +1106,25 @@ constexpr int kLlCatchupGroup = 8;
 // S->catchup_early while block row t-1 is solved; only the last step's
 // product (K = nb) stays on the chain of solves.  The rows [c0, n) receive
 // L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
-// rows come in, and each group's solved rows go to the host at once on
-// sink.out.  Against the step-by-step catch-up this saves the per-step
+// rows come in (the chunk's rows [c0, n) may still be arriving when the
+// chain starts: rows_in marks them in), and each group's solved rows go to
+// the host at once on sink.out.  Against the step-by-step catch-up this saves the per-step
 // passes over all rows below each block row (the chain of solves runs
 // beside fewer, larger updates); the sums are rounded once per update
 // instead of once per step, as in the grouped bulk passes of the
 // factorization itself.
 static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t lda,
                              LlCatchup* cu, int* err, int64_t c0, int64_t c1, DevStreams* S,
-                             const ColumnSink& sink) {
+                             const ColumnSink& sink, cudaEvent_t rows_in) {
   const int64_t n = p.n, nb = p.nb, nc = c1 - c0;
   const TcOperand kind = tc_kind(p.outer);
   const int64_t es = tc_operand_bytes(kind);
   cudaStream_t sb = S->catchup_bulk, se = S->catchup_early;
   LUB_CUDA_TRY(cudaEventRecord(S->cu_join, st));
   LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_join, 0));
+  // the passes over the rows [c0, n) wait for them to arrive (rows_in); the
+  // chain of block rows needs only the rows above c0
+  LUB_CUDA_TRY(cudaStreamWaitEvent(sb, rows_in, 0));
   LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_join, 0));
   const int ctas = std::max(1, sm_count() * 3 / 4);
   const int64_t nsteps = ceil_div(c0, nb);
@@ -1676,19 +1682,38 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         (!la || ok(cudaStreamWaitEvent(cu, S->fork, 0)))) {
       int q = 0;
       for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
-        {
-          ProfScope ps("copy_h2d", ci, 4.0 * (double)n * (std::min(n, c0 + cw) - c0));
-          if (!ok(h2d(ci, c0, std::min(n, c0 + cw)))) break;
+        const int64_t c1 = std::min(n, c0 + cw);
+        if (llc && q > 0) {
+          // the rows above c0 first: the chunk's catch-up chain starts on
+          // them while its lower rows are still on the way
+          {
+            ProfScope ps("copy_h2d", ci, 4.0 * (double)c0 * (c1 - c0));
+            if (!ok(cudaMemcpy2DAsync(d_a + c0 * ldda, (size_t)ldda * 4, h_a + c0 * lda,
+                                      (size_t)lda * 4, (size_t)c0 * 4, (size_t)(c1 - c0),
+                                      cudaMemcpyHostToDevice, ci)))
+              break;
+          }
+          if (!ok(cudaEventRecord(S->chunk_top[q], ci))) break;
+          ProfScope ps("copy_h2d", ci, 4.0 * (double)(n - c0) * (c1 - c0));
+          if (!ok(cudaMemcpy2DAsync(d_a + c0 + c0 * ldda, (size_t)ldda * 4, h_a + c0 + c0 * lda,
+                                    (size_t)lda * 4, (size_t)(n - c0) * 4, (size_t)(c1 - c0),
+                                    cudaMemcpyHostToDevice, ci)))
+            break;
+        } else {
+          ProfScope ps("copy_h2d", ci, 4.0 * (double)n * (c1 - c0));
+          if (!ok(h2d(ci, c0, c1))) break;
         }
         if (!ok(cudaEventRecord(S->chunk_in[q], ci))) break;
       }
       q = 0;
       for (int64_t c0 = 0; c0 < n && s == LU_SUCCESS; c0 += cw, ++q) {
         const int64_t c1 = std::min(n, c0 + cw);
-        if (!ok(cudaStreamWaitEvent(cu, S->chunk_in[q], 0))) break;
+        if (!ok(cudaStreamWaitEvent(cu, llc && q > 0 ? S->chunk_top[q] : S->chunk_in[q], 0)))
+          break;
         if (q > 0 && llc) {
           // (its rows above c0 go out group by group inside)
-          if ((s = catch_up_ll(p, cu, d_a, ldda, &llb, err, c0, c1, S, sink)) != LU_SUCCESS)
+          if ((s = catch_up_ll(p, cu, d_a, ldda, &llb, err, c0, c1, S, sink, S->chunk_in[q])) !=
+              LU_SUCCESS)
             break;
         } else if (q > 0) {
           s = catch_up(p, cu, d_a, ldda, cubuf, wcu, err, c0, c1, la ? S : nullptr);

@@ -345,16 +345,16 @@ def time_to_solution(rb, torch, base, n, nb, outer, la, tol=1e-14, reps=2, solve
 def isolated_update_roofline(rb, torch, outer, n, nb, la, peaks, reps=3) -> dict:
     """The dominant kernel alone: the factorization's largest trailing-update
     launch shape -- under look-ahead with fp16 / bf16 updates the first bulk
-    pass of four outer steps (M = N = n - 6 nb, K = 4 nb, the CTA-pair
+    pass of six outer steps (M = N = n - 8 nb, K = 6 nb, the CTA-pair
     kernel), else the first step's bulk (M = N = n - 3 nb, K = nb) -- run
     through the library's update entry on one stream with nothing
     concurrent; the tensor-core launch is timed with CUDA events on its
     stream (the operand packing, a separate launch, is not counted).  At
-    K = 4 nb = 1024 each C element's 8 bytes carry 2K = 2048 flops (AI 256
-    flop/B, at the ridge of the measured peaks), so the bound reported is
-    the tensor pipe; the HBM fraction is given beside it."""
+    K = 6 nb = 1536 each C element's 8 bytes carry 2K = 3072 flops (AI 384
+    flop/B, above the ridge of the measured peaks), so the bound reported
+    is the tensor pipe; the HBM fraction is given beside it."""
     grouped = la and outer in (rb.TC32, rb.compute_type.TC32_BF16)
-    q = 4 if grouped else 1
+    q = 6 if grouped else 1
     m = n - (q + 2 if grouped else 3) * nb
     k = q * nb
     g = torch.Generator(device="cuda")
@@ -373,7 +373,7 @@ def isolated_update_roofline(rb, torch, outer, n, nb, la, peaks, reps=3) -> dict
     gbs = e["bytes"] / sec / 1e9
     tfs = e["flops"] / sec / 1e12
     alg = e["bytes"] / e["launches"]
-    prof_name = "tc_update_pair_update_m8192_k1024" if grouped else "tc_update_update_m8192_k512"
+    prof_name = "tc_update_pair_update_m8192_k1536" if grouped else "tc_update_update_m8192_k512"
     tr = profiled_traffic(prof_name)
     del a, b, c
     torch.cuda.empty_cache()

@@ -89,7 +89,7 @@ typedef struct lu_opts {
                            src/lu_nopiv_ll.hxx:172-201); 0 rounds the update
                            to fp16 first (OP = fp16).  Ignored for fp32 storage. */
   int32_t bulk_steps;   /* right-looking with look-ahead and fp16 / bf16 trailing
-                           updates: q = 2, 3 or 4 consecutive outer steps'
+                           updates: q = 2 .. 8 consecutive outer steps'
                            updates of the bulk of the trailing matrix in one
                            pass (C - (L_k U_k + ... + L_k+q-1 U_k+q-1), one
                            fp32 accumulator, C read and written once per q

@@ -143,7 +143,7 @@ def lu_nopiv_rl(a: torch.Tensor, nb: int = 256, inner=FP32, outer=FP32,
     """In-place right-looking no-pivot LU of the column-major CUDA matrix `a`
     (remifa::lu_nopiv_rl).  Returns the device info tensor (0 = success,
     k > 0 = first bad pivot, 1-based).  Asynchronous on `stream`.
-    bulk_steps: q = 2, 3 or 4 lets q consecutive outer steps share one pass
+    bulk_steps: q = 2 .. 8 lets q consecutive outer steps share one pass
     over the bulk of the trailing matrix (fp16 / bf16 updates with
     look-ahead; 0 = the default, 4), 1 applies every step separately (the
     reference's rounding order)."""

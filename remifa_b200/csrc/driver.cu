@@ -175,6 +175,7 @@ static lu_status tc_update_fp32(cudaStream_t st, TcOperand kind, int64_t M,
 // Internal streams of one device: panel work runs at the highest priority,
 // the bulk of each trailing update at the lowest, ordered by two events.
 constexpr int kMaxChunks = 16;  // column chunks of the host-memory entry
+constexpr int kMaxBulkSteps = 8;  // outer steps per bulk pass (bulk_steps)
 
 struct DevStreams {
   cudaStream_t panel = nullptr, update = nullptr, copy = nullptr, side = nullptr;
@@ -200,7 +201,7 @@ struct DevStreams {
   cudaEvent_t copied = nullptr;
   cudaEvent_t fork = nullptr, join_p = nullptr, join_u = nullptr;
   cudaEvent_t packed = nullptr, updated = nullptr;
-  cudaEvent_t done_with[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // U2 done reading buffer b
+  cudaEvent_t done_with[kMaxBulkSteps + 2] = {};  // U2 done reading buffer b
   // left-looking look-ahead: the previous block is queued (ll_ready); the
   // early partial products of the block of each parity are done (ll_early)
   cudaEvent_t ll_ready = nullptr, ll_early[2] = {nullptr, nullptr};
@@ -235,12 +236,13 @@ static lu_status dev_streams(DevStreams** out) {
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t* e : {&d.fork, &d.join_p, &d.join_u, &d.packed, &d.updated,
-                           &d.done_with[0], &d.done_with[1], &d.done_with[2],
-                           &d.done_with[3], &d.done_with[4], &d.done_with[5], &d.copied,
+                           &d.copied,
                            &d.diag_done, &d.small_done, &d.big_done, &d.diag1_done,
                            &d.u1_done, &d.join_s,
                            &d.spack_done, &d.ll_ready, &d.ll_early[0], &d.ll_early[1]})
       LUB_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (cudaEvent_t& e : d.done_with)
+      LUB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     it = cache.emplace(dev, d).first;
   }
   *out = &it->second;
@@ -293,9 +295,10 @@ static size_t ll_part_layout(Plan* p, size_t off) {
 }
 
 // Outer steps whose bulk trailing updates share one pass by default: the
-// pass then has K = 4 nb = 1024 (AI 256 flop/B of C traffic, where the
-// CTA-pair update reaches ~1 PFLOP/s on B200).
-constexpr int kBulkSteps = 4;
+// pass then has K = 6 nb = 1536 (AI 384 flop/B of C traffic).  B200, TC32,
+// nb = 256: n = 16384 273 / 275 / 272 TF/s and n = 32768 490 / 516 / 512
+// TF/s with 4 / 6 / 8 steps per pass.
+constexpr int kBulkSteps = 6;
 
 lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
                     Plan* p) {
@@ -374,9 +377,9 @@ lu_status make_plan(const lu_opts& o, int64_t m, int64_t n, lu_dtype dtype,
     return LU_SUCCESS;
   }
   // several outer steps per bulk pass (look-ahead, unscaled fp16 / bf16
-  // operands): bulk_steps 0 (default: kBulkSteps) or 2..4; 1 keeps one pass
-  // per step
-  if (o.bulk_steps < 0 || o.bulk_steps > 4) return LU_ERR_INVALID_ARG;
+  // operands): bulk_steps 0 (default: kBulkSteps) or 2..kMaxBulkSteps; 1
+  // keeps one pass per step
+  if (o.bulk_steps < 0 || o.bulk_steps > kMaxBulkSteps) return LU_ERR_INVALID_ARG;
   const bool grouping = is_tc(p->outer) && !tc_scaled(tc_kind(p->outer)) && p->lookahead;
   p->bulk_group = grouping ? (o.bulk_steps == 0 ? kBulkSteps : o.bulk_steps) : 1;
   p->bulk_pair = p->bulk_group >= 2;
@@ -604,7 +607,7 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   // columns)
   const int q = p.bulk_group;
   const int nbuf = q >= 2 ? q + 2 : 3;
-  TcWs w2[6];
+  TcWs w2[kMaxBulkSteps + 2];
   if (tc && n > nb) {
     w2[0] = tc_ws_layout(256, n - nb, n - nb, nb, tc_kind(p.outer));
     const size_t shift = w2[0].bytes;
@@ -667,8 +670,8 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
   // steps of the current group whose bulk (rows and columns beyond their
   // trailing origin + 3 nb) waits to be applied together with later steps'
   int ngrp = 0;
-  int grp_buf[4] = {0, 0, 0, 0};
-  int64_t grp_step[4] = {0, 0, 0, 0};
+  int grp_buf[kMaxBulkSteps] = {};
+  int64_t grp_step[kMaxBulkSteps] = {};
   const int64_t ldk = tc && n > nb ? tc_packed_k(kind, nb) : 0;
   const int64_t es = tc ? tc_operand_bytes(kind) : 0;
   // block column [ofs, ofs + in) is final once the panel work queued so far
@@ -878,9 +881,9 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
         auto group_update = [&](int64_t r0, int64_t rows, int64_t c0, int64_t cols,
                                 int tiles_, int ctas_) -> lu_status {
           if (rows <= 0 || cols <= 0) return LU_SUCCESS;
-          int64_t ks[4];
-          const void* as[4];
-          const void* bs[4];
+          int64_t ks[kMaxBulkSteps];
+          const void* as[kMaxBulkSteps];
+          const void* bs[kMaxBulkSteps];
           int ns = 0;
           for (int g = 0; g <= ngrp; ++g) {
             const bool own = g == ngrp;

@@ -44,7 +44,7 @@ using namespace sm100;
 
 constexpr int BM = 128;
 constexpr int BN = 256;
-constexpr int kMaxSets = 4;  // operand sets summed in one pass
+constexpr int kMaxSets = 8;  // operand sets summed in one pass
 constexpr int kRowBytes = 128;                  // bytes of K per tile row
 constexpr int kStageA = BM * kRowBytes;         // 16 KB
 constexpr int kStageB = BN * kRowBytes;         // 32 KB
@@ -122,6 +122,10 @@ struct TcParams {
                        // columns [s N, (s + 1) N) of tmap_c) instead of the
                        // reduce-add into C
 };
+// the update kernels take (TcMaps, CUtensorMap, TcParams, uint32_t) by value:
+// within the 4 KB of kernel parameters
+static_assert(sizeof(TcMaps) + sizeof(CUtensorMap) + sizeof(TcParams) + 16 <= 4096,
+              "update kernel parameters exceed 4 KB");
 
 // KIND 0: kind::f16 (fp16/bf16), 1: kind::f8f6f4 (e4m3).
 // EPI  0: C loaded/stored by the epilogue threads; 1: TMA reduce-add;
@@ -769,9 +773,9 @@ constexpr int kPairMinTiles = 2 * 148;
 // B[q] (K[q] x N, column-major, ldb_p), summed in one accumulator.
 struct OpSets {
   int n = 1;
-  int64_t K[kMaxSets] = {0, 0, 0, 0};
-  const void* A[kMaxSets] = {nullptr, nullptr, nullptr, nullptr};
-  const void* B[kMaxSets] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t K[kMaxSets] = {};
+  const void* A[kMaxSets] = {};
+  const void* B[kMaxSets] = {};
 };
 
 OpSets one_set(int64_t K, const void* A, const void* B) {

@@ -45,7 +45,7 @@ lu_status launch_tc_update2(cudaStream_t st, TcOperand kind, int64_t M, int64_t 
                             const void* A2, const void* B2, int64_t ld_p, float* C,
                             int64_t ldc, int* err, int max_ctas = 0, int tiles_per_cta = 0);
 
-// C -= sum_q A[q] B[q] in one pass over C: up to four K-major operand sets
+// C -= sum_q A[q] B[q] in one pass over C: up to eight K-major operand sets
 // (unscaled fp16 or bf16, the same leading dimension ld_p, K[q] columns
 // each) summed in one fp32 accumulator, so C is read and written once for
 // several outer steps' updates.  Persistent launches (tiles_per_cta = 0) of

@@ -17,7 +17,7 @@ The second form runs the trailing (Schur) update alone: C (M x M, fp32) -=
 A (M x K) B (K x M) through the library's update entry (operands packed, then
 one persistent tensor-core launch over all SMs: CTA pairs from K = 512 up)
 `reps` times -- the shape class of the factorization's largest launches
-(K = 4 nb = 1024 when four outer steps share a pass) at a size whose C
+(K = 6 nb = 1536 when six outer steps share a pass) at a size whose C
 (M = 8192: 256 MB) is larger than L2 and small enough for a full capture.
 
 The third form factors an fp16 matrix with the left-looking driver and fp16

@@ -291,10 +291,11 @@ def test_lookahead_is_bit_identical(built, compute, n, nb):
                                          (rb.compute_type.TC32_BF16, O.FMT_BF16)])
 @pytest.mark.parametrize("n,nb,q", [(2048, 256, 2), (1800, 128, 2), (3000, 256, 2),
                                     (3000, 128, 3), (2500, 128, 4), (4096, 256, 4),
-                                    (3000, 256, 0)])
+                                    (3000, 256, 0), (3300, 128, 6), (4096, 256, 8),
+                                    (2900, 128, 8)])
 def test_grouped_bulk_pass(built, compute, fmt, n, nb, q):
-    """bulk_steps q (0: the default, 4, under look-ahead): q outer steps'
-    updates of the bulk of the trailing matrix in one pass,
+    """bulk_steps q (2 .. 8; 0: the default, under look-ahead): q outer
+    steps' updates of the bulk of the trailing matrix in one pass,
     C - (L_k U_k + ... + L_k+q-1 U_k+q-1) with one fp32 accumulator, the
     block row and column each step's successors need applied at once with
     every pending product.  Only that rounding differs from the

@@ -351,99 +351,61 @@ diag_factor_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
 
 // ---------------------------------------------------------------------------
 // Diagonal block of the left-looking (Crout) variant, w <= 128, one CTA.
-// Per tile T, in the reference's order (src/lu_nopiv_inner_ll.hxx:197-370):
+// The reference's order (src/lu_nopiv_inner_ll.hxx:197-370), per tile T:
 // the tile column (rows >= 8T) and the tile row (columns right of the tile)
-// receive one update summing all earlier columns of the block (acc over
-// k < 8T, subtracted once), then the tile is factored and the L rows and U
-// columns of the block are eliminated with it.
-__global__ void __launch_bounds__(kThreads)
+// receive one update summing all earlier columns of the block (acc =
+// sum_k fma(L[i][k], U[k][j], acc) from 0 over k < 8T, subtracted once),
+// then the tile is factored and the L rows / U columns of the block are
+// eliminated with it.  Each element's sum is one fma chain in k order, so
+// it can be carried along tile by tile: ACC (w x w) holds every trailing
+// element's chain, extended by each tile's 8 columns as soon as the tile's
+// L rows / U columns are known (a rank-8 step over the whole trailing block,
+// like diag_factor_kernel's Phase C, with ACC in place of the subtraction)
+// and subtracted from the element when its own tile comes.  Bit for bit the
+// reference's sums and subtractions; the work per tile is spread over the
+// whole trailing block instead of the tile's column and row.
+__global__ void __launch_bounds__(kDiagT)
 diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
                   int* first_bad) {
   extern __shared__ __align__(16) float smem[];
   const int LD = ((w + 3) / 4) * 4 + 4;
   float* D = smem;
-  float* inv = D + (size_t)LD * w;  // 8
+  float* ACC = D + (size_t)LD * w;
+  float* Ls = ACC + (size_t)LD * w;   // [8][128]
+  float* Us = Ls + 8 * 128;           // [8][128]
+  float* inv = Us + 8 * 128;          // [8]
   const int tid = threadIdx.x;
-  stage_cols_async<kThreads>(D, LD, a, lda, w, w);
+
+  stage_cols_async<kDiagT>(D, LD, a, lda, w, w);
+  for (int i = tid; i < LD * w; i += kDiagT) ACC[i] = 0.0f;
   cp_async_wait_all();
+  __syncthreads();
+
+  // tile 0: no earlier columns
+  if (tid == 0) {
+    const int tw0 = min(8, w);
+    if (!(tw0 == 8 && factor_tile8_fast(D, LD, inv)))
+      factor_tile_thread(D, LD, tw0, inv, col0, first_bad);
+  }
   __syncthreads();
   const int nt = (w + 7) / 8;
   for (int t = 0; t < nt; ++t) {
     const int t0 = 8 * t;
-    const int tw = min(8, w - t0);
-    if (t0 > 0) {
-      // (a) tile column: rows [t0, w) x cols [t0, t0+tw); tile row: rows
-      // [t0, t0+tw) x cols [t0+tw, w).  Items of 4 rows x 2 columns (tile
-      // column) or 4 rows x 1 column (tile row), K walked 4 at a time with
-      // 16-byte reads of L (4 rows of column k) and U (4 k of column c);
-      // every element's sum still runs k = 0, 1, ..., t0 - 1 in order.
-      const int RG = (w + 3) >> 2;  // 4-row groups (rows >= w never stored)
-      const int g0 = t0 >> 2;
-      const int ncg = RG - g0;
-      const int nci = ncg * ((tw + 1) >> 1);
-      const int nri = 2 * (w - t0 - tw);  // tw == 8 whenever this is > 0
-      for (int e = tid; e < nci + nri; e += kThreads) {
-        int i0, c, nc;
-        if (e < nci) {
-          i0 = 4 * (g0 + e % ncg);
-          c = t0 + 2 * (e / ncg);
-          nc = min(2, t0 + tw - c);
-        } else {
-          const int f = e - nci;
-          i0 = t0 + 4 * (f & 1);
-          c = t0 + tw + (f >> 1);
-          nc = 1;
-        }
-        float acc0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, acc1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        const float* U0 = D + (size_t)c * LD;
-        const float* U1 = D + (size_t)(nc > 1 ? c + 1 : c) * LD;
-        for (int k = 0; k < t0; k += 4) {
-          float l[4][4];
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            const float4 v = *reinterpret_cast<const float4*>(D + i0 + (size_t)(k + kk) * LD);
-            l[kk][0] = v.x; l[kk][1] = v.y; l[kk][2] = v.z; l[kk][3] = v.w;
-          }
-          const float4 a4 = *reinterpret_cast<const float4*>(U0 + k);
-          const float4 b4 = *reinterpret_cast<const float4*>(U1 + k);
-          const float u0[4] = {a4.x, a4.y, a4.z, a4.w};
-          const float u1[4] = {b4.x, b4.y, b4.z, b4.w};
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              acc0[r] = __fmaf_rn(l[kk][r], u0[kk], acc0[r]);
-              acc1[r] = __fmaf_rn(l[kk][r], u1[kk], acc1[r]);
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          if (i0 + r < w) {
-            float* p0 = D + (i0 + r) + (size_t)c * LD;
-            *p0 = __fsub_rn(*p0, acc0[r]);
-            if (nc > 1) {
-              float* p1 = p0 + LD;
-              *p1 = __fsub_rn(*p1, acc1[r]);
-            }
-          }
-        }
-      }
-      __syncthreads();
-    }
-    // (b) factor the tile (in registers when its pivots are in the fast
-    // reciprocal's range, else the exact path that also reports them)
-    if (tid == 0 && !(tw == 8 && factor_tile8_fast(D + t0 + t0 * LD, LD, inv)))
-      factor_tile_thread(D + t0 + t0 * LD, LD, tw, inv, col0 + t0, first_bad);
-    __syncthreads();
-    const int s = w - t0 - tw;
+    const int s = w - t0 - 8;  // trailing extent inside the block
     if (s <= 0) break;
-    // (c) eliminate the block's L rows / U columns with the tile
+    // The tile's L rows below it (threads 0..127) and U columns right of it
+    // (threads 128..255): first the subtraction of the element's sum over
+    // the earlier tiles, then the elimination with the tile; results also
+    // go to the strip buffers.
     if (tid < 128) {
       if (tid < s) {
-        const int i = t0 + tw + tid;
+        const int i = t0 + 8 + tid;
         float row[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) row[c] = D[i + (t0 + c) * LD];
+        for (int c = 0; c < 8; ++c) {
+          row[c] = D[i + (t0 + c) * LD];
+          if (t0 > 0) row[c] = __fsub_rn(row[c], ACC[i + (t0 + c) * LD]);
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           row[k] = __fmul_rn(row[k], inv[k]);
@@ -452,27 +414,104 @@ diag_crout_kernel(float* __restrict__ a, int64_t lda, int w, int64_t col0,
             row[c] = __fmaf_rn(-row[k], D[(t0 + k) + (t0 + c) * LD], row[c]);
         }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) D[i + (t0 + c) * LD] = row[c];
+        for (int c = 0; c < 8; ++c) {
+          D[i + (t0 + c) * LD] = row[c];
+          Ls[c * 128 + (i - t0 - 8)] = row[c];
+        }
       }
-    } else {
+    } else if (tid < 256) {
       const int q = tid - 128;
       if (q < s) {
-        const int j = t0 + tw + q;
+        const int j = t0 + 8 + q;
         float col[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) col[r] = D[(t0 + r) + j * LD];
+        for (int r = 0; r < 8; ++r) {
+          col[r] = D[(t0 + r) + j * LD];
+          if (t0 > 0) col[r] = __fsub_rn(col[r], ACC[(t0 + r) + j * LD]);
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k)
 #pragma unroll
           for (int r = k + 1; r < 8; ++r)
             col[r] = __fmaf_rn(-D[(t0 + r) + (t0 + k) * LD], col[k], col[r]);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) D[(t0 + r) + j * LD] = col[r];
+        for (int r = 0; r < 8; ++r) {
+          D[(t0 + r) + j * LD] = col[r];
+          Us[r * 128 + q] = col[r];
+        }
+      }
+    }
+    __syncthreads();
+    // The tile's 8 columns appended to every trailing element's sum.
+    // Look-ahead: warp 0 finishes the next tile's block (its sum, one
+    // subtraction) and its lane 0 factors it, while warps 1.. extend ACC.
+    const int t1w = min(8, s);  // width of tile t+1
+    if (tid < 32) {
+      float* T1 = D + (t0 + 8) + (t0 + 8) * LD;
+      const float* A1 = ACC + (t0 + 8) + (t0 + 8) * LD;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int e = tid + 32 * h, i = e & 7, j = e >> 3;
+        if (i < t1w && j < t1w) {
+          float acc = A1[i + j * LD];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc = __fmaf_rn(Ls[k * 128 + i], Us[k * 128 + j], acc);
+          T1[i + j * LD] = __fsub_rn(T1[i + j * LD], acc);
+        }
+      }
+      __syncwarp();
+      if (tid == 0 && !(t1w == 8 && factor_tile8_fast(T1, LD, inv)))
+        factor_tile_thread(T1, LD, t1w, inv, col0 + t0 + 8, first_bad);
+    }
+    const int nb4 = (s + 3) / 4;
+    const bool vec = (s % 4 == 0);
+    for (int b = tid - 32; b < nb4 * nb4; b += kDiagT - 32) {
+      if (b < 0) break;
+      const int li = 4 * (b % nb4), lj = 4 * (b / nb4);  // local to the block
+      if (li < 8 && lj < 8) continue;  // the next tile: warp 0
+      const int i0 = t0 + 8 + li, j0 = t0 + 8 + lj;
+      float acc[4][4];
+      if (vec) {
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const float4 c4 = *reinterpret_cast<const float4*>(&ACC[i0 + (j0 + jj) * LD]);
+          acc[0][jj] = c4.x; acc[1][jj] = c4.y; acc[2][jj] = c4.z; acc[3][jj] = c4.w;
+        }
+      } else {
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            acc[ii][jj] = (i0 + ii < w && j0 + jj < w) ? ACC[(i0 + ii) + (j0 + jj) * LD] : 0.0f;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float4 l4 = *reinterpret_cast<const float4*>(&Ls[k * 128 + li]);
+        const float4 u4 = *reinterpret_cast<const float4*>(&Us[k * 128 + lj]);
+        const float l[4] = {l4.x, l4.y, l4.z, l4.w};
+        const float u[4] = {u4.x, u4.y, u4.z, u4.w};
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = __fmaf_rn(l[ii], u[jj], acc[ii][jj]);
+      }
+      if (vec) {
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+          *reinterpret_cast<float4*>(&ACC[i0 + (j0 + jj) * LD]) =
+              make_float4(acc[0][jj], acc[1][jj], acc[2][jj], acc[3][jj]);
+      } else {
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            if (i0 + ii < w && j0 + jj < w) ACC[(i0 + ii) + (j0 + jj) * LD] = acc[ii][jj];
       }
     }
     __syncthreads();
   }
-  store_cols<kThreads>(a, lda, D, LD, w, w);
+
+  store_cols<kDiagT>(a, lda, D, LD, w, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -922,9 +961,9 @@ lu_status launch_diag_crout(cudaStream_t st, float* a, int64_t lda, int w,
                             int64_t col0, int* first_bad) {
   if (w <= 0 || w > 128) return LU_ERR_INVALID_ARG;
   const int LD = ((w + 3) / 4) * 4 + 4;
-  const size_t sm = ((size_t)LD * w + 8) * sizeof(float);
+  const size_t sm = ((size_t)2 * LD * w + 2 * 8 * 128 + 8) * sizeof(float);
   LUB_CUDA_TRY(set_smem_limit((const void*)diag_crout_kernel, sm));
-  diag_crout_kernel<<<1, kThreads, sm, st>>>(a, lda, w, col0, first_bad);
+  diag_crout_kernel<<<1, kDiagT, sm, st>>>(a, lda, w, col0, first_bad);
   LUB_LAUNCH_CHECK();
   return LU_SUCCESS;
 }

@@ -1744,6 +1744,10 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         cudaStreamWaitEvent(st, S->cu_done, 0);
         cudaEventRecord(S->cu_join, S->catchup_bulk);
         cudaStreamWaitEvent(st, S->cu_join, 0);
+        if (llc) {
+          cudaEventRecord(S->cu_join, S->catchup_early);
+          cudaStreamWaitEvent(st, S->cu_join, 0);
+        }
       }
       cudaEventRecord(S->out_done, co);
       cudaStreamWaitEvent(st, S->out_done, 0);

@@ -56,6 +56,16 @@ def test_workspace_size_validation(built):
     assert _ws(o, 64, 64)[0] == _lib.ERR_UNSUPPORTED          # ib is 8
     o = rb.make_opts(diag_width=129)
     assert _ws(o, 64, 64)[0] == _lib.ERR_INVALID_ARG
+    # steps per bulk pass: 0 (default) and 1 .. 8; the workspace grows with q
+    # (q + 2 operand buffers under look-ahead with fp16 updates)
+    sizes = []
+    for q in (0, 1, 2, 4, 6, 8):
+        st, sz = _ws(rb.make_opts(outer=rb.TC32, bulk_steps=q), 4096, 4096)
+        assert st == _lib.SUCCESS, q
+        sizes.append(sz)
+    assert sizes[0] == sizes[4] and sizes[2] < sizes[3] < sizes[4] < sizes[5]
+    for q in (-1, 9):
+        assert _ws(rb.make_opts(bulk_steps=q), 64, 64)[0] == _lib.ERR_INVALID_ARG
 
 
 def _rl(m=64, n=64, a=1, lda=64, info=1, dtype=_lib.F32, ws=None, ws_bytes=0):

@@ -378,12 +378,15 @@ def test_host_entry_matches_device_entry(built, n, nb, outer, la, pad):
 
 
 @pytest.mark.parametrize("n,nb,outer", [(4096, 256, rb.TC32), (3000, 128, rb.compute_type.TC32_BF16),
-                                        (8192, 256, rb.TC32)])
+                                        (8192, 256, rb.TC32), (5000, 256, rb.TC32),
+                                        (6144, 128, rb.compute_type.TC32_BF16)])
 def test_host_entry_two_step_bulk(built, n, nb, outer):
-    """The host entry with two steps per bulk pass (the default, in its chunk
-    factorizations and in the catch-up of arriving chunks): same factors as
-    the step-by-step order up to the one rounding per pass it saves, and as
-    the oracle's restatement."""
+    """The host entry with several steps per bulk pass (the default): the
+    chunk factorizations group their bulk passes and arriving chunks are
+    caught up in left-looking order (block-row updates over all earlier
+    steps, then the row's solves); same factors as the oracle's
+    step-by-step restatement up to those roundings, ragged last chunks and
+    blocks included."""
     fmt = O.FMT_FP16 if outer == rb.TC32 else O.FMT_BF16
     a = O.gen_matrix(n, seed=n + 7, kind=1, alpha=1.5)
     h = torch.empty((n, n), dtype=torch.float32, pin_memory=True).t()[:n, :]

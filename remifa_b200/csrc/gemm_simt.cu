@@ -161,6 +161,99 @@ sgemm_update_kernel(int64_t M, int64_t N, int64_t K, float alpha,
   }
 }
 
+// The same product on 64 x 64 tiles (4 x 4 outputs per thread), for
+// shapes whose 128 x 128 grid would leave most SMs idle (the narrow FP32
+// updates inside a left-looking block: n rows x 128 columns, K = 128).
+// Every output's sum runs over K in the same order from 0 and gets the
+// same final rounding as in sgemm_update_kernel, so the results are equal.
+template <bool VEC>
+__global__ void __launch_bounds__(NT)
+sgemm_update64_kernel(int64_t M, int64_t N, int64_t K, float alpha,
+                      const float* __restrict__ A, int64_t lda,
+                      const float* __restrict__ B, int64_t ldb, float beta,
+                      float* __restrict__ C, int64_t ldc) {
+  constexpr int TB = 64;
+  __shared__ __align__(16) float As[2][BK][TB];
+  __shared__ __align__(16) float Bs[2][BK][TB];
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  const int64_t m0 = (int64_t)blockIdx.x * TB;
+  const int64_t n0 = (int64_t)blockIdx.y * TB;
+  // A tile TB x BK: 2 consecutive rows of one column per thread; B tile
+  // BK x TB: 2 consecutive k of one column per thread
+  const int a_col = tid / 32, a_row = (tid % 32) * 2;
+  const int b_col = tid / 4, b_k = (tid % 4) * 2;
+  float ra[2], rb[2];
+  auto load_tiles = [&](int64_t k0) {
+    const int64_t ak = k0 + a_col, ar = m0 + a_row;
+    if (VEC && ak < K && ar + 1 < M) {
+      const float2 v = *reinterpret_cast<const float2*>(A + ar + ak * lda);
+      ra[0] = v.x; ra[1] = v.y;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) ra[i] = (ak < K && ar + i < M) ? A[ar + i + ak * lda] : 0.0f;
+    }
+    const int64_t bc = n0 + b_col, bk = k0 + b_k;
+    if (VEC && bc < N && bk + 1 < K) {
+      const float2 v = *reinterpret_cast<const float2*>(B + bk + bc * ldb);
+      rb[0] = v.x; rb[1] = v.y;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) rb[i] = (bc < N && bk + i < K) ? B[bk + i + bc * ldb] : 0.0f;
+    }
+  };
+  auto store_tiles = [&](int buf) {
+    *reinterpret_cast<float2*>(&As[buf][a_col][a_row]) = make_float2(ra[0], ra[1]);
+    Bs[buf][b_k][b_col] = rb[0];
+    Bs[buf][b_k + 1][b_col] = rb[1];
+  };
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  const int64_t nk = (K + BK - 1) / BK;
+  load_tiles(0);
+  store_tiles(0);
+  __syncthreads();
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int buf = (int)(kt & 1);
+    if (kt + 1 < nk) load_tiles((kt + 1) * BK);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      const float4 a4 = *reinterpret_cast<const float4*>(&As[buf][k][tx * 4]);
+      const float4 b4 = *reinterpret_cast<const float4*>(&Bs[buf][k][ty * 4]);
+      const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+      const float b[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+    }
+    if (kt + 1 < nk) {
+      store_tiles(buf ^ 1);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t r = m0 + tx * 4 + i;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t c = n0 + ty * 4 + j;
+      if (c >= N) continue;
+      float* p = C + r + c * ldc;
+      if (alpha == -1.0f && beta == 1.0f)
+        *p = __fsub_rn(*p, acc[i][j]);
+      else if (beta == 0.0f)
+        *p = __fmul_rn(alpha, acc[i][j]);
+      else
+        *p = __fmaf_rn(alpha, acc[i][j], __fmul_rn(beta, *p));
+    }
+  }
+}
+
 // Rank-8-chunked update C -= A * B over up to two independent regions in one
 // launch (the rest of an outer block column and of its block row), TM x TM
 // outputs per thread on CB x CB tiles (CB = 16 TM: 64 for the wide updates,
@@ -339,6 +432,19 @@ lu_status launch_sgemm_update(cudaStream_t st, int64_t M, int64_t N, int64_t K,
                    ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0);
   dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN));
   if (grid.y > 65535) return LU_ERR_INVALID_ARG;
+  if (!chunk8 && (int64_t)grid.x * grid.y < 2 * sm_count()) {
+    // too few 128 x 128 tiles to fill the GPU: 64 x 64 tiles, same results
+    dim3 g64((unsigned)ceil_div(M, 64), (unsigned)ceil_div(N, 64));
+    if (g64.y > 65535) return LU_ERR_INVALID_ARG;
+    const bool v2 = (lda % 2 == 0) && (ldb % 2 == 0) && ((uintptr_t)A % 8 == 0) &&
+                    ((uintptr_t)B % 8 == 0);
+    if (v2)
+      sgemm_update64_kernel<true><<<g64, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      sgemm_update64_kernel<false><<<g64, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    LUB_LAUNCH_CHECK();
+    return LU_SUCCESS;
+  }
   if (chunk8) {
     if (vec)
       sgemm_update_kernel<true, true><<<grid, NT, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);

@@ -1111,11 +1111,11 @@ constexpr int kLlCatchupGroup = 8;
 // L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
 // rows come in (the chunk's rows [c0, n) may still be arriving when the
 // chain starts: rows_in marks them in), and each group's solved rows go to
-// the host at once on sink.out.  Against the step-by-step catch-up this saves the per-step
-// passes over all rows below each block row (the chain of solves runs
-// beside fewer, larger updates); the sums are rounded once per update
-// instead of once per step, as in the grouped bulk passes of the
-// factorization itself.
+// the host at once on sink.out.  Against the step-by-step catch-up this
+// saves the per-step passes over all rows below each block row (the chain
+// of solves runs beside fewer, larger updates); the sums are rounded once
+// per update instead of once per step, as in the grouped bulk passes of
+// the factorization itself.
 static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t lda,
                              LlCatchup* cu, int* err, int64_t c0, int64_t c1, DevStreams* S,
                              const ColumnSink& sink, cudaEvent_t rows_in) {

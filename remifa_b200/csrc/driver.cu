@@ -1225,8 +1225,11 @@ static int ll_split(int64_t updm, int64_t in, int64_t ofs, int64_t es) {
 // kernel and the left-looking L / U panels eliminate it.  For in <= kLlSub
 // this is exactly the reference's inner Crout loop
 // (src/lu_nopiv_inner_ll.hxx:197-370); wider blocks nest one more level.
+// With lcopy given, the L panels also write their rows' fp16 copies
+// (rounded as the fp16 matrix stores them) into the operand copy.
 static lu_status ll_block(cudaStream_t st, float* x, int64_t ldx, int64_t n, int64_t ofs,
-                          int64_t in, int* first_bad, DevStreams* S) {
+                          int64_t in, int* first_bad, DevStreams* S, void* lcopy = nullptr,
+                          int64_t ldk = 0) {
   for (int64_t c = ofs; c < ofs + in; c += kLlSub) {
     const int64_t w = std::min(kLlSub, ofs + in - c);
     const int64_t rest = n - c - w;
@@ -1257,7 +1260,15 @@ static lu_status ll_block(cudaStream_t st, float* x, int64_t ldx, int64_t n, int
     }
     if (rest > 0) {
       ProfScope ps("lupanel", st, 16.0 * rest * w, 2.0 * rest * (double)w * w);
-      LUB_TRY(launch_lupanel(st, dg, ldx, (int)w, rest, rest, true));
+      // lcopy: the finished L rows also go to the fp16 A operand copy
+      // (row i, column k at lcopy[i * ldk + k])
+      LuPack pk;
+      pk.pa = lcopy;
+      pk.ldk = ldk;
+      pk.row0 = c + w;
+      pk.k0 = (int)c;
+      LUB_TRY(launch_lupanel(st, dg, ldx, (int)w, rest, rest, true, 0, 0,
+                             lcopy ? &pk : nullptr));
     }
   }
   return LU_SUCCESS;
@@ -1497,19 +1508,14 @@ static lu_status ll_factor_f16(const Plan& p, cudaStream_t st, __half* a, int64_
         LUB_TRY(join_side(st, S));
       }
     }
-    LUB_TRY(ll_block(st, Sh, lds, n, ofs, in, first_bad, S));
+    // (the L panels write the L operand copy of the rows below the block)
+    LUB_TRY(ll_block(st, Sh, lds, n, ofs, in, first_bad, S, Lc, ldk));
     {
       ProfScope ps("convert", st, 6.0 * (double)in * (updm + rest));
       LUB_TRY(launch_convert(st, updm, in, sblk, LU_F32, lds, blk, LU_F16, lda, 0));
       if (rest > 0)
         LUB_TRY(launch_convert(st, in, rest, sblk + in * lds, LU_F32, lds, blk + in * lda,
                                LU_F16, lda, 0));
-    }
-    if (rest > 0) {
-      // L rows [ofs+in, n) of the block's columns, rounded exactly as stored
-      ProfScope ps("pack_operands", st, 6.0 * (double)rest * in);
-      LUB_TRY(launch_pack_a(st, TcOperand::F16, rest, in, sblk + in, lds,
-                            Lc + ((ofs + in) * ldk + ofs) * 2, ldk, nullptr));
     }
   }
   // the low-priority stream joins the caller's stream

@@ -453,6 +453,32 @@ LU_API lu_status lu_selftest_wait_solve_c(lu_stream_t stream, unsigned long long
                                           double* d_x, void* d_scratch, size_t bytes,
                                           unsigned* d_expired);
 
+/* One block row of the host entry's left-looking chunk catch-up, for tests
+ * and measurement (no reference counterpart; for one block row it stands
+ * for the U-panel solves of src/lu_nopiv_inner_rl.hxx:155-190 that the
+ * reference runs per outer step).  d_a holds, column-major with leading
+ * dimension lda, a factored in x in diagonal block at (0, 0) (its unit
+ * lower part is used) and the block row R (in x nc) at column coff >= in.
+ * First R loses the sum of nslabs fp32 slabs of partial products (slab s,
+ * column q, row i at d_part[s * slab + q * ldp + i], ldp = in rounded up to
+ * a multiple of 4, slab a multiple of 4; summed in slab order, then one
+ * subtraction, as the split-K finish does; nslabs = 0: none).  Then R -= La
+ * Xb with K = kl (kl = 0: nothing; fp16 operands, bf16 if bf16 != 0; La row
+ * i at d_la + i * lda_k elements, Xb column q at d_xb + q * ldx), then R =
+ * L^{-1} R in place, and R's fp16 / bf16 copy to d_xo (column q at d_xo + q
+ * * ldx).  fused = 1: one launch (in and kl multiples of 32, in <= 256, ldx
+ * and lda_k multiples of 8, operand pointers 16-byte aligned); fused = 0:
+ * the split-K finish, the tensor-core update and the blocked U-panel
+ * solves.  Everything but the order of the sum La Xb is the same bit for
+ * bit either way.  d_err: device int, the update's error word (0 on
+ * success). */
+LU_API lu_status lu_catchup_row_step_c(lu_stream_t stream, int fused, int bf16, int64_t in,
+                                       int64_t nc, int64_t coff, int64_t kl, float* d_a,
+                                       int64_t lda, const void* d_la, int64_t lda_k,
+                                       const void* d_xb, void* d_xo, int64_t ldx,
+                                       const float* d_part, int64_t slab, int64_t ldp,
+                                       int nslabs, int* d_err);
+
 /* ---- profiling (new; the reference only wall-clocks whole calls) ------- */
 typedef struct lu_profile_entry {
   char name[32];     /* kernel class, e.g. "tc_update", "diag_factor" */

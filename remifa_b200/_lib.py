@@ -144,6 +144,8 @@ SIGNATURES = {
                                          _vp]),
     "lu_selftest_wait_solve_c": (_int, [_vp, ctypes.c_ulonglong, _i64, _vp, _i64, _vp, _vp,
                                         ctypes.c_size_t, _vp]),
+    "lu_catchup_row_step_c": (_int, [_vp, _int, _int, _i64, _i64, _i64, _i64, _vp, _i64, _vp,
+                                     _i64, _vp, _vp, _i64, _vp, _i64, _i64, _int, _vp]),
     "lu_profile_begin": (None, []),
     "lu_profile_end": (_int, [ctypes.POINTER(LuProfileEntry), _int]),
     "lu_launch_count": (ctypes.c_longlong, []),

@@ -17,6 +17,7 @@
 #include "driver.cuh"
 #include "tc_gemm.cuh"
 #include "profile.cuh"
+#include "rowsolve.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -183,6 +184,8 @@ struct DevStreams {
   cudaStream_t catchup = nullptr;   // the host entry's catch_up of arrived chunks
   cudaStream_t catchup_bulk = nullptr;  // its bulk updates (look-ahead)
   cudaStream_t catchup_early = nullptr;  // left-looking catch-up: early partial products
+  cudaStream_t catchup_chain = nullptr;  // left-looking catch-up: the chain of block rows
+  cudaStream_t catchup_pack = nullptr;   // left-looking catch-up: the steps' L operand copies
   cudaEvent_t cu_done = nullptr;
   cudaEvent_t cu_packed = nullptr, cu_u2[2] = {nullptr, nullptr}, cu_join = nullptr;
   cudaEvent_t cu_out = nullptr;  // a chunk's catch-up done: its rows above it can go out
@@ -192,6 +195,7 @@ struct DevStreams {
   // per outer step of the host entry: the step's block column is final
   // once what was queued on the panel (p) and side (s) streams has run
   std::vector<cudaEvent_t> step_p, step_s;
+  std::vector<cudaEvent_t> cu_pk;  // left-looking catch-up: step u's L columns packed
   cudaEvent_t chunk_in[kMaxChunks] = {};
   cudaEvent_t chunk_top[kMaxChunks] = {};  // the rows above a chunk's first column are in
   cudaEvent_t out_done = nullptr;
@@ -230,6 +234,8 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_bulk, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_early, cudaStreamNonBlocking, greatest));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_chain, cudaStreamNonBlocking, greatest));
+    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_pack, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
     for (cudaEvent_t* e : {&d.cu_packed, &d.cu_u2[0], &d.cu_u2[1], &d.cu_join, &d.cu_out,
                            &d.cu_xp, &d.cu_early[0], &d.cu_early[1]})
@@ -254,11 +260,13 @@ static lu_status step_events(DevStreams* S, int64_t steps) {
   static std::mutex mu;
   std::lock_guard<std::mutex> lk(mu);
   while ((int64_t)S->step_p.size() < steps) {
-    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    cudaEvent_t e1 = nullptr, e2 = nullptr, e3 = nullptr;
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+    LUB_CUDA_TRY(cudaEventCreateWithFlags(&e3, cudaEventDisableTiming));
     S->step_p.push_back(e1);
     S->step_s.push_back(e2);
+    S->cu_pk.push_back(e3);
   }
   return LU_SUCCESS;
 }
@@ -1098,16 +1106,73 @@ constexpr int kLlCatchupSplitMax = 8;
 // outer steps per pass over the chunk's rows below c0, and per copy out
 constexpr int kLlCatchupGroup = 8;
 
+// One block row of the left-looking catch-up, on a block whose diagonal
+// block (in x in, factored) sits at blk (leading dimension lda) and whose
+// block row (in x nc, the earlier products but the last one subtracted)
+// starts coff columns right of it: R -= La Xb (K = kl; kl = 0: nothing to
+// subtract), then the unit-lower solve in place, its fp16 / bf16 copy to xo
+// (column q, row i at xo[q * ldx + i]).  fused: one ll_rowsolve launch;
+// otherwise the tensor-core update and the blocked U-panel solves (diag_w
+// rows at a time, rank-8 updates between them) -- the same solve, bit for
+// bit.
+lu_status catchup_row_step(cudaStream_t st, bool fused, bool bf16, float* blk, int64_t lda,
+                           int64_t in, int64_t coff, int64_t nc, int64_t kl, const void* la,
+                           int64_t lda_k, const void* xb, void* xo, int64_t ldx, int diag_w,
+                           int* err, const EarlyPart& ep) {
+  const TcOperand kind = bf16 ? TcOperand::BF16 : TcOperand::F16;
+  float* rows = blk + coff * lda;
+  const int64_t es = tc_operand_bytes(kind);
+  if (fused) {
+    ProfScope ps("rowsolve", st, 8.0 * in * nc + 2.0 * in * in + es * (in + nc) * kl,
+                 2.0 * in * (double)nc * kl + (double)in * in * nc);
+    RowSolveArgs g;
+    g.r = rows;
+    g.ldr = lda;
+    g.l = blk;
+    g.ldl = lda;
+    g.la = la;
+    g.lda_k = lda_k;
+    g.xb = xb;
+    g.xo = xo;
+    g.ldx = ldx;
+    g.nc = nc;
+    g.in = (int)in;
+    g.kl = (int)kl;
+    g.part = ep.part;
+    g.ns = ep.ns;
+    g.slab = ep.slab;
+    g.ldp = ep.ldp;
+    return launch_ll_rowsolve(st, bf16, g);
+  }
+  if (ep.ns > 0) {
+    ProfScope ps("splitk_finish", st, 4.0 * (ep.ns + 2) * (double)in * nc);
+    LUB_TRY(launch_splitk_finish(st, in, nc, ep.ns, ep.part, -1.0f, rows, false, lda, nullptr,
+                                 0));
+  }
+  if (kl > 0) {
+    ProfScope ps("tc_update", st, 8.0 * in * nc + (double)es * (in + nc) * kl,
+                 2.0 * in * (double)nc * kl);
+    LUB_TRY(launch_tc_update(st, kind, in, nc, kl, -1.0f, la, lda_k, xb, ldx, rows, lda,
+                             nullptr, nullptr, err));
+  }
+  Plan q;
+  q.diag_w = diag_w;
+  return u_solve_cols(q, st, blk, lda, 0, in, coff, nc, xo, ldx, bf16);
+}
+
 // The catch-up of the columns [c0, c1) in left-looking order (unscaled fp16 /
 // bf16 operands, several outer steps per bulk pass): block row t of the
 // chunk (rows [t nb, (t+1) nb)) first receives the products of all earlier
-// steps (K = t nb), then the U part of step t (u_solve_cols), whose solves
-// also write the solved rows as the B operand of the later block rows.  The
-// products with the solved rows of steps up to t-2 (the early part, K =
-// (t-1) nb: split-K partial products in fixed slabs, summed in split order,
-// so every run gives the same result) are computed and subtracted on
-// S->catchup_early while block row t-1 is solved; only the last step's
-// product (K = nb) stays on the chain of solves.  The rows [c0, n) receive
+// steps (K = t nb), then the U part of step t (the unit-lower solve with
+// its diagonal block), which also writes the solved rows as the B operand of
+// the later block rows.  The products with the solved rows of steps up to
+// t-2 (the early part, K = (t-1) nb: split-K partial products in fixed
+// slabs, summed in split order, so every run gives the same result) are
+// computed and subtracted on S->catchup_early while block row t-1 is
+// solved; only the last step's product (K = nb) stays on the chain of
+// solves, fused with the solve into one launch (ll_rowsolve) where the
+// block fits it.  Each step's L columns are packed as A rows on
+// S->catchup_early too, a step ahead of the chain.  The rows [c0, n) receive
 // L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
 // rows come in (the chunk's rows [c0, n) may still be arriving when the
 // chain starts: rows_in marks them in), and each group's solved rows go to
@@ -1131,51 +1196,74 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
   LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_join, 0));
   const int ctas = std::max(1, sm_count() * 3 / 4);
   const int64_t nsteps = ceil_div(c0, nb);
+  // one fused launch per block row (late product + solve, and the sum of
+  // its early partial products) where it fits
+  const bool fused = rowsolve_supported(nb, nb, cu->ldx) && cu->ldl % 8 == 0;
+  // Every step's L columns (rows u nb.., final once its step events fire)
+  // as A rows, on their own stream, queued at once: cu_pk[u] marks steps
+  // up to u packed.  The chain needs step u's a block row later.
+  cudaStream_t sp = S->catchup_pack;
+  LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->cu_join, 0));
+  for (int64_t u = cu->npacked; u < nsteps; ++u) {
+    const int64_t o = u * nb, w = std::min(nb, c0 - o);
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->step_p[u], 0));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->step_s[u], 0));
+    {
+      ProfScope ps("pack_operands", sp, (4.0 + es) * (double)(n - o) * w);
+      LUB_TRY(launch_pack_a(sp, kind, n - o, w, a + o + o * lda, lda,
+                            cu->lp + (o * cu->ldl + o) * es, cu->ldl, nullptr));
+    }
+    LUB_CUDA_TRY(cudaEventRecord(S->cu_pk[u], sp));
+  }
+  cu->npacked = std::max(cu->npacked, nsteps);
+  // the partial products of block row r go to slab set r % 2
+  std::vector<int> nslabs(nsteps, 0);
+  const int64_t set_floats = (int64_t)cu->ksplit_max * cu->slab;
   int64_t k0 = 0;  // first row of the group whose bulk pass is pending
   for (int64_t t = 0; t < nsteps; ++t) {
     const int64_t ofs = t * nb, in = std::min(nb, c0 - ofs);
     LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[t], 0));
     LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[t], 0));
-    if (t >= cu->npacked) {
-      // step t's L columns (rows ofs.., final now) as A rows
-      ProfScope ps("pack_operands", st, (4.0 + es) * (double)(n - ofs) * in);
-      LUB_TRY(launch_pack_a(st, kind, n - ofs, in, a + ofs + ofs * lda, lda,
-                            cu->lp + (ofs * cu->ldl + ofs) * es, cu->ldl, nullptr));
-      cu->npacked = t + 1;
+    if (t > 0) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_pk[t - 1], 0));
+    // row t's products with the solved rows up to t-2 (on se, two
+    // iterations ago)
+    if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_early[t % 2], 0));
+    const int64_t k_late = ofs - nb;
+    EarlyPart ep;
+    if (fused && nslabs[t] > 0) {
+      ep.part = cu->part + (t % 2) * set_floats;
+      ep.ns = nslabs[t];
+      ep.slab = splitk_slab_floats(in, nc);
+      ep.ldp = (in + 3) / 4 * 4;
     }
-    float* rows = a + ofs + c0 * lda;
-    if (t > 0) {
-      // the product with the solved rows of step t-1 (the earlier ones were
-      // subtracted on se)
-      const int64_t k_late = ofs - nb;
-      if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_early[t % 2], 0));
-      ProfScope ps("tc_update", st, 8.0 * in * nc + (double)es * (in + nc) * nb,
-                   2.0 * in * (double)nc * nb);
-      LUB_TRY(launch_tc_update(st, kind, in, nc, nb, -1.0f,
-                               cu->lp + (ofs * cu->ldl + k_late) * es, cu->ldl,
-                               cu->xp + k_late * es, cu->ldx, rows, lda, nullptr, nullptr, err));
-    }
-    LUB_TRY(u_solve_cols(p, st, a, lda, ofs, in, c0, nc, cu->xp, cu->ldx,
-                         kind == TcOperand::BF16));
-    // block row t+2's early part (K = (t+1) nb: the solved rows up to this
-    // one) beside the solve of block row t+1
+    LUB_TRY(catchup_row_step(st, fused, kind == TcOperand::BF16, a + ofs + ofs * lda, lda, in,
+                             c0 - ofs, nc, t > 0 ? nb : 0,
+                             t > 0 ? cu->lp + (ofs * cu->ldl + k_late) * es : nullptr, cu->ldl,
+                             t > 0 ? cu->xp + k_late * es : nullptr, cu->xp + ofs * es,
+                             cu->ldx, p.diag_w, err, ep));
+    // on se: block row t+2's early part (K = (t+1) nb: the solved rows up to
+    // this one) beside the solve of block row t+1; its slab set was last
+    // read by the solve of block row t, just done
+    LUB_CUDA_TRY(cudaEventRecord(S->cu_xp, st));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_xp, 0));
     if (t + 2 < nsteps) {
+      LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_pk[t], 0));
       const int64_t o2 = ofs + 2 * nb, ke = ofs + nb;
-      LUB_CUDA_TRY(cudaEventRecord(S->cu_xp, st));
-      LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_xp, 0));
       const int64_t in2 = std::min(nb, c0 - o2);
       const int64_t tiles = ceil_div(in2, 128) * ceil_div(nc, 256);
       const int ks = tc_split_choice(tiles, ke, (int)es, sm_count(), cu->ksplit_max);
+      float* set = cu->part + (t % 2) * set_floats;
       int ns = 0;
       {
         ProfScope ps("tc_update", se, 4.0 * ks * in2 * nc + (double)es * (in2 + nc) * ke,
                      2.0 * in2 * (double)nc * ke);
         LUB_TRY(launch_tc_partials(se, kind, in2, nc, ke, cu->lp + o2 * cu->ldl * es, cu->ldl,
-                                   cu->xp, cu->ldx, ks, cu->part, 0, &ns, err));
+                                   cu->xp, cu->ldx, ks, set, 0, &ns, err));
       }
-      {
+      nslabs[t + 2] = ns;
+      if (!fused) {
         ProfScope ps("splitk_finish", se, 4.0 * (ns + 2) * (double)in2 * nc);
-        LUB_TRY(launch_splitk_finish(se, in2, nc, ns, cu->part, -1.0f, a + o2 + c0 * lda, false,
+        LUB_TRY(launch_splitk_finish(se, in2, nc, ns, set, -1.0f, a + o2 + c0 * lda, false,
                                      lda, nullptr, 0));
       }
       LUB_CUDA_TRY(cudaEventRecord(S->cu_early[t % 2], se));
@@ -1184,6 +1272,7 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
     if ((t + 1) % kLlCatchupGroup != 0 && t + 1 < nsteps) continue;
     LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
     LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
+    LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_pk[t], 0));  // the packs up to step t
     if (n > c0) {
       ProfScope ps("tc_update", sb, 8.0 * (n - c0) * nc + (double)es * (n - c0 + nc) * (k1 - k0),
                    2.0 * (n - c0) * (double)nc * (k1 - k0));
@@ -1204,6 +1293,8 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
   LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sb));
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   LUB_CUDA_TRY(cudaEventRecord(S->cu_join, se));
+  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
+  LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sp));
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   return LU_SUCCESS;
 }
@@ -1662,6 +1753,7 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
     // several steps per bulk pass: the left-looking catch-up (catch_up_ll);
     // one pass per step keeps the step-by-step order of the device entry
     const bool llc = la && tc && !tc_scaled(kind) && p.bulk_group >= 2;
+    if (llc && S) cu = S->catchup_chain;  // the chain of block rows comes first
     LlCatchup llb;
     if (s == LU_SUCCESS && llc) {
       const int64_t c_last = (ceil_div(n, cw) - 1) * cw;  // first column of the last chunk
@@ -1672,7 +1764,9 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
       const size_t lp_bytes = align_up((size_t)n * llb.ldl * es, 1024);
       const size_t xp_bytes = align_up((size_t)llb.ldx * cw * es, 1024);
       llb.slab = splitk_slab_floats(nb, cw);
-      const size_t part_bytes = (size_t)kLlCatchupSplitMax * llb.slab * 4;
+      // two sets of slabs: a block row's partial products stay until its
+      // solve has read them while the next row's are computed
+      const size_t part_bytes = 2 * (size_t)kLlCatchupSplitMax * llb.slab * 4;
       if (pool_malloc_async((void**)&cu_alloc, lp_bytes + xp_bytes + part_bytes, st) !=
           cudaSuccess)
         s = LU_ERR_ALLOC;
@@ -1752,6 +1846,8 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         cudaStreamWaitEvent(st, S->cu_join, 0);
         if (llc) {
           cudaEventRecord(S->cu_join, S->catchup_early);
+          cudaStreamWaitEvent(st, S->cu_join, 0);
+          cudaEventRecord(S->cu_join, S->catchup_pack);
           cudaStreamWaitEvent(st, S->cu_join, 0);
         }
       }

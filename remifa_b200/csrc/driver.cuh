@@ -54,4 +54,26 @@ lu_status gemm_update_ex(lu_compute compute, cudaStream_t st, int64_t m, int64_t
                          const void* b, lu_dtype tb, int64_t ldb, double beta, void* c,
                          lu_dtype tc, int64_t ldc, void* workspace, size_t ws_bytes);
 
+// A block row's early products as split-K partial slabs (slab s, column q,
+// row i at part[s * slab + q * ldp + i]), summed in slab order and
+// subtracted before anything else; ns = 0: none.
+struct EarlyPart {
+  const float* part = nullptr;
+  int64_t slab = 0, ldp = 0;
+  int ns = 0;
+};
+
+// One block row of the host entry's left-looking chunk catch-up: on the
+// block whose factored in x in diagonal block sits at blk, the block row
+// coff columns right of it (in x nc) gets R -= La Xb (K = kl, fp16 / bf16
+// operands: La row i at la[i * lda_k], Xb column q at xb[q * ldx]), then the
+// unit-lower solve in place, whose fp16 / bf16 copy goes to xo[q * ldx + i];
+// with ep, R first loses the sum of its early partial products.  fused: one
+// launch; otherwise the unfused kernels (split-K finish, tensor-core update,
+// U-panel solves of diag_w rows, rank-8 updates between them).
+lu_status catchup_row_step(cudaStream_t st, bool fused, bool bf16, float* blk, int64_t lda,
+                           int64_t in, int64_t coff, int64_t nc, int64_t kl, const void* la,
+                           int64_t lda_k, const void* xb, void* xo, int64_t ldx, int diag_w,
+                           int* err, const EarlyPart& ep = EarlyPart());
+
 }  // namespace lub

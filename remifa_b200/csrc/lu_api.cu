@@ -8,6 +8,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "driver.cuh"
+#include "rowsolve.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -155,6 +156,30 @@ lu_status lu_gen_matrix_c(lu_stream_t stream, int64_t n, float* d_a,
   LUB_TRY(check_device());
   return launch_gen_matrix((cudaStream_t)stream, n, d_a, lda, seed, kind,
                            alpha, kscale, gamma_bits);
+}
+
+lu_status lu_catchup_row_step_c(lu_stream_t stream, int fused, int bf16, int64_t in, int64_t nc,
+                                int64_t coff, int64_t kl, float* d_a, int64_t lda,
+                                const void* d_la, int64_t lda_k, const void* d_xb, void* d_xo,
+                                int64_t ldx, const float* d_part, int64_t slab, int64_t ldp,
+                                int nslabs, int* d_err) {
+  if (in <= 0 || nc < 0 || coff < in || kl < 0 || !d_a || !d_xo || !d_err || nslabs < 0)
+    return LU_ERR_INVALID_ARG;
+  if (nslabs > 0 && (!d_part || ldp != (in + 3) / 4 * 4 || slab < ldp * nc || slab % 4 != 0))
+    return LU_ERR_INVALID_ARG;
+  if (lda < in || ldx < in || (kl > 0 && (!d_la || !d_xb || lda_k < kl || ldx < kl)))
+    return LU_ERR_INVALID_ARG;
+  if (fused && !rowsolve_supported(in, kl, ldx)) return LU_ERR_UNSUPPORTED;
+  if (!fused && (in % 8 != 0 || kl % 8 != 0 || ldx % 8 != 0 || lda_k % 8 != 0))
+    return LU_ERR_UNSUPPORTED;
+  LUB_TRY(check_device());
+  EarlyPart ep;
+  ep.part = d_part;
+  ep.slab = slab;
+  ep.ldp = ldp;
+  ep.ns = nslabs;
+  return catchup_row_step((cudaStream_t)stream, fused != 0, bf16 != 0, d_a, lda, in, coff, nc,
+                          kl, d_la, lda_k, d_xb, d_xo, ldx, 128, d_err, ep);
 }
 
 }  // extern "C"

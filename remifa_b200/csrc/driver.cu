@@ -1105,6 +1105,8 @@ struct LlCatchup {
 constexpr int kLlCatchupSplitMax = 8;
 // outer steps per pass over the chunk's rows below c0, and per copy out
 constexpr int kLlCatchupGroup = 8;
+// column chunks of the host entry with the left-looking catch-up
+constexpr int kLlChunks = 8;
 
 // One block row of the left-looking catch-up, on a block whose diagonal
 // block (in x in, factored) sits at blk (leading dimension lda) and whose
@@ -1707,9 +1709,13 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
   const bool tc = is_tc(p.outer);
   const TcOperand kind = tc_kind(p.outer);
   const int64_t nblk = ceil_div(std::max<int64_t>(n, 1), nb);
-  // four chunks of whole outer blocks (B200 at n = 16384: 4 chunks 40 ms,
-  // 2 or 3 chunks 41-42 ms, 8 chunks 46 ms, one 47 ms)
-  const int64_t cw = ceil_div(nblk, 4) * nb;
+  // Column chunks of whole outer blocks: four with the step-order catch-up
+  // (B200 at n = 16384: 4 chunks 40 ms, 2 or 3 chunks 41-42 ms, 8 chunks 46
+  // ms, one 47 ms); kLlChunks with the left-looking one, whose chain per
+  // earlier step is short, so a smaller last chunk -- less left to do and
+  // to send back after the last rows arrive -- wins.
+  const bool ll_order = p.lookahead && tc && !tc_scaled(kind) && p.bulk_group >= 2;
+  const int64_t cw = ceil_div(nblk, ll_order ? kLlChunks : 4) * nb;
   const bool chunked = n > 2 * nb && !(tc && tc_scaled(kind) && nb % 128 != 0) &&
                        ceil_div(n, cw) <= kMaxChunks;
   auto h2d = [&](cudaStream_t sm, int64_t c0, int64_t c1) {

@@ -105,9 +105,9 @@ ll_rowsolve_kernel(RowSolveArgs g) {
   // (slab order, then one fused subtraction: fma(-1, sum, r))
   {
     const float* R = g.r + col0 * g.ldr;
-    const int q4 = in / 4;
-    for (int idx = tid; idx < kRsCols * q4; idx += kRsT) {
-      const int c = idx / q4, p = 4 * (idx % q4);
+    // warp w: columns w, w + 8, ...; its lanes stride down the column
+    for (int c = warp; c < kRsCols; c += 8)
+    for (int p = 4 * lane; p < in; p += 128) {
       float* d = S + c * ls + p;
       if (c >= ncols) {
         *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -141,18 +141,17 @@ ll_rowsolve_kernel(RowSolveArgs g) {
       }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
+    // panel T, column k = warp: rows [8T, in) down the lanes
     for (int T = 0; T < nt; ++T) {
-      const int rows = in - 8 * T, r4 = rows / 4;
-      float* dst = Fp + rs_panel_off(in, T);
-      const float* src = g.l + 8 * T + (int64_t)(8 * T) * g.ldl;
-      for (int idx = tid; idx < 8 * r4; idx += kRsT) {
-        const int k = idx / r4, p = 4 * (idx % r4);
-        const float* s = src + p + (int64_t)k * g.ldl;
+      const int rows = in - 8 * T;
+      float* dst = Fp + rs_panel_off(in, T) + warp * rows;
+      const float* src = g.l + 8 * T + (int64_t)(8 * T + warp) * g.ldl;
+      for (int p = 4 * lane; p < rows; p += 128) {
         if (g.l_vec) {
-          cp_async16(dst + k * rows + p, s);
+          cp_async16(dst + p, src + p);
         } else {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) cp_async4(dst + k * rows + p + e, s + e);
+          for (int e = 0; e < 4; ++e) cp_async4(dst + p + e, src + p + e);
         }
       }
     }
@@ -310,9 +309,8 @@ ll_rowsolve_kernel(RowSolveArgs g) {
   // xo[(col0 + c) * ldx + p])
   {
     float* R = g.r + col0 * g.ldr;
-    const int q4 = in / 4;
-    for (int idx = tid; idx < ncols * q4; idx += kRsT) {
-      const int c = idx / q4, p = 4 * (idx % q4);
+    for (int c = warp; c < ncols; c += 8)
+    for (int p = 4 * lane; p < in; p += 128) {
       const float4 v = *reinterpret_cast<const float4*>(S + c * ls + p);
       float* d = R + p + (int64_t)c * g.ldr;
       if (g.r_vec) {
@@ -322,9 +320,8 @@ ll_rowsolve_kernel(RowSolveArgs g) {
       }
     }
     E* xo = static_cast<E*>(g.xo);
-    const int q8 = in / 8;
-    for (int idx = tid; idx < ncols * q8; idx += kRsT) {
-      const int c = idx / q8, p = 8 * (idx % q8);
+    for (int c = warp; c < ncols; c += 8)
+    for (int p = 8 * lane; p < in; p += 256) {
       float v[8];
       rs_ld8(S + c * ls + p, v);
       uint4 o;

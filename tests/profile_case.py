@@ -3,6 +3,7 @@
     python tests/profile_case.py [n] [compute] [reps]
     python tests/profile_case.py update M K [compute] [reps]
     python tests/profile_case.py ll16 [n] [nb] [reps]
+    python tests/profile_case.py rowstep [nc] [reps]
 
 The first form factors the seeded matrix A = R + D (R ~ N(0,1)/sqrt(n), row
 dominance 1.5, the generator of the benchmarks) `reps` times on cuda:0 with
@@ -23,6 +24,12 @@ one persistent tensor-core launch over all SMs: CTA pairs from K = 512 up)
 The third form factors an fp16 matrix with the left-looking driver and fp16
 tensor-core updates (fp16 storage, nb = 256 by default): its block-column
 updates have K up to n and N = nb, the shapes of the fp16-storage workload.
+
+The fourth form runs one block-row step of the host entry's left-looking
+chunk catch-up (lu_catchup_row_step_c, fused: the K = 256 fp16 product with
+the previous block row, then the 256-row unit-lower solve) on a 256 x nc
+block row (nc = 4096 by default, the columns of one chunk at n = 16384 with
+four chunks) `reps` times, in place.
 """
 import os
 import sys
@@ -77,12 +84,40 @@ def factor_f16(argv) -> None:
     print("ok", float(lu.float().abs().max()))
 
 
+def rowstep(argv) -> None:
+    import ctypes
+    from remifa_b200 import _lib
+    nc = int(argv[0]) if len(argv) > 0 else 4096
+    reps = int(argv[1]) if len(argv) > 1 else 2
+    inn = kl = 256
+    ldx = inn + 8
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    d = api.colmajor(torch.randn(inn, inn + nc, device="cuda", generator=g))
+    d[:, :inn] = torch.tril(d[:, :inn], -1) * 0.01 + torch.eye(inn, device="cuda")
+    la = (torch.rand(inn, ldx, device="cuda", generator=g) * 0.1).half()
+    xb = torch.rand(nc * ldx, device="cuda", generator=g).half()
+    xo = torch.zeros(nc * ldx, device="cuda", dtype=torch.float16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    for _ in range(reps):
+        s = _lib.lib().lu_catchup_row_step_c(st, 1, 0, inn, nc, inn, kl, p(d), inn, p(la), ldx,
+                                             p(xb), p(xo), ldx, None, 0, 0, 0, p(err))
+        assert s == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    print("ok", float(d[:, inn:].abs().max()))
+
+
 def main(argv=None) -> None:
     argv = list(sys.argv[1:] if argv is None else argv)
     if argv and argv[0] == "update":
         update(argv[1:])
     elif argv and argv[0] == "ll16":
         factor_f16(argv[1:])
+    elif argv and argv[0] == "rowstep":
+        rowstep(argv[1:])
     else:
         factor(argv)
 

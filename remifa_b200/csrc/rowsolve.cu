@@ -24,13 +24,15 @@
 // sub-blocks give, so X_t is bit-identical to the unfused solve for the
 // same R.
 //
-// CTA = 32 columns, 8 warps.  Shared memory: the block row (column c at
+// CTA = 32 columns, 16 warps.  Shared memory: the block row (column c at
 // S[c * ls + p]) and the strictly-lower part of L_tt by panels of 8 columns
 // (panel T: rows [8T, in) of columns 8T..8T+7, column-major), fp32 --
 // 135 KB at in = 256.  Per tile T, after one barrier, warp 0 (one lane per
 // column) applies tile T to tile T+1 and eliminates tile T+1 (look-ahead),
-// while warps 1-7 apply tile T to the rows below tile T+1 in register
-// micro-tiles of 4 columns x 8 rows.
+// while warps 1-15 apply tile T to the rows below tile T+1 in register
+// micro-tiles of 2 columns x 8 rows (16 warps rather than 8 with 4 x 8
+// tiles: more warps to cover the dependent chains; 31.1 -> 29.1 us per step
+// at 256 x 4096 x K 256).
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -40,7 +42,8 @@ namespace lub {
 namespace {
 
 constexpr int kRsCols = 32;   // columns per CTA
-constexpr int kRsT = 256;     // threads
+constexpr int kRsT = 512;     // threads
+constexpr int kRsW = kRsT / 32;  // warps
 
 __device__ __forceinline__ void rs_ld8(const float* p, float (&v)[8]) {
   const float4 a = *reinterpret_cast<const float4*>(p);
@@ -106,7 +109,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
   {
     const float* R = g.r + col0 * g.ldr;
     // warp w: columns w, w + 8, ...; its lanes stride down the column
-    for (int c = warp; c < kRsCols; c += 8)
+    for (int c = warp; c < kRsCols; c += kRsW)
     for (int p = 4 * lane; p < in; p += 128) {
       float* d = S + c * ls + p;
       if (c >= ncols) {
@@ -141,12 +144,13 @@ ll_rowsolve_kernel(RowSolveArgs g) {
       }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
-    // panel T, column k = warp: rows [8T, in) down the lanes
+    // panel T, column k = warp % 8: rows [8T, in) down the lanes, the two
+    // halves of the warps on alternate 128-row stretches
     for (int T = 0; T < nt; ++T) {
-      const int rows = in - 8 * T;
-      float* dst = Fp + rs_panel_off(in, T) + warp * rows;
-      const float* src = g.l + 8 * T + (int64_t)(8 * T + warp) * g.ldl;
-      for (int p = 4 * lane; p < rows; p += 128) {
+      const int rows = in - 8 * T, k = warp & 7;
+      float* dst = Fp + rs_panel_off(in, T) + k * rows;
+      const float* src = g.l + 8 * T + (int64_t)(8 * T + k) * g.ldl;
+      for (int p = 4 * lane + 128 * (warp >> 3); p < rows; p += 256) {
         if (g.l_vec) {
           cp_async16(dst + p, src + p);
         } else {
@@ -176,13 +180,13 @@ ll_rowsolve_kernel(RowSolveArgs g) {
       for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0f;
-    const bool has0 = warp < mt, has1 = warp + 8 < mt;
+    const bool has0 = warp < mt, has1 = warp + kRsW < mt;
 #pragma unroll 2
     for (int kc = 0; kc < g.kl; kc += 32) {
       uint4 a[2][2], b[4];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
-        const int m = (warp + 8 * i) * 16 + gid;
+        const int m = (warp + kRsW * i) * 16 + gid;
         const bool h = i == 0 ? has0 : has1;
 #pragma unroll
         for (int r = 0; r < 2; ++r)
@@ -210,7 +214,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       if (i == 0 ? !has0 : !has1) continue;
-      const int m = (warp + 8 * i) * 16 + gid;
+      const int m = (warp + kRsW * i) * 16 + gid;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int c = 8 * j + 2 * tig;
@@ -273,12 +277,12 @@ ll_rowsolve_kernel(RowSolveArgs g) {
     } else {
       const int q0 = p0 + 8;
       const int npos = (in - q0) / 8;
-      for (int m = tid - 32; m < npos * 8; m += kRsT - 32) {
-        const int ig = m & 7, pp = q0 + 8 * (m >> 3);
-        float xv[4][8], acc[4][8];
+      for (int m = tid - 32; m < npos * 16; m += kRsT - 32) {
+        const int ig = m & 15, pp = q0 + 8 * (m >> 4);
+        float xv[2][8], acc[2][8];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          rs_ld8(S + (ig + 8 * a) * ls + t0, xv[a]);
+        for (int a = 0; a < 2; ++a) {
+          rs_ld8(S + (ig + 16 * a) * ls + t0, xv[a]);
 #pragma unroll
           for (int b = 0; b < 8; ++b) acc[a][b] = 0.0f;
         }
@@ -287,13 +291,13 @@ ll_rowsolve_kernel(RowSolveArgs g) {
           float f[8];
           rs_ld8(FT + k * rows + (pp - t0), f);  // L[pp + b][t0 + k]
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+          for (int a = 0; a < 2; ++a)
 #pragma unroll
             for (int b = 0; b < 8; ++b) acc[a][b] = __fmaf_rn(xv[a][k], f[b], acc[a][b]);
         }
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          float* row = S + (ig + 8 * a) * ls + pp;
+        for (int a = 0; a < 2; ++a) {
+          float* row = S + (ig + 16 * a) * ls + pp;
           float c[8];
           rs_ld8(row, c);
 #pragma unroll
@@ -309,7 +313,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
   // xo[(col0 + c) * ldx + p])
   {
     float* R = g.r + col0 * g.ldr;
-    for (int c = warp; c < ncols; c += 8)
+    for (int c = warp; c < ncols; c += kRsW)
     for (int p = 4 * lane; p < in; p += 128) {
       const float4 v = *reinterpret_cast<const float4*>(S + c * ls + p);
       float* d = R + p + (int64_t)c * g.ldr;
@@ -320,7 +324,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
       }
     }
     E* xo = static_cast<E*>(g.xo);
-    for (int c = warp; c < ncols; c += 8)
+    for (int c = warp; c < ncols; c += kRsW)
     for (int p = 8 * lane; p < in; p += 256) {
       float v[8];
       rs_ld8(S + c * ls + p, v);

@@ -108,7 +108,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
   // (slab order, then one fused subtraction: fma(-1, sum, r))
   {
     const float* R = g.r + col0 * g.ldr;
-    // warp w: columns w, w + 8, ...; its lanes stride down the column
+    // warp w: columns w and w + 16; its lanes stride down the column
     for (int c = warp; c < kRsCols; c += kRsW)
     for (int p = 4 * lane; p < in; p += 128) {
       float* d = S + c * ls + p;
@@ -164,7 +164,7 @@ ll_rowsolve_kernel(RowSolveArgs g) {
     __syncthreads();
   }
 
-  // 2. R -= L_{t,t-1} X_{t-1}: warp w owns the 16-row tiles w and w + 8 and
+  // 2. R -= L_{t,t-1} X_{t-1}: warp w owns the 16-row tile w (and w + 16) and
   // all four 8-column tiles.  Each lane loads 8 consecutive k of its A row
   // and B column per 32-k slab and feeds them to two MMAs (k permuted the
   // same way in A and B, so the products pair up).

@@ -105,6 +105,38 @@ def test_host_entry_argument_validation_without_device(built):
     assert _rl_host(n=-1) == _lib.ERR_INVALID_ARG
 
 
+def test_catchup_row_step_validation_without_device(built):
+    """lu_catchup_row_step_c (one block row of the host entry's chunk
+    catch-up) rejects bad arguments, and shapes the fused kernel does not
+    take, before any device call."""
+    L = _lib.lib()
+    ok = ctypes.c_void_p(256)
+
+    def step(fused=1, inn=256, nc=64, coff=256, kl=256, a=ok, lda=256, la=ok, lda_k=264,
+             xb=ok, xo=ok, ldx=264, part=None, slab=0, ldp=0, ns=0, err=ok):
+        return L.lu_catchup_row_step_c(None, fused, 0, inn, nc, coff, kl, a, lda, la, lda_k,
+                                       xb, xo, ldx, part, slab, ldp, ns, err)
+
+    bad = _lib.ERR_INVALID_ARG
+    assert step(coff=100) == bad          # the block row overlaps the diagonal block
+    assert step(a=None) == bad and step(xo=None) == bad and step(err=None) == bad
+    assert step(lda=100) == bad and step(ldx=200) == bad
+    assert step(la=None) == bad and step(xb=None) == bad and step(lda_k=100) == bad
+    assert step(ns=-1) == bad
+    assert step(ns=2) == bad              # slabs without a pointer
+    assert step(ns=2, part=ok, ldp=128, slab=128 * 64) == bad     # ldp != in
+    assert step(ns=2, part=ok, ldp=256, slab=256 * 63) == bad     # slab too small
+    uns = _lib.ERR_UNSUPPORTED
+    assert step(inn=288, coff=288, lda=288, ldx=296) == uns       # more than 256 rows
+    assert step(inn=48, coff=48, lda=48, ldx=264) == uns          # rows not a multiple of 32
+    assert step(kl=40, lda_k=48) == uns                           # K not a multiple of 32
+    assert step(fused=0, kl=12, lda_k=16) == uns                  # unfused: K % 8
+    import torch
+    if not torch.cuda.is_available():
+        # valid arguments without a device: no fallback
+        assert step() == _lib.ERR_NO_DEVICE
+
+
 def test_no_cpu_fallback(built):
     import torch
     if torch.cuda.is_available():

@@ -185,7 +185,6 @@ struct DevStreams {
   cudaStream_t catchup_bulk = nullptr;  // its bulk updates (look-ahead)
   cudaStream_t catchup_early = nullptr;  // left-looking catch-up: early partial products
   cudaStream_t catchup_chain = nullptr;  // left-looking catch-up: the chain of block rows
-  cudaStream_t catchup_pack = nullptr;   // left-looking catch-up: the steps' L operand copies
   cudaEvent_t cu_done = nullptr;
   cudaEvent_t cu_packed = nullptr, cu_u2[2] = {nullptr, nullptr}, cu_join = nullptr;
   cudaEvent_t cu_out = nullptr;  // a chunk's catch-up done: its rows above it can go out
@@ -195,7 +194,6 @@ struct DevStreams {
   // per outer step of the host entry: the step's block column is final
   // once what was queued on the panel (p) and side (s) streams has run
   std::vector<cudaEvent_t> step_p, step_s;
-  std::vector<cudaEvent_t> cu_pk;  // left-looking catch-up: step u's L columns packed
   cudaEvent_t chunk_in[kMaxChunks] = {};
   cudaEvent_t chunk_top[kMaxChunks] = {};  // the rows above a chunk's first column are in
   cudaEvent_t out_done = nullptr;
@@ -235,7 +233,6 @@ static lu_status dev_streams(DevStreams** out) {
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_bulk, cudaStreamNonBlocking, least));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_early, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_chain, cudaStreamNonBlocking, greatest));
-    LUB_CUDA_TRY(cudaStreamCreateWithPriority(&d.catchup_pack, cudaStreamNonBlocking, greatest));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&d.cu_done, cudaEventDisableTiming));
     for (cudaEvent_t* e : {&d.cu_packed, &d.cu_u2[0], &d.cu_u2[1], &d.cu_join, &d.cu_out,
                            &d.cu_xp, &d.cu_early[0], &d.cu_early[1]})
@@ -260,13 +257,11 @@ static lu_status step_events(DevStreams* S, int64_t steps) {
   static std::mutex mu;
   std::lock_guard<std::mutex> lk(mu);
   while ((int64_t)S->step_p.size() < steps) {
-    cudaEvent_t e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
     LUB_CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
-    LUB_CUDA_TRY(cudaEventCreateWithFlags(&e3, cudaEventDisableTiming));
     S->step_p.push_back(e1);
     S->step_s.push_back(e2);
-    S->cu_pk.push_back(e3);
   }
   return LU_SUCCESS;
 }
@@ -412,6 +407,10 @@ struct PackTarget {
   const TcWs* w = nullptr;
   int64_t ldk = 0, nb = 0;
   int bf16 = 0;
+  // also the host entry's catch-up copy of the step's L columns (global
+  // row r, column c at lp[r * ldl + c]); the step starts at column ofs
+  char* lp = nullptr;
+  int64_t ldl = 0, ofs = 0;
   // the launch of sub-block p0 (width wd) whose L rows / U columns start
   // offL / offU past the sub-block's edge
   LuPack at(int64_t p0, int wd, int64_t offL, int64_t offU) const {
@@ -424,6 +423,12 @@ struct PackTarget {
     k.col0 = p0 + wd + offU - nb;
     k.k0 = (int)p0;
     k.bf16 = bf16;
+    if (lp) {
+      k.pa2 = lp;
+      k.ldk2 = ldl;
+      k.row02 = ofs + p0 + wd + offL;
+      k.k02 = (int)(ofs + p0);
+    }
     return k;
   }
 };
@@ -602,6 +607,10 @@ struct ColumnSink {
   float* h = nullptr;
   int64_t ldh = 0;
   cudaStream_t out = nullptr;
+  // the left-looking catch-up's fp16 / bf16 copy of the L columns [0,
+  // lp_cols), written by the panels of the steps inside that range
+  char* lp = nullptr;
+  int64_t ldl = 0, lp_cols = 0;
 };
 
 static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
@@ -703,7 +712,12 @@ static lu_status rl_factor(const Plan& p, cudaStream_t st, float* a,
     const int64_t tcn = col_end - (ofs + nb); // trailing columns
     const int buf = (int)(step % nbuf);
     const TcWs& wk = w2[buf];
-    const PackTarget pt = pack_target(p, ws, wk);
+    PackTarget pt = pack_target(p, ws, wk);
+    if (pt.ws && sink && sink->lp && ofs + in <= sink->lp_cols) {
+      pt.lp = sink->lp;
+      pt.ldl = sink->ldl;
+      pt.ofs = ofs;
+    }
     // this step's panel writes operand buffer `buf`: the bulk update that
     // last read it (step k - nbuf's) must have finished
     if (tc && step >= nbuf && (!ok(cudaStreamWaitEvent(sp, S->done_with[buf], 0)) ||
@@ -1097,10 +1111,9 @@ struct LlCatchup {
   int64_t ldl = 0;
   char* xp = nullptr;
   int64_t ldx = 0;
-  float* part = nullptr;  // kLlCatchupSplitMax slabs of `slab` floats
+  float* part = nullptr;  // two sets of kLlCatchupSplitMax slabs of `slab` floats
   int64_t slab = 0;
   int ksplit_max = 1;
-  int64_t npacked = 0;  // outer steps whose L columns are in lp
 };
 constexpr int kLlCatchupSplitMax = 8;
 // outer steps per pass over the chunk's rows below c0, and per copy out
@@ -1173,9 +1186,9 @@ lu_status catchup_row_step(cudaStream_t st, bool fused, bool bf16, float* blk, i
 // computed and subtracted on S->catchup_early while block row t-1 is
 // solved; only the last step's product (K = nb) stays on the chain of
 // solves, fused with the solve into one launch (ll_rowsolve) where the
-// block fits it.  Each step's L columns are packed as A rows on
-// S->catchup_early too, a step ahead of the chain.  The rows [c0, n) receive
-// L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
+// block fits it.  The L columns of the earlier steps (A rows) come from the
+// factorization's own panel kernels (ColumnSink::lp).  The rows [c0, n)
+// receive L X in passes of kLlCatchupGroup steps on S->catchup_bulk as the solved
 // rows come in (the chunk's rows [c0, n) may still be arriving when the
 // chain starts: rows_in marks them in), and each group's solved rows go to
 // the host at once on sink.out.  Against the step-by-step catch-up this
@@ -1201,23 +1214,8 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
   // one fused launch per block row (late product + solve, and the sum of
   // its early partial products) where it fits
   const bool fused = rowsolve_supported(nb, nb, cu->ldx) && cu->ldl % 8 == 0;
-  // Every step's L columns (rows u nb.., final once its step events fire)
-  // as A rows, on their own stream, queued at once: cu_pk[u] marks steps
-  // up to u packed.  The chain needs step u's a block row later.
-  cudaStream_t sp = S->catchup_pack;
-  LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->cu_join, 0));
-  for (int64_t u = cu->npacked; u < nsteps; ++u) {
-    const int64_t o = u * nb, w = std::min(nb, c0 - o);
-    LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->step_p[u], 0));
-    LUB_CUDA_TRY(cudaStreamWaitEvent(sp, S->step_s[u], 0));
-    {
-      ProfScope ps("pack_operands", sp, (4.0 + es) * (double)(n - o) * w);
-      LUB_TRY(launch_pack_a(sp, kind, n - o, w, a + o + o * lda, lda,
-                            cu->lp + (o * cu->ldl + o) * es, cu->ldl, nullptr));
-    }
-    LUB_CUDA_TRY(cudaEventRecord(S->cu_pk[u], sp));
-  }
-  cu->npacked = std::max(cu->npacked, nsteps);
+  // The L columns of every earlier step are in lp already: the
+  // factorization's panels wrote them with the step (its step events).
   // the partial products of block row r go to slab set r % 2
   std::vector<int> nslabs(nsteps, 0);
   const int64_t set_floats = (int64_t)cu->ksplit_max * cu->slab;
@@ -1226,7 +1224,6 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
     const int64_t ofs = t * nb, in = std::min(nb, c0 - ofs);
     LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_p[t], 0));
     LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->step_s[t], 0));
-    if (t > 0) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_pk[t - 1], 0));
     // row t's products with the solved rows up to t-2 (on se, two
     // iterations ago)
     if (t >= 2) LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_early[t % 2], 0));
@@ -1249,7 +1246,6 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
     LUB_CUDA_TRY(cudaEventRecord(S->cu_xp, st));
     LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_xp, 0));
     if (t + 2 < nsteps) {
-      LUB_CUDA_TRY(cudaStreamWaitEvent(se, S->cu_pk[t], 0));
       const int64_t o2 = ofs + 2 * nb, ke = ofs + nb;
       const int64_t in2 = std::min(nb, c0 - o2);
       const int64_t tiles = ceil_div(in2, 128) * ceil_div(nc, 256);
@@ -1274,7 +1270,6 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
     if ((t + 1) % kLlCatchupGroup != 0 && t + 1 < nsteps) continue;
     LUB_CUDA_TRY(cudaEventRecord(S->cu_packed, st));
     LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_packed, 0));
-    LUB_CUDA_TRY(cudaStreamWaitEvent(sb, S->cu_pk[t], 0));  // the packs up to step t
     if (n > c0) {
       ProfScope ps("tc_update", sb, 8.0 * (n - c0) * nc + (double)es * (n - c0 + nc) * (k1 - k0),
                    2.0 * (n - c0) * (double)nc * (k1 - k0));
@@ -1295,8 +1290,6 @@ static lu_status catch_up_ll(const Plan& p, cudaStream_t st, float* a, int64_t l
   LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sb));
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   LUB_CUDA_TRY(cudaEventRecord(S->cu_join, se));
-  LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
-  LUB_CUDA_TRY(cudaEventRecord(S->cu_join, sp));
   LUB_CUDA_TRY(cudaStreamWaitEvent(st, S->cu_join, 0));
   return LU_SUCCESS;
 }
@@ -1779,6 +1772,11 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
       llb.lp = static_cast<char*>(cu_alloc);
       llb.xp = llb.lp + lp_bytes;
       llb.part = reinterpret_cast<float*>(llb.xp + xp_bytes);
+      // the factorization's panels write the L columns left of the last
+      // chunk into lp as they finish them (no packing pass)
+      sink.lp = llb.lp;
+      sink.ldl = llb.ldl;
+      sink.lp_cols = c_last;
     } else if (s == LU_SUCCESS && la && tc) {
       wcu[0] = tc_ws_layout(0, n - nb, n - nb, nb, kind);
       wcu[1] = tc_ws_layout(wcu[0].bytes, n - nb, n - nb, nb, kind);
@@ -1852,8 +1850,6 @@ lu_status factorize_host(const lu_opts& o, cudaStream_t st, int64_t n, float* h_
         cudaStreamWaitEvent(st, S->cu_join, 0);
         if (llc) {
           cudaEventRecord(S->cu_join, S->catchup_early);
-          cudaStreamWaitEvent(st, S->cu_join, 0);
-          cudaEventRecord(S->cu_join, S->catchup_pack);
           cudaStreamWaitEvent(st, S->cu_join, 0);
         }
       }

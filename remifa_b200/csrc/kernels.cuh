@@ -22,6 +22,11 @@ struct LuPack {
   int64_t row0 = 0, col0 = 0;
   int k0 = 0;
   int bf16 = 0;
+  // a second copy of the L rows (row r at pa2[(row02 + r) * ldk2 + k02 + c]),
+  // every row of the launch
+  void* pa2 = nullptr;
+  int64_t ldk2 = 0, row02 = 0;
+  int k02 = 0;
 };
 
 // L rows (M of them, below) and U columns (N, right) of the w x w factored

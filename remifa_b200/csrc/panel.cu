@@ -750,11 +750,15 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
   else store_cols<kPanelT>(A + item0 * lda, lda, S, ls, w, nitems);
   // the finished items as tensor-core operands: item qq's w values are
   // contiguous along K in both copies (consecutive threads, consecutive k)
-  void* dst = is_l ? pk.pa : pk.pb;
-  if (dst) {
+  // destination 0: the tensor-core operand copy; 1: the second L copy
+  for (int dsel = 0; dsel < 2; ++dsel) {
+    void* dst = dsel == 0 ? (is_l ? pk.pa : pk.pb) : (is_l ? pk.pa2 : nullptr);
+    if (!dst) continue;
     const int64_t lim = is_l ? M : N;
-    const int64_t base = (is_l ? pk.row0 : pk.col0) + item0;
-    if (w % 8 == 0 && pk.ldk % 8 == 0 && pk.k0 % 8 == 0) {
+    const int64_t base = (dsel == 1 ? pk.row02 : is_l ? pk.row0 : pk.col0) + item0;
+    const int64_t ldk = dsel == 1 ? pk.ldk2 : pk.ldk;
+    const int k0 = dsel == 1 ? pk.k02 : pk.k0;
+    if (w % 8 == 0 && ldk % 8 == 0 && k0 % 8 == 0) {
       // 8 values -> one 16-byte store
       const int w8 = w / 8;  // <= 16
       for (int idx = tid; idx < kItems * 16; idx += kPanelT) {
@@ -775,8 +779,7 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
               o32[e] = *reinterpret_cast<const uint32_t*>(&h);
             }
           }
-          *reinterpret_cast<uint4*>(static_cast<uint16_t*>(dst) + pr * pk.ldk + pk.k0 +
-                                    8 * c8) = out;
+          *reinterpret_cast<uint4*>(static_cast<uint16_t*>(dst) + pr * ldk + k0 + 8 * c8) = out;
         }
       }
     } else {
@@ -785,7 +788,7 @@ lupanel_kernel(float* __restrict__ dg, int64_t lda, int w, int64_t M,
         const int64_t pr = base + qq;
         if (item0 + qq < lim && pr >= 0) {
           const float v = S[qq * ls + c];
-          const int64_t o = pr * pk.ldk + pk.k0 + c;
+          const int64_t o = pr * ldk + k0 + c;
           if (pk.bf16) static_cast<__nv_bfloat16*>(dst)[o] = __float2bfloat16_rn(v);
           else static_cast<__half*>(dst)[o] = __float2half_rn(v);
         }
